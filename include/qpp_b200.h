@@ -1,0 +1,215 @@
+/*
+ * qpp_b200.h -- C ABI of the B200-native Quantum++ gate-application and
+ * subsystem-manipulation path.
+ *
+ * Conventions (identical to Quantum++ 7.0.3, include/qpp/types.hpp:127-178):
+ *   - complex numbers are interleaved (re, im) pairs of double (c128) or
+ *     float (c64); gate matrices passed to this ABI are always c128;
+ *   - a ket is a D x 1 column, a density matrix is a D x D matrix stored
+ *     column-major (element (r, c) at r + c * D);
+ *   - multi-indices are big-endian mixed radix: subsystem 0 is the most
+ *     significant digit (include/qpp/internal/util.hpp:58-116);
+ *   - a gate on k target subsystems is a DA x DA matrix, DA = prod dims[t],
+ *     whose row/column index is the big-endian multi-index over `target`
+ *     in the order given.
+ *
+ * Ownership: host arrays are borrowed for the duration of a call. Device
+ * states are owned by qgpu_state handles; ops on a handle work in place in
+ * HBM (the resident path). The qgpu_host_* entry points keep Quantum++'s
+ * value semantics: the input is const, the result is written to a caller
+ * buffer.
+ *
+ * Errors: every entry point returns a qgpu_status. Validation follows the
+ * order of the corresponding qpp function, so the first error reported is
+ * the one qpp would throw; qgpu_last_error_where()/what() return qpp's
+ * (where, what) strings, e.g. ("qpp::apply()", "dims/target").
+ *
+ * Threading: a context may be used from several threads; a state handle may
+ * not be used by two threads at once. Errors are recorded per thread.
+ */
+#ifndef QPP_B200_H_
+#define QPP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One value per qpp::exception type used on this path
+ * (include/qpp/classes/exception.hpp:129-655), plus device-side codes. */
+typedef enum qgpu_status {
+    QGPU_OK = 0,
+    QGPU_ERR_ZERO_SIZE = 1,                     /* exception::ZeroSize */
+    QGPU_ERR_MATRIX_NOT_SQUARE = 2,             /* exception::MatrixNotSquare */
+    QGPU_ERR_MATRIX_NOT_SQUARE_NOR_CVECTOR = 3, /* MatrixNotSquareNorCvector */
+    QGPU_ERR_MATRIX_MISMATCH_SUBSYS = 4,        /* MatrixMismatchSubsys */
+    QGPU_ERR_DIMS_INVALID = 5,                  /* DimsInvalid */
+    QGPU_ERR_DIMS_NOT_EQUAL = 6,                /* DimsNotEqual */
+    QGPU_ERR_DIMS_MISMATCH_MATRIX = 7,          /* DimsMismatchMatrix */
+    QGPU_ERR_DIMS_MISMATCH_CVECTOR = 8,         /* DimsMismatchCvector */
+    QGPU_ERR_SUBSYS_MISMATCH_DIMS = 9,          /* SubsysMismatchDims */
+    QGPU_ERR_PERM_INVALID = 10,                 /* PermInvalid */
+    QGPU_ERR_PERM_MISMATCH_DIMS = 11,           /* PermMismatchDims */
+    QGPU_ERR_OUT_OF_RANGE = 12,                 /* OutOfRange */
+    QGPU_ERR_TYPE_MISMATCH = 13,                /* TypeMismatch */
+    QGPU_ERR_SIZE_MISMATCH = 14,                /* SizeMismatch */
+    QGPU_ERR_QUDIT_ALREADY_MEASURED = 15,       /* QuditAlreadyMeasured */
+    QGPU_ERR_MATRIX_NOT_SQUARE_NOR_VECTOR = 16, /* MatrixNotSquareNorVector */
+    QGPU_ERR_DIVISION_BY_ZERO = 17, /* std::overflow_error in normalize() */
+    /* device-side and library codes (no qpp counterpart) */
+    QGPU_ERR_CUDA = 100,         /* a CUDA runtime call failed */
+    QGPU_ERR_OUT_OF_MEMORY = 101, /* device allocation or admission refused */
+    QGPU_ERR_TIMEOUT = 102,      /* a bounded device wait gave up */
+    QGPU_ERR_INVALID_HANDLE = 103,
+    QGPU_ERR_NOT_SUPPORTED = 104, /* size or form outside what is built */
+    QGPU_ERR_INVALID_ARGUMENT = 105
+} qgpu_status;
+
+typedef enum qgpu_kind { QGPU_KET = 0, QGPU_RHO = 1 } qgpu_kind;
+typedef enum qgpu_prec { QGPU_C128 = 0, QGPU_C64 = 1 } qgpu_prec;
+
+typedef struct qgpu_ctx qgpu_ctx;
+typedef struct qgpu_state qgpu_state;
+
+/* ---------------------------------------------------------------- errors */
+const char* qgpu_last_error_where(void);
+const char* qgpu_last_error_what(void);
+const char* qgpu_status_name(qgpu_status s);
+/* Library version string. */
+const char* qgpu_version(void);
+
+/* --------------------------------------------------------------- context */
+/* A context binds one CUDA device and owns the stream every op runs on. */
+qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out);
+qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx);
+qgpu_status qgpu_ctx_synchronize(qgpu_ctx* ctx);
+/* Device bytes currently free / total (cudaMemGetInfo on the ctx device). */
+qgpu_status qgpu_ctx_mem_info(qgpu_ctx* ctx, uint64_t* free_bytes,
+                              uint64_t* total_bytes);
+/* Number of kernels this library launched on the context since creation. */
+uint64_t qgpu_ctx_launch_count(const qgpu_ctx* ctx);
+/* The cudaStream_t every op of this context is issued on, as void*. */
+void* qgpu_ctx_stream(qgpu_ctx* ctx);
+
+/* ---------------------------------------------------------------- states */
+/* Allocate a ket (D x 1) or density matrix (D x D) over `dims` in HBM,
+ * zero-initialised. Fails with QGPU_ERR_DIMS_INVALID for empty dims or a
+ * zero dimension (internal::check_dims, util.hpp:158-166). */
+qgpu_status qgpu_state_create(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
+                              const uint64_t* dims, uint32_t n,
+                              qgpu_state** out);
+qgpu_status qgpu_state_destroy(qgpu_state* s);
+qgpu_status qgpu_state_clone(const qgpu_state* s, qgpu_state** out);
+/* Copy host data in the state's own precision (interleaved, column-major). */
+qgpu_status qgpu_state_upload(qgpu_state* s, const void* host);
+qgpu_status qgpu_state_download(const qgpu_state* s, void* host);
+/* Copy c128 host data, converting on the device for c64 states. */
+qgpu_status qgpu_state_upload_c128(qgpu_state* s, const double* host);
+qgpu_status qgpu_state_download_c128(const qgpu_state* s, double* host);
+qgpu_status qgpu_state_info(const qgpu_state* s, qgpu_kind* kind,
+                            qgpu_prec* prec, uint32_t* n, uint64_t* dims,
+                            uint64_t* D);
+/* Device pointer of the amplitudes (c128: double2*, c64: float2*). */
+void* qgpu_state_device_ptr(qgpu_state* s);
+/* Fill with i.i.d. complex Gaussian entries (re, im ~ N(0, 1)) from the
+ * counter-based Philox4x32-10 generator keyed by `seed` (element index as
+ * the counter), then normalise as qpp::normalize does. The same stream is
+ * reproducible on the host. */
+qgpu_status qgpu_state_fill_gaussian(qgpu_state* s, uint64_t seed);
+/* Copy a state into another of the same kind and dims, converting the
+ * precision on the device (c128 <-> c64). */
+qgpu_status qgpu_state_convert(const qgpu_state* src, qgpu_state* dst);
+
+/* ------------------------------------------------- resident ops (in HBM) */
+/* qpp::apply(state, A, target, dims), operations.hpp:72-372; in place. */
+qgpu_status qgpu_apply(qgpu_state* s, const double* A, uint64_t DA,
+                       const uint64_t* target, uint32_t k);
+/* qpp::applyCTRL(state, A, ctrl, target, dims, shift), operations.hpp:616-887.
+ * shift may be NULL (std::nullopt). */
+qgpu_status qgpu_apply_ctrl(qgpu_state* s, const double* A, uint64_t DA,
+                            const uint64_t* ctrl, uint32_t nc,
+                            const uint64_t* target, uint32_t k,
+                            const uint64_t* shift);
+/* qpp::applyCTRL_fan(...), operations.hpp:961-1234 (A is d x d). */
+qgpu_status qgpu_apply_ctrl_fan(qgpu_state* s, const double* A, uint64_t DA,
+                                const uint64_t* ctrl, uint32_t nc,
+                                const uint64_t* target, uint32_t k,
+                                const uint64_t* shift);
+/* qpp::apply(A, Ks, target, dims), operations.hpp:476-560: the channel
+ * sum_i K_i rho K_i^dagger on the subsystems `target`, in place.
+ * Ks holds nK consecutive DA x DA column-major c128 matrices. */
+qgpu_status qgpu_apply_kraus(qgpu_state* s, const double* Ks, uint32_t nK,
+                             uint64_t DA, const uint64_t* target, uint32_t k);
+/* qpp::ptrace(A, target, dims), operations.hpp:1908-2114: writes a new
+ * density-matrix state over the complement of `target`. */
+qgpu_status qgpu_ptrace(const qgpu_state* s, const uint64_t* target,
+                        uint32_t k, qgpu_state** out);
+/* qpp::ptranspose(A, target, dims), operations.hpp:2167-2335: a new
+ * D x D density-matrix state (a ket input gives (|psi><psi|)^{T_target}). */
+qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
+                            uint32_t k, qgpu_state** out);
+/* qpp::syspermute(A, perm, dims), operations.hpp:2386-2514: subsystem
+ * perm[i] moves to position i; writes a new state of the same kind. */
+qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
+                            uint32_t n, qgpu_state** out);
+/* Squared norm (ket) or trace (rho, real and imaginary parts), FP64
+ * accumulation. */
+qgpu_status qgpu_norm2(const qgpu_state* s, double* out);
+qgpu_status qgpu_trace(const qgpu_state* s, double* re, double* im);
+/* qpp::normalize(A), functions.hpp:304-333, in place (ket / norm,
+ * rho / trace). */
+qgpu_status qgpu_normalize(qgpu_state* s);
+/* <a|b> for two kets over the same dims (FP64 accumulation). */
+qgpu_status qgpu_inner(const qgpu_state* a, const qgpu_state* b, double* re,
+                       double* im);
+
+/* ------------------------------------- value-semantics entry points (host)
+ * These mirror qpp's free functions exactly: the state is a host array with
+ * `rows` x `cols` (cols == 1 for a ket, rows == cols for a density matrix),
+ * the result goes to a host buffer. Each call uploads, runs the device op
+ * and downloads; they exist so that a caller binding qpp's signatures can
+ * switch without keeping states resident. */
+qgpu_status qgpu_host_apply(qgpu_ctx* ctx, const double* state, uint64_t rows,
+                            uint64_t cols, const double* A, uint64_t A_rows,
+                            uint64_t A_cols, const uint64_t* target,
+                            uint32_t k, const uint64_t* dims, uint32_t n,
+                            double* result);
+qgpu_status qgpu_host_apply_ctrl(qgpu_ctx* ctx, const double* state,
+                                 uint64_t rows, uint64_t cols, const double* A,
+                                 uint64_t A_rows, uint64_t A_cols,
+                                 const uint64_t* ctrl, uint32_t nc,
+                                 const uint64_t* target, uint32_t k,
+                                 const uint64_t* dims, uint32_t n,
+                                 const uint64_t* shift, int fan,
+                                 double* result);
+qgpu_status qgpu_host_apply_kraus(qgpu_ctx* ctx, const double* state,
+                                  uint64_t rows, uint64_t cols,
+                                  const double* Ks, uint32_t nK,
+                                  uint64_t K_rows, uint64_t K_cols,
+                                  const uint64_t* target, uint32_t k,
+                                  const uint64_t* dims, uint32_t n,
+                                  double* result);
+/* result is Dbar x Dbar, Dbar = D / prod dims[target]. */
+qgpu_status qgpu_host_ptrace(qgpu_ctx* ctx, const double* state, uint64_t rows,
+                             uint64_t cols, const uint64_t* target, uint32_t k,
+                             const uint64_t* dims, uint32_t n, double* result);
+/* result is D x D. */
+qgpu_status qgpu_host_ptranspose(qgpu_ctx* ctx, const double* state,
+                                 uint64_t rows, uint64_t cols,
+                                 const uint64_t* target, uint32_t k,
+                                 const uint64_t* dims, uint32_t n,
+                                 double* result);
+/* result has the input's shape. */
+qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
+                                 uint64_t rows, uint64_t cols,
+                                 const uint64_t* perm, uint32_t nperm,
+                                 const uint64_t* dims, uint32_t n,
+                                 double* result);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* QPP_B200_H_ */

@@ -1,0 +1,216 @@
+"""ctypes front-end of the CPU oracle (oracle/qpp_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline leg of bench.py. The product package (qpp_b200) never imports it.
+
+Each function mirrors the Quantum++ 7.0.3 free function of the same name
+(include/qpp/operations.hpp, instruments.hpp) with value semantics: numpy
+complex128 arrays in (kets as 1-D arrays or (D, 1) columns, density matrices
+as (D, D)), a fresh numpy array out. Errors raise OracleError carrying qpp's
+(where, what) pair and the shared status code of include/qpp_b200.h.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+u64p = ct.POINTER(ct.c_uint64)
+dp = ct.POINTER(ct.c_double)
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code, where, what):
+        super().__init__(f"{where}: {what} (status {code})")
+        self.code, self.where, self.what = code, where, what
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ct.CDLL(_LIB_PATH)
+        L.oracle_last_where.restype = ct.c_char_p
+        L.oracle_last_what.restype = ct.c_char_p
+        _lib = L
+    return _lib
+
+
+def _u64(v):
+    if v is None:
+        return None, None
+    a = np.ascontiguousarray(np.asarray(v, dtype=np.uint64).reshape(-1))
+    return a, a.ctypes.data_as(u64p)
+
+
+def _cplx(a):
+    a = np.asarray(a, dtype=np.complex128)
+    return a
+
+
+def _state(a):
+    a = _cplx(a)
+    if a.ndim == 1:
+        rows, cols = a.shape[0], 1
+        buf = np.ascontiguousarray(a)
+    else:
+        rows, cols = a.shape
+        buf = np.asfortranarray(a)
+    return buf, rows, cols
+
+
+def _check(rc):
+    if rc != 0:
+        L = lib()
+        raise OracleError(rc, L.oracle_last_where().decode(), L.oracle_last_what().decode())
+
+
+def _out_like(rows, cols, shape_1d):
+    if cols == 1 and shape_1d:
+        return np.zeros(rows, dtype=np.complex128)
+    return np.zeros((rows, cols), dtype=np.complex128, order="F")
+
+
+def _dp(a):
+    return a.ctypes.data_as(dp)
+
+
+def apply(state, A, target, dims, path=0):
+    """qpp::apply(state, A, target, dims), operations.hpp:72-372.
+    path=1 takes the qubit-kernel loops (apply.hpp) for 1q/2q kets."""
+    buf, rows, cols = _state(state)
+    Am = np.asfortranarray(_cplx(A))
+    ar, ac = (Am.shape + (1,))[:2] if Am.ndim == 2 else (Am.shape[0], 1)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    out = _out_like(rows, cols, np.asarray(state).ndim == 1)
+    _check(lib().oracle_apply(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), _dp(Am),
+                              ct.c_uint64(ar), ct.c_uint64(ac), tp, ct.c_uint32(len(t)),
+                              dpp, ct.c_uint32(len(d)), _dp(out), ct.c_int(path)))
+    return out
+
+
+def applyCTRL(state, A, ctrl, target, dims, shift=None, path=0, fan=False):
+    """qpp::applyCTRL / applyCTRL_fan, operations.hpp:616-1234."""
+    buf, rows, cols = _state(state)
+    Am = np.asfortranarray(_cplx(A))
+    c, cp = _u64(ctrl)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    s, sp = _u64(shift)
+    out = _out_like(rows, cols, np.asarray(state).ndim == 1)
+    _check(lib().oracle_apply_ctrl(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), _dp(Am),
+                                   ct.c_uint64(Am.shape[0]), ct.c_uint64(Am.shape[1]),
+                                   cp, ct.c_uint32(len(c)), tp, ct.c_uint32(len(t)),
+                                   dpp, ct.c_uint32(len(d)), sp, ct.c_int(1 if fan else 0),
+                                   _dp(out), ct.c_int(path)))
+    return out
+
+
+def applyCTRL_fan(state, A, ctrl, target, dims, shift=None, path=0):
+    return applyCTRL(state, A, ctrl, target, dims, shift, path, fan=True)
+
+
+def apply_kraus(rho, Ks, target, dims):
+    """qpp::apply(A, Ks, target, dims), operations.hpp:476-560."""
+    buf, rows, cols = _state(rho)
+    Ks = [np.asfortranarray(_cplx(K)) for K in Ks]
+    kr, kc = Ks[0].shape if Ks else (0, 0)
+    packed = np.concatenate([K.reshape(-1, order="F") for K in Ks]) if Ks else np.zeros(1, np.complex128)
+    packed = np.ascontiguousarray(packed)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    out = np.zeros((rows, cols), dtype=np.complex128, order="F")
+    _check(lib().oracle_apply_kraus(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), _dp(packed),
+                                    ct.c_uint32(len(Ks)), ct.c_uint64(kr), ct.c_uint64(kc),
+                                    tp, ct.c_uint32(len(t)), dpp, ct.c_uint32(len(d)), _dp(out)))
+    return out
+
+
+def ptrace(state, target, dims):
+    """qpp::ptrace(A, target, dims), operations.hpp:1908-2114."""
+    buf, rows, cols = _state(state)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    DS = 1
+    for i in target:
+        if 0 <= int(i) < len(dims):
+            DS *= int(dims[int(i)])
+    Db = rows // DS if rows % DS == 0 else 1
+    out = np.zeros((max(Db, 1), max(Db, 1)), dtype=np.complex128, order="F")
+    _check(lib().oracle_ptrace(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                               ct.c_uint32(len(t)), dpp, ct.c_uint32(len(d)), _dp(out)))
+    return out
+
+
+def ptranspose(state, target, dims, compat=False):
+    """qpp::ptranspose(A, target, dims), operations.hpp:2167-2335.
+    compat=True reproduces internal/kernels/qubit/ptranspose.hpp."""
+    buf, rows, cols = _state(state)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    out = np.zeros((rows, rows), dtype=np.complex128, order="F")
+    _check(lib().oracle_ptranspose(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                                   ct.c_uint32(len(t)), dpp, ct.c_uint32(len(d)), _dp(out),
+                                   ct.c_int(1 if compat else 0)))
+    return out
+
+
+def syspermute(state, perm, dims, compat=False):
+    """qpp::syspermute(A, perm, dims), operations.hpp:2386-2514.
+    compat=True reproduces internal/kernels/qubit/syspermute.hpp."""
+    buf, rows, cols = _state(state)
+    p, pp = _u64(perm)
+    d, dpp = _u64(dims)
+    out = _out_like(rows, cols, np.asarray(state).ndim == 1)
+    _check(lib().oracle_syspermute(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), pp,
+                                   ct.c_uint32(len(p)), dpp, ct.c_uint32(len(d)), _dp(out),
+                                   ct.c_int(1 if compat else 0)))
+    return out
+
+
+def normalize(state):
+    """qpp::normalize(A), functions.hpp:304-333."""
+    buf, rows, cols = _state(state)
+    buf = buf.copy(order="F" if cols > 1 else "C")
+    _check(lib().oracle_normalize(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols)))
+    return buf
+
+
+def measure_seq(state, target, dims, destructive=True, forced=None, seed=0):
+    """qpp::measure_seq(A, target, dims, destructive), instruments.hpp:985-1111.
+    forced: outcome dits to take instead of sampling (replay mode).
+    Returns (results, probs, post-measurement state, its dims)."""
+    buf, rows, cols = _state(state)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    f, fp = _u64(forced)
+    k = len(t)
+    res = np.zeros(max(k, 1), dtype=np.uint64)
+    probs = np.zeros(max(k, 1), dtype=np.float64)
+    out = np.zeros(rows * cols, dtype=np.complex128)
+    od = np.zeros(max(len(d), 1), dtype=np.uint64)
+    ond = ct.c_uint32(0)
+    _check(lib().oracle_measure_seq(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                                    ct.c_uint32(k), dpp, ct.c_uint32(len(d)),
+                                    ct.c_int(1 if destructive else 0), fp, ct.c_uint64(seed),
+                                    res.ctypes.data_as(u64p), _dp(probs), _dp(out),
+                                    od.ctypes.data_as(u64p), ct.byref(ond)))
+    nd = [int(x) for x in od[: ond.value]]
+    Dn = int(np.prod(nd)) if nd else 1
+    if cols == 1:
+        st = out[:Dn].copy()
+    else:
+        st = out[: Dn * Dn].reshape((Dn, Dn), order="F").copy()
+    return [int(x) for x in res[:k]], [float(x) for x in probs[:k]], st, nd

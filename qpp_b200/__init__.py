@@ -1,0 +1,393 @@
+"""qpp_b200 -- B200-native Quantum++ gate-application and subsystem path.
+
+Python host mirror of the C ABI in include/qpp_b200.h (libqpp_b200.so,
+built in-tree for sm_100a). The free functions keep Quantum++'s names,
+argument meaning and value semantics (include/qpp/operations.hpp):
+
+    apply(state, A, target, dims)                       operations.hpp:72
+    applyCTRL(state, A, ctrl, target, dims, shift)      operations.hpp:616
+    applyCTRL_fan(state, A, ctrl, target, dims, shift)  operations.hpp:961
+    apply_kraus(rho, Ks, target, dims)                  operations.hpp:476
+    ptrace(state, target, dims)                         operations.hpp:1908
+    ptranspose(state, target, dims)                     operations.hpp:2167
+    syspermute(state, perm, dims)                       operations.hpp:2386
+
+Errors raise the qpp exception type of the same name (ZeroSize,
+DimsInvalid, SubsysMismatchDims, ...) with qpp's (where, what) text.
+`State` is the resident form: a ket or density matrix kept in HBM, mutated
+in place by its methods. There is no CPU fallback: importing on a machine
+without the built library raises, and every op needs a B200.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqpp_b200.so")
+
+u64p = ct.POINTER(ct.c_uint64)
+dp = ct.POINTER(ct.c_double)
+vp = ct.c_void_p
+
+KET, RHO = 0, 1
+C128, C64 = 0, 1
+
+_STATUS = {
+    1: "ZeroSize", 2: "MatrixNotSquare", 3: "MatrixNotSquareNorCvector",
+    4: "MatrixMismatchSubsys", 5: "DimsInvalid", 6: "DimsNotEqual",
+    7: "DimsMismatchMatrix", 8: "DimsMismatchCvector", 9: "SubsysMismatchDims",
+    10: "PermInvalid", 11: "PermMismatchDims", 12: "OutOfRange",
+    13: "TypeMismatch", 14: "SizeMismatch", 15: "QuditAlreadyMeasured",
+    16: "MatrixNotSquareNorVector", 17: "DivisionByZero", 100: "CudaError",
+    101: "OutOfMemory", 102: "Timeout", 103: "InvalidHandle",
+    104: "NotSupported", 105: "InvalidArgument",
+}
+
+
+class QppError(RuntimeError):
+    """Base of the qpp exception mirror (include/qpp/classes/exception.hpp)."""
+
+    def __init__(self, code, where, what):
+        super().__init__(f"{where}: {what}")
+        self.code, self.where, self.what = code, where, what
+
+
+_EXC = {code: type(name, (QppError,), {}) for code, name in _STATUS.items()}
+globals().update({cls.__name__: cls for cls in _EXC.values()})
+
+_lib = None
+
+
+def lib():
+    """The loaded libqpp_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              "`make -C qpp_b200` (nvcc, sm_100a)")
+        L = ct.CDLL(LIB_PATH)
+        L.qgpu_last_error_where.restype = ct.c_char_p
+        L.qgpu_last_error_what.restype = ct.c_char_p
+        L.qgpu_version.restype = ct.c_char_p
+        L.qgpu_status_name.restype = ct.c_char_p
+        L.qgpu_ctx_launch_count.restype = ct.c_uint64
+        L.qgpu_ctx_stream.restype = vp
+        L.qgpu_state_device_ptr.restype = vp
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        L = lib()
+        where = L.qgpu_last_error_where().decode()
+        what = L.qgpu_last_error_what().decode()
+        raise _EXC.get(rc, QppError)(rc, where, what)
+
+
+def _u64(v):
+    if v is None:
+        return None, None, 0
+    a = np.ascontiguousarray(np.asarray(list(v), dtype=np.uint64).reshape(-1))
+    if a.size == 0:
+        a = np.zeros(1, dtype=np.uint64)
+        return a, a.ctypes.data_as(u64p), 0
+    return a, a.ctypes.data_as(u64p), a.size
+
+
+def _mat(A):
+    A = np.asfortranarray(np.asarray(A, dtype=np.complex128))
+    if A.ndim == 1:
+        A = A.reshape(-1, 1, order="F")
+    return A
+
+
+def _host_state(state):
+    a = np.asarray(state, dtype=np.complex128)
+    if a.ndim == 1:
+        return np.ascontiguousarray(a), a.shape[0], 1, True
+    return np.asfortranarray(a), a.shape[0], a.shape[1], False
+
+
+def _dp(a):
+    return a.ctypes.data_as(dp)
+
+
+class Context:
+    """A CUDA device plus the stream all ops on it are issued on."""
+
+    def __init__(self, device=0):
+        self.h = vp()
+        check(lib().qgpu_ctx_create(ct.c_int(device), ct.byref(self.h)))
+        self.device = device
+
+    def synchronize(self):
+        check(lib().qgpu_ctx_synchronize(self.h))
+
+    def launches(self):
+        return int(lib().qgpu_ctx_launch_count(self.h))
+
+    def stream(self):
+        return lib().qgpu_ctx_stream(self.h)
+
+    def mem_info(self):
+        f, t = ct.c_uint64(), ct.c_uint64()
+        check(lib().qgpu_ctx_mem_info(self.h, ct.byref(f), ct.byref(t)))
+        return f.value, t.value
+
+    def close(self):
+        if self.h:
+            check(lib().qgpu_ctx_destroy(self.h))
+            self.h = None
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class State:
+    """A ket (kind=KET) or density matrix (kind=RHO) resident in HBM."""
+
+    def __init__(self, ctx, kind, dims, prec=C128, handle=None):
+        self.ctx = ctx
+        if handle is None:
+            handle = vp()
+            d, dpp, nd = _u64(dims)
+            check(lib().qgpu_state_create(ctx.h, ct.c_int(kind), ct.c_int(prec), dpp,
+                                          ct.c_uint32(nd), ct.byref(handle)))
+        self.h = handle
+        self._info()
+
+    def _info(self):
+        k, p, n, D = ct.c_int(), ct.c_int(), ct.c_uint32(), ct.c_uint64()
+        check(lib().qgpu_state_info(self.h, ct.byref(k), ct.byref(p), ct.byref(n), None,
+                                    ct.byref(D)))
+        dims = np.zeros(max(n.value, 1), dtype=np.uint64)
+        check(lib().qgpu_state_info(self.h, None, None, None, dims.ctypes.data_as(u64p), None))
+        self.kind, self.prec, self.D = k.value, p.value, D.value
+        self.dims = [int(x) for x in dims[: n.value]]
+
+    @classmethod
+    def from_numpy(cls, ctx, arr, dims, prec=C128):
+        a = np.asarray(arr, dtype=np.complex128)
+        kind = KET if a.ndim == 1 or (a.ndim == 2 and a.shape[1] == 1) else RHO
+        s = cls(ctx, kind, dims, prec)
+        s.upload(a)
+        return s
+
+    def upload(self, arr):
+        a = np.asarray(arr, dtype=np.complex128)
+        a = np.ascontiguousarray(a.reshape(-1)) if self.kind == KET else np.asfortranarray(a)
+        check(lib().qgpu_state_upload_c128(self.h, _dp(a)))
+
+    def numpy(self):
+        n = self.D if self.kind == KET else self.D * self.D
+        out = np.zeros(n, dtype=np.complex128)
+        check(lib().qgpu_state_download_c128(self.h, _dp(out)))
+        if self.kind == KET:
+            return out
+        return out.reshape((self.D, self.D), order="F")
+
+    def device_ptr(self):
+        return lib().qgpu_state_device_ptr(self.h)
+
+    def fill_gaussian(self, seed):
+        """i.i.d. complex Gaussian entries (Philox4x32-10 keyed by seed),
+        normalised."""
+        check(lib().qgpu_state_fill_gaussian(self.h, ct.c_uint64(seed)))
+        return self
+
+    def convert_from(self, other):
+        check(lib().qgpu_state_convert(other.h, self.h))
+        return self
+
+    # resident (in-place) ops
+    def apply(self, A, target):
+        A = _mat(A)
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_apply(self.h, _dp(A), ct.c_uint64(A.shape[0]), tp, ct.c_uint32(nt)))
+        return self
+
+    def apply_ctrl(self, A, ctrl, target, shift=None, fan=False):
+        A = _mat(A)
+        c, cp, nc = _u64(ctrl)
+        t, tp, nt = _u64(target)
+        s, sp, _ = _u64(shift)
+        fn = lib().qgpu_apply_ctrl_fan if fan else lib().qgpu_apply_ctrl
+        check(fn(self.h, _dp(A), ct.c_uint64(A.shape[0]), cp, ct.c_uint32(nc), tp,
+                 ct.c_uint32(nt), sp))
+        return self
+
+    def apply_kraus(self, Ks, target):
+        packed, DA = _pack_kraus(Ks)
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_apply_kraus(self.h, _dp(packed), ct.c_uint32(len(Ks)),
+                                     ct.c_uint64(DA), tp, ct.c_uint32(nt)))
+        return self
+
+    def ptrace(self, target):
+        t, tp, nt = _u64(target)
+        h = vp()
+        check(lib().qgpu_ptrace(self.h, tp, ct.c_uint32(nt), ct.byref(h)))
+        return State(self.ctx, RHO, None, handle=h)
+
+    def ptranspose(self, target):
+        t, tp, nt = _u64(target)
+        h = vp()
+        check(lib().qgpu_ptranspose(self.h, tp, ct.c_uint32(nt), ct.byref(h)))
+        return State(self.ctx, RHO, None, handle=h)
+
+    def syspermute(self, perm):
+        p, pp, npm = _u64(perm)
+        h = vp()
+        check(lib().qgpu_syspermute(self.h, pp, ct.c_uint32(npm), ct.byref(h)))
+        return State(self.ctx, self.kind, None, handle=h)
+
+    def norm2(self):
+        v = ct.c_double()
+        check(lib().qgpu_norm2(self.h, ct.byref(v)))
+        return v.value
+
+    def trace(self):
+        r, i = ct.c_double(), ct.c_double()
+        check(lib().qgpu_trace(self.h, ct.byref(r), ct.byref(i)))
+        return complex(r.value, i.value)
+
+    def normalize(self):
+        check(lib().qgpu_normalize(self.h))
+        return self
+
+    def inner(self, other):
+        r, i = ct.c_double(), ct.c_double()
+        check(lib().qgpu_inner(self.h, other.h, ct.byref(r), ct.byref(i)))
+        return complex(r.value, i.value)
+
+    def clone(self):
+        h = vp()
+        check(lib().qgpu_state_clone(self.h, ct.byref(h)))
+        return State(self.ctx, self.kind, None, handle=h)
+
+    def free(self):
+        if self.h:
+            check(lib().qgpu_state_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            if self.h and lib() is not None:
+                lib().qgpu_state_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def _pack_kraus(Ks):
+    Ks = [_mat(K) for K in Ks]
+    if not Ks:
+        return np.zeros(1, dtype=np.complex128), 0
+    packed = np.ascontiguousarray(np.concatenate([K.reshape(-1, order="F") for K in Ks]))
+    return packed, Ks[0].shape[0]
+
+
+# ------------------------------------------ value-semantics free functions
+def apply(state, A, target, dims, ctx=None):
+    """qpp::apply(state, A, target, dims) (operations.hpp:72-372)."""
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(state)
+    A = _mat(A)
+    t, tp, nt = _u64(target)
+    d, dpp, nd = _u64(dims)
+    out = np.zeros(s.shape, dtype=np.complex128, order="F")
+    check(lib().qgpu_host_apply(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols), _dp(A),
+                                ct.c_uint64(A.shape[0]), ct.c_uint64(A.shape[1]), tp,
+                                ct.c_uint32(nt), dpp, ct.c_uint32(nd), _dp(out)))
+    return out
+
+
+def applyCTRL(state, A, ctrl, target, dims, shift=None, ctx=None, fan=False):
+    """qpp::applyCTRL(state, A, ctrl, target, dims, shift) (operations.hpp:616)."""
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(state)
+    A = _mat(A)
+    c, cp, nc = _u64(ctrl)
+    t, tp, nt = _u64(target)
+    d, dpp, nd = _u64(dims)
+    sh, sp, _ = _u64(shift)
+    out = np.zeros(s.shape, dtype=np.complex128, order="F")
+    check(lib().qgpu_host_apply_ctrl(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols),
+                                     _dp(A), ct.c_uint64(A.shape[0]), ct.c_uint64(A.shape[1]),
+                                     cp, ct.c_uint32(nc), tp, ct.c_uint32(nt), dpp,
+                                     ct.c_uint32(nd), sp, ct.c_int(1 if fan else 0), _dp(out)))
+    return out
+
+
+def applyCTRL_fan(state, A, ctrl, target, dims, shift=None, ctx=None):
+    """qpp::applyCTRL_fan(state, A, ctrl, target, dims, shift) (operations.hpp:961)."""
+    return applyCTRL(state, A, ctrl, target, dims, shift, ctx=ctx, fan=True)
+
+
+def apply_kraus(rho, Ks, target, dims, ctx=None):
+    """qpp::apply(A, Ks, target, dims) (operations.hpp:476-560)."""
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(rho)
+    Kl = [_mat(K) for K in Ks]
+    packed, _ = _pack_kraus(Kl)
+    kr, kc = (Kl[0].shape if Kl else (0, 0))
+    t, tp, nt = _u64(target)
+    d, dpp, nd = _u64(dims)
+    out = np.zeros((rows, cols), dtype=np.complex128, order="F")
+    check(lib().qgpu_host_apply_kraus(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols),
+                                      _dp(packed), ct.c_uint32(len(Kl)), ct.c_uint64(kr),
+                                      ct.c_uint64(kc), tp, ct.c_uint32(nt), dpp,
+                                      ct.c_uint32(nd), _dp(out)))
+    return out
+
+
+def ptrace(state, target, dims, ctx=None):
+    """qpp::ptrace(A, target, dims) (operations.hpp:1908-2114)."""
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(state)
+    t, tp, nt = _u64(target)
+    d, dpp, nd = _u64(dims)
+    DS = 1
+    for i in (target or []):
+        if 0 <= int(i) < len(dims):
+            DS *= int(dims[int(i)])
+    Db = max(rows // DS, 1) if rows % DS == 0 else 1
+    out = np.zeros((Db, Db), dtype=np.complex128, order="F")
+    check(lib().qgpu_host_ptrace(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                                 ct.c_uint32(nt), dpp, ct.c_uint32(nd), _dp(out)))
+    return out
+
+
+def ptranspose(state, target, dims, ctx=None):
+    """qpp::ptranspose(A, target, dims) (operations.hpp:2167-2335)."""
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(state)
+    t, tp, nt = _u64(target)
+    d, dpp, nd = _u64(dims)
+    out = np.zeros((rows, rows), dtype=np.complex128, order="F")
+    check(lib().qgpu_host_ptranspose(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                                     ct.c_uint32(nt), dpp, ct.c_uint32(nd), _dp(out)))
+    return out
+
+
+def syspermute(state, perm, dims, ctx=None):
+    """qpp::syspermute(A, perm, dims) (operations.hpp:2386-2514)."""
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(state)
+    p, pp, npm = _u64(perm)
+    d, dpp, nd = _u64(dims)
+    out = np.zeros(s.shape, dtype=np.complex128, order="F")
+    check(lib().qgpu_host_syspermute(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols), pp,
+                                     ct.c_uint32(npm), dpp, ct.c_uint32(nd), _dp(out)))
+    return out

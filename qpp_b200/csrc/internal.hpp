@@ -1,0 +1,78 @@
+// internal.hpp -- host-side structures of libqpp_b200 (context, state,
+// errors). Pure C++17 + CUDA runtime API; no torch and no Eigen.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qpp_b200.h"
+
+struct qgpu_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    std::atomic<uint64_t> launches{0};
+    std::mutex mu;
+    // Device scratch owned by the context (FP64 block partials, large gate
+    // matrices, offset tables). Grown on demand; used in stream order only.
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // Pinned host buffer for small device -> host results.
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+struct qgpu_state {
+    qgpu_ctx* ctx = nullptr;
+    qgpu_kind kind = QGPU_KET;
+    qgpu_prec prec = QGPU_C128;
+    std::vector<uint64_t> dims;
+    uint64_t D = 0;     // prod(dims)
+    uint64_t elems = 0; // D (ket) or D * D (rho)
+    void* data = nullptr;
+    size_t elem_bytes() const { return prec == QGPU_C128 ? 16 : 8; }
+    size_t bytes() const { return elems * elem_bytes(); }
+};
+
+namespace qgpu {
+
+// Internal exception; converted to a qgpu_status at the C boundary.
+struct Exc {
+    qgpu_status code;
+    std::string where;
+    std::string what;
+};
+
+[[noreturn]] inline void raise(qgpu_status c, const std::string& where,
+                               const std::string& what) {
+    throw Exc{c, where, what};
+}
+
+void record_error(qgpu_status c, const std::string& where,
+                  const std::string& what);
+void clear_error();
+
+#define QG_CUDA(call)                                                       \
+    do {                                                                    \
+        cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess)                                              \
+            ::qgpu::raise(e_ == cudaErrorMemoryAllocation                   \
+                              ? QGPU_ERR_OUT_OF_MEMORY                      \
+                              : QGPU_ERR_CUDA,                              \
+                          #call, cudaGetErrorString(e_));                   \
+    } while (0)
+
+// Checks the last launch on this thread and counts it on the context.
+void after_launch(qgpu_ctx* ctx, const char* name);
+
+// Context scratch of at least `bytes` (stream-ordered reuse).
+void* ctx_scratch(qgpu_ctx* ctx, size_t bytes);
+// Pinned host buffer of at least `bytes`.
+void* ctx_pinned(qgpu_ctx* ctx, size_t bytes);
+
+} // namespace qgpu

@@ -1,0 +1,86 @@
+// kernels.hpp -- host-callable launchers of the sm_100a kernels.
+//
+// All launchers enqueue on the context stream and return immediately; they
+// throw qgpu::Exc on a launch error. Matrices are c128 column-major; the
+// launcher converts them to the state precision.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace qgpu {
+
+using cd = std::complex<double>;
+
+// Number of SMs and resident blocks of 256 threads used to size grids.
+int grid_blocks(qgpu_ctx* ctx, int blocks_per_sm);
+
+// --- gate application (kernels_gate.cu), all in place -------------------
+// Qubit ket, one target at bit position `bit` (LSB = 0) of a 2^nbits state.
+void launch_qubit_1q(qgpu_ctx* ctx, qgpu_prec prec, void* data, int nbits,
+                     int bit, const cd* A);
+// Qubit ket, two targets: A's row index is 2 * b(bit0) + b(bit1).
+void launch_qubit_2q(qgpu_ctx* ctx, qgpu_prec prec, void* data, int nbits,
+                     int bit0, int bit1, const cd* A);
+// Generic: for every group g of `outer`, the DA amplitudes at
+// base(g) + off[m] are replaced by A * (those amplitudes).
+void launch_apply_generic(qgpu_ctx* ctx, qgpu_prec prec, void* data,
+                          const SegPlan& outer,
+                          const std::vector<uint64_t>& off, const cd* A,
+                          uint64_t DA);
+
+// --- subsystem kernels (kernels_subsys.cu) --------------------------------
+// out[o] = in[map(o)], o over map.count.
+void launch_gather(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
+                   const SegPlan& map);
+// out[o] = in[mapA(o)] * conj(in[mapB(o)]) (ket -> density-matrix forms).
+void launch_gather_outer(qgpu_ctx* ctx, qgpu_prec prec, const void* in,
+                         void* out, const SegPlan& mapA, const SegPlan& mapB);
+// Partial trace: out[o] = sum_a in[mapA(o) + toff[a]] (rho), or
+// sum_a in[mapA(o) + toff[a]] * conj(in[mapB(o) + toff[a]]) (ket, is_ket).
+void launch_ptrace(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
+                   const SegPlan& mapA, const SegPlan& mapB,
+                   const std::vector<uint64_t>& toff, bool is_ket);
+
+// --- reductions and elementwise (kernels_reduce.cu) ----------------------
+// sum |x|^2 over n elements, FP64 accumulation; result to *host_out.
+double reduce_norm2(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
+                    uint64_t n);
+// sum_i x[i * stride] (complex, FP64 accumulation): the trace for stride D+1.
+cd reduce_strided_sum(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
+                      uint64_t n, uint64_t stride);
+// sum conj(a[i]) b[i], FP64 accumulation.
+cd reduce_inner(qgpu_ctx* ctx, qgpu_prec prec, const void* a, const void* b,
+                uint64_t n);
+// x[i] *= s
+void launch_scale(qgpu_ctx* ctx, qgpu_prec prec, void* data, uint64_t n,
+                  cd s);
+// Marginal probabilities over the target digits of a ket (|x|^2) or of the
+// diagonal of a density matrix: p[m] = sum_g w(base(g) + off[m]), FP64.
+std::vector<double> reduce_marginals(qgpu_ctx* ctx, qgpu_prec prec,
+                                     const void* data, const SegPlan& outer,
+                                     const std::vector<uint64_t>& off,
+                                     bool diag_of_rho, uint64_t D);
+// Index of the first element whose inclusive prefix sum of weights exceeds
+// `threshold` (FP64); weights are |x_i|^2 (ket) or Re rho(i, i).
+uint64_t prefix_search(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
+                       uint64_t D, bool diag_of_rho, double threshold,
+                       double* total_out);
+// Keep the elements whose digit (index / dig_stride) % dig_dim equals
+// dig_val (for rho: in both the row and the column index), scale them by
+// `scale`, zero the rest.
+void launch_project(qgpu_ctx* ctx, qgpu_prec prec, void* data, uint64_t n,
+                    uint64_t D, bool is_rho, uint64_t dig_stride,
+                    uint64_t dig_dim, uint64_t dig_val, double scale);
+// Philox4x32-10 counter-based normal samples: x = (N(0,1), N(0,1)).
+void launch_fill_gaussian(qgpu_ctx* ctx, qgpu_prec prec, void* data,
+                          uint64_t n, uint64_t seed);
+// c128 <-> c64 conversion on the device.
+void launch_convert(qgpu_ctx* ctx, const void* in, qgpu_prec in_prec,
+                    void* out, qgpu_prec out_prec, uint64_t n);
+
+} // namespace qgpu
