@@ -317,12 +317,12 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic",
-            "config": {"workload": f"{n}-qubit ket (2^{n} complex128, 16 GiB), layered depth-{DEPTH} "
+            "config": {"workload": f"{n}-qubit ket (2^{n} complex128, {16 * D / 2**30:g} GiB), layered depth-{DEPTH} "
                                    "random circuit, plain form: one in-place pass per gate; "
                                    "step = one layer (30 1q + 15 2q gates)",
                        "qubits": n, "depth": DEPTH, "gates_per_step": len(layers[0]),
                        "parallelism": f"replicas x{world}",
-                       "l2": "state is 16 GiB (136x L2): no flush needed"},
+                       "l2": f"state is {16 * D / 2**30:g} GiB, {16 * D / (126 * 2**20):.0f}x the 126 MB L2: no flush needed"},
             "roofline": {"bound": "hbm", "kernel": "k_qubit_1q", "achieved": ach1, "peak": peak,
                          "unit": "GB/s", "frac": ach1 / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": gbytes, "mean_launch_ms": statistics.mean(d1),

@@ -58,6 +58,7 @@ typedef enum qgpu_status {
     QGPU_ERR_QUDIT_ALREADY_MEASURED = 15,       /* QuditAlreadyMeasured */
     QGPU_ERR_MATRIX_NOT_SQUARE_NOR_VECTOR = 16, /* MatrixNotSquareNorVector */
     QGPU_ERR_DIVISION_BY_ZERO = 17, /* std::overflow_error in normalize() */
+    QGPU_ERR_DUPLICATES = 18,       /* exception::Duplicates */
     /* device-side and library codes (no qpp counterpart) */
     QGPU_ERR_CUDA = 100,         /* a CUDA runtime call failed */
     QGPU_ERR_OUT_OF_MEMORY = 101, /* device allocation or admission refused */
@@ -207,6 +208,54 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* perm, uint32_t nperm,
                                  const uint64_t* dims, uint32_t n,
                                  double* result);
+
+/* --------------------------------------------------------------- circuits
+ * The step list of qpp::QCircuit (include/qpp/classes/qcircuit.hpp) over nq
+ * qudits of dimension d with nc classical dits. Step checks follow
+ * QCircuit's (qcircuit.hpp:1166-1483), with "Step <i>: <what>" messages. */
+typedef struct qgpu_circuit qgpu_circuit;
+qgpu_status qgpu_circuit_create(uint32_t nq, uint64_t d, uint32_t nc,
+                                qgpu_circuit** out);
+qgpu_status qgpu_circuit_destroy(qgpu_circuit* c);
+/* QCircuit::gate(U, target), qcircuit.hpp:1166-1483 (U is d^k x d^k). */
+qgpu_status qgpu_circuit_gate(qgpu_circuit* c, const double* U, uint64_t DU,
+                              const uint64_t* target, uint32_t k);
+/* QCircuit::gate_fan(U, target): the d x d U on every target. */
+qgpu_status qgpu_circuit_gate_fan(qgpu_circuit* c, const double* U,
+                                  uint64_t DU, const uint64_t* target,
+                                  uint32_t k);
+/* QCircuit::CTRL / CTRL_fan(U, ctrl, target, shift), qcircuit.hpp:1985-2322;
+ * shift may be NULL. */
+qgpu_status qgpu_circuit_ctrl(qgpu_circuit* c, const double* U, uint64_t DU,
+                              const uint64_t* ctrl, uint32_t nc,
+                              const uint64_t* target, uint32_t k,
+                              const uint64_t* shift, int fan);
+/* QCircuit::cCTRL / cCTRL_fan: controlled on classical dits ctrl_dits. */
+qgpu_status qgpu_circuit_cctrl(qgpu_circuit* c, const double* U, uint64_t DU,
+                               const uint64_t* ctrl_dits, uint32_t nc,
+                               const uint64_t* target, uint32_t k,
+                               const uint64_t* shift, int fan);
+/* QCircuit::measure / measure_many in the Z basis (qcircuit.hpp:2983):
+ * the first outcome goes to classical dit c_reg. */
+qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target,
+                                 uint32_t k, uint64_t c_reg, int destructive);
+qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq,
+                              uint64_t* n_steps);
+/* Number of state passes of the fused plan with blocks of <= max_k qubits
+ * (host-side planning only). */
+qgpu_status qgpu_circuit_fuse(qgpu_circuit* c, uint32_t max_k,
+                              uint64_t* n_passes);
+
+/* Execution forms of the unitary steps of a circuit on a resident state. */
+typedef enum qgpu_form {
+    QGPU_FORM_PLAIN = 0, /* one pass per qpp call, in the state precision */
+    QGPU_FORM_FUSED = 1  /* fused blocks: c64 -> 6-qubit tcgen05 3xTF32 */
+} qgpu_form;
+qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form);
+/* One gate of k <= 6 qubits on a complex64 qubit ket of >= 13 qubits, as a
+ * 64 x 64 block on the tensor cores (split-TF32, FP32 accumulation). */
+qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U,
+                          const uint64_t* target, uint32_t k);
 
 #ifdef __cplusplus
 } /* extern "C" */

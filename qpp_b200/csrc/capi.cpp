@@ -336,6 +336,7 @@ const char* qgpu_status_name(qgpu_status s) {
         case QGPU_ERR_QUDIT_ALREADY_MEASURED: return "QuditAlreadyMeasured";
         case QGPU_ERR_MATRIX_NOT_SQUARE_NOR_VECTOR: return "MatrixNotSquareNorVector";
         case QGPU_ERR_DIVISION_BY_ZERO: return "DivisionByZero";
+        case QGPU_ERR_DUPLICATES: return "Duplicates";
         case QGPU_ERR_CUDA: return "CudaError";
         case QGPU_ERR_OUT_OF_MEMORY: return "OutOfMemory";
         case QGPU_ERR_TIMEOUT: return "Timeout";
@@ -377,6 +378,7 @@ qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
         if (ctx->scratch) cudaFree(ctx->scratch);
         if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        if (ctx->dev_flag) cudaFree(ctx->dev_flag);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
     });

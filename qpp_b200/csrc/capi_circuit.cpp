@@ -1,0 +1,266 @@
+// capi_circuit.cpp -- extern "C" entry points for circuits, the fused form
+// and single tensor-core blocks.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "capi_common.hpp"
+#include "circuit.hpp"
+#include "kernels.hpp"
+#include "ops.hpp"
+
+using qgpu::cd;
+using qgpu::guarded;
+using qgpu::need_handle;
+using qgpu::raise;
+using qgpu::vec_of;
+
+namespace qgpu {
+void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
+                      const float* dB);
+void fused6_matrix(const cd* U, float* B);
+int fused_error(qgpu_ctx* ctx);
+} // namespace qgpu
+
+namespace {
+
+std::string ctx_of(const qgpu_circuit* c) {
+    return "Step " + std::to_string(c->steps.size()) + ": ";
+}
+
+// QCircuit::gate target checks (qcircuit.hpp:1453-1483)
+void check_targets(const qgpu_circuit* c, const char* W,
+                   const std::vector<uint64_t>& t, const char* what,
+                   const std::vector<char>& measured) {
+    if (t.empty()) raise(QGPU_ERR_ZERO_SIZE, W, ctx_of(c) + what);
+    for (uint64_t x : t) {
+        if (x >= c->nq) raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + what);
+        if (measured[x]) raise(QGPU_ERR_QUDIT_ALREADY_MEASURED, W, ctx_of(c) + what);
+    }
+    std::vector<uint64_t> s = t;
+    std::sort(s.begin(), s.end());
+    if (std::adjacent_find(s.begin(), s.end()) != s.end())
+        raise(QGPU_ERR_DUPLICATES, W, ctx_of(c) + what);
+}
+
+std::vector<char> measured_of(const qgpu_circuit* c) {
+    std::vector<char> m(c->nq, 0);
+    for (auto& s : c->steps)
+        if (s.kind == qgpu::StepKind::Measure && s.destructive)
+            for (uint64_t t : s.target) m[t] = 1;
+    return m;
+}
+
+uint64_t ipow(uint64_t d, size_t k) {
+    uint64_t r = 1;
+    for (size_t i = 0; i < k; ++i) r *= d;
+    return r;
+}
+
+} // namespace
+
+extern "C" {
+
+qgpu_status qgpu_circuit_create(uint32_t nq, uint64_t d, uint32_t nc,
+                                qgpu_circuit** out) {
+    return guarded([&] {
+        if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_circuit_create()", "out");
+        if (nq == 0) raise(QGPU_ERR_ZERO_SIZE, "qpp::QCircuit::QCircuit()", "nq");
+        if (d < 2) raise(QGPU_ERR_DIMS_INVALID, "qpp::QCircuit::QCircuit()", "d");
+        auto* c = new qgpu_circuit;
+        c->nq = nq;
+        c->d = d;
+        c->nc = nc;
+        *out = c;
+    });
+}
+
+qgpu_status qgpu_circuit_destroy(qgpu_circuit* c) {
+    return guarded([&] { delete c; });
+}
+
+qgpu_status qgpu_circuit_gate(qgpu_circuit* c, const double* U, uint64_t DU,
+                              const uint64_t* target, uint32_t k) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = "qpp::QCircuit::gate()";
+        auto t = vec_of(target, k);
+        check_targets(c, W, t, "target", measured_of(c));
+        if (DU != ipow(c->d, t.size()))
+            raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, W, ctx_of(c) + "U");
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::Gate;
+        s.U.assign(reinterpret_cast<const cd*>(U), reinterpret_cast<const cd*>(U) + DU * DU);
+        s.DU = DU;
+        s.target = t;
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+qgpu_status qgpu_circuit_gate_fan(qgpu_circuit* c, const double* U, uint64_t DU,
+                                  const uint64_t* target, uint32_t k) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = "qpp::QCircuit::gate_fan()";
+        auto t = vec_of(target, k);
+        check_targets(c, W, t, "target", measured_of(c));
+        if (DU != c->d) raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, W, ctx_of(c) + "U");
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::Fan;
+        s.U.assign(reinterpret_cast<const cd*>(U), reinterpret_cast<const cd*>(U) + DU * DU);
+        s.DU = DU;
+        s.target = t;
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+qgpu_status qgpu_circuit_ctrl(qgpu_circuit* c, const double* U, uint64_t DU,
+                              const uint64_t* ctrl, uint32_t nc,
+                              const uint64_t* target, uint32_t k,
+                              const uint64_t* shift, int fan) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = fan ? "qpp::QCircuit::CTRL_fan()" : "qpp::QCircuit::CTRL()";
+        auto cv = vec_of(ctrl, nc), t = vec_of(target, k);
+        auto meas = measured_of(c);
+        check_targets(c, W, cv, "ctrl", meas);
+        check_targets(c, W, t, "target", meas);
+        for (uint64_t x : cv)
+            if (std::find(t.begin(), t.end(), x) != t.end())
+                raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + "ctrl/target");
+        uint64_t want = fan ? c->d : ipow(c->d, t.size());
+        if (DU != want) raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, W, ctx_of(c) + "U");
+        qgpu::Step s;
+        s.kind = fan ? qgpu::StepKind::CtrlFan : qgpu::StepKind::Ctrl;
+        s.U.assign(reinterpret_cast<const cd*>(U), reinterpret_cast<const cd*>(U) + DU * DU);
+        s.DU = DU;
+        s.ctrl = cv;
+        s.target = t;
+        if (shift) {
+            s.has_shift = true;
+            s.shift = vec_of(shift, nc);
+            for (uint64_t x : s.shift)
+                if (x >= c->d) raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + "shift");
+        }
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+qgpu_status qgpu_circuit_cctrl(qgpu_circuit* c, const double* U, uint64_t DU,
+                               const uint64_t* ctrl_dits, uint32_t nc,
+                               const uint64_t* target, uint32_t k,
+                               const uint64_t* shift, int fan) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = fan ? "qpp::QCircuit::cCTRL_fan()" : "qpp::QCircuit::cCTRL()";
+        auto cv = vec_of(ctrl_dits, nc), t = vec_of(target, k);
+        if (cv.empty()) raise(QGPU_ERR_ZERO_SIZE, W, ctx_of(c) + "ctrl_dits");
+        for (uint64_t x : cv)
+            if (x >= c->nc) raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + "ctrl_dits");
+        check_targets(c, W, t, "target", measured_of(c));
+        uint64_t want = fan ? c->d : ipow(c->d, t.size());
+        if (DU != want) raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, W, ctx_of(c) + "U");
+        qgpu::Step s;
+        s.kind = fan ? qgpu::StepKind::CCtrlFan : qgpu::StepKind::CCtrl;
+        s.U.assign(reinterpret_cast<const cd*>(U), reinterpret_cast<const cd*>(U) + DU * DU);
+        s.DU = DU;
+        s.ctrl = cv;
+        s.target = t;
+        if (shift) {
+            s.has_shift = true;
+            s.shift = vec_of(shift, nc);
+        }
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target, uint32_t k,
+                                 uint64_t c_reg, int destructive) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = k > 1 ? "qpp::QCircuit::measure_many()" : "qpp::QCircuit::measure()";
+        auto t = vec_of(target, k);
+        check_targets(c, W, t, "target", measured_of(c));
+        if (c_reg >= c->nc) raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + "c_reg");
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::Measure;
+        s.target = t;
+        s.c_reg = c_reg;
+        s.destructive = destructive != 0;
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq, uint64_t* n_steps) {
+    return guarded([&] {
+        need_handle(c);
+        if (nq) *nq = c->nq;
+        if (n_steps) *n_steps = c->steps.size();
+    });
+}
+
+qgpu_status qgpu_circuit_fuse(qgpu_circuit* c, uint32_t max_k, uint64_t* n_passes) {
+    return guarded([&] {
+        need_handle(c);
+        if (c->d != 2) raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_circuit_fuse()", "qubit circuits only");
+        if (max_k < 1 || max_k > 12)
+            raise(QGPU_ERR_OUT_OF_RANGE, "qgpu_circuit_fuse()", "max_k");
+        auto plan = qgpu::fuse(c->steps, c->nq, max_k);
+        if (n_passes) *n_passes = plan.size();
+    });
+}
+
+qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form) {
+    return guarded([&] {
+        need_handle(s);
+        need_handle(c);
+        if (s->dims.size() != c->nq)
+            raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, "qgpu_run_gates()", "state/circuit");
+        for (uint64_t x : s->dims)
+            if (x != c->d) raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, "qgpu_run_gates()", "state/circuit");
+        qgpu::run_gates(s, c, form, 0, c->steps.size());
+    });
+}
+
+qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U, const uint64_t* target, uint32_t k) {
+    return guarded([&] {
+        need_handle(s);
+        const char* W = "qgpu_apply_tc()";
+        auto t = vec_of(target, k);
+        if (s->kind != QGPU_KET || s->prec != QGPU_C64)
+            raise(QGPU_ERR_NOT_SUPPORTED, W, "complex64 kets only");
+        for (uint64_t x : s->dims)
+            if (x != 2) raise(QGPU_ERR_NOT_SUPPORTED, W, "qubits only");
+        int n = int(s->dims.size());
+        if (n < 13) raise(QGPU_ERR_NOT_SUPPORTED, W, "needs at least 13 qubits");
+        if (t.empty() || t.size() > 6) raise(QGPU_ERR_OUT_OF_RANGE, W, "target");
+        std::vector<int> q;
+        for (uint64_t x : t) {
+            if (x >= uint64_t(n)) raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
+            q.push_back(int(x));
+        }
+        std::vector<int> q6 = q;
+        for (int x = 0; q6.size() < 6; ++x)
+            if (std::find(q6.begin(), q6.end(), x) == q6.end()) q6.push_back(x);
+        uint64_t DA = uint64_t(1) << q.size();
+        std::vector<cd> G(reinterpret_cast<const cd*>(U), reinterpret_cast<const cd*>(U) + DA * DA);
+        std::vector<cd> U6 = qgpu::embed(G, q, q6);
+        std::vector<float> B(128 * 128);
+        qgpu::fused6_matrix(U6.data(), B.data());
+        float* dB = static_cast<float*>(qgpu::ctx_scratch(s->ctx, B.size() * sizeof(float)));
+        QG_CUDA(cudaMemcpyAsync(dB, B.data(), B.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                s->ctx->stream));
+        int tb[6];
+        for (int j = 0; j < 6; ++j) tb[j] = n - 1 - q6[size_t(j)];
+        qgpu::launch_fused6_tc(s->ctx, s->data, n, tb, dB);
+        if (qgpu::fused_error(s->ctx))
+            raise(QGPU_ERR_TIMEOUT, W, "tensor-core pass timed out");
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,273 @@
+// circuit.cpp -- gate fusion planner and the plain / fused execution forms.
+#include "circuit.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+
+#include "kernels.hpp"
+#include "ops.hpp"
+
+qgpu_circuit::~qgpu_circuit() {
+    if (dB) cudaFree(dB);
+}
+
+namespace qgpu {
+
+void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
+                      const float* dB);
+void fused6_matrix(const cd* U, float* B);
+int fused_error(qgpu_ctx* ctx);
+
+// E on block qubits bq (big-endian), with G acting on gq (subset of bq).
+std::vector<cd> embed(const std::vector<cd>& G, const std::vector<int>& gq,
+                      const std::vector<int>& bq) {
+    int kb = int(bq.size()), kg = int(gq.size());
+    uint64_t Db = uint64_t(1) << kb, Dg = uint64_t(1) << kg;
+    std::vector<int> pos(kg); // bit of the block index holding gq[j]
+    uint64_t mask = 0;
+    for (int j = 0; j < kg; ++j) {
+        int p = int(std::find(bq.begin(), bq.end(), gq[j]) - bq.begin());
+        pos[j] = kb - 1 - p;
+        mask |= uint64_t(1) << pos[j];
+    }
+    std::vector<cd> E(Db * Db, 0.0);
+    for (uint64_t c = 0; c < Db; ++c) {
+        uint64_t gc = 0;
+        for (int j = 0; j < kg; ++j) gc |= ((c >> pos[j]) & 1) << (kg - 1 - j);
+        for (uint64_t gr = 0; gr < Dg; ++gr) {
+            uint64_t r = c & ~mask;
+            for (int j = 0; j < kg; ++j) r |= ((gr >> (kg - 1 - j)) & 1) << pos[j];
+            E[r + c * Db] = G[gr + gc * Dg];
+        }
+    }
+    return E;
+}
+
+static std::vector<cd> matmul(const std::vector<cd>& A, const std::vector<cd>& B,
+                              uint64_t m) {
+    std::vector<cd> C(m * m, 0.0);
+    for (uint64_t j = 0; j < m; ++j)
+        for (uint64_t l = 0; l < m; ++l) {
+            cd b = B[l + j * m];
+            if (b == cd(0.0)) continue;
+            for (uint64_t i = 0; i < m; ++i) C[i + j * m] += A[i + l * m] * b;
+        }
+    return C;
+}
+
+static std::vector<cd> kron_pow(const std::vector<cd>& U, int m) {
+    std::vector<cd> R{cd(1.0)};
+    uint64_t dr = 1;
+    for (int i = 0; i < m; ++i) {
+        R = kron_mat(R, dr, U, 2);
+        dr *= 2;
+    }
+    return R;
+}
+
+bool step_dense(const Step& s, uint32_t max_k, std::vector<int>& qubits,
+                std::vector<cd>& U) {
+    qubits.clear();
+    switch (s.kind) {
+        case StepKind::Gate:
+            for (uint64_t t : s.target) qubits.push_back(int(t));
+            if (qubits.size() > max_k) return false;
+            U = s.U;
+            return true;
+        case StepKind::Fan:
+            for (uint64_t t : s.target) qubits.push_back(int(t));
+            if (qubits.size() > max_k) return false;
+            U = kron_pow(s.U, int(s.target.size()));
+            return true;
+        case StepKind::Ctrl:
+        case StepKind::CtrlFan: {
+            for (uint64_t c : s.ctrl) qubits.push_back(int(c));
+            for (uint64_t t : s.target) qubits.push_back(int(t));
+            if (qubits.size() > max_k) return false;
+            int nc = int(s.ctrl.size()), nt = int(s.target.size());
+            std::vector<cd> G = s.kind == StepKind::Ctrl ? s.U : kron_pow(s.U, nt);
+            uint64_t Dt = uint64_t(1) << nt, D = uint64_t(1) << (nc + nt);
+            // control pattern: the gate acts when every control bit equals
+            // (shift_inv + 1) % 2 with shift_inv = (2 - shift) % 2 = shift
+            uint64_t want = 0;
+            for (int i = 0; i < nc; ++i) {
+                uint64_t sh = s.has_shift ? s.shift[i] % 2 : 0;
+                if (((sh + 1) % 2) == 1) want |= uint64_t(1) << (nc - 1 - i);
+            }
+            U.assign(D * D, 0.0);
+            for (uint64_t c = 0; c < D; ++c) {
+                uint64_t cc = c >> nt, ct = c & (Dt - 1);
+                if (cc != want) {
+                    U[c + c * D] = 1.0;
+                    continue;
+                }
+                for (uint64_t rt = 0; rt < Dt; ++rt) U[(cc << nt | rt) + c * D] = G[rt + ct * Dt];
+            }
+            return true;
+        }
+        default:
+            return false;
+    }
+}
+
+std::vector<Block> fuse(const std::vector<Step>& steps, uint32_t nq, uint32_t max_k) {
+    std::vector<Block> plan;
+    std::vector<Block> open;
+    std::vector<int> owner(nq, -1); // qubit -> index in `open`, -1 none
+    auto rebuild_owner = [&] {
+        std::fill(owner.begin(), owner.end(), -1);
+        for (size_t b = 0; b < open.size(); ++b)
+            for (int q : open[b].qubits) owner[size_t(q)] = int(b);
+    };
+    auto emit = [&](std::vector<int> ids) {
+        std::sort(ids.begin(), ids.end());
+        ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+        for (int id : ids) plan.push_back(open[size_t(id)]);
+        for (size_t i = ids.size(); i-- > 0;) open.erase(open.begin() + ids[i]);
+        rebuild_owner();
+    };
+    for (size_t i = 0; i < steps.size(); ++i) {
+        std::vector<int> q;
+        std::vector<cd> G;
+        if (!step_dense(steps[i], max_k, q, G)) {
+            std::vector<int> all(open.size());
+            for (size_t b = 0; b < open.size(); ++b) all[b] = int(b);
+            emit(all);
+            Block pass;
+            pass.step = int(i);
+            plan.push_back(pass);
+            continue;
+        }
+        std::vector<int> touched;
+        for (int x : q)
+            if (owner[size_t(x)] >= 0) touched.push_back(owner[size_t(x)]);
+        std::sort(touched.begin(), touched.end());
+        touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+        std::vector<int> uq;
+        for (int b : touched)
+            for (int x : open[size_t(b)].qubits) uq.push_back(x);
+        for (int x : q)
+            if (std::find(uq.begin(), uq.end(), x) == uq.end()) uq.push_back(x);
+        Block nb;
+        if (uq.size() <= max_k) {
+            nb.qubits = uq;
+            uint64_t Db = uint64_t(1) << uq.size();
+            std::vector<cd> M(Db * Db, 0.0);
+            for (uint64_t j = 0; j < Db; ++j) M[j + j * Db] = 1.0;
+            for (int b : touched) M = matmul(embed(open[size_t(b)].U, open[size_t(b)].qubits, uq), M, Db);
+            nb.U = matmul(embed(G, q, uq), M, Db);
+            std::vector<int> rm = touched;
+            for (size_t r = rm.size(); r-- > 0;) open.erase(open.begin() + rm[r]);
+        } else {
+            emit(touched);
+            nb.qubits = q;
+            nb.U = G;
+        }
+        open.push_back(nb);
+        rebuild_owner();
+    }
+    std::vector<int> all(open.size());
+    for (size_t b = 0; b < open.size(); ++b) all[b] = int(b);
+    emit(all);
+    return plan;
+}
+
+void apply_step(qgpu_state* s, const Step& st) {
+    auto shift_inv = [&](uint64_t d) {
+        std::vector<uint64_t> r(st.ctrl.size(), 0);
+        if (st.has_shift)
+            for (size_t i = 0; i < r.size(); ++i) r[i] = (d - st.shift[i] % d) % d;
+        return r;
+    };
+    switch (st.kind) {
+        case StepKind::Gate:
+            op_apply(s, st.U.data(), st.DU, st.target);
+            break;
+        case StepKind::Fan:
+            for (uint64_t t : st.target) op_apply(s, st.U.data(), st.DU, {t});
+            break;
+        case StepKind::Ctrl:
+        case StepKind::CtrlFan: {
+            uint64_t d = s->dims[st.ctrl[0]];
+            op_apply_ctrl(s, st.U.data(), st.DU, st.ctrl, st.target, shift_inv(d),
+                          st.kind == StepKind::CtrlFan);
+            break;
+        }
+        case StepKind::Nop:
+            break;
+        default:
+            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
+                  "measurement or classically controlled step: use the engine");
+    }
+}
+
+static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
+    if (c->plan_k != k) {
+        c->plan = fuse(c->steps, c->nq, k);
+        c->plan_k = k;
+        if (c->dB) {
+            cudaFree(c->dB);
+            c->dB = nullptr;
+        }
+        c->block_slot.clear();
+    }
+    bool tc = s->prec == QGPU_C64 && c->nq >= 13 && k == 6;
+    if (!tc || c->dB) return;
+    c->block_slot.assign(c->plan.size(), -1);
+    int64_t nslot = 0;
+    for (size_t i = 0; i < c->plan.size(); ++i)
+        if (c->plan[i].step < 0 && c->plan[i].qubits.size() >= 3) c->block_slot[i] = nslot++;
+    if (nslot == 0) return;
+    std::vector<float> host(size_t(nslot) * 128 * 128);
+    for (size_t i = 0; i < c->plan.size(); ++i) {
+        if (c->block_slot[i] < 0) continue;
+        const Block& b = c->plan[i];
+        std::vector<int> q6 = b.qubits;
+        for (int x = 0; int(q6.size()) < 6 && x < int(c->nq); ++x)
+            if (std::find(q6.begin(), q6.end(), x) == q6.end()) q6.push_back(x);
+        std::vector<cd> U6 = embed(b.U, b.qubits, q6);
+        c->plan[i].qubits = q6; // executed as a 6-qubit block
+        c->plan[i].U = U6;
+        fused6_matrix(U6.data(), host.data() + size_t(c->block_slot[i]) * 128 * 128);
+    }
+    QG_CUDA(cudaMalloc(&c->dB, host.size() * sizeof(float)));
+    QG_CUDA(cudaMemcpy(c->dB, host.data(), host.size() * sizeof(float),
+                       cudaMemcpyHostToDevice));
+    c->plan_ctx = s->ctx;
+}
+
+void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_t count) {
+    if (form == 0) {
+        for (uint64_t i = first; i < first + count && i < c->steps.size(); ++i)
+            apply_step(s, c->steps[i]);
+        return;
+    }
+    if (s->kind != QGPU_KET || c->d != 2)
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
+    if (first != 0 || count < c->steps.size())
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form runs whole circuits");
+    uint32_t k = s->prec == QGPU_C64 ? 6 : 3;
+    prepare_plan(s, c, k);
+    VSpace vs = vspace_ket(s->dims);
+    int nb = int(c->nq);
+    for (size_t i = 0; i < c->plan.size(); ++i) {
+        const Block& b = c->plan[i];
+        if (b.step >= 0) {
+            apply_step(s, c->steps[size_t(b.step)]);
+            continue;
+        }
+        if (!c->block_slot.empty() && c->block_slot[i] >= 0) {
+            int tb[6];
+            for (int j = 0; j < 6; ++j) tb[j] = nb - 1 - b.qubits[size_t(j)];
+            launch_fused6_tc(s->ctx, s->data, nb, tb,
+                             c->dB + size_t(c->block_slot[i]) * 128 * 128);
+            continue;
+        }
+        vapply(s, vs, b.qubits, {}, b.U.data(), uint64_t(1) << b.qubits.size());
+    }
+    if (!c->block_slot.empty() && fused_error(s->ctx))
+        raise(QGPU_ERR_TIMEOUT, "qgpu_run_gates()", "tensor-core pass timed out");
+}
+
+} // namespace qgpu

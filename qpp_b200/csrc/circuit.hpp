@@ -1,0 +1,90 @@
+// circuit.hpp -- circuit description, gate fusion and execution forms.
+//
+// A qgpu_circuit mirrors the steps of qpp::QCircuit that the engines execute
+// (include/qpp/classes/qcircuit.hpp: gate :1166-1444, CTRL :1985-2322,
+// measure :2983; step kinds internal/classes/qcircuit_gate_step.hpp and
+// qcircuit_measurement_step.hpp). Gate matrices are stored once per step on
+// the host and uploaded on use.
+//
+// Fusion (no reference counterpart): consecutive unitary steps on qubit
+// circuits are merged greedily into dense blocks of at most k qubits. Open
+// blocks act on disjoint qubits, so they commute; a gate joins (and merges)
+// the open blocks it touches while the union stays within k qubits,
+// otherwise those blocks are emitted first. Non-unitary steps flush every
+// open block.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "internal.hpp"
+
+namespace qgpu {
+
+using cd = std::complex<double>;
+
+enum class StepKind {
+    Gate,      // apply(U, target)           GType SINGLE/TWO/THREE/JOINT
+    Fan,       // apply(U, {t}) for each t   GType FAN
+    Ctrl,      // applyCTRL                  GType CTRL
+    CtrlFan,   // applyCTRL_fan              GType CTRL_FAN
+    CCtrl,     // classically controlled     GType cCTRL
+    CCtrlFan,  // classically controlled fan GType cCTRL_FAN
+    Measure,   // Z-basis measure_seq        MType MEASURE / MEASURE_MANY (+ _ND)
+    Reset,     // reset targets to |0>
+    Nop
+};
+
+struct Step {
+    StepKind kind = StepKind::Nop;
+    std::vector<cd> U;
+    uint64_t DU = 0;
+    std::vector<uint64_t> target, ctrl, shift;
+    bool has_shift = false;
+    uint64_t c_reg = 0;
+    bool destructive = true;
+};
+
+struct Block {
+    std::vector<int> qubits; // big-endian order of the block index
+    std::vector<cd> U;       // 2^k x 2^k, column-major
+    int step = -1;           // >= 0: not fused, run step `step` as is
+};
+
+} // namespace qgpu
+
+struct qgpu_circuit {
+    uint32_t nq = 0;
+    uint64_t d = 2;
+    uint32_t nc = 0; // classical dits
+    std::vector<qgpu::Step> steps;
+    // fused plan cache
+    uint32_t plan_k = 0;
+    std::vector<qgpu::Block> plan;
+    // device copies of the tensor-core block matrices (fp32, 128 x 128 each)
+    qgpu_ctx* plan_ctx = nullptr;
+    float* dB = nullptr;
+    std::vector<int64_t> block_slot; // plan index -> slot in dB, or -1
+    ~qgpu_circuit();
+};
+
+namespace qgpu {
+
+// Dense matrix of the step on its qubits (ctrl + target order), for steps
+// that can be fused; false if the step is not unitary or too wide.
+bool step_dense(const Step& s, uint32_t max_k, std::vector<int>& qubits,
+                std::vector<cd>& U);
+std::vector<cd> embed(const std::vector<cd>& G, const std::vector<int>& gq,
+                      const std::vector<int>& bq);
+std::vector<Block> fuse(const std::vector<Step>& steps, uint32_t nq,
+                        uint32_t max_k);
+
+// Runs the unitary steps [first, first + count) of `c` on `s`:
+// form 0 = plain (one pass per qpp call), form 1 = fused blocks.
+void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first,
+               uint64_t count);
+void apply_step(qgpu_state* s, const Step& st);
+
+} // namespace qgpu

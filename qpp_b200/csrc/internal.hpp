@@ -25,6 +25,8 @@ struct qgpu_ctx {
     // Pinned host buffer for small device -> host results.
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // Device word where kernels with bounded waits record a timeout.
+    int* dev_flag = nullptr;
 };
 
 struct qgpu_state {
