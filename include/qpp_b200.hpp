@@ -1,0 +1,308 @@
+// qpp_b200.hpp -- C++17 drop-in layer over the C ABI (qpp_b200.h).
+//
+// Mirrors the Quantum++ 7.0.3 free functions of the gate-application and
+// subsystem path with the same names, argument meaning, value semantics and
+// exception types (include/qpp/operations.hpp, classes/exception.hpp):
+//
+//   qpp_b200::apply(state, A, target, dims)                 operations.hpp:72
+//   qpp_b200::apply(state, A, target, d)                    operations.hpp:386
+//   qpp_b200::applyCTRL(state, A, ctrl, target, dims, shift) operations.hpp:616
+//   qpp_b200::applyCTRL_fan(...)                            operations.hpp:961
+//   qpp_b200::apply(rho, Ks, target, dims)                  operations.hpp:476
+//   qpp_b200::ptrace(A, target, dims)                       operations.hpp:1908
+//   qpp_b200::ptranspose(A, target, dims)                   operations.hpp:2167
+//   qpp_b200::syspermute(A, perm, dims)                     operations.hpp:2386
+//
+// Matrices are qpp_b200::cmat (column-major std::complex<double>, rows x
+// cols; a ket is D x 1). When Eigen is available the same functions accept
+// and return Eigen::MatrixXcd / VectorXcd, so code written against qpp::
+// compiles against qpp_b200:: unchanged. Errors throw
+// qpp_b200::exception::<QppName> carrying qpp's (where, what) strings.
+// Header-only; link with libqpp_b200.so.
+#ifndef QPP_B200_HPP_
+#define QPP_B200_HPP_
+
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "qpp_b200.h"
+
+#if defined(__has_include)
+#if __has_include(<Eigen/Dense>)
+#include <Eigen/Dense>
+#define QPP_B200_HAS_EIGEN 1
+#endif
+#endif
+
+namespace qpp_b200 {
+
+using idx = std::size_t;
+using cplx = std::complex<double>;
+
+struct cmat {
+    idx rows_ = 0, cols_ = 0;
+    std::vector<cplx> data_; // column-major
+    cmat() = default;
+    cmat(idx r, idx c) : rows_(r), cols_(c), data_(r * c, cplx(0.0)) {}
+    idx rows() const { return rows_; }
+    idx cols() const { return cols_; }
+    cplx& operator()(idx r, idx c) { return data_[r + c * rows_]; }
+    const cplx& operator()(idx r, idx c) const { return data_[r + c * rows_]; }
+    cplx& operator()(idx i) { return data_[i]; }
+    const cplx& operator()(idx i) const { return data_[i]; }
+    const double* raw() const { return reinterpret_cast<const double*>(data_.data()); }
+    double* raw() { return reinterpret_cast<double*>(data_.data()); }
+};
+using ket = cmat;
+
+namespace exception {
+// qpp::exception::Exception (classes/exception.hpp:68-127): what() is
+// "IN " + where + ": Exception <type>! " + description.
+class Exception : public std::runtime_error {
+  public:
+    Exception(std::string type, std::string where, std::string what)
+        : std::runtime_error("IN " + where + ": Exception " + type + "! " + what),
+          type_(std::move(type)), where_(std::move(where)), what_(std::move(what)) {}
+    const std::string& type_description() const { return type_; }
+    const std::string& where() const { return where_; }
+    const std::string& detail() const { return what_; }
+
+  private:
+    std::string type_, where_, what_;
+};
+#define QPP_B200_EXC(Name)                                                    \
+    class Name : public Exception {                                          \
+      public:                                                                \
+        Name(std::string where, std::string what)                            \
+            : Exception(#Name, std::move(where), std::move(what)) {}         \
+    };
+QPP_B200_EXC(ZeroSize)
+QPP_B200_EXC(MatrixNotSquare)
+QPP_B200_EXC(MatrixNotSquareNorCvector)
+QPP_B200_EXC(MatrixMismatchSubsys)
+QPP_B200_EXC(DimsInvalid)
+QPP_B200_EXC(DimsNotEqual)
+QPP_B200_EXC(DimsMismatchMatrix)
+QPP_B200_EXC(DimsMismatchCvector)
+QPP_B200_EXC(SubsysMismatchDims)
+QPP_B200_EXC(PermInvalid)
+QPP_B200_EXC(PermMismatchDims)
+QPP_B200_EXC(OutOfRange)
+QPP_B200_EXC(TypeMismatch)
+QPP_B200_EXC(SizeMismatch)
+QPP_B200_EXC(QuditAlreadyMeasured)
+QPP_B200_EXC(MatrixNotSquareNorVector)
+QPP_B200_EXC(Duplicates)
+QPP_B200_EXC(DeviceError)
+#undef QPP_B200_EXC
+} // namespace exception
+
+namespace detail {
+
+[[noreturn]] inline void throw_status(qgpu_status s) {
+    std::string w = qgpu_last_error_where(), m = qgpu_last_error_what();
+    using namespace exception;
+    switch (s) {
+        case QGPU_ERR_ZERO_SIZE: throw ZeroSize(w, m);
+        case QGPU_ERR_MATRIX_NOT_SQUARE: throw MatrixNotSquare(w, m);
+        case QGPU_ERR_MATRIX_NOT_SQUARE_NOR_CVECTOR: throw MatrixNotSquareNorCvector(w, m);
+        case QGPU_ERR_MATRIX_MISMATCH_SUBSYS: throw MatrixMismatchSubsys(w, m);
+        case QGPU_ERR_DIMS_INVALID: throw DimsInvalid(w, m);
+        case QGPU_ERR_DIMS_NOT_EQUAL: throw DimsNotEqual(w, m);
+        case QGPU_ERR_DIMS_MISMATCH_MATRIX: throw DimsMismatchMatrix(w, m);
+        case QGPU_ERR_DIMS_MISMATCH_CVECTOR: throw DimsMismatchCvector(w, m);
+        case QGPU_ERR_SUBSYS_MISMATCH_DIMS: throw SubsysMismatchDims(w, m);
+        case QGPU_ERR_PERM_INVALID: throw PermInvalid(w, m);
+        case QGPU_ERR_PERM_MISMATCH_DIMS: throw PermMismatchDims(w, m);
+        case QGPU_ERR_OUT_OF_RANGE: throw OutOfRange(w, m);
+        case QGPU_ERR_TYPE_MISMATCH: throw TypeMismatch(w, m);
+        case QGPU_ERR_SIZE_MISMATCH: throw SizeMismatch(w, m);
+        case QGPU_ERR_QUDIT_ALREADY_MEASURED: throw QuditAlreadyMeasured(w, m);
+        case QGPU_ERR_MATRIX_NOT_SQUARE_NOR_VECTOR: throw MatrixNotSquareNorVector(w, m);
+        case QGPU_ERR_DUPLICATES: throw Duplicates(w, m);
+        case QGPU_ERR_DIVISION_BY_ZERO: throw std::overflow_error(w + ": " + m);
+        default: throw DeviceError(w, std::string(qgpu_status_name(s)) + ": " + m);
+    }
+}
+
+inline void check(qgpu_status s) {
+    if (s != QGPU_OK) throw_status(s);
+}
+
+// One context per thread on device 0 unless set_device() chose another.
+inline int& device_slot() {
+    static thread_local int dev = 0;
+    return dev;
+}
+struct CtxHolder {
+    qgpu_ctx* c = nullptr;
+    int dev = -1;
+    ~CtxHolder() {
+        if (c) qgpu_ctx_destroy(c);
+    }
+};
+inline qgpu_ctx* ctx() {
+    static thread_local CtxHolder h;
+    if (!h.c || h.dev != device_slot()) {
+        if (h.c) qgpu_ctx_destroy(h.c);
+        h.c = nullptr;
+        check(qgpu_ctx_create(device_slot(), &h.c));
+        h.dev = device_slot();
+    }
+    return h.c;
+}
+
+inline std::vector<uint64_t> u64(const std::vector<idx>& v) {
+    return std::vector<uint64_t>(v.begin(), v.end());
+}
+inline const uint64_t* ptr(const std::vector<uint64_t>& v) {
+    return v.empty() ? nullptr : v.data();
+}
+
+// get_num_subsys (internal/util.hpp:389-397)
+inline std::vector<idx> dims_of(idx D, idx d) {
+    idx n = static_cast<idx>(std::llround(std::log2(static_cast<double>(D)) /
+                                          std::log2(static_cast<double>(d))));
+    return std::vector<idx>(n, d);
+}
+
+} // namespace detail
+
+// Select the CUDA device used by the calling thread.
+inline void set_device(int device) { detail::device_slot() = device; }
+
+inline cmat apply(const cmat& state, const cmat& A, const std::vector<idx>& target,
+                  const std::vector<idx>& dims) {
+    auto t = detail::u64(target), d = detail::u64(dims);
+    cmat out(state.rows(), state.cols());
+    detail::check(qgpu_host_apply(detail::ctx(), state.raw(), state.rows(), state.cols(),
+                                  A.raw(), A.rows(), A.cols(), detail::ptr(t),
+                                  uint32_t(t.size()), detail::ptr(d), uint32_t(d.size()),
+                                  out.raw()));
+    return out;
+}
+
+inline cmat apply(const cmat& state, const cmat& A, const std::vector<idx>& target,
+                  idx d = 2) {
+    if (state.rows() * state.cols() == 0)
+        throw exception::ZeroSize("qpp::apply()", "state");
+    if (d < 2) throw exception::DimsInvalid("qpp::apply()", "d");
+    return apply(state, A, target, detail::dims_of(state.rows(), d));
+}
+
+inline cmat applyCTRL(const cmat& state, const cmat& A, const std::vector<idx>& ctrl,
+                      const std::vector<idx>& target, const std::vector<idx>& dims,
+                      std::optional<std::vector<idx>> shift = std::nullopt) {
+    auto c = detail::u64(ctrl), t = detail::u64(target), d = detail::u64(dims);
+    std::vector<uint64_t> s;
+    if (shift) s = detail::u64(*shift);
+    cmat out(state.rows(), state.cols());
+    detail::check(qgpu_host_apply_ctrl(
+        detail::ctx(), state.raw(), state.rows(), state.cols(), A.raw(), A.rows(), A.cols(),
+        detail::ptr(c), uint32_t(c.size()), detail::ptr(t), uint32_t(t.size()),
+        detail::ptr(d), uint32_t(d.size()), shift ? s.data() : nullptr, 0, out.raw()));
+    return out;
+}
+
+inline cmat applyCTRL_fan(const cmat& state, const cmat& A, const std::vector<idx>& ctrl,
+                          const std::vector<idx>& target, const std::vector<idx>& dims,
+                          std::optional<std::vector<idx>> shift = std::nullopt) {
+    auto c = detail::u64(ctrl), t = detail::u64(target), d = detail::u64(dims);
+    std::vector<uint64_t> s;
+    if (shift) s = detail::u64(*shift);
+    cmat out(state.rows(), state.cols());
+    detail::check(qgpu_host_apply_ctrl(
+        detail::ctx(), state.raw(), state.rows(), state.cols(), A.raw(), A.rows(), A.cols(),
+        detail::ptr(c), uint32_t(c.size()), detail::ptr(t), uint32_t(t.size()),
+        detail::ptr(d), uint32_t(d.size()), shift ? s.data() : nullptr, 1, out.raw()));
+    return out;
+}
+
+inline cmat apply(const cmat& rho, const std::vector<cmat>& Ks,
+                  const std::vector<idx>& target, const std::vector<idx>& dims) {
+    auto t = detail::u64(target), d = detail::u64(dims);
+    std::vector<cplx> packed;
+    idx kr = Ks.empty() ? 0 : Ks[0].rows(), kc = Ks.empty() ? 0 : Ks[0].cols();
+    for (auto& K : Ks) {
+        if (K.rows() != kr || K.cols() != kc)
+            throw exception::DimsNotEqual("qpp::apply()", "K");
+        packed.insert(packed.end(), K.data_.begin(), K.data_.end());
+    }
+    cmat out(rho.rows(), rho.cols());
+    detail::check(qgpu_host_apply_kraus(
+        detail::ctx(), rho.raw(), rho.rows(), rho.cols(),
+        reinterpret_cast<const double*>(packed.data()), uint32_t(Ks.size()), kr, kc,
+        detail::ptr(t), uint32_t(t.size()), detail::ptr(d), uint32_t(d.size()), out.raw()));
+    return out;
+}
+
+inline cmat ptrace(const cmat& A, const std::vector<idx>& target, const std::vector<idx>& dims) {
+    auto t = detail::u64(target), d = detail::u64(dims);
+    idx DS = 1;
+    for (idx x : target)
+        if (x < dims.size()) DS *= dims[x];
+    idx Db = (DS && A.rows() % DS == 0) ? A.rows() / DS : 1;
+    cmat out(Db, Db);
+    detail::check(qgpu_host_ptrace(detail::ctx(), A.raw(), A.rows(), A.cols(), detail::ptr(t),
+                                   uint32_t(t.size()), detail::ptr(d), uint32_t(d.size()),
+                                   out.raw()));
+    return out;
+}
+
+inline cmat ptranspose(const cmat& A, const std::vector<idx>& target,
+                       const std::vector<idx>& dims) {
+    auto t = detail::u64(target), d = detail::u64(dims);
+    cmat out(A.rows(), A.rows());
+    detail::check(qgpu_host_ptranspose(detail::ctx(), A.raw(), A.rows(), A.cols(),
+                                       detail::ptr(t), uint32_t(t.size()), detail::ptr(d),
+                                       uint32_t(d.size()), out.raw()));
+    return out;
+}
+
+inline cmat syspermute(const cmat& A, const std::vector<idx>& perm, const std::vector<idx>& dims) {
+    auto p = detail::u64(perm), d = detail::u64(dims);
+    cmat out(A.rows(), A.cols());
+    detail::check(qgpu_host_syspermute(detail::ctx(), A.raw(), A.rows(), A.cols(),
+                                       detail::ptr(p), uint32_t(p.size()), detail::ptr(d),
+                                       uint32_t(d.size()), out.raw()));
+    return out;
+}
+
+#ifdef QPP_B200_HAS_EIGEN
+// Eigen adapters: same calls on Eigen::MatrixXcd / VectorXcd.
+namespace detail {
+template <typename D>
+cmat from_eigen(const Eigen::MatrixBase<D>& m) {
+    Eigen::MatrixXcd e = m.template cast<cplx>();
+    cmat r(idx(e.rows()), idx(e.cols()));
+    for (idx j = 0; j < r.cols(); ++j)
+        for (idx i = 0; i < r.rows(); ++i) r(i, j) = e(Eigen::Index(i), Eigen::Index(j));
+    return r;
+}
+inline Eigen::MatrixXcd to_eigen(const cmat& m) {
+    Eigen::MatrixXcd e(Eigen::Index(m.rows()), Eigen::Index(m.cols()));
+    for (idx j = 0; j < m.cols(); ++j)
+        for (idx i = 0; i < m.rows(); ++i) e(Eigen::Index(i), Eigen::Index(j)) = m(i, j);
+    return e;
+}
+} // namespace detail
+template <typename D1, typename D2>
+Eigen::MatrixXcd apply(const Eigen::MatrixBase<D1>& s, const Eigen::MatrixBase<D2>& A,
+                       const std::vector<idx>& target, const std::vector<idx>& dims) {
+    return detail::to_eigen(apply(detail::from_eigen(s), detail::from_eigen(A), target, dims));
+}
+template <typename D>
+Eigen::MatrixXcd ptrace(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+                        const std::vector<idx>& dims) {
+    return detail::to_eigen(ptrace(detail::from_eigen(A), target, dims));
+}
+#endif
+
+} // namespace qpp_b200
+
+#endif // QPP_B200_HPP_

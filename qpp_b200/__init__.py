@@ -41,7 +41,7 @@ _STATUS = {
     7: "DimsMismatchMatrix", 8: "DimsMismatchCvector", 9: "SubsysMismatchDims",
     10: "PermInvalid", 11: "PermMismatchDims", 12: "OutOfRange",
     13: "TypeMismatch", 14: "SizeMismatch", 15: "QuditAlreadyMeasured",
-    16: "MatrixNotSquareNorVector", 17: "DivisionByZero", 100: "CudaError",
+    16: "MatrixNotSquareNorVector", 17: "DivisionByZero", 18: "Duplicates", 100: "CudaError",
     101: "OutOfMemory", 102: "Timeout", 103: "InvalidHandle",
     104: "NotSupported", 105: "InvalidArgument",
 }
@@ -391,3 +391,97 @@ def syspermute(state, perm, dims, ctx=None):
     check(lib().qgpu_host_syspermute(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols), pp,
                                      ct.c_uint32(npm), dpp, ct.c_uint32(nd), _dp(out)))
     return out
+
+
+# ------------------------------------------------------------------ circuits
+PLAIN, FUSED = 0, 1
+
+
+class Circuit:
+    """Step list of qpp::QCircuit (include/qpp/classes/qcircuit.hpp): gates,
+    fan gates, (classically) controlled gates and Z-basis measurements."""
+
+    def __init__(self, nq, d=2, nc=0):
+        self.h = vp()
+        check(lib().qgpu_circuit_create(ct.c_uint32(nq), ct.c_uint64(d), ct.c_uint32(nc),
+                                        ct.byref(self.h)))
+        self.nq, self.d, self.nc = nq, d, nc
+
+    def gate(self, U, target):
+        U = _mat(U)
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_circuit_gate(self.h, _dp(U), ct.c_uint64(U.shape[0]), tp, ct.c_uint32(nt)))
+        return self
+
+    def gate_fan(self, U, target):
+        U = _mat(U)
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_circuit_gate_fan(self.h, _dp(U), ct.c_uint64(U.shape[0]), tp,
+                                          ct.c_uint32(nt)))
+        return self
+
+    def CTRL(self, U, ctrl, target, shift=None, fan=False):
+        U = _mat(U)
+        c, cp, nc = _u64(ctrl)
+        t, tp, nt = _u64(target)
+        s, sp, _ = _u64(shift)
+        check(lib().qgpu_circuit_ctrl(self.h, _dp(U), ct.c_uint64(U.shape[0]), cp, ct.c_uint32(nc),
+                                      tp, ct.c_uint32(nt), sp, ct.c_int(1 if fan else 0)))
+        return self
+
+    def cCTRL(self, U, ctrl_dits, target, shift=None, fan=False):
+        U = _mat(U)
+        c, cp, nc = _u64(ctrl_dits)
+        t, tp, nt = _u64(target)
+        s, sp, _ = _u64(shift)
+        check(lib().qgpu_circuit_cctrl(self.h, _dp(U), ct.c_uint64(U.shape[0]), cp,
+                                       ct.c_uint32(nc), tp, ct.c_uint32(nt), sp,
+                                       ct.c_int(1 if fan else 0)))
+        return self
+
+    def measure(self, target, c_reg=0, destructive=True):
+        t, tp, nt = _u64(target if isinstance(target, (list, tuple)) else [target])
+        check(lib().qgpu_circuit_measure(self.h, tp, ct.c_uint32(nt), ct.c_uint64(c_reg),
+                                         ct.c_int(1 if destructive else 0)))
+        return self
+
+    def steps(self):
+        n = ct.c_uint64()
+        check(lib().qgpu_circuit_info(self.h, None, ct.byref(n)))
+        return n.value
+
+    def fused_passes(self, max_k=6):
+        n = ct.c_uint64()
+        check(lib().qgpu_circuit_fuse(self.h, ct.c_uint32(max_k), ct.byref(n)))
+        return n.value
+
+    def run(self, state, form=PLAIN):
+        """Apply the unitary steps to a resident State (in place)."""
+        check(lib().qgpu_run_gates(state.h, self.h, ct.c_int(form)))
+        return state
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().qgpu_circuit_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def apply_tc(state, U, target):
+    """One <= 6-qubit gate on a complex64 ket as a 64 x 64 tensor-core block."""
+    U = _mat(U)
+    t, tp, nt = _u64(target)
+    check(lib().qgpu_apply_tc(state.h, _dp(U), tp, ct.c_uint32(nt)))
+    return state
+
+
+def layered_circuit(n, depth, seed):
+    """The seeded layered circuit of qpp_b200.workloads as a Circuit."""
+    from . import workloads
+    c = Circuit(n)
+    for layer in workloads.layered_circuit(n, depth, seed):
+        for U, t in layer:
+            c.gate(U, t)
+    return c

@@ -120,10 +120,43 @@ std::vector<Block> fuse(const std::vector<Step>& steps, uint32_t nq, uint32_t ma
         for (size_t b = 0; b < open.size(); ++b)
             for (int q : open[b].qubits) owner[size_t(q)] = int(b);
     };
+    // Emitted blocks act on disjoint qubits, so they commute: pack them
+    // first-fit (largest first) into passes of at most max_k qubits.
     auto emit = [&](std::vector<int> ids) {
         std::sort(ids.begin(), ids.end());
         ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
-        for (int id : ids) plan.push_back(open[size_t(id)]);
+        std::vector<Block> out;
+        for (int id : ids) out.push_back(open[size_t(id)]);
+        std::stable_sort(out.begin(), out.end(), [](const Block& a, const Block& b) {
+            return a.qubits.size() > b.qubits.size();
+        });
+        std::vector<std::vector<Block>> bins;
+        for (auto& b : out) {
+            bool placed = false;
+            for (auto& bin : bins) {
+                size_t w = 0;
+                for (auto& x : bin) w += x.qubits.size();
+                if (w + b.qubits.size() <= max_k) {
+                    bin.push_back(b);
+                    placed = true;
+                    break;
+                }
+            }
+            if (!placed) bins.push_back({b});
+        }
+        for (auto& bin : bins) {
+            if (bin.size() == 1) {
+                plan.push_back(bin[0]);
+                continue;
+            }
+            Block m;
+            for (auto& x : bin) m.qubits.insert(m.qubits.end(), x.qubits.begin(), x.qubits.end());
+            uint64_t Dm = uint64_t(1) << m.qubits.size();
+            m.U.assign(Dm * Dm, 0.0);
+            for (uint64_t j = 0; j < Dm; ++j) m.U[j + j * Dm] = 1.0;
+            for (auto& x : bin) m.U = matmul(embed(x.U, x.qubits, m.qubits), m.U, Dm);
+            plan.push_back(m);
+        }
         for (size_t i = ids.size(); i-- > 0;) open.erase(open.begin() + ids[i]);
         rebuild_owner();
     };
