@@ -55,6 +55,16 @@ void* ctx_scratch(qgpu_ctx* ctx, size_t bytes) {
     return ctx->scratch;
 }
 
+void destroy_ctx(qgpu_ctx* ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->dev_flag) cudaFree(ctx->dev_flag);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
 void* ctx_pinned(qgpu_ctx* ctx, size_t bytes) {
     if (bytes <= ctx->pinned_bytes) return ctx->pinned;
     size_t nb = std::max<size_t>(bytes, 4096);
@@ -374,13 +384,10 @@ qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out) {
 qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx) {
     return guard([&] {
         check_handle(ctx);
-        cudaSetDevice(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
-        if (ctx->scratch) cudaFree(ctx->scratch);
-        if (ctx->pinned) cudaFreeHost(ctx->pinned);
-        if (ctx->dev_flag) cudaFree(ctx->dev_flag);
-        cudaStreamDestroy(ctx->stream);
-        delete ctx;
+        // states still alive keep the context (their memory lives on its
+        // stream); the last qgpu_state_destroy tears it down
+        ctx->closing.store(true);
+        if (ctx->live_states.load() == 0) qgpu::destroy_ctx(ctx);
     });
 }
 

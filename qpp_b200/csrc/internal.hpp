@@ -27,6 +27,10 @@ struct qgpu_ctx {
     size_t pinned_bytes = 0;
     // Device word where kernels with bounded waits record a timeout.
     int* dev_flag = nullptr;
+    // States created on this context that are still alive; a destroyed
+    // context is torn down only when the last of them is freed.
+    std::atomic<int64_t> live_states{0};
+    std::atomic<bool> closing{false};
 };
 
 struct qgpu_state {
@@ -71,6 +75,9 @@ void clear_error();
 
 // Checks the last launch on this thread and counts it on the context.
 void after_launch(qgpu_ctx* ctx, const char* name);
+
+// Frees the context's stream, buffers and the context itself.
+void destroy_ctx(qgpu_ctx* ctx);
 
 // Context scratch of at least `bytes` (stream-ordered reuse).
 void* ctx_scratch(qgpu_ctx* ctx, size_t bytes);

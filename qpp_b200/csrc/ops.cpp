@@ -188,14 +188,23 @@ qgpu_state* new_state(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
         raise(QGPU_ERR_OUT_OF_MEMORY, "qgpu_state_create()",
               "device allocation failed");
     }
-    if (zero) QG_CUDA(cudaMemsetAsync(s->data, 0, s->bytes(), ctx->stream));
+    ctx->live_states.fetch_add(1);
+    if (zero) {
+        cudaError_t z = cudaMemsetAsync(s->data, 0, s->bytes(), ctx->stream);
+        if (z != cudaSuccess) {
+            free_state(s);
+            raise(QGPU_ERR_CUDA, "qgpu_state_create()", cudaGetErrorString(z));
+        }
+    }
     return s;
 }
 
 void free_state(qgpu_state* s) {
     if (!s) return;
-    if (s->data) cudaFreeAsync(s->data, s->ctx->stream);
+    qgpu_ctx* ctx = s->ctx;
+    if (s->data) cudaFreeAsync(s->data, ctx->stream);
     delete s;
+    if (ctx->live_states.fetch_sub(1) == 1 && ctx->closing.load()) destroy_ctx(ctx);
 }
 
 static bool all_two(const std::vector<uint64_t>& d) {

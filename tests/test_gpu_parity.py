@@ -254,3 +254,17 @@ def test_config1_ket_gates(ctx):
         s.apply_ctrl(U, sub[:nc], sub[nc:])
         ref = orc.applyCTRL(ref, U, sub[:nc], sub[nc:], dims, path=1)
     assert relerr(s.numpy(), ref) < TOL128
+
+
+def test_states_outlive_a_closed_context():
+    """Destroying a context while states are alive defers the teardown to the
+    last state's destruction (no use after free)."""
+    import qpp_b200 as qb
+    c = qb.Context(0)
+    a = qb.State(c, qb.KET, [2] * 10).fill_gaussian(1)
+    b = a.ptrace([0, 1])
+    c.close()
+    assert abs(a.norm2() - 1) < 1e-12
+    del a
+    assert b.numpy().shape == (256, 256)
+    del b
