@@ -155,6 +155,26 @@ qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
  * perm[i] moves to position i; writes a new state of the same kind. */
 qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
                             uint32_t n, qgpu_state** out);
+/* Partial trace that allocates nothing. No counterpart in the reference:
+ * Quantum++ always returns a freshly allocated matrix. This entry point is
+ * for callers that cannot allocate device memory when they need the trace --
+ * an application whose own memory pool holds all of the GPU's free memory, or
+ * a latency-critical loop that cannot afford the device-wide synchronisation
+ * of cudaMalloc / cudaFree. The result (the Dbar x Dbar density matrix over
+ * the kept subsystems, column-major, in the state's precision, Dbar = D /
+ * prod dims[target]) is written to d_out, device memory the caller owns.
+ * The table of traced offsets lives in a fixed array of 65536 entries
+ * (512 KB) that the library keeps on every GPU that loads it until the
+ * process exits; a traced dimension prod dims[target] above 65536 is
+ * rejected with QGPU_ERR_NOT_SUPPORTED. The first call on a device looks up
+ * the array's device address (once per device) and should therefore come
+ * before any stream capture. Every call shares that one array: calls whose
+ * work overlaps on the GPU (different streams, different contexts of the
+ * same device) race on it, so serialise them. The work is queued on the
+ * state's context stream; synchronise that stream before reading d_out
+ * elsewhere. */
+qgpu_status qgpu_ptrace_noalloc(const qgpu_state* s, const uint64_t* target,
+                                uint32_t k, void* d_out);
 /* Squared norm (ket) or trace (rho, real and imaginary parts), FP64
  * accumulation. */
 qgpu_status qgpu_norm2(const qgpu_state* s, double* out);

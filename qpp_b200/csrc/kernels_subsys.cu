@@ -180,3 +180,198 @@ void launch_ptrace(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
 }
 
 } // namespace qgpu
+
+// ======================================================================
+// Allocation-free partial trace (qgpu_ptrace_noalloc).
+//
+// Some callers cannot allocate device memory at the moment they need a
+// partial trace: a host application whose memory pool owns all of the
+// GPU's free memory, or a latency-critical loop where the implicit device
+// synchronisation of cudaMalloc/cudaFree is not acceptable. For them the
+// table of traced offsets lives in a fixed array in device memory that the
+// library reserves when it is loaded (512 KB on every GPU that loads it,
+// held until the process exits), and the result goes to a buffer the caller
+// already owns. Nothing is allocated on the device or the host on the
+// success path.
+// ======================================================================
+#include <mutex>
+
+#include "capi_common.hpp"
+
+namespace qgpu {
+
+constexpr uint64_t kNoAllocMaxTraced = 65536; // entries of the offset table
+
+static __device__ __align__(256) uint64_t g_noalloc_toff[kNoAllocMaxTraced];
+
+struct TraceDigits {
+    int k;
+    uint64_t dim[64];
+    uint64_t stride[64]; // element stride of each traced digit (row + column for rho)
+};
+
+// toff[a] = sum_j digit_j(a) * stride[j], digits big-endian over the traced
+// subsystems in the order given.
+__global__ void __launch_bounds__(256)
+    k_fill_toff(uint64_t* __restrict__ toff, uint64_t DS, const __grid_constant__ TraceDigits td) {
+    for (uint64_t a = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; a < DS;
+         a += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t r = a, o = 0;
+        for (int j = td.k - 1; j >= 0; --j) {
+            o += (r % td.dim[j]) * td.stride[j];
+            r /= td.dim[j];
+        }
+        toff[a] = o;
+    }
+}
+
+// Device address of g_noalloc_toff, looked up once per device with that
+// device current (the host-side symbol is only a stand-in, never a device
+// address).
+static uint64_t* noalloc_table(int device) {
+    static std::mutex mu;
+    static uint64_t* addr[64] = {nullptr};
+    if (device < 0 || device >= 64)
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_ptrace_noalloc()", "device index above 63");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_toff);
+        if (e != cudaSuccess)
+            raise(QGPU_ERR_CUDA, "qgpu_ptrace_noalloc()", cudaGetErrorString(e));
+        addr[device] = static_cast<uint64_t*>(p);
+    }
+    return addr[device];
+}
+
+// Merged gather plan over fixed-size arrays (same rule as plan_gather).
+static void plan_gather_fixed(const uint64_t* od, const uint64_t* src, int n, SegPlan& p) {
+    std::memset(&p, 0, sizeof(p));
+    bool run = false;
+    uint64_t cs = 1, cst = 0;
+    auto push = [&](uint64_t size, uint64_t stride) {
+        if (size == 1) return;
+        if (p.nseg >= kMaxSeg)
+            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_ptrace_noalloc()", "too many index segments");
+        p.size[p.nseg] = size;
+        p.stride[p.nseg] = stride;
+        ++p.nseg;
+    };
+    for (int v = n - 1; v >= 0; --v) {
+        if (od[v] == 1) continue;
+        if (!run) {
+            cs = od[v];
+            cst = src[v];
+            run = true;
+        } else if (src[v] == cst * cs) {
+            cs *= od[v];
+        } else {
+            push(cs, cst);
+            cs = od[v];
+            cst = src[v];
+        }
+    }
+    if (run) push(cs, cst);
+    p.count = 1;
+    p.pow2 = 1;
+    for (int s = 0; s < p.nseg; ++s) {
+        p.count *= p.size[s];
+        if (p.size[s] & (p.size[s] - 1)) p.pow2 = 0;
+        int sh = 0;
+        while ((uint64_t(1) << sh) < p.size[s]) ++sh;
+        p.shift[s] = uint8_t(sh);
+    }
+}
+
+template <typename R>
+static void noalloc_launch(qgpu_ctx* ctx, const void* in, void* out, const SegPlan& ma,
+                           const SegPlan& mb, const uint64_t* toff, uint64_t DS, bool ket) {
+    const Cplx<R>* i = static_cast<const Cplx<R>*>(in);
+    Cplx<R>* o = static_cast<Cplx<R>*>(out);
+    bool warp = ma.count < uint64_t(ctx->num_sms) * 2048 && DS >= 32;
+    int b = blocks_for(ctx, warp ? ma.count * 32 : ma.count, 8);
+    if (warp) {
+        if (ket) k_ptrace_warp<R, true><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, toff, DS);
+        else k_ptrace_warp<R, false><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, toff, DS);
+    } else {
+        if (ket) k_ptrace_thread<R, true><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, toff, DS);
+        else k_ptrace_thread<R, false><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, toff, DS);
+    }
+    after_launch(ctx, "k_ptrace (no-alloc)");
+}
+
+} // namespace qgpu
+
+extern "C" qgpu_status qgpu_ptrace_noalloc(const qgpu_state* s, const uint64_t* target,
+                                           uint32_t k, void* d_out) {
+    using namespace qgpu;
+    return guarded([&] {
+        const char* W = "qgpu_ptrace_noalloc()";
+        need_handle(s);
+        if (!d_out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "d_out");
+        const int n = int(s->dims.size());
+        if (n > 64) raise(QGPU_ERR_NOT_SUPPORTED, W, "more than 64 subsystems");
+        if (k > uint32_t(n) || (k > 0 && !target))
+            raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, "qpp::ptrace()", "dims/target");
+        bool traced[64] = {false};
+        for (uint32_t j = 0; j < k; ++j) {
+            if (target[j] >= uint64_t(n) || traced[target[j]])
+                raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, "qpp::ptrace()", "dims/target");
+            traced[target[j]] = true;
+        }
+        uint64_t stride[64];
+        stride[n - 1] = 1;
+        for (int q = n - 1; q > 0; --q) stride[q - 1] = stride[q] * s->dims[size_t(q)];
+        const bool ket = s->kind == QGPU_KET;
+        const uint64_t D = s->D;
+        TraceDigits td;
+        td.k = int(k);
+        uint64_t DS = 1;
+        for (uint32_t j = 0; j < k; ++j) {
+            uint64_t q = target[j];
+            td.dim[j] = s->dims[q];
+            td.stride[j] = ket ? stride[q] : stride[q] * (D + 1);
+            DS *= s->dims[q];
+        }
+        if (DS > kNoAllocMaxTraced)
+            raise(QGPU_ERR_NOT_SUPPORTED, W,
+                  "traced dimension above 65536 (the fixed offset table)");
+        // output digits: [column digits of the kept subsystems, row digits]
+        uint64_t od[128], sa[128], sb[128];
+        int no = 0;
+        for (int q = 0; q < n; ++q)
+            if (!traced[q]) {
+                od[no] = s->dims[size_t(q)];
+                sa[no] = ket ? 0 : stride[q] * D;
+                sb[no] = ket ? stride[q] : 0;
+                ++no;
+            }
+        for (int q = 0; q < n; ++q)
+            if (!traced[q]) {
+                od[no] = s->dims[size_t(q)];
+                sa[no] = stride[q];
+                sb[no] = 0;
+                ++no;
+            }
+        SegPlan ma, mb;
+        plan_gather_fixed(od, sa, no, ma);
+        plan_gather_fixed(od, sb, no, mb);
+        int prev = 0;
+        QG_CUDA(cudaGetDevice(&prev));
+        QG_CUDA(cudaSetDevice(s->ctx->device));
+        try {
+            uint64_t* toff = noalloc_table(s->ctx->device);
+            int fb = int(std::min<uint64_t>((DS + 255) / 256, 1024));
+            k_fill_toff<<<fb, 256, 0, s->ctx->stream>>>(toff, DS, td);
+            after_launch(s->ctx, "k_fill_toff");
+            if (s->prec == QGPU_C128)
+                noalloc_launch<double>(s->ctx, s->data, d_out, ma, mb, toff, DS, ket);
+            else
+                noalloc_launch<float>(s->ctx, s->data, d_out, ma, mb, toff, DS, ket);
+        } catch (...) {
+            cudaSetDevice(prev);
+            throw;
+        }
+        QG_CUDA(cudaSetDevice(prev));
+    });
+}
