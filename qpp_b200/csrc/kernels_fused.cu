@@ -171,18 +171,25 @@ __global__ void __launch_bounds__(512, 1)
     const uint32_t bh_addr = smem_u32(Bh), bl_addr = smem_u32(Bl);
     uint32_t parity = 0;
 
-    for (uint64_t tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
-        uint64_t g = tile * 128 + uint64_t(quarter * 32 + lane);
-        uint64_t base = g;
+    // Software pipeline over this CTA's tiles (D double-buffered in TMEM
+    // columns [256,384) and [384,512)):
+    //   loads of tile i+1 are in flight while MMA(i) runs;
+    //   MMA(i+1) runs while tile i is read back from TMEM and stored.
+    auto tile_base = [&](uint64_t tile) {
+        uint64_t base = tile * 128 + uint64_t(quarter * 32 + lane);
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             int b = p.tb_sorted[i];
             uint64_t low = (uint64_t(1) << b) - 1;
             base = ((base & ~low) << 1) | (base & low);
         }
-        float2 v[16];
+        return base;
+    };
+    auto load = [&](uint64_t base, float2 (&v)[16]) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) v[j] = psi[base + p.off[kpart * 16 + j]];
+    };
+    auto stage = [&](const float2 (&v)[16]) {
         uint32_t hi[32], lo[32];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
@@ -195,10 +202,11 @@ __global__ void __launch_bounds__(512, 1)
         tmem_st32(tbase + lane_off + 128u + uint32_t(kpart * 32), lo);
         asm volatile("tcgen05.wait::st.sync.aligned;");
         asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
+    };
+    auto issue = [&](uint32_t dcol) { // after a __syncthreads
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t d = tbase + 256u;
+            const uint32_t d = tbase + dcol;
 #pragma unroll 1
             for (int ks = 0; ks < 16; ++ks) {
                 uint32_t koff = uint32_t((ks >> 2) * 16384 + (ks & 3) * 32);
@@ -211,30 +219,56 @@ __global__ void __launch_bounds__(512, 1)
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                     mb));
         }
-        bool ok = mbar_wait(mb, parity);
-        if (!ok) {
-            if (lane == 0) {
+    };
+
+    uint64_t tile = blockIdx.x;
+    if (tile < p.ntiles) {
+        float2 v[16];
+        uint64_t base_cur = tile_base(tile);
+        load(base_cur, v);
+        stage(v);
+        __syncthreads();
+        issue(256u);
+        uint32_t dsel = 0;
+        for (;;) {
+            const uint64_t next = tile + gridDim.x;
+            const bool has_next = next < p.ntiles;
+            uint64_t base_next = 0;
+            if (has_next) {
+                base_next = tile_base(next);
+                load(base_next, v);
+            }
+            bool ok = mbar_wait(mb, parity);
+            if (!ok && lane == 0) {
                 atomicExch(p.err, 1);
                 abort_sh = 1;
             }
-        }
-        __syncthreads();
-        if (abort_sh) {
-            // let MMAs still in flight drain (bounded) before freeing TMEM
-            if (tid == 0) mbar_wait(mb, parity);
-            break;
-        }
-        parity ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        uint32_t dv[32];
-        tmem_ld32(tbase + lane_off + 256u + uint32_t(kpart * 32), dv);
-        asm volatile("tcgen05.wait::ld.sync.aligned;");
+            __syncthreads();
+            if (abort_sh) {
+                // let MMAs still in flight drain (bounded) before freeing TMEM
+                if (tid == 0) mbar_wait(mb, parity);
+                break;
+            }
+            parity ^= 1u;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (has_next) {
+                stage(v);
+                __syncthreads();
+                issue(256u + 128u * (dsel ^ 1u));
+            }
+            uint32_t dv[32];
+            tmem_ld32(tbase + lane_off + 256u + 128u * dsel + uint32_t(kpart * 32), dv);
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-            psi[base + p.off[kpart * 16 + j]] =
-                make_float2(__uint_as_float(dv[2 * j]), __uint_as_float(dv[2 * j + 1]));
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
+            for (int j = 0; j < 16; ++j)
+                psi[base_cur + p.off[kpart * 16 + j]] =
+                    make_float2(__uint_as_float(dv[2 * j]), __uint_as_float(dv[2 * j + 1]));
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            if (!has_next) break;
+            tile = next;
+            base_cur = base_next;
+            dsel ^= 1u;
+        }
     }
     __syncthreads();
     if (warp == 0) {
