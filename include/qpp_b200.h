@@ -259,6 +259,13 @@ qgpu_status qgpu_circuit_cctrl(qgpu_circuit* c, const double* U, uint64_t DU,
  * the first outcome goes to classical dit c_reg. */
 qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target,
                                  uint32_t k, uint64_t c_reg, int destructive);
+/* A Kraus channel sum_i K_i . K_i^+ on `target` (nK consecutive DK x DK
+ * operators). No QCircuit counterpart: density-matrix engines apply it
+ * exactly (qpp::apply(rho, Ks, target, dims), operations.hpp:476-560); ket
+ * engines draw one branch with probability ||K_i psi||^2 and renormalise. */
+qgpu_status qgpu_circuit_channel(qgpu_circuit* c, const double* Ks,
+                                 uint32_t nK, uint64_t DK,
+                                 const uint64_t* target, uint32_t k);
 qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq,
                               uint64_t* n_steps);
 /* Number of state passes of the fused plan with blocks of <= max_k qubits
@@ -276,6 +283,98 @@ qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form);
  * 64 x 64 block on the tensor cores (split-TF32, FP32 accumulation). */
 qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U,
                           const uint64_t* target, uint32_t k);
+
+/* ---------------------------------------------------------------- engines
+ * QEngine / QDensityEngine / QNoisyEngine over a qgpu_circuit
+ * (include/qpp/classes/qengine.hpp:1271-1405, qnoisy_engine.hpp:105-139).
+ * The state stays in HBM across gates, measurements and noise; kind
+ * QGPU_KET runs a QEngine, QGPU_RHO a QDensityEngine. Randomness is one
+ * std::mt19937 per engine drawn in qpp's order (one full-basis index per
+ * measurement step, one Kraus index per non-measured qudit before every step
+ * when noisy); every draw is recorded and can be replayed. */
+typedef struct qgpu_engine qgpu_engine;
+qgpu_status qgpu_engine_create(qgpu_ctx* ctx, qgpu_circuit* c, qgpu_kind kind,
+                               qgpu_prec prec, qgpu_engine** out);
+qgpu_status qgpu_engine_destroy(qgpu_engine* e);
+qgpu_status qgpu_engine_set_seed(qgpu_engine* e, uint64_t seed);
+/* QNoisyEngine noise model (noise.hpp:75-380): nK Kraus operators on one
+ * qudit (d x d each, consecutive, column-major); probs != NULL gives a
+ * state-independent model (e.g. QubitDepolarizingNoise {1-p, p/3, p/3,
+ * p/3}), probs == NULL a state-dependent one (p_i = tr(K_i rho_q K_i^+)).
+ * nK == 0 removes the noise. */
+qgpu_status qgpu_engine_set_noise(qgpu_engine* e, const double* Ks,
+                                  uint32_t nK, uint64_t d,
+                                  const double* probs);
+/* QEngineT::set_state (qengine.hpp:1191-1214): the initial state of every
+ * repetition (default |0...0>). */
+qgpu_status qgpu_engine_set_state(qgpu_engine* e, const qgpu_state* s);
+/* Force the random choices: measurement outcome dits in execution order and
+ * Kraus indices step by step, qudit by qudit (NULL, 0 to stop replaying). */
+qgpu_status qgpu_engine_set_replay(qgpu_engine* e, const uint64_t* outcomes,
+                                   uint64_t n_out, const uint64_t* noise,
+                                   uint64_t n_noise);
+/* QEngineT::execute(reps) (qengine.hpp:1341-1405): reps independent runs
+ * from the initial state; dits / probs / state hold the last run. */
+qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps);
+qgpu_status qgpu_engine_get_dits(const qgpu_engine* e, uint64_t* dits,
+                                 double* probs);
+/* A new state handle holding a copy of the engine's current state. */
+qgpu_status qgpu_engine_get_state(const qgpu_engine* e, qgpu_state** out);
+/* Outcome statistics of the last execute (QEngineStatistics): the number of
+ * distinct dit vectors, then their counts and the vectors (nc dits each). */
+qgpu_status qgpu_engine_get_stats(const qgpu_engine* e, uint64_t* n_distinct,
+                                  uint64_t* counts, uint64_t* outcomes);
+/* The random choices of the last execute (sizes first, arrays when given). */
+qgpu_status qgpu_engine_get_record(const qgpu_engine* e, uint64_t* n_out,
+                                   uint64_t* outcomes, uint64_t* n_noise,
+                                   uint64_t* noise);
+
+/* ------------------------------------------------ trajectory batches
+ * All `shots` stochastic trajectories of a QNoisyEngine request (qubit
+ * circuit of at most 14 qubits; 1- and 2-qubit gates, fan gates, controlled
+ * 1-qubit gates, Z measurements) in one launch, one CTA per trajectory with
+ * the state in shared memory. Noise: before every step each non-measured
+ * qubit draws from the depolarising channel {I, X, Y, Z} with probabilities
+ * {1 - p, p/3, p/3, p/3} (qnoisy_engine.hpp:105-121, noise.hpp:388-412).
+ * Outputs (any may be NULL): samples[shots] = the final full-basis sample of
+ * each shot; dits[shots * max(nc, 1)] = measurement outcomes; dump[shots * 2
+ * * 2^n] = final states (complex64 widened to double, for parity checks);
+ * events[shots * max_events * 2] = noise events as (instruction, bit |
+ * pauli << 16), unused slots 0xffffffff. Draws come from Philox4x32-10
+ * keyed by seed with counter (shot, instruction, qubit). */
+qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double p_depol,
+                              uint64_t shots, uint64_t seed,
+                              uint64_t* samples, uint32_t* dits, double* dump,
+                              uint32_t* events, uint32_t max_events);
+
+/* ------------------------------------------------------------ serving loop
+ * QNoisyEngine requests on one GPU. A worker thread drains the queue.
+ * mode 0 (batched): requests that arrive while a launch runs are admitted in
+ * arrival order while their estimated HBM footprint fits hbm_budget, and all
+ * their trajectories share the next trajectory-kernel launch; requests the
+ * kernel cannot run (density matrices, > 20 qubits, wider gates) run on the
+ * resident engine on a second stream at the same time. mode 1 (plain): one
+ * request at a time on the resident engine in complex128, one launch per
+ * gate. A request's circuit must stay alive until its wait returns. */
+typedef struct qgpu_server qgpu_server;
+qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode,
+                               qgpu_server** out);
+/* kind QGPU_KET: `shots` trajectories with depolarising probability p per
+ * qubit per step; kind QGPU_RHO: one exact density-matrix run (noise from
+ * the circuit's channels), then `shots` samples of the final diagonal. */
+qgpu_status qgpu_server_submit(qgpu_server* s, qgpu_circuit* c,
+                               qgpu_kind kind, double p, uint64_t shots,
+                               uint64_t seed, uint64_t* id);
+/* Blocks until request `id` finished (timeout_s < 0: no limit); latency is
+ * submit -> result on the host; samples[shots] and dits[shots * max(nc, 1)]
+ * are copied when given. The request is released afterwards. */
+qgpu_status qgpu_server_wait(qgpu_server* s, uint64_t id, double timeout_s,
+                             double* latency_s, uint64_t* samples,
+                             uint32_t* dits);
+qgpu_status qgpu_server_stats(qgpu_server* s, uint64_t* batches,
+                              uint64_t* trajectories, uint64_t* engine_runs,
+                              double* busy_s);
+qgpu_status qgpu_server_destroy(qgpu_server* s);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -485,3 +485,81 @@ def layered_circuit(n, depth, seed):
         for U, t in layer:
             c.gate(U, t)
     return c
+
+
+# ------------------------------------------------------------------- engines
+class Engine:
+    """QEngine (kind=KET) / QDensityEngine (kind=RHO) / QNoisyEngine (after
+    set_noise) over a Circuit, state resident in HBM
+    (include/qpp/classes/qengine.hpp, qnoisy_engine.hpp)."""
+
+    def __init__(self, ctx, circuit, kind=KET, prec=C128):
+        self.h = vp()
+        self.ctx, self.circuit = ctx, circuit
+        check(lib().qgpu_engine_create(ctx.h, circuit.h, ct.c_int(kind), ct.c_int(prec),
+                                       ct.byref(self.h)))
+
+    def set_seed(self, seed):
+        check(lib().qgpu_engine_set_seed(self.h, ct.c_uint64(seed)))
+        return self
+
+    def set_noise(self, Ks, probs=None):
+        packed, d = _pack_kraus(Ks)
+        pr = None if probs is None else np.ascontiguousarray(np.asarray(probs, dtype=np.float64))
+        check(lib().qgpu_engine_set_noise(self.h, _dp(packed), ct.c_uint32(len(Ks)),
+                                          ct.c_uint64(d), None if pr is None else _dp(pr)))
+        return self
+
+    def set_state(self, state):
+        check(lib().qgpu_engine_set_state(self.h, state.h))
+        return self
+
+    def set_replay(self, outcomes=None, noise=None):
+        o, op, no = _u64(outcomes) if outcomes is not None else (None, None, 0)
+        k, kp, nk = _u64(noise) if noise is not None else (None, None, 0)
+        check(lib().qgpu_engine_set_replay(self.h, op, ct.c_uint64(no), kp, ct.c_uint64(nk)))
+        return self
+
+    def execute(self, reps=1):
+        check(lib().qgpu_engine_execute(self.h, ct.c_uint64(reps)))
+        return self
+
+    def get_dits(self):
+        nc = self.circuit.nc
+        d = np.zeros(max(nc, 1), dtype=np.uint64)
+        p = np.zeros(max(nc, 1), dtype=np.float64)
+        check(lib().qgpu_engine_get_dits(self.h, d.ctypes.data_as(u64p), _dp(p)))
+        return [int(x) for x in d[:nc]], [float(x) for x in p[:nc]]
+
+    def get_state(self):
+        h = vp()
+        check(lib().qgpu_engine_get_state(self.h, ct.byref(h)))
+        return State(self.ctx, KET, None, handle=h)
+
+    def get_stats(self):
+        n = ct.c_uint64()
+        check(lib().qgpu_engine_get_stats(self.h, ct.byref(n), None, None))
+        nc = self.circuit.nc
+        counts = np.zeros(max(n.value, 1), dtype=np.uint64)
+        outs = np.zeros(max(n.value * nc, 1), dtype=np.uint64)
+        check(lib().qgpu_engine_get_stats(self.h, None, counts.ctypes.data_as(u64p),
+                                          outs.ctypes.data_as(u64p)))
+        return {tuple(int(x) for x in outs[i * nc:(i + 1) * nc]): int(counts[i])
+                for i in range(n.value)}
+
+    def get_record(self):
+        no, nn = ct.c_uint64(), ct.c_uint64()
+        check(lib().qgpu_engine_get_record(self.h, ct.byref(no), None, ct.byref(nn), None))
+        o = np.zeros(max(no.value, 1), dtype=np.uint64)
+        k = np.zeros(max(nn.value, 1), dtype=np.uint64)
+        check(lib().qgpu_engine_get_record(self.h, None, o.ctypes.data_as(u64p), None,
+                                           k.ctypes.data_as(u64p)))
+        return [int(x) for x in o[:no.value]], [int(x) for x in k[:nn.value]]
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().qgpu_engine_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass

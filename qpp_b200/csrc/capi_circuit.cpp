@@ -196,6 +196,27 @@ qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target, uint32
     });
 }
 
+qgpu_status qgpu_circuit_channel(qgpu_circuit* c, const double* Ks, uint32_t nK, uint64_t DK,
+                                 const uint64_t* target, uint32_t k) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = "qgpu_circuit_channel()";
+        auto t = vec_of(target, k);
+        check_targets(c, W, t, "target", measured_of(c));
+        if (nK == 0) raise(QGPU_ERR_ZERO_SIZE, W, ctx_of(c) + "Ks");
+        if (DK != ipow(c->d, t.size())) raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, W, ctx_of(c) + "Ks");
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::Channel;
+        const cd* K = reinterpret_cast<const cd*>(Ks);
+        s.U.assign(K, K + size_t(nK) * DK * DK);
+        s.DU = DK;
+        s.nK = nK;
+        s.target = t;
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
 qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq, uint64_t* n_steps) {
     return guarded([&] {
         need_handle(c);

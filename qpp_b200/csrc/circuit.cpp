@@ -227,6 +227,12 @@ void apply_step(qgpu_state* s, const Step& st) {
                           st.kind == StepKind::CtrlFan);
             break;
         }
+        case StepKind::Channel:
+            if (s->kind != QGPU_RHO)
+                raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
+                      "a channel on a ket needs the engine (sampled branch)");
+            op_apply_kraus(s, st.U.data(), st.nK, st.DU, st.target);
+            break;
         case StepKind::Nop:
             break;
         default:

@@ -34,13 +34,16 @@ enum class StepKind {
     CCtrlFan,  // classically controlled fan GType cCTRL_FAN
     Measure,   // Z-basis measure_seq        MType MEASURE / MEASURE_MANY (+ _ND)
     Reset,     // reset targets to |0>
+    Channel,   // Kraus channel sum_i K_i . K_i^+ on the targets (no QCircuit step:
+               // exact on density matrices, one sampled branch on kets)
     Nop
 };
 
 struct Step {
     StepKind kind = StepKind::Nop;
-    std::vector<cd> U;
+    std::vector<cd> U; // Channel: nK consecutive DU x DU Kraus operators
     uint64_t DU = 0;
+    uint32_t nK = 0;
     std::vector<uint64_t> target, ctrl, shift;
     bool has_shift = false;
     uint64_t c_reg = 0;

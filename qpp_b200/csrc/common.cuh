@@ -59,6 +59,37 @@ __host__ __device__ inline uint64_t seg_offset(const SegPlan& p, uint64_t g) {
     return off;
 }
 
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11): 10 rounds of the
+// published multipliers and Weyl key increments on a 128-bit counter.
+__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = uint64_t(0xD2511F53u) * c[0];
+        uint64_t p1 = uint64_t(0xCD9E8D57u) * c[2];
+        uint32_t hi0 = uint32_t(p0 >> 32), lo0 = uint32_t(p0);
+        uint32_t hi1 = uint32_t(p1 >> 32), lo1 = uint32_t(p1);
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Two uniforms in [0, 1) with 53 random bits each, for counter (a, b, c, d).
+__host__ __device__ inline void philox_uniform2(uint64_t key, uint32_t a, uint32_t b,
+                                                uint32_t c, uint32_t d, double& u0,
+                                                double& u1) {
+    uint32_t x[4] = {a, b, c, d};
+    philox4x32_10(x, uint32_t(key), uint32_t(key >> 32));
+    uint64_t m0 = (uint64_t(x[0]) << 21) ^ (uint64_t(x[1]) >> 11);
+    uint64_t m1 = (uint64_t(x[2]) << 21) ^ (uint64_t(x[3]) >> 11);
+    u0 = double(m0 & ((uint64_t(1) << 53) - 1)) * 0x1.0p-53;
+    u1 = double(m1 & ((uint64_t(1) << 53) - 1)) * 0x1.0p-53;
+}
+
 template <typename C>
 __device__ __forceinline__ C cmul(C a, C b) {
     return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};

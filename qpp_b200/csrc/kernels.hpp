@@ -65,10 +65,12 @@ std::vector<double> reduce_marginals(qgpu_ctx* ctx, qgpu_prec prec,
                                      const void* data, const SegPlan& outer,
                                      const std::vector<uint64_t>& off,
                                      bool diag_of_rho, uint64_t D);
-// Index of the first element whose inclusive prefix sum of weights exceeds
-// `threshold` (FP64); weights are |x_i|^2 (ket) or Re rho(i, i).
+// Index of the first element whose inclusive prefix sum of weights reaches
+// fraction * (sum of all weights) (FP64); weights are |x_i|^2 (ket) or
+// Re rho(i, i). This is std::discrete_distribution's draw for a uniform u
+// = fraction.
 uint64_t prefix_search(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
-                       uint64_t D, bool diag_of_rho, double threshold,
+                       uint64_t D, bool diag_of_rho, double fraction,
                        double* total_out);
 // Keep the elements whose digit (index / dig_stride) % dig_dim equals
 // dig_val (for rho: in both the row and the column index), scale them by

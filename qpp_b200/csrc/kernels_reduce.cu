@@ -238,23 +238,6 @@ __global__ void __launch_bounds__(256)
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter = element
 // index, key = seed; Box-Muller on the first two words gives (re, im).
-__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0,
-                                              uint32_t k1) {
-    for (int r = 0; r < 10; ++r) {
-        uint64_t p0 = uint64_t(0xD2511F53u) * c[0];
-        uint64_t p1 = uint64_t(0xCD9E8D57u) * c[2];
-        uint32_t hi0 = uint32_t(p0 >> 32), lo0 = uint32_t(p0);
-        uint32_t hi1 = uint32_t(p1 >> 32), lo1 = uint32_t(p1);
-        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = lo1;
-        c[2] = n2;
-        c[3] = lo0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-}
-
 template <typename R>
 __global__ void __launch_bounds__(256)
     k_fill_gaussian(Cplx<R>* __restrict__ x, uint64_t n, uint64_t seed) {
@@ -420,7 +403,7 @@ std::vector<double> reduce_marginals(qgpu_ctx* ctx, qgpu_prec prec,
 }
 
 uint64_t prefix_search(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
-                       uint64_t D, bool diag, double threshold,
+                       uint64_t D, bool diag, double fraction,
                        double* total_out) {
     int nb = std::min(kRedBlocks, nblocks(ctx, D));
     uint64_t chunk = (D + nb - 1) / nb;
@@ -447,7 +430,7 @@ uint64_t prefix_search(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
     double total = 0;
     for (double p : ps) total += p;
     if (total_out) *total_out = total;
-    double thr = threshold;
+    double thr = fraction * total;
     double cum = 0;
     int b = 0;
     for (; b < nb; ++b) {

@@ -1,0 +1,290 @@
+// kernels_traj.cu -- noisy circuit trajectories with the whole state in
+// shared memory: one CTA runs one trajectory (one shot) of a QNoisyEngine
+// request from start to finish, and one launch carries the trajectories of
+// many requests (the serving loop's batched form).
+//
+// Semantics follow include/qpp/classes/qnoisy_engine.hpp:105-139: before every
+// circuit step each non-measured qubit draws one Kraus index of the
+// depolarising channel {I, X, Y, Z} with probabilities {1-p, p/3, p/3, p/3}
+// (noise.hpp:388-412); Z-basis measurements follow measure_seq
+// (instruments.hpp:985-1111) one qubit at a time; a destructively measured
+// qubit stays in the register fixed at its outcome and is never touched
+// again (equivalent to qpp removing it). After the last step one full-basis
+// index is sampled from |psi|^2 (the shot's result).
+//
+// Arithmetic: amplitudes in complex64 with FP32 arithmetic; measurement
+// probabilities, renormalisation factors and the final sampling prefix sums
+// in FP64. Randomness: Philox4x32-10 keyed by the request seed with counter
+// (shot, instruction, qubit, purpose), so every draw is reproducible.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "kernels.hpp"
+#include "traj.hpp"
+
+namespace qgpu {
+
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 c_fma(float2 a, float2 b, float2 c) {
+    c.x = fmaf(a.x, b.x, c.x);
+    c.x = fmaf(-a.y, b.y, c.x);
+    c.y = fmaf(a.x, b.y, c.y);
+    c.y = fmaf(a.y, b.x, c.y);
+    return c;
+}
+
+__device__ __forceinline__ uint32_t ins0(uint32_t x, int b) {
+    uint32_t low = (1u << b) - 1;
+    return ((x & ~low) << 1) | (x & low);
+}
+
+// block-wide FP64 sum (256 threads), result broadcast to every thread
+__device__ double block_sum_d(double v, double* red) {
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_down_sync(0xffffffffu, v, s);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double t = 0;
+    for (int i = 0; i < int(blockDim.x >> 5); ++i) t += red[i];
+    return t;
+}
+
+__global__ void __launch_bounds__(256)
+    k_traj(const TWork* __restrict__ work, int nwork, uint32_t* __restrict__ dits,
+           int maxcreg, uint64_t* __restrict__ samples, float2* __restrict__ dump,
+           TEvent* __restrict__ events, int max_events, float2* __restrict__ gscratch,
+           uint64_t gslot) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    // registers of up to 2^14 amplitudes live in shared memory; larger ones
+    // in this CTA's own slot of a global scratch buffer (L2 / HBM), which
+    // __syncthreads makes coherent between the block's threads
+    float2* psi = gscratch ? gscratch + uint64_t(blockIdx.x) * gslot
+                           : reinterpret_cast<float2*>(sm);
+    __shared__ double red[8];
+    __shared__ double part[256];
+    __shared__ uint32_t xmask_sh, zmask_sh, ny_sh, nev_sh;
+    __shared__ int outcome_sh;
+    const int tid = threadIdx.x, nt = blockDim.x;
+
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const TWork W = work[w];
+        const int n = W.n;
+        const uint32_t N = 1u << n;
+        for (uint32_t i = tid; i < N; i += nt) psi[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
+        uint32_t alive = (n == 32) ? 0xffffffffu : ((1u << n) - 1);
+        if (tid == 0) nev_sh = 0;
+        __syncthreads();
+        for (uint32_t k = 0; k < W.nins; ++k) {
+            const TInstr I = W.prog[k];
+            if ((I.flags & kTNewStep) && W.p_noise > 0.f) {
+                // one Kraus pick per non-measured qubit (thread b <-> bit b)
+                if (tid == 0) {
+                    xmask_sh = 0;
+                    zmask_sh = 0;
+                    ny_sh = 0;
+                }
+                __syncthreads();
+                if (tid < n && ((alive >> tid) & 1u)) {
+                    double u0, u1;
+                    philox_uniform2(W.seed, W.shot, k, uint32_t(tid), 0x6e6f6973u, u0, u1);
+                    if (u0 < double(W.p_noise)) {
+                        int pk = 1 + min(int(u1 * 3.0), 2); // 1 X, 2 Y, 3 Z
+                        if (pk != 3) atomicOr(&xmask_sh, 1u << tid);
+                        if (pk != 1) atomicOr(&zmask_sh, 1u << tid);
+                        if (pk == 2) atomicAdd(&ny_sh, 1u);
+                        if (events) {
+                            uint32_t e = atomicAdd(&nev_sh, 1u);
+                            if (int(e) < max_events)
+                                events[size_t(W.out) * max_events + e] =
+                                    TEvent{k, uint16_t(tid), uint16_t(pk)};
+                        }
+                    }
+                }
+                __syncthreads();
+                const uint32_t xm = xmask_sh, zm = zmask_sh, ny = ny_sh;
+                if (xm | zm) {
+                    // P|i> = i^ny (-1)^popc(i & zm) |i ^ xm>
+                    float2 gph = ny % 4 == 0 ? make_float2(1, 0)
+                               : ny % 4 == 1 ? make_float2(0, 1)
+                               : ny % 4 == 2 ? make_float2(-1, 0) : make_float2(0, -1);
+                    if (xm == 0) {
+                        for (uint32_t i = tid; i < N; i += nt) {
+                            float2 a = c_mul(gph, psi[i]);
+                            if (__popc(i & zm) & 1) a = make_float2(-a.x, -a.y);
+                            psi[i] = a;
+                        }
+                    } else {
+                        int hb = 31 - __clz(xm); // pair (i, i ^ xm) with bit hb of i clear
+                        for (uint32_t p = tid; p < N / 2; p += nt) {
+                            uint32_t i = ins0(p, hb), j = i ^ xm;
+                            float2 a = c_mul(gph, psi[i]), b = c_mul(gph, psi[j]);
+                            if (__popc(i & zm) & 1) a = make_float2(-a.x, -a.y);
+                            if (__popc(j & zm) & 1) b = make_float2(-b.x, -b.y);
+                            psi[j] = a;
+                            psi[i] = b;
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            switch (I.op) {
+                case kTG1: {
+                    const float2* m = W.mats + I.mat; // column-major 2 x 2
+                    const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
+                    const uint32_t s = 1u << I.b0;
+                    for (uint32_t p = tid; p < N / 2; p += nt) {
+                        uint32_t i = ins0(p, I.b0);
+                        float2 v0 = psi[i], v1 = psi[i + s];
+                        psi[i] = c_fma(a01, v1, c_mul(a00, v0));
+                        psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
+                    }
+                    break;
+                }
+                case kTCG1: {
+                    const float2* m = W.mats + I.mat;
+                    const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
+                    const uint32_t s = 1u << I.b0;
+                    for (uint32_t p = tid; p < N / 2; p += nt) {
+                        uint32_t i = ins0(p, I.b0);
+                        if ((i & I.cmask) != I.cval) continue;
+                        float2 v0 = psi[i], v1 = psi[i + s];
+                        psi[i] = c_fma(a01, v1, c_mul(a00, v0));
+                        psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
+                    }
+                    break;
+                }
+                case kTG2: {
+                    const float2* m = W.mats + I.mat; // column-major 4 x 4
+                    const int lo = min(I.b0, I.b1), hi = max(I.b0, I.b1);
+                    const uint32_t s0 = 1u << I.b0, s1 = 1u << I.b1;
+                    for (uint32_t p = tid; p < N / 4; p += nt) {
+                        uint32_t i = ins0(ins0(p, lo), hi);
+                        float2 v[4] = {psi[i], psi[i + s1], psi[i + s0], psi[i + s0 + s1]};
+                        float2 r[4];
+#pragma unroll
+                        for (int row = 0; row < 4; ++row) {
+                            float2 acc = c_mul(m[row], v[0]);
+                            acc = c_fma(m[row + 4], v[1], acc);
+                            acc = c_fma(m[row + 8], v[2], acc);
+                            acc = c_fma(m[row + 12], v[3], acc);
+                            r[row] = acc;
+                        }
+                        psi[i] = r[0];
+                        psi[i + s1] = r[1];
+                        psi[i + s0] = r[2];
+                        psi[i + s0 + s1] = r[3];
+                    }
+                    break;
+                }
+                case kTMeas: {
+                    const uint32_t bit = 1u << I.b0;
+                    double p1 = 0, tot = 0;
+                    for (uint32_t i = tid; i < N; i += nt) {
+                        double w2 = double(psi[i].x) * psi[i].x + double(psi[i].y) * psi[i].y;
+                        tot += w2;
+                        if (i & bit) p1 += w2;
+                    }
+                    tot = block_sum_d(tot, red);
+                    p1 = block_sum_d(p1, red);
+                    if (tid == 0) {
+                        double u0, u1;
+                        philox_uniform2(W.seed, W.shot, k, 0xffffu, 0x6d656173u, u0, u1);
+                        // first outcome whose cumulative probability reaches u
+                        outcome_sh = (u0 * tot <= tot - p1 && tot - p1 > 0) ? 0 : 1;
+                        if (I.mat < uint32_t(maxcreg))
+                            dits[size_t(W.out) * maxcreg + I.mat] = uint32_t(outcome_sh);
+                    }
+                    __syncthreads();
+                    const int o = outcome_sh;
+                    const double pk = o ? p1 : tot - p1;
+                    const float sc = float(1.0 / sqrt(pk));
+                    for (uint32_t i = tid; i < N; i += nt) {
+                        bool keep = (((i & bit) != 0) == (o == 1));
+                        float2 a = psi[i];
+                        psi[i] = keep ? make_float2(a.x * sc, a.y * sc) : make_float2(0.f, 0.f);
+                    }
+                    if (I.flags & kTDestructive) alive &= ~bit;
+                    break;
+                }
+                default:
+                    break;
+            }
+            __syncthreads();
+        }
+        // final full-basis sample: FP64 prefix sums over thread chunks
+        {
+            const uint32_t chunk = (N + nt - 1) / nt;
+            double s = 0;
+            const uint32_t lo = tid * chunk, hi = min(N, lo + chunk);
+            for (uint32_t i = lo; i < hi; ++i)
+                s += double(psi[i].x) * psi[i].x + double(psi[i].y) * psi[i].y;
+            part[tid] = s;
+            __syncthreads();
+            if (tid == 0) {
+                double tot = 0;
+                for (int t = 0; t < nt; ++t) tot += part[t];
+                double u0, u1;
+                philox_uniform2(W.seed, W.shot, 0xffffffffu, 0u, 0x66696e6cu, u0, u1);
+                double thr = u0 * tot, cum = 0;
+                uint64_t idx = N - 1;
+                int t = 0;
+                for (; t < nt; ++t) {
+                    if (cum + part[t] >= thr && part[t] > 0) break;
+                    cum += part[t];
+                }
+                if (t < nt) {
+                    for (uint32_t i = t * chunk; i < min(N, (t + 1) * chunk); ++i) {
+                        cum += double(psi[i].x) * psi[i].x + double(psi[i].y) * psi[i].y;
+                        if (cum >= thr) {
+                            idx = i;
+                            break;
+                        }
+                    }
+                }
+                samples[W.out] = idx;
+            }
+            __syncthreads();
+        }
+        if (dump)
+            for (uint32_t i = tid; i < N; i += nt) dump[size_t(W.out) * N + i] = psi[i];
+        __syncthreads();
+    }
+}
+
+int traj_global_grid(qgpu_ctx* ctx, int nwork) {
+    return std::min(nwork, ctx->num_sms * 8);
+}
+
+void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
+                 int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
+                 int max_events, float2* gscratch) {
+    if (nwork == 0) return;
+    if (nmax > kTrajMaxQubits) {
+        if (!gscratch)
+            raise(QGPU_ERR_INVALID_ARGUMENT, "launch_traj()", "registers above 14 qubits need scratch");
+        int grid = traj_global_grid(ctx, nwork);
+        k_traj<<<grid, 256, 0, ctx->stream>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump,
+                                               devents, max_events, gscratch,
+                                               uint64_t(1) << nmax);
+        after_launch(ctx, "k_traj (global)");
+        return;
+    }
+    size_t smem = (size_t(1) << nmax) * sizeof(float2);
+    if (smem > 48 * 1024)
+        QG_CUDA(cudaFuncSetAttribute(k_traj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(smem)));
+    int per_sm = int(std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / (smem + 4096))));
+    int grid = std::min(nwork, ctx->num_sms * per_sm);
+    k_traj<<<grid, 256, smem, ctx->stream>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump,
+                                             devents, max_events, nullptr, 0);
+    after_launch(ctx, "k_traj");
+}
+
+} // namespace qgpu

@@ -1,0 +1,65 @@
+// traj.hpp -- compiled trajectory programs for the shared-memory kernel.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "internal.hpp"
+
+namespace qgpu {
+
+enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4 };
+enum : uint8_t { kTNewStep = 1, kTDestructive = 2 };
+
+// One instruction; qubits are bit positions (LSB = 0) of the full register.
+struct TInstr {
+    uint8_t op;
+    uint8_t b0, b1; // targets (G2: row index = 2 * bit(b0) + bit(b1))
+    uint8_t flags;  // kTNewStep: noise is drawn before this instruction
+    uint32_t mat;   // gate: float2 offset of the column-major matrix; meas: c_reg
+    uint32_t cmask; // controlled gate: control bits
+    uint32_t cval;  // controlled gate: required values of the control bits
+};
+
+// One trajectory (shot) of one request.
+struct TWork {
+    const TInstr* prog;
+    const float2* mats;
+    uint32_t nins;
+    uint8_t n;
+    uint8_t pad0;
+    uint16_t pad1;
+    float p_noise;  // depolarising probability per qubit per step
+    uint32_t shot;  // trajectory index inside its request (Philox counter)
+    uint32_t out;   // global output slot
+    uint64_t seed;  // request seed (Philox key)
+};
+
+// Recorded noise event: before instruction `ins`, Pauli `pauli` (1 X, 2 Y,
+// 3 Z) on bit `bit`.
+struct TEvent {
+    uint32_t ins;
+    uint16_t bit;
+    uint16_t pauli;
+};
+
+// Largest register held in shared memory (2^14 complex64 = 128 KB); up to
+// kTrajMaxGlobalQubits a CTA works on its own slot of a global scratch
+// buffer instead (traj_global_grid(ctx, nwork) slots of 2^n amplitudes).
+constexpr int kTrajMaxQubits = 14;
+constexpr int kTrajMaxGlobalQubits = 20;
+int traj_global_grid(qgpu_ctx* ctx, int nwork);
+
+struct TProgram {
+    uint32_t n = 0;
+    uint32_t ncreg = 0;
+    std::vector<TInstr> ins;
+    std::vector<float> mats; // interleaved complex64
+};
+
+void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
+                 int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
+                 int max_events, float2* gscratch);
+bool compile_traj(const qgpu_circuit* c, TProgram& P);
+
+} // namespace qgpu
