@@ -174,6 +174,19 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def reduce_over_ranks(dist, ms_local, bytes_local, device=None):
+    """Replicas: the job time is the slowest rank's device time and the job
+    work is the sum of every rank's work. Returns (max ms, total bytes)."""
+    if dist is None or not dist.is_initialized():
+        return ms_local, bytes_local
+    import torch
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    b = torch.tensor([float(bytes_local)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(b.item())
+
+
 def cpu_sample_gates(layers, count):
     """The first `count` gates of the circuit in layer order, taking 1q and
     2q gates in the circuit's 2:1 ratio."""
@@ -321,14 +334,12 @@ def main():
     ctx.synchronize()
     launches = ctx.launches() - l0
     clk = clocks.stop()
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
     n_gates = sum(len(layers[s % DEPTH]) for s in range(args.steps))
-    value = world * n_gates * gbytes / (ms / 1e3) / 1e9
+    ms, job_bytes = reduce_over_ranks(dist, start.elapsed_time(end), n_gates * gbytes,
+                                      device="cuda")
+    if dist:
+        dist.barrier()
+    value = job_bytes / (ms / 1e3) / 1e9
     d1 = [a.elapsed_time(b) for k, a, b in ev if k == 1]
     d2 = [a.elapsed_time(b) for k, a, b in ev if k == 2]
     peak, peak_kind = peaks()

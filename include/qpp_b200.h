@@ -347,6 +347,23 @@ qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double p_depol,
                               uint64_t* samples, uint32_t* dits, double* dump,
                               uint32_t* events, uint32_t max_events);
 
+/* ------------------------------------------------------ batched instances
+ * n_inst independent instances, instance i running circuits[i] on
+ * states[i] in place (kets or density matrices of uneven sizes). form
+ * QGPU_FORM_FUSED (1): every complex64 instance of <= 22 (virtual) qubits is
+ * compiled into a trajectory program (a density matrix as a ket over 2n
+ * virtual qubits: 1-qubit gates and 1-qubit channels as 4 x 4
+ * superoperators, 2-qubit gates as U on the rows then conj(U) on the
+ * columns) and all of them run as ONE CUDA-graph launch holding one
+ * trajectory-kernel launch per register size; instances it cannot compile
+ * run in the plain form afterwards. form QGPU_FORM_PLAIN (0): a loop over
+ * the instances, one kernel launch per gate. graph_kernels (may be NULL)
+ * receives the number of kernels in the graph. No reference counterpart. */
+qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst,
+                           qgpu_circuit* const* circuits,
+                           qgpu_state* const* states, int form,
+                           uint64_t* graph_kernels);
+
 /* ------------------------------------------------------------ serving loop
  * QNoisyEngine requests on one GPU. A worker thread drains the queue.
  * mode 0 (batched): requests that arrive while a launch runs are admitted in

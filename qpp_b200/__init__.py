@@ -477,6 +477,18 @@ def apply_tc(state, U, target):
     return state
 
 
+def run_batch(ctx, circuits, states, form=FUSED):
+    """Independent instances circuits[i] on states[i] (in place): FUSED runs
+    every complex64 instance that compiles as one CUDA-graph launch, PLAIN
+    loops with one launch per gate. Returns the kernels in the graph."""
+    n = len(circuits)
+    C = (vp * n)(*[c.h for c in circuits])
+    S = (vp * n)(*[s.h for s in states])
+    k = ct.c_uint64()
+    check(lib().qgpu_run_batch(ctx.h, ct.c_uint32(n), C, S, ct.c_int(form), ct.byref(k)))
+    return k.value
+
+
 def layered_circuit(n, depth, seed):
     """The seeded layered circuit of qpp_b200.workloads as a Circuit."""
     from . import workloads

@@ -1,0 +1,252 @@
+"""Measurements of the other benchmark configurations (one GPU).
+
+  config1  20-qubit Gaussian ket (16 MiB, L2-resident), 1000 Haar gates
+           (70% 1-qubit, 30% 2-qubit on ordered pairs) then 100 applyCTRL
+           with 1-3 controls; complex128, one pass per gate.
+  config2  12-qubit density matrix (4096 x 4096, rank 64), 200 steps of
+           {16-operator pair channel, ptrace over 6, ptranspose over 6,
+           syspermute}; plus the mixed-dimension variant dims
+           [3,3,2,2,3,2,2,3] with Haar 3x3 / 6x6 gates; complex128.
+  config4  2048 kets of 10-22 qubits and 512 density matrices of 6-11
+           qubits (rank 8), each with its own depth-20 layered circuit
+           (density matrices: depolarising p=0.005 on every qubit after each
+           layer), complex64: one CUDA-graph launch versus the plain loop of
+           per-instance launches (and that loop in complex128).
+
+Device times are CUDA events on the library's stream. The CPU figures time
+the oracle (the CPU restatement of qpp, all host cores) on a bounded sample
+of the same work; the oracle is test infrastructure and is imported only
+for these baseline samples.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, State, run_batch
+from .workloads import haar_unitary, ket_gate_sequence
+
+
+def _events(torch, stream):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return a, b
+
+
+def config1(ctx, torch, stream, cpu=True):
+    n = 20
+    seq = ket_gate_sequence(n, seed=1)
+    s = State(ctx, KET, [2] * n, C128).fill_gaussian(1)
+    for U, c, t in seq[:50]:  # warm-up
+        s.apply_ctrl(U, c, t) if c else s.apply(U, t)
+    a, b = _events(torch, stream)
+    a.record(stream)
+    for U, c, t in seq:
+        s.apply_ctrl(U, c, t) if c else s.apply(U, t)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    D = 2 ** n
+    byts = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq)
+    out = {"gates": len(seq), "ms": ms, "gates_per_s": len(seq) / (ms / 1e3),
+           "GBps": byts / (ms / 1e3) / 1e9,
+           "note": "16 MiB state stays in the 126 MB L2: bandwidth is L2, not HBM"}
+    if cpu:
+        from oracle import oracle as orc  # CPU baseline sample only
+        psi = s.numpy()
+        t0 = time.perf_counter()
+        for U, c, t in seq[:200]:
+            psi = orc.applyCTRL(psi, U, c, t, [2] * n, path=1) if c else \
+                orc.apply(psi, U, t, [2] * n, path=1)
+        cpu_s = time.perf_counter() - t0
+        cb = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq[:200])
+        out["cpu"] = {"gates_per_s": 200 / cpu_s, "GBps": cb / cpu_s / 1e9,
+                      "cores": os.cpu_count(), "sample": "first 200 gates", "kind": "port"}
+    s.free()
+    return out
+
+
+def _inv(p):
+    q = [0] * len(p)
+    for i, x in enumerate(p):
+        q[x] = i
+    return q
+
+
+def config2(ctx, torch, stream, cpu=True, steps=200):
+    from .serving import pair_channel
+    rng = np.random.default_rng(2)
+    n, D = 12, 4096
+    W = rng.standard_normal((D, 64)) + 1j * rng.standard_normal((D, 64))
+    rho = W @ W.conj().T
+    rho /= np.trace(rho).real
+    s = State.from_numpy(ctx, rho, [2] * n)
+    Ks = pair_channel()
+    plan = []
+    for _ in range(steps):
+        plan.append(([int(x) for x in rng.choice(n, 2, replace=False)],
+                     [int(x) for x in rng.choice(n, 6, replace=False)],
+                     [int(x) for x in rng.choice(n, 6, replace=False)],
+                     [int(x) for x in rng.permutation(n)]))
+    t = {"channel": 0.0, "ptrace": 0.0, "ptranspose": 0.0, "syspermute": 0.0}
+    for i, (pair, A, T, perm) in enumerate(plan):
+        ev = [_events(torch, stream) for _ in range(4)]
+        ev[0][0].record(stream)
+        s.apply_kraus(Ks, pair)
+        ev[0][1].record(stream)
+        ev[1][0].record(stream)
+        r = s.ptrace(A)
+        ev[1][1].record(stream)
+        ev[2][0].record(stream)
+        p = s.ptranspose(T)
+        ev[2][1].record(stream)
+        ev[3][0].record(stream)
+        s2 = s.syspermute(perm)
+        ev[3][1].record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:  # first two steps are warm-up
+            for k, key in enumerate(t):
+                t[key] += ev[k][0].elapsed_time(ev[k][1])
+        r.free()
+        p.free()
+        s.free()
+        s = s2
+    m = steps - 2
+    full = 2 * 16 * D * D
+    out = {"steps": steps}
+    for key, byts in (("channel", full), ("ptrace", 16 * 64 ** 3 + 16 * 64 * 64),
+                      ("ptranspose", full), ("syspermute", full)):
+        ms = t[key] / m
+        out[key] = {"ms": ms, "GBps": byts / (ms / 1e3) / 1e9, "bytes": byts}
+    trace_err = abs(s.trace() - 1)
+    out["trace_error_after"] = trace_err
+    if cpu:
+        from oracle import oracle as orc
+        x = s.numpy()
+        pair, A, T, perm = plan[0]
+        c = {}
+        t0 = time.perf_counter()
+        orc.ptrace(x, A, [2] * n)
+        c["ptrace_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        orc.ptranspose(x, T, [2] * n)
+        c["ptranspose_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        orc.syspermute(x, perm, [2] * n)
+        c["syspermute_s"] = time.perf_counter() - t0
+        c["sample"] = "one step of ptrace / ptranspose / syspermute on the 4096^2 matrix " \
+                      "(the 16-operator channel is left out: the restated generic loop " \
+                      "takes minutes at this size)"
+        c["kind"] = "port"
+        c["cores"] = os.cpu_count()
+        out["cpu"] = c
+    s.free()
+    # mixed dimensions
+    dims = [3, 3, 2, 2, 3, 2, 2, 3]
+    Dm = int(np.prod(dims))
+    Wm = rng.standard_normal((Dm, 64)) + 1j * rng.standard_normal((Dm, 64))
+    rm = Wm @ Wm.conj().T
+    rm /= np.trace(rm).real
+    sm = State.from_numpy(ctx, rm, dims)
+    a, b = _events(torch, stream)
+    a.record(stream)
+    for _ in range(20):
+        q3 = int(rng.choice([0, 1, 4, 7]))
+        sm.apply(haar_unitary(rng, 3), [q3])
+        sm.apply(haar_unitary(rng, 6), [int(rng.choice([0, 1, 4, 7])), int(rng.choice([2, 3, 5, 6]))])
+        half = [int(x) for x in rng.choice(8, 4, replace=False)]
+        sm.ptrace(half).free()
+        sm.ptranspose(half).free()
+        nxt = sm.syspermute([int(x) for x in rng.permutation(8)])
+        sm.free()
+        sm = nxt
+    b.record(stream)
+    torch.cuda.synchronize()
+    out["mixed_dims"] = {"dims": dims, "steps": 20, "ms_per_step": a.elapsed_time(b) / 20,
+                         "trace_error_after": abs(sm.trace() - 1)}
+    sm.free()
+    return out
+
+
+def _layered(rng, n, depth, rho, bank1, bank2, chan):
+    from .serving import c_channel
+    c = Circuit(n)
+    for _ in range(depth):
+        for q in range(n):
+            c.gate(bank1[int(rng.integers(len(bank1)))], [q])
+        perm = rng.permutation(n)
+        for i in range(n // 2):
+            c.gate(bank2[int(rng.integers(len(bank2)))], [int(perm[2 * i]), int(perm[2 * i + 1])])
+        if rho:
+            for q in range(n):
+                c_channel(c, chan, [q])
+    return c
+
+
+def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
+    from .serving import _depol
+    rng = np.random.default_rng(4)
+    bank1 = [haar_unitary(rng, 2) for _ in range(64)]
+    bank2 = [haar_unitary(rng, 4) for _ in range(64)]
+    chan = _depol(0.005)
+    ns = [int(x) for x in rng.integers(10, 23, size=n_kets)]
+    nr = [int(x) for x in rng.integers(6, 12, size=n_rho)]
+    circs = [_layered(rng, n, depth, False, bank1, bank2, chan) for n in ns] + \
+            [_layered(rng, n, depth, True, bank1, bank2, chan) for n in nr]
+    kinds = [KET] * n_kets + [RHO] * n_rho
+    sizes = ns + nr
+
+    def states(prec):
+        out = []
+        for i, (k, n) in enumerate(zip(kinds, sizes)):
+            s = State(ctx, k, [2] * n, prec)
+            if k == KET:
+                s.fill_gaussian(100 + i)
+            else:
+                from .workloads import haar_unitary as _h  # noqa: F401
+                s.fill_gaussian(100 + i)  # random Hermitian-free start; unit trace
+            out.append(s)
+        return out
+
+    res = {"instances": {"kets": n_kets, "rho": n_rho, "depth": depth,
+                         "ket_qubits": "10-22", "rho_qubits": "6-11"}}
+    for prec, name in ((C64, "c64"), (C128, "c128")):
+        st = states(prec)
+        ctx.synchronize()
+        forms = (("graph", FUSED), ("plain_loop", PLAIN)) if prec == C64 else (("plain_loop", PLAIN),)
+        for label, form in forms:
+            if label == "graph":
+                run_batch(ctx, circs[:8], st[:8], form)  # warm-up
+            a, b = _events(torch, stream)
+            a.record(stream)
+            t0 = time.perf_counter()
+            k = run_batch(ctx, circs, st, form)
+            b.record(stream)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            res[f"{name}_{label}"] = {"s": wall, "device_ms": a.elapsed_time(b),
+                                      "instances_per_s": len(circs) / wall,
+                                      "graph_kernels": k}
+        for s in st:
+            s.free()
+    res["graph_speedup_vs_plain_c64"] = res["c64_plain_loop"]["s"] / res["c64_graph"]["s"]
+    return res
+
+
+def main():
+    import torch
+    cpu = "--no-cpu" not in sys.argv
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    out = {"config1": config1(ctx, torch, stream, cpu),
+           "config2": config2(ctx, torch, stream, cpu),
+           "config4": config4(ctx, torch, stream)}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

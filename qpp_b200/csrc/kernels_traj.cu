@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
@@ -77,7 +78,10 @@ __global__ void __launch_bounds__(256)
         const TWork W = work[w];
         const int n = W.n;
         const uint32_t N = 1u << n;
-        for (uint32_t i = tid; i < N; i += nt) psi[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
+        if (W.init)
+            for (uint32_t i = tid; i < N; i += nt) psi[i] = W.init[i];
+        else
+            for (uint32_t i = tid; i < N; i += nt) psi[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
         uint32_t alive = (n == 32) ? 0xffffffffu : ((1u << n) - 1);
         if (tid == 0) nev_sh = 0;
         __syncthreads();
@@ -254,12 +258,24 @@ __global__ void __launch_bounds__(256)
         }
         if (dump)
             for (uint32_t i = tid; i < N; i += nt) dump[size_t(W.out) * N + i] = psi[i];
+        if (W.fin)
+            for (uint32_t i = tid; i < N; i += nt) W.fin[i] = psi[i];
         __syncthreads();
     }
 }
 
-int traj_global_grid(qgpu_ctx* ctx, int nwork) {
-    return std::min(nwork, ctx->num_sms * 8);
+void traj_prepare() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        QG_CUDA(cudaFuncSetAttribute(k_traj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int((size_t(1) << kTrajMaxQubits) * sizeof(float2))));
+    });
+}
+
+int traj_global_grid(qgpu_ctx* ctx, int nwork, int n) {
+    const uint64_t slot = (uint64_t(1) << n) * sizeof(float2);
+    const uint64_t by_mem = std::max<uint64_t>(1, (uint64_t(4) << 30) / slot);
+    return int(std::min<uint64_t>(std::min<uint64_t>(nwork, uint64_t(ctx->num_sms) * 8), by_mem));
 }
 
 void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
@@ -269,7 +285,7 @@ void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_
     if (nmax > kTrajMaxQubits) {
         if (!gscratch)
             raise(QGPU_ERR_INVALID_ARGUMENT, "launch_traj()", "registers above 14 qubits need scratch");
-        int grid = traj_global_grid(ctx, nwork);
+        int grid = traj_global_grid(ctx, nwork, nmax);
         k_traj<<<grid, 256, 0, ctx->stream>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump,
                                                devents, max_events, gscratch,
                                                uint64_t(1) << nmax);
@@ -277,9 +293,7 @@ void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_
         return;
     }
     size_t smem = (size_t(1) << nmax) * sizeof(float2);
-    if (smem > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_traj, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(smem)));
+    traj_prepare();
     int per_sm = int(std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / (smem + 4096))));
     int grid = std::min(nwork, ctx->num_sms * per_sm);
     k_traj<<<grid, 256, smem, ctx->stream>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump,

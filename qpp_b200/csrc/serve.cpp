@@ -5,21 +5,24 @@
 // probability per qubit per step (kets, stochastic trajectories as in
 // qnoisy_engine.hpp:105-139), a shot count and a seed; its result is one
 // classical register (the measurement dits) and one final full-basis sample
-// per shot. Requests are queued by any thread; one worker thread drains the
-// queue:
+// per shot. Requests are queued by any thread and routed to one of three
+// lanes, each with its own worker thread and CUDA stream, so small requests
+// never wait behind large ones:
 //
-//   batched mode  every request that arrived while the previous launch ran
-//                 is admitted (by an estimate of its HBM footprint against the
-//                 budget) and all their trajectories go into the next launch
-//                 of the shared-memory / per-CTA-slot trajectory kernel, one
-//                 launch per register size. Requests the kernel cannot run
-//                 (density matrices, > 20 qubits, wider gates) run on the
-//                 resident engine on a second stream, overlapping the batch.
-//   plain mode    one request at a time on the resident engine, one kernel
-//                 launch per gate, complex128 (the comparison form).
+//   lane 0  kets of <= 14 qubits: trajectories with the state in shared
+//           memory; every request that arrived while the lane's previous
+//           launch ran is admitted (in arrival order, by an estimate of its
+//           HBM footprint against the budget) into the next launch;
+//   lane 1  kets of 15-20 qubits: the same kernel with each CTA on its own
+//           slot of global scratch (L2 / HBM), batched the same way;
+//   lane 2  everything the kernel cannot run (density matrices, > 20 qubits,
+//           wider gates, classical control): the resident engine, one
+//           request at a time.
+//   plain mode: every request on lane 2 in complex128, one at a time (the
+//           comparison form: one kernel launch per gate).
 //
-// Latency is measured from submit to the moment the worker has the result
-// on the host.
+// Latency is measured from submit to the moment the lane has the result on
+// the host.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -49,6 +52,7 @@ struct Request {
     double p = 0;
     uint64_t shots = 1;
     uint64_t seed = 0;
+    const TProgram* prog = nullptr; // compiled trajectory program, or null
     Clock::time_point t_submit, t_done;
     bool done = false;
     qgpu_status status = QGPU_OK;
@@ -57,18 +61,21 @@ struct Request {
     std::vector<uint64_t> samples; // shots
 };
 
+struct Lane {
+    qgpu_ctx* ctx = nullptr;
+    std::deque<Request*> q;
+    std::thread th;
+};
+
 } // namespace qgpu
 
 struct qgpu_server {
-    qgpu_ctx* ctx = nullptr;  // batches
-    qgpu_ctx* ctx2 = nullptr; // engine path
     int mode = 0;
     uint64_t budget = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<qgpu::Request*> queue;
+    qgpu::Lane lanes[3];
     std::unordered_map<uint64_t, qgpu::Request*> all;
-    std::thread worker;
     bool stop = false;
     uint64_t next_id = 1;
     uint64_t batches = 0, launched_traj = 0, engine_runs = 0;
@@ -78,13 +85,6 @@ struct qgpu_server {
 
 namespace qgpu {
 namespace {
-
-uint64_t state_bytes(const Request* r, qgpu_prec prec) {
-    uint64_t D = 1;
-    for (uint32_t i = 0; i < r->c->nq; ++i) D *= r->c->d;
-    uint64_t e = prec == QGPU_C128 ? 16 : 8;
-    return r->kind == QGPU_KET ? D * e : D * D * e;
-}
 
 // Engine path: trajectories one shot at a time on the resident engine; a
 // density matrix evolves once (its noise is in the circuit's channels) and
@@ -136,22 +136,36 @@ void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec) {
     }
 }
 
-const TProgram* program_of(qgpu_server* S, Request* r) {
-    auto it = S->progs.find(r->c);
+// caller holds S->mu
+const TProgram* program_of(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind) {
+    if (kind != QGPU_KET) return nullptr;
+    auto it = S->progs.find(c);
     if (it == S->progs.end()) {
         TProgram P;
-        bool ok = r->kind == QGPU_KET && compile_traj(r->c, P);
-        it = S->progs.emplace(r->c, std::make_pair(ok, std::move(P))).first;
+        bool ok = compile_traj(c, P);
+        it = S->progs.emplace(c, std::make_pair(ok, std::move(P))).first;
     }
     return it->second.first ? &it->second.second : nullptr;
 }
 
-// One launch (per register size) for all trajectories of `batch`.
-void run_batch(qgpu_server* S, std::vector<Request*>& batch) {
-    qgpu_ctx* ctx = S->ctx;
-    // group by register size
+void finish(qgpu_server* S, Request* r) {
+    std::lock_guard<std::mutex> lock(S->mu);
+    r->t_done = Clock::now();
+    r->done = true;
+    S->cv_done.notify_all();
+}
+
+void fail(qgpu_server* S, Request* r, qgpu_status code, const std::string& msg) {
+    r->status = code;
+    r->err = msg;
+    finish(S, r);
+}
+
+// One launch per register size for all trajectories of `batch`; each size
+// class is finished as soon as its results are on the host.
+void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
     std::map<uint32_t, std::vector<Request*>> by_n;
-    for (Request* r : batch) by_n[program_of(S, r)->n].push_back(r);
+    for (Request* r : batch) by_n[r->prog->n].push_back(r);
     for (auto& kv : by_n) {
         const uint32_t n = kv.first;
         auto& rs = kv.second;
@@ -161,7 +175,7 @@ void run_batch(qgpu_server* S, std::vector<Request*>& batch) {
         std::vector<float> mats;
         std::vector<std::pair<size_t, size_t>> pofs; // (ins offset, mat offset) per request
         for (Request* r : rs) {
-            const TProgram* P = program_of(S, r);
+            const TProgram* P = r->prog;
             pofs.push_back({ins.size(), mats.size() / 2});
             ins.insert(ins.end(), P->ins.begin(), P->ins.end());
             mats.insert(mats.end(), P->mats.begin(), P->mats.end());
@@ -176,7 +190,7 @@ void run_batch(qgpu_server* S, std::vector<Request*>& batch) {
         size_t b_dits = nwork * maxcreg * sizeof(uint32_t);
         size_t b_samp = nwork * sizeof(uint64_t);
         size_t b_g = n > uint32_t(kTrajMaxQubits)
-                         ? size_t(traj_global_grid(ctx, int(nwork))) * N * sizeof(float2)
+                         ? size_t(traj_global_grid(ctx, int(nwork), int(n))) * N * sizeof(float2)
                          : 0;
         size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_dits) + al(b_samp) + al(b_g);
         unsigned char* buf = nullptr;
@@ -197,7 +211,7 @@ void run_batch(qgpu_server* S, std::vector<Request*>& batch) {
         work.reserve(nwork);
         uint32_t out = 0;
         for (size_t i = 0; i < rs.size(); ++i) {
-            const TProgram* P = program_of(S, rs[i]);
+            const TProgram* P = rs[i]->prog;
             for (uint64_t s = 0; s < rs[i]->shots; ++s) {
                 TWork w{};
                 w.prog = dins + pofs[i].first;
@@ -226,7 +240,6 @@ void run_batch(qgpu_server* S, std::vector<Request*>& batch) {
         QG_CUDA(cudaMemcpyAsync(hs.data(), dsamp, b_samp, cudaMemcpyDeviceToHost, ctx->stream));
         QG_CUDA(cudaFreeAsync(buf, ctx->stream));
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
-        S->launched_traj += nwork;
         out = 0;
         for (Request* r : rs) {
             const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
@@ -236,92 +249,63 @@ void run_batch(qgpu_server* S, std::vector<Request*>& batch) {
                 r->samples[s] = hs[out];
                 for (uint32_t i = 0; i < nc; ++i) r->dits[s * nc + i] = hd[size_t(out) * maxcreg + i];
             }
+            finish(S, r);
         }
+        std::lock_guard<std::mutex> lock(S->mu);
+        S->launched_traj += nwork;
     }
 }
 
-void finish(qgpu_server* S, Request* r) {
-    std::lock_guard<std::mutex> lock(S->mu);
-    r->t_done = Clock::now();
-    r->done = true;
-    S->cv_done.notify_all();
-}
-
-void worker_loop(qgpu_server* S) {
-    cudaSetDevice(S->ctx->device);
+void lane_loop(qgpu_server* S, int li) {
+    Lane& L = S->lanes[li];
+    cudaSetDevice(L.ctx->device);
+    const bool batching = li < 2;
     for (;;) {
         std::vector<Request*> got;
         {
             std::unique_lock<std::mutex> lock(S->mu);
-            S->cv_work.wait(lock, [&] { return S->stop || !S->queue.empty(); });
-            if (S->stop && S->queue.empty()) return;
-            if (S->mode == 1) {
-                got.push_back(S->queue.front());
-                S->queue.pop_front();
+            S->cv_work.wait(lock, [&] { return S->stop || !L.q.empty(); });
+            if (S->stop && L.q.empty()) return;
+            if (!batching) {
+                got.push_back(L.q.front());
+                L.q.pop_front();
             } else {
-                // admit in arrival order while the estimated footprint fits
+                // admit in arrival order while the estimated footprint fits:
+                // per-CTA slots for >= 15 qubits, outputs otherwise
                 uint64_t used = 0;
-                while (!S->queue.empty()) {
-                    Request* r = S->queue.front();
-                    uint64_t need = program_of(S, r) ? r->shots * 64 : 2 * state_bytes(r, QGPU_C64);
+                while (!L.q.empty()) {
+                    Request* r = L.q.front();
+                    uint64_t need = r->shots * 64 + (r->prog->n > uint32_t(kTrajMaxQubits)
+                                                          ? (uint64_t(8) << r->prog->n) * 8
+                                                          : 0);
                     if (!got.empty() && used + need > S->budget) break;
                     used += need;
                     got.push_back(r);
-                    S->queue.pop_front();
+                    L.q.pop_front();
                 }
             }
         }
         auto t0 = Clock::now();
-        std::vector<Request*> batch, rest;
-        for (Request* r : got) (S->mode == 0 && program_of(S, r) ? batch : rest).push_back(r);
-        try {
-            if (!batch.empty()) {
-                std::thread side;
-                std::vector<std::pair<Request*, std::string>> side_err;
-                // engine-path requests overlap the batch on the second stream
-                if (!rest.empty())
-                    side = std::thread([&] {
-                        cudaSetDevice(S->ctx2->device);
-                        for (Request* r : rest) {
-                            try {
-                                run_engine(S->ctx2, r, QGPU_C64);
-                            } catch (const Exc& e) {
-                                r->status = e.code;
-                                r->err = e.where + ": " + e.what;
-                            }
-                            finish(S, r);
-                        }
-                    });
+        if (batching) {
+            try {
+                run_batch(S, L.ctx, got);
+            } catch (const Exc& e) {
+                for (Request* r : got)
+                    if (!r->done) fail(S, r, e.code, e.where + ": " + e.what);
+            }
+        } else {
+            for (Request* r : got) {
                 try {
-                    run_batch(S, batch);
-                } catch (const Exc& e) {
-                    for (Request* r : batch) {
-                        r->status = e.code;
-                        r->err = e.where + ": " + e.what;
-                    }
-                }
-                for (Request* r : batch) finish(S, r);
-                if (side.joinable()) side.join();
-                ++S->batches;
-            } else {
-                for (Request* r : rest) {
-                    try {
-                        run_engine(S->ctx2, r, S->mode == 1 ? QGPU_C128 : QGPU_C64);
-                    } catch (const Exc& e) {
-                        r->status = e.code;
-                        r->err = e.where + ": " + e.what;
-                    }
-                    ++S->engine_runs;
+                    run_engine(L.ctx, r, S->mode == 1 ? QGPU_C128 : QGPU_C64);
                     finish(S, r);
+                } catch (const Exc& e) {
+                    fail(S, r, e.code, e.where + ": " + e.what);
                 }
             }
-        } catch (...) {
-            for (Request* r : got)
-                if (!r->done) {
-                    r->status = QGPU_ERR_CUDA;
-                    finish(S, r);
-                }
         }
+        std::lock_guard<std::mutex> lock(S->mu);
+        if (batching) ++S->batches;
+        else S->engine_runs += got.size();
         S->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
     }
 }
@@ -341,16 +325,18 @@ qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode, qgpu_s
         if (mode != 0 && mode != 1)
             raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_server_create()", "mode");
         auto* S = new qgpu_server;
-        qgpu_status st = qgpu_ctx_create(device, &S->ctx);
-        if (st == QGPU_OK) st = qgpu_ctx_create(device, &S->ctx2);
-        if (st != QGPU_OK) {
-            if (S->ctx) qgpu_ctx_destroy(S->ctx);
-            delete S;
-            raise(st, "qgpu_server_create()", "context");
-        }
         S->mode = mode;
         S->budget = hbm_budget;
-        S->worker = std::thread(qgpu::worker_loop, S);
+        for (auto& L : S->lanes) {
+            qgpu_status st = qgpu_ctx_create(device, &L.ctx);
+            if (st != QGPU_OK) {
+                for (auto& M : S->lanes)
+                    if (M.ctx) qgpu_ctx_destroy(M.ctx);
+                delete S;
+                raise(st, "qgpu_server_create()", "context");
+            }
+        }
+        for (int i = 0; i < 3; ++i) S->lanes[i].th = std::thread(qgpu::lane_loop, S, i);
         *out = S;
     });
 }
@@ -372,9 +358,14 @@ qgpu_status qgpu_server_submit(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind, 
             std::lock_guard<std::mutex> lock(S->mu);
             r->id = S->next_id++;
             S->all[r->id] = r;
-            S->queue.push_back(r);
+            int lane = 2;
+            if (S->mode == 0) {
+                r->prog = qgpu::program_of(S, c, kind);
+                if (r->prog) lane = r->prog->n > uint32_t(qgpu::kTrajMaxQubits) ? 1 : 0;
+            }
+            S->lanes[lane].q.push_back(r);
         }
-        S->cv_work.notify_one();
+        S->cv_work.notify_all();
         if (id) *id = r->id;
     });
 }
@@ -427,10 +418,10 @@ qgpu_status qgpu_server_destroy(qgpu_server* S) {
             S->stop = true;
         }
         S->cv_work.notify_all();
-        if (S->worker.joinable()) S->worker.join();
+        for (auto& L : S->lanes)
+            if (L.th.joinable()) L.th.join();
         for (auto& kv : S->all) delete kv.second;
-        qgpu_ctx_destroy(S->ctx2);
-        qgpu_ctx_destroy(S->ctx);
+        for (auto& L : S->lanes) qgpu_ctx_destroy(L.ctx);
         delete S;
     });
 }

@@ -130,7 +130,8 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
         size_t b_dump = dump ? shots * N * sizeof(float2) : 0;
         size_t b_ev = events ? shots * size_t(max_events) * sizeof(qgpu::TEvent) : 0;
         size_t b_g = P.n > uint32_t(qgpu::kTrajMaxQubits)
-                         ? size_t(qgpu::traj_global_grid(ctx, int(shots))) * N * sizeof(float2)
+                         ? size_t(qgpu::traj_global_grid(ctx, int(shots), int(P.n))) * N *
+                               sizeof(float2)
                          : 0;
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
         size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_dits) + al(b_samp) + al(b_dump) +

@@ -33,6 +33,8 @@ struct TWork {
     uint32_t shot;  // trajectory index inside its request (Philox counter)
     uint32_t out;   // global output slot
     uint64_t seed;  // request seed (Philox key)
+    const float2* init; // initial register (null: |0...0>)
+    float2* fin;        // where the final register goes (null: nowhere)
 };
 
 // Recorded noise event: before instruction `ins`, Pauli `pauli` (1 X, 2 Y,
@@ -47,8 +49,12 @@ struct TEvent {
 // kTrajMaxGlobalQubits a CTA works on its own slot of a global scratch
 // buffer instead (traj_global_grid(ctx, nwork) slots of 2^n amplitudes).
 constexpr int kTrajMaxQubits = 14;
-constexpr int kTrajMaxGlobalQubits = 20;
-int traj_global_grid(qgpu_ctx* ctx, int nwork);
+constexpr int kTrajMaxGlobalQubits = 22;
+// CTAs (= scratch slots) for a launch of nwork trajectories of n qubits:
+// at most 8 per SM and at most 4 GiB of slots.
+int traj_global_grid(qgpu_ctx* ctx, int nwork, int n);
+// Raises the kernel's shared-memory limit once (outside any stream capture).
+void traj_prepare();
 
 struct TProgram {
     uint32_t n = 0;
@@ -61,5 +67,10 @@ void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_
                  int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
                  int max_events, float2* gscratch);
 bool compile_traj(const qgpu_circuit* c, TProgram& P);
+// A density-matrix run of `c` as a ket over 2n virtual qubits [column
+// digits, row digits]: 1-qubit gates and 1-qubit channels become 4 x 4
+// superoperators on (column t, row t); 2-qubit gates become U on the row
+// digits and conj(U) on the column digits. False for anything else.
+bool compile_traj_rho(const qgpu_circuit* c, TProgram& P);
 
 } // namespace qgpu
