@@ -186,6 +186,28 @@ qgpu_status qgpu_normalize(qgpu_state* s);
 qgpu_status qgpu_inner(const qgpu_state* a, const qgpu_state* b, double* re,
                        double* im);
 
+/* ----------------------------------------- Z-basis sampling and measurement
+ * Replaces qpp::sample(num_samples, A, target, dims)
+ * (instruments.hpp:856-940): num_samples full-basis draws of |A_i|^2 (ket)
+ * or Re A(i, i) (density matrix); results[i * k + j] = digit of target[j] in
+ * draw i. The draws are std::discrete_distribution's: u = the caller's
+ * uniforms in [0, 1) when u != NULL, else generate_canonical<double, 53> of a
+ * std::mt19937 seeded with `seed` (qpp's generator, seeded); index = the first
+ * whose FP64 prefix sum reaches u * total. One pass over the state plus one
+ * 4096-weight chunk scanned per draw. */
+qgpu_status qgpu_sample(const qgpu_state* s, const uint64_t* target, uint32_t k,
+                        uint64_t num_samples, uint64_t seed, const double* u,
+                        uint64_t* results);
+/* Replaces qpp::measure_seq(A, target, dims, destructive)
+ * (instruments.hpp:985-1111), value semantics: one full-basis draw (seeded
+ * as above; forced != NULL gives the outcomes instead), then each target is
+ * projected and renormalised (probs = qpp's conditional probabilities);
+ * destructive drops the measured subsystems. *out is a new state; `s` is
+ * unchanged. */
+qgpu_status qgpu_measure_seq(const qgpu_state* s, const uint64_t* target, uint32_t k,
+                             int destructive, uint64_t seed, const uint64_t* forced,
+                             uint64_t* results, double* probs, qgpu_state** out);
+
 /* ------------------------------------- value-semantics entry points (host)
  * These mirror qpp's free functions exactly: the state is a host array with
  * `rows` x `cols` (cols == 1 for a ket, rows == cols for a density matrix),
@@ -305,22 +327,38 @@ qgpu_status qgpu_engine_set_seed(qgpu_engine* e, uint64_t seed);
 qgpu_status qgpu_engine_set_noise(qgpu_engine* e, const double* Ks,
                                   uint32_t nK, uint64_t d,
                                   const double* probs);
-/* QEngineT::set_state (qengine.hpp:1191-1214): the initial state of every
- * repetition (default |0...0>). */
+/* QEngineT::set_state (qengine.hpp:1191-1214): replaces the engine's
+ * current state (a copy); its dimension must be d^(qudits not measured
+ * destructively), else QGPU_ERR_DIMS_NOT_EQUAL; a density matrix for a ket
+ * engine (or the reverse) is QGPU_ERR_TYPE_MISMATCH. */
 qgpu_status qgpu_engine_set_state(qgpu_engine* e, const qgpu_state* s);
+/* QEngineT::reset / QNoisyEngineT::reset (qengine.hpp:1251-1260): the state
+ * back to |0...0>, dits / probabilities / measured qudits cleared; the
+ * statistics too when reset_stats != 0. */
+qgpu_status qgpu_engine_reset(qgpu_engine* e, int reset_stats);
 /* Force the random choices: measurement outcome dits in execution order and
  * Kraus indices step by step, qudit by qudit (NULL, 0 to stop replaying). */
 qgpu_status qgpu_engine_set_replay(qgpu_engine* e, const uint64_t* outcomes,
                                    uint64_t n_out, const uint64_t* noise,
                                    uint64_t n_noise);
-/* QEngineT::execute(reps) (qengine.hpp:1341-1405): reps independent runs
- * from the initial state; dits / probs / state hold the last run. */
+/* QEngineT::execute(reps) (qengine.hpp:1341-1405). A noiseless engine
+ * starts from its current state (which must be full size), clears the dits,
+ * and for reps > 1 reorders the circuit as qpp's canonical_form (classical
+ * controls, then measurements, pushed to the end past steps they commute
+ * with); the steps before the first measurement run once, the rest reps
+ * times from that point. When the rest holds only measurements, one run
+ * gives the engine state and the other reps - 1 are full-basis samples of
+ * the pre-measurement state (qengine.hpp:374-481), drawn in qpp's RNG order.
+ * A noisy engine (qnoisy_engine.hpp:129-139) runs every step reps times from
+ * its current engine state. Either way the engine keeps the FIRST
+ * repetition's state, dits and probabilities, and the statistics accumulate
+ * across calls until a reset. reps == 0: QGPU_ERR_OUT_OF_RANGE. */
 qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps);
 qgpu_status qgpu_engine_get_dits(const qgpu_engine* e, uint64_t* dits,
                                  double* probs);
 /* A new state handle holding a copy of the engine's current state. */
 qgpu_status qgpu_engine_get_state(const qgpu_engine* e, qgpu_state** out);
-/* Outcome statistics of the last execute (QEngineStatistics): the number of
+/* Outcome statistics since the last reset (QEngineStatistics): the number of
  * distinct dit vectors, then their counts and the vectors (nc dits each). */
 qgpu_status qgpu_engine_get_stats(const qgpu_engine* e, uint64_t* n_distinct,
                                   uint64_t* counts, uint64_t* outcomes);

@@ -12,6 +12,8 @@
 //   qpp_b200::ptrace(A, target, dims)                       operations.hpp:1908
 //   qpp_b200::ptranspose(A, target, dims)                   operations.hpp:2167
 //   qpp_b200::syspermute(A, perm, dims)                     operations.hpp:2386
+//   qpp_b200::sample(num_samples, A, target, dims, seed)    instruments.hpp:856
+//   qpp_b200::measure_seq(A, target, dims, destructive, seed) instruments.hpp:985
 //
 // Matrices are qpp_b200::cmat (column-major std::complex<double>, rows x
 // cols; a ket is D x 1). When Eigen is available the same functions accept
@@ -24,6 +26,8 @@
 
 #include <cmath>
 #include <complex>
+#include <map>
+#include <tuple>
 #include <cstdint>
 #include <optional>
 #include <stdexcept>
@@ -271,6 +275,78 @@ inline cmat syspermute(const cmat& A, const std::vector<idx>& perm, const std::v
                                        detail::ptr(p), uint32_t(p.size()), detail::ptr(d),
                                        uint32_t(d.size()), out.raw()));
     return out;
+}
+
+namespace detail {
+// qpp's state checks for sample / measure_seq (instruments.hpp:757-781,
+// :996-1017), then the state uploaded as a resident handle
+struct StateHolder {
+    qgpu_state* s = nullptr;
+    ~StateHolder() {
+        if (s) qgpu_state_destroy(s);
+    }
+};
+inline void upload_checked(const cmat& A, const std::vector<idx>& dims, const char* W,
+                           StateHolder& h) {
+    using namespace exception;
+    if (A.rows() * A.cols() == 0) throw ZeroSize(W, "A");
+    idx D = 1;
+    bool ok = !dims.empty();
+    for (idx x : dims) {
+        ok = ok && x != 0;
+        D *= x;
+    }
+    if (!ok) throw DimsInvalid(W, "dims");
+    const bool is_ket = A.cols() == 1;
+    if (is_ket) {
+        if (D != A.rows()) throw DimsMismatchCvector(W, "A/dims");
+    } else if (A.rows() == A.cols()) {
+        if (D != A.rows()) throw DimsMismatchMatrix(W, "A/dims");
+    } else {
+        throw MatrixNotSquareNorCvector(W, "A");
+    }
+    auto d = u64(dims);
+    check(qgpu_state_create(ctx(), is_ket ? QGPU_KET : QGPU_RHO, QGPU_C128, ptr(d),
+                            uint32_t(d.size()), &h.s));
+    check(qgpu_state_upload_c128(h.s, A.raw()));
+}
+} // namespace detail
+
+// qpp::sample(num_samples, A, target, dims) (instruments.hpp:856-940), with
+// the draws of a std::mt19937 seeded with `seed`.
+inline std::map<std::vector<idx>, idx> sample(idx num_samples, const cmat& A,
+                                              const std::vector<idx>& target,
+                                              const std::vector<idx>& dims, uint64_t seed = 0) {
+    detail::StateHolder h;
+    detail::upload_checked(A, dims, "qpp::sample()", h);
+    auto t = detail::u64(target);
+    std::vector<uint64_t> r(num_samples * t.size() + 1);
+    detail::check(qgpu_sample(h.s, detail::ptr(t), uint32_t(t.size()), num_samples, seed,
+                              nullptr, r.data()));
+    std::map<std::vector<idx>, idx> out;
+    for (idx i = 0; i < num_samples; ++i)
+        ++out[std::vector<idx>(r.begin() + i * t.size(), r.begin() + (i + 1) * t.size())];
+    return out;
+}
+
+// qpp::measure_seq(A, target, dims, destructive) (instruments.hpp:985-1111):
+// (outcomes, probabilities, post-measurement state).
+inline std::tuple<std::vector<idx>, std::vector<double>, cmat>
+measure_seq(const cmat& A, const std::vector<idx>& target, const std::vector<idx>& dims,
+            bool destructive = true, uint64_t seed = 0) {
+    detail::StateHolder h, o;
+    detail::upload_checked(A, dims, "qpp::measure_seq()", h);
+    auto t = detail::u64(target);
+    std::vector<uint64_t> res(t.size() + 1);
+    std::vector<double> ps(t.size() + 1);
+    detail::check(qgpu_measure_seq(h.s, detail::ptr(t), uint32_t(t.size()), destructive ? 1 : 0,
+                                   seed, nullptr, res.data(), ps.data(), &o.s));
+    uint64_t D = 0;
+    detail::check(qgpu_state_info(o.s, nullptr, nullptr, nullptr, nullptr, &D));
+    cmat out(D, A.cols() == 1 ? 1 : D);
+    detail::check(qgpu_state_download_c128(o.s, out.raw()));
+    return {std::vector<idx>(res.begin(), res.begin() + t.size()),
+            std::vector<double>(ps.begin(), ps.begin() + t.size()), out};
 }
 
 #ifdef QPP_B200_HAS_EIGEN

@@ -214,3 +214,19 @@ def measure_seq(state, target, dims, destructive=True, forced=None, seed=0):
     else:
         st = out[: Dn * Dn].reshape((Dn, Dn), order="F").copy()
     return [int(x) for x in res[:k]], [float(x) for x in probs[:k]], st, nd
+
+
+def sample(state, target, dims, num_samples, seed=0):
+    """qpp::sample(num_samples, A, target, dims), instruments.hpp:856-940, with
+    std::mt19937(seed): the target digits of every draw, in draw order
+    (num_samples x len(target))."""
+    buf, rows, cols = _state(state)
+    t, tp = _u64(target)
+    d, dpp = _u64(dims)
+    k = len(t)
+    out = np.zeros(max(num_samples * k, 1), dtype=np.uint64)
+    _check(lib().oracle_sample(_dp(buf), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                               ct.c_uint32(k), dpp, ct.c_uint32(len(d)),
+                               ct.c_uint64(num_samples), ct.c_uint64(seed),
+                               out.ctypes.data_as(u64p)))
+    return out[: num_samples * k].reshape(num_samples, k).astype(np.int64)

@@ -901,7 +901,7 @@ int oracle_measure_seq(const double* state, idx rows, idx cols,
             std::vector<cplx> B(ket ? Dn : Dn * Dn);
             if (ket) {
                 for (idx i = 0; i < Dc; ++i) {
-                    idx dg[kMaxN], dn[kMaxN];
+                    idx dg[kMaxN] = {}, dn[kMaxN];
                     to_digits(i, n, cd.data(), dg);
                     if (dg[t] != res[ip]) continue;
                     idx m = 0;
@@ -931,6 +931,37 @@ int oracle_measure_seq(const double* state, idx rows, idx cols,
     std::memcpy(out_state, A.data(), A.size() * sizeof(cplx));
     for (idx i = 0; i < cd.size(); ++i) out_dims[i] = cd[i];
     *out_nd = static_cast<uint32_t>(cd.size());
+    return 0;
+}
+
+// qpp::sample(num_samples, A, target, dims), instruments.hpp:856-940:
+// num_samples draws of one std::discrete_distribution over the full basis
+// (|A_i|^2 for a ket, Re A(i, i) for a density matrix) from
+// std::mt19937(seed); results[i * k + j] = digit target[j] of draw i.
+int oracle_sample(const double* state, idx rows, idx cols, const uint64_t* target_p,
+                  uint32_t k, const uint64_t* dims_p, uint32_t nd, uint64_t num_samples,
+                  uint64_t seed, uint64_t* results) {
+    const char* W = "qpp::sample()";
+    std::vector<idx> target = vec(target_p, k), dims = vec(dims_p, nd);
+    if (rows * cols == 0) return fail({QGPU_ERR_ZERO_SIZE, W, "A"});
+    if (!dims_ok(dims)) return fail({QGPU_ERR_DIMS_INVALID, W, "dims"});
+    if (int e = check_state_shape(rows, cols, dims, W, "A/dims", "A/dims", "A"))
+        return e;
+    if (!subsys_ok(target, dims))
+        return fail({QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target"});
+    if (num_samples == 0) return fail({QGPU_ERR_OUT_OF_RANGE, W, "num_samples"});
+    const bool ket = cols == 1;
+    const idx D = rows;
+    const cplx* A = C(state);
+    std::vector<double> pbs(D);
+    for (idx i = 0; i < D; ++i) pbs[i] = ket ? std::norm(A[i]) : A[i + i * D].real();
+    std::mt19937 gen(static_cast<uint32_t>(seed));
+    std::discrete_distribution<idx> dd(pbs.begin(), pbs.end());
+    for (uint64_t r = 0; r < num_samples; ++r) {
+        idx dg[kMaxN];
+        to_digits(dd(gen), dims.size(), dims.data(), dg);
+        for (uint32_t j = 0; j < k; ++j) results[r * k + j] = dg[target[j]];
+    }
     return 0;
 }
 

@@ -276,6 +276,42 @@ class State:
         check(lib().qgpu_state_clone(self.h, ct.byref(h)))
         return State(self.ctx, self.kind, None, handle=h)
 
+    def sample_draws(self, target, num_samples, seed=0, u=None):
+        """qpp::sample(num_samples, ...) draws in order: an array of
+        num_samples x len(target) digits (std::mt19937(seed), or the given
+        uniforms u)."""
+        t, tp, nt = _u64(target)
+        out = np.zeros(max(num_samples * nt, 1), dtype=np.uint64)
+        up = None
+        if u is not None:
+            u = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
+            up = _dp(u)
+        check(lib().qgpu_sample(self.h, tp, ct.c_uint32(nt), ct.c_uint64(num_samples),
+                                ct.c_uint64(seed), up, out.ctypes.data_as(u64p)))
+        return out[: num_samples * nt].reshape(num_samples, nt).astype(np.int64)
+
+    def sample(self, target, num_samples, seed=0, u=None):
+        """qpp::sample(num_samples, A, target, dims): {outcome tuple: count}."""
+        res = {}
+        for row in self.sample_draws(target, num_samples, seed, u):
+            key = tuple(int(x) for x in row)
+            res[key] = res.get(key, 0) + 1
+        return res
+
+    def measure_seq(self, target, destructive=True, seed=0, forced=None):
+        """qpp::measure_seq(A, target, dims, destructive): (results, probs,
+        post-measurement State); this state is unchanged."""
+        t, tp, nt = _u64(target)
+        f, fp, _ = _u64(forced)
+        res = np.zeros(max(nt, 1), dtype=np.uint64)
+        probs = np.zeros(max(nt, 1), dtype=np.float64)
+        h = vp()
+        check(lib().qgpu_measure_seq(self.h, tp, ct.c_uint32(nt), ct.c_int(1 if destructive else 0),
+                                     ct.c_uint64(seed), fp, res.ctypes.data_as(u64p), _dp(probs),
+                                     ct.byref(h)))
+        return ([int(x) for x in res[:nt]], [float(x) for x in probs[:nt]],
+                State(self.ctx, self.kind, None, handle=h))
+
     def free(self):
         if self.h:
             check(lib().qgpu_state_destroy(self.h))
@@ -516,6 +552,10 @@ class Engine:
         return self
 
     def set_noise(self, Ks, probs=None):
+        """A Kraus list (+ probabilities; None: state-dependent), or one of
+        the models of qpp_b200.noise."""
+        if hasattr(Ks, "Ks"):
+            Ks, probs = Ks.Ks, Ks.probs
         packed, d = _pack_kraus(Ks)
         pr = None if probs is None else np.ascontiguousarray(np.asarray(probs, dtype=np.float64))
         check(lib().qgpu_engine_set_noise(self.h, _dp(packed), ct.c_uint32(len(Ks)),
@@ -532,7 +572,16 @@ class Engine:
         check(lib().qgpu_engine_set_replay(self.h, op, ct.c_uint64(no), kp, ct.c_uint64(nk)))
         return self
 
+    def reset(self, reset_stats=True):
+        """State back to |0...0>, registers cleared (statistics too unless
+        reset_stats is False)."""
+        check(lib().qgpu_engine_reset(self.h, ct.c_int(1 if reset_stats else 0)))
+        return self
+
     def execute(self, reps=1):
+        """qpp's execute(reps): from the engine's current state; the engine
+        keeps the first repetition's state and dits; statistics accumulate
+        until reset()."""
         check(lib().qgpu_engine_execute(self.h, ct.c_uint64(reps)))
         return self
 

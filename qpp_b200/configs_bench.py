@@ -154,14 +154,18 @@ def config2(ctx, torch, stream, cpu=True, steps=200):
     sm = State.from_numpy(ctx, rm, dims)
     a, b = _events(torch, stream)
     a.record(stream)
+    cur = list(dims)  # dims follow the permutations
     for _ in range(20):
-        q3 = int(rng.choice([0, 1, 4, 7]))
-        sm.apply(haar_unitary(rng, 3), [q3])
-        sm.apply(haar_unitary(rng, 6), [int(rng.choice([0, 1, 4, 7])), int(rng.choice([2, 3, 5, 6]))])
+        threes = [q for q in range(8) if cur[q] == 3]
+        twos = [q for q in range(8) if cur[q] == 2]
+        sm.apply(haar_unitary(rng, 3), [int(rng.choice(threes))])
+        sm.apply(haar_unitary(rng, 6), [int(rng.choice(threes)), int(rng.choice(twos))])
         half = [int(x) for x in rng.choice(8, 4, replace=False)]
         sm.ptrace(half).free()
         sm.ptranspose(half).free()
-        nxt = sm.syspermute([int(x) for x in rng.permutation(8)])
+        perm = [int(x) for x in rng.permutation(8)]
+        nxt = sm.syspermute(perm)
+        cur = [cur[p] for p in perm]
         sm.free()
         sm = nxt
     b.record(stream)
@@ -203,12 +207,14 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
     def states(prec):
         out = []
         for i, (k, n) in enumerate(zip(kinds, sizes)):
-            s = State(ctx, k, [2] * n, prec)
             if k == KET:
-                s.fill_gaussian(100 + i)
+                s = State(ctx, KET, [2] * n, prec).fill_gaussian(100 + i)
             else:
-                from .workloads import haar_unitary as _h  # noqa: F401
-                s.fill_gaussian(100 + i)  # random Hermitian-free start; unit trace
+                # rank 8: W (2^n x 8 Gaussian, unit norm) as a ket over
+                # [2]*n + [8]; tracing out the last subsystem gives W W^dagger
+                w = State(ctx, KET, [2] * n + [8], prec).fill_gaussian(100 + i)
+                s = w.ptrace([n])
+                w.free()
             out.append(s)
         return out
 

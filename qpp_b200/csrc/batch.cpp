@@ -5,13 +5,16 @@
 // form compiles every instance into a trajectory program (a density matrix
 // as a ket over 2n virtual qubits, see compile_traj_rho), groups instances
 // by register size, and captures one trajectory-kernel launch per size into
-// a single CUDA graph, so the whole batch is one graph launch; every
-// instance reads its initial state from, and writes its final state back to,
-// its own qgpu_state. The plain form loops over the instances with one
-// kernel launch per gate (qgpu_run_gates, QGPU_FORM_PLAIN).
+// a single CUDA graph (one parallel branch per size), so the whole batch is
+// one graph launch. One CTA runs one instance: registers of up to 2^14
+// amplitudes are copied into shared memory and back to the instance's own
+// qgpu_state; larger ones are worked on in place in that state (HBM). The
+// plain form loops over the instances with one kernel launch per gate
+// (qgpu_run_gates, QGPU_FORM_PLAIN).
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <set>
 
 #include "capi_common.hpp"
 #include "circuit.hpp"
@@ -75,14 +78,30 @@ bool compile_traj_rho(const qgpu_circuit* c, TProgram& P) {
                 break;
             }
             case StepKind::Channel: {
-                if (s.target.size() != 1 || s.DU != 2) return false;
-                std::vector<cd> S(16, 0.0);
+                const uint64_t DK = s.DU;
+                if (!((s.target.size() == 1 && DK == 2) || (s.target.size() == 2 && DK == 4)))
+                    return false;
+                const uint64_t DS = DK * DK;
+                std::vector<cd> S(DS * DS, 0.0);
                 for (uint32_t i = 0; i < s.nK; ++i) {
-                    std::vector<cd> K(s.U.begin() + 4 * i, s.U.begin() + 4 * (i + 1));
-                    std::vector<cd> t = kron_mat(conj_mat(K), 2, K, 2);
-                    for (int j = 0; j < 16; ++j) S[j] += t[j];
+                    std::vector<cd> K(s.U.begin() + DK * DK * i, s.U.begin() + DK * DK * (i + 1));
+                    std::vector<cd> t = kron_mat(conj_mat(K), DK, K, DK);
+                    for (size_t j = 0; j < t.size(); ++j) S[j] += t[j];
                 }
-                super1(int(s.target[0]), S, first);
+                if (s.target.size() == 1) {
+                    super1(int(s.target[0]), S, first);
+                } else {
+                    // sum_i conj(K_i) (x) K_i on (col a, col b, row a, row b)
+                    int a = int(s.target[0]), b = int(s.target[1]);
+                    TInstr I{};
+                    I.op = kTG4;
+                    I.b0 = vbit(a);
+                    I.b1 = vbit(b);
+                    I.cmask = uint32_t(vbit(nq + a)) | (uint32_t(vbit(nq + b)) << 8);
+                    I.flags = first;
+                    I.mat = add_mat(S);
+                    P.ins.push_back(I);
+                }
                 break;
             }
             case StepKind::Nop:
@@ -106,9 +125,13 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
     return guarded([&] {
         need_handle(ctx);
         const char* W = "qgpu_run_batch()";
+        if (n_inst && (!circuits || !states)) raise(QGPU_ERR_INVALID_ARGUMENT, W, "arrays");
+        std::set<const qgpu_state*> seen;
         for (uint32_t i = 0; i < n_inst; ++i) {
             need_handle(circuits[i]);
             need_handle(states[i]);
+            // instances run concurrently, each in its own state
+            if (!seen.insert(states[i]).second) raise(QGPU_ERR_DUPLICATES, W, "states");
             const qgpu_state* s = states[i];
             if (s->dims.size() != circuits[i]->nq)
                 raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, W, "state/circuit");
@@ -143,13 +166,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             size_t b_mat = std::max<size_t>(mats.size() * sizeof(float), 16);
             size_t b_work = prog.size() * sizeof(qgpu::TWork);
             size_t b_out = prog.size() * (sizeof(uint64_t) + sizeof(uint32_t) * 8);
-            size_t b_g = 0;
-            for (auto& kv : by_n)
-                if (kv.first > uint32_t(qgpu::kTrajMaxQubits))
-                    b_g = std::max(b_g, al(size_t(qgpu::traj_global_grid(ctx, int(kv.second.size()),
-                                                                         int(kv.first))) *
-                                           (size_t(1) << kv.first) * sizeof(float2)));
-            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_out) + b_g;
+            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_out);
             unsigned char* buf = nullptr;
             QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), total, ctx->stream));
             unsigned char* p = buf;
@@ -163,7 +180,6 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             auto* dwork = reinterpret_cast<qgpu::TWork*>(take(b_work));
             auto* dsamp = reinterpret_cast<uint64_t*>(take(prog.size() * sizeof(uint64_t)));
             auto* ddits = reinterpret_cast<uint32_t*>(take(prog.size() * sizeof(uint32_t) * 8));
-            auto* dg = reinterpret_cast<float2*>(b_g ? take(b_g) : nullptr);
             std::vector<qgpu::TWork> work;
             std::vector<std::pair<uint32_t, std::pair<size_t, size_t>>> ranges; // n -> [lo, hi)
             for (auto& kv : by_n) {
@@ -180,6 +196,8 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     w.seed = prog[k].first;
                     w.init = static_cast<const float2*>(states[prog[k].first]->data);
                     w.fin = static_cast<float2*>(states[prog[k].first]->data);
+                    // above shared-memory size the CTA works in the state itself
+                    w.inplace = kv.first > uint32_t(qgpu::kTrajMaxQubits) ? 1 : 0;
                     work.push_back(w);
                 }
                 ranges.push_back({kv.first, {lo, work.size()}});
@@ -191,17 +209,38 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                                         cudaMemcpyHostToDevice, ctx->stream));
             QG_CUDA(cudaMemcpyAsync(dwork, work.data(), b_work, cudaMemcpyHostToDevice,
                                     ctx->stream));
-            // one graph: a launch per register size, back to back
+            // one graph: a launch per register size, each on its own branch
+            // (the groups touch disjoint states), so the small-register
+            // launches fill the SMs that the few large instances leave idle
             qgpu::traj_prepare();
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
+            std::vector<cudaStream_t> side(ranges.size(), nullptr);
+            std::vector<cudaEvent_t> ev(ranges.size() + 1, nullptr);
+            struct Rel {
+                std::vector<cudaStream_t>& s;
+                std::vector<cudaEvent_t>& e;
+                ~Rel() {
+                    for (cudaStream_t x : s)
+                        if (x) cudaStreamDestroy(x);
+                    for (cudaEvent_t x : e)
+                        if (x) cudaEventDestroy(x);
+                }
+            } rel{side, ev};
+            for (auto& x : side) QG_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+            for (auto& x : ev) QG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
             QG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
             try {
-                for (auto& rg : ranges)
+                QG_CUDA(cudaEventRecord(ev[0], ctx->stream));
+                for (size_t g = 0; g < ranges.size(); ++g) {
+                    const auto& rg = ranges[g];
+                    QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
                     qgpu::launch_traj(ctx, dwork + rg.second.first,
                                       int(rg.second.second - rg.second.first), int(rg.first), ddits, 1,
-                                      dsamp, nullptr, nullptr, 0,
-                                      rg.first > uint32_t(qgpu::kTrajMaxQubits) ? dg : nullptr);
+                                      dsamp, nullptr, nullptr, 0, nullptr, side[g]);
+                    QG_CUDA(cudaEventRecord(ev[g + 1], side[g]));
+                    QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
+                }
             } catch (...) {
                 cudaStreamEndCapture(ctx->stream, &graph);
                 if (graph) cudaGraphDestroy(graph);

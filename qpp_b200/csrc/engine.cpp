@@ -24,6 +24,7 @@
 #include <cstring>
 #include <map>
 #include <random>
+#include <set>
 
 #include "capi_common.hpp"
 #include "circuit.hpp"
@@ -45,9 +46,9 @@ struct qgpu_engine {
     std::vector<double> kprobs;
     std::vector<int> kclass; // 0 general, 1 identity-like, 2 unitary-like
     std::vector<std::vector<cd>> kunit; // normalised unitary for class 2
-    // optional initial state
-    qgpu_state* init = nullptr;
-    // run state
+    // engine state (qengine_state.hpp:52-157): the current state (null:
+    // |0...0> not materialised yet), dits, probabilities, and which qudits
+    // were measured destructively
     qgpu_state* st = nullptr;
     std::vector<uint64_t> dits;
     std::vector<double> probs;
@@ -58,10 +59,7 @@ struct qgpu_engine {
     bool replay = false;
     std::vector<uint64_t> forced_outcomes, forced_noise;
     size_t fo_pos = 0, fn_pos = 0;
-    ~qgpu_engine() {
-        qgpu::free_state(st);
-        qgpu::free_state(init);
-    }
+    ~qgpu_engine() { qgpu::free_state(st); }
 };
 
 namespace qgpu {
@@ -78,31 +76,76 @@ uint64_t rel_pos(const qgpu_engine* e, uint64_t q) {
     return r;
 }
 
-void reset_state(qgpu_engine* e) {
-    free_state(e->st);
-    e->st = nullptr;
-    std::vector<uint64_t> dims(e->circ->nq, e->circ->d);
-    if (e->init) {
-        e->st = new_state(e->ctx, e->init->kind, e->prec, e->init->dims, false);
-        QG_CUDA(cudaMemcpyAsync(e->st->data, e->init->data, e->init->bytes(),
-                                cudaMemcpyDeviceToDevice, e->ctx->stream));
-    } else {
-        e->st = new_state(e->ctx, e->kind, e->prec, dims, true);
-        if (e->prec == QGPU_C128) {
-            static const double one[2] = {1.0, 0.0};
-            QG_CUDA(cudaMemcpyAsync(e->st->data, one, sizeof(one), cudaMemcpyHostToDevice,
-                                    e->ctx->stream));
-        } else {
-            static const float one[2] = {1.0f, 0.0f};
-            QG_CUDA(cudaMemcpyAsync(e->st->data, one, sizeof(one), cudaMemcpyHostToDevice,
-                                    e->ctx->stream));
-        }
-    }
+// dits, probabilities and measured flags back to their initial values
+// (QEngineState::reset, qengine_state.hpp:115-157)
+void clear_registers(qgpu_engine* e) {
     e->dits.assign(e->circ->nc, 0);
     e->probs.assign(e->circ->nc, 0.0);
     e->measured.assign(e->circ->nq, 0);
-    e->noise_results.assign(e->circ->steps.size(), {});
 }
+
+// materialise |0...0> (ket) or |0...0><0...0| when the engine has no state
+void ensure_state(qgpu_engine* e) {
+    if (e->dits.size() != e->circ->nc) clear_registers(e);
+    if (e->noise_results.size() != e->circ->steps.size())
+        e->noise_results.resize(e->circ->steps.size());
+    if (e->st) return;
+    std::vector<uint64_t> dims(e->circ->nq, e->circ->d);
+    e->st = new_state(e->ctx, e->kind, e->prec, dims, true);
+    if (e->prec == QGPU_C128) {
+        static const double one[2] = {1.0, 0.0};
+        QG_CUDA(cudaMemcpyAsync(e->st->data, one, sizeof(one), cudaMemcpyHostToDevice,
+                                e->ctx->stream));
+    } else {
+        static const float one[2] = {1.0f, 0.0f};
+        QG_CUDA(cudaMemcpyAsync(e->st->data, one, sizeof(one), cudaMemcpyHostToDevice,
+                                e->ctx->stream));
+    }
+}
+
+qgpu_state* copy_state(const qgpu_state* s) {
+    qgpu_state* c = new_state(s->ctx, s->kind, s->prec, s->dims, false);
+    QG_CUDA(cudaMemcpyAsync(c->data, s->data, s->bytes(), cudaMemcpyDeviceToDevice,
+                            s->ctx->stream));
+    return c;
+}
+
+// A copy of the engine state (qeng_st_ copies in qengine.hpp:316-345).
+struct Snapshot {
+    qgpu_state* st = nullptr;
+    std::vector<uint64_t> dits;
+    std::vector<double> probs;
+    std::vector<char> measured;
+    void take(qgpu_engine* e) { // move the engine's state in
+        st = e->st;
+        e->st = nullptr;
+        dits = e->dits;
+        probs = e->probs;
+        measured = e->measured;
+    }
+    void copy_from(const qgpu_engine* e) {
+        st = copy_state(e->st);
+        dits = e->dits;
+        probs = e->probs;
+        measured = e->measured;
+    }
+    void restore_copy(qgpu_engine* e) const {
+        free_state(e->st);
+        e->st = copy_state(st);
+        e->dits = dits;
+        e->probs = probs;
+        e->measured = measured;
+    }
+    void restore_move(qgpu_engine* e) {
+        free_state(e->st);
+        e->st = st;
+        st = nullptr;
+        e->dits = dits;
+        e->probs = probs;
+        e->measured = measured;
+    }
+    ~Snapshot() { free_state(st); }
+};
 
 // Draw from weights w with std::discrete_distribution semantics.
 uint64_t draw(std::mt19937& gen, const std::vector<double>& w) {
@@ -164,48 +207,78 @@ qgpu_state* drop(qgpu_state* s, const std::vector<uint64_t>& ts,
 }
 
 // qpp::measure_seq on the engine state (instruments.hpp:985-1111).
+// big-endian mixed-radix digits of a full-basis index (util.hpp:58-84)
+std::vector<uint64_t> digits_of(uint64_t idx, const std::vector<uint64_t>& dims) {
+    std::vector<uint64_t> dg(dims.size());
+    for (size_t q = dims.size(); q-- > 0;) {
+        dg[q] = idx % dims[q];
+        idx /= dims[q];
+    }
+    return dg;
+}
+
+double canonical(std::mt19937& gen) {
+    return std::generate_canonical<double, std::numeric_limits<double>::digits>(gen);
+}
+
+} // namespace
+
+// The collapse of qpp::measure_seq (instruments.hpp:1024-1093) for given
+// outcomes: project each target on its outcome and renormalise (ps = the
+// conditional probabilities); destructive: drop the targets (one at a time
+// in descending order, or all at the end for density matrices of <= 10
+// subsystems, as qpp does). `s` may be replaced by a smaller state.
+void collapse_seq(qgpu_state*& s, const std::vector<uint64_t>& tgt, bool destructive,
+                  const std::vector<uint64_t>& res, std::vector<double>& ps) {
+    const size_t k = tgt.size();
+    ps.assign(k, 0.0);
+    const bool small_rho = s->kind == QGPU_RHO && s->dims.size() <= 10;
+    std::vector<size_t> order(k);
+    for (size_t i = 0; i < k; ++i) order[i] = i;
+    if (destructive && !small_rho)
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return tgt[a] > tgt[b]; });
+    for (size_t c = 0; c < k; ++c) {
+        size_t i = order[c];
+        ps[i] = project(s, tgt[i], res[i]);
+        if (destructive && !small_rho) {
+            qgpu_state* nxt = drop(s, {tgt[i]}, {res[i]});
+            free_state(s);
+            s = nxt;
+        }
+    }
+    if (destructive && small_rho) {
+        qgpu_state* nxt = drop(s, tgt, res);
+        free_state(s);
+        s = nxt;
+    }
+}
+
+// One full-basis draw (qpp::sample, instruments.hpp:746-818): the digits of
+// the targets.
+std::vector<uint64_t> sample_once(const qgpu_state* s, const std::vector<uint64_t>& tgt,
+                                  double u) {
+    uint64_t idx =
+        prefix_search(s->ctx, s->prec, s->data, s->D, s->kind == QGPU_RHO, u, nullptr);
+    std::vector<uint64_t> dg = digits_of(idx, s->dims), res(tgt.size());
+    for (size_t i = 0; i < tgt.size(); ++i) res[i] = dg[tgt[i]];
+    return res;
+}
+
+namespace {
+
 void measure_seq(qgpu_engine* e, const std::vector<uint64_t>& rel, bool destructive,
                  std::vector<uint64_t>& res, std::vector<double>& ps) {
-    qgpu_state* s = e->st;
     const size_t k = rel.size();
     res.assign(k, 0);
-    ps.assign(k, 0.0);
     if (e->replay) {
         if (e->fo_pos + k > e->forced_outcomes.size())
             raise(QGPU_ERR_OUT_OF_RANGE, kExec, "replay list exhausted (outcomes)");
         for (size_t i = 0; i < k; ++i) res[i] = e->forced_outcomes[e->fo_pos++];
     } else {
-        double u = std::generate_canonical<double, std::numeric_limits<double>::digits>(e->gen);
-        uint64_t idx = prefix_search(s->ctx, s->prec, s->data, s->D, s->kind == QGPU_RHO, u,
-                                     nullptr);
-        uint64_t r = idx;
-        std::vector<uint64_t> dg(s->dims.size());
-        for (size_t q = s->dims.size(); q-- > 0;) {
-            dg[q] = r % s->dims[q];
-            r /= s->dims[q];
-        }
-        for (size_t i = 0; i < k; ++i) res[i] = dg[rel[i]];
+        res = sample_once(e->st, rel, canonical(e->gen));
     }
     for (uint64_t v : res) e->rec_outcomes.push_back(v);
-    bool small_rho = s->kind == QGPU_RHO && s->dims.size() <= 10;
-    std::vector<size_t> order(k);
-    for (size_t i = 0; i < k; ++i) order[i] = i;
-    if (destructive && !small_rho)
-        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return rel[a] > rel[b]; });
-    for (size_t c = 0; c < k; ++c) {
-        size_t i = order[c];
-        ps[i] = project(e->st, rel[i], res[i]);
-        if (destructive && !small_rho) {
-            qgpu_state* nxt = drop(e->st, {rel[i]}, {res[i]});
-            free_state(e->st);
-            e->st = nxt;
-        }
-    }
-    if (destructive && small_rho) {
-        qgpu_state* nxt = drop(e->st, rel, res);
-        free_state(e->st);
-        e->st = nxt;
-    }
+    collapse_seq(e->st, rel, destructive, res, ps);
 }
 
 void apply_noise(qgpu_engine* e, size_t step_idx) {
@@ -386,6 +459,147 @@ int classify(const std::vector<cd>& K, uint64_t d, std::vector<cd>& unit) {
     return idl ? 1 : 2;
 }
 
+bool is_measurement(const Step& s) { return s.kind == StepKind::Measure || s.kind == StepKind::Reset; }
+bool is_cctrl(const Step& s) { return s.kind == StepKind::CCtrl || s.kind == StepKind::CCtrlFan; }
+
+// (ctrl, target, c_reg) of a step as qpp's
+// extract_ctrl_target_ps_vals_c_reg sees them (qcircuit.hpp:7371-7440)
+void step_sets(const Step& s, std::vector<uint64_t>& ctrl, std::vector<uint64_t>& target,
+               std::vector<uint64_t>& creg) {
+    ctrl.clear();
+    creg.clear();
+    target = s.target;
+    switch (s.kind) {
+        case StepKind::Measure:
+            for (size_t i = 0; i < s.target.size(); ++i) creg.push_back(s.c_reg + i);
+            break;
+        case StepKind::CCtrl:
+        case StepKind::CCtrlFan:
+            creg = s.ctrl;
+            break;
+        case StepKind::Ctrl:
+        case StepKind::CtrlFan:
+            ctrl = s.ctrl;
+            break;
+        default:
+            break;
+    }
+}
+
+bool overlap(const std::vector<uint64_t>& a, const std::vector<uint64_t>& b) {
+    for (uint64_t x : a)
+        if (std::find(b.begin(), b.end(), x) != b.end()) return true;
+    return false;
+}
+
+// qpp::internal::can_swap (qcircuit.hpp:7465-7492): controls, targets and
+// classical dits pairwise disjoint (a control may meet a target)
+bool can_swap(const Step& a, const Step& b) {
+    std::vector<uint64_t> c1, t1, r1, c2, t2, r2;
+    step_sets(a, c1, t1, r1);
+    step_sets(b, c2, t2, r2);
+    return !overlap(c1, c2) && !overlap(t1, t2) && !overlap(r1, r2);
+}
+
+// qpp::internal::canonical_form (qcircuit.hpp:7556-7631): from the first
+// measurement on, classically controlled steps and then measurements are
+// bubbled towards the end past the steps they can swap with (stable: two
+// steps of the same class are never exchanged). Only for reps > 1.
+std::vector<size_t> canonical_order(const qgpu_circuit* c, bool canonical) {
+    const size_t ns = c->steps.size();
+    std::vector<size_t> order(ns);
+    for (size_t i = 0; i < ns; ++i) order[i] = i;
+    if (!canonical) return order;
+    size_t first = 0;
+    while (first < ns && !is_measurement(c->steps[first])) ++first;
+    auto push_back_class = [&](bool (*cls)(const Step&)) {
+        for (size_t r = ns; r-- > first;) {
+            if (!cls(c->steps[order[r]])) continue;
+            for (size_t j = r; j + 1 < ns; ++j) {
+                const Step& cur = c->steps[order[j]];
+                const Step& nxt = c->steps[order[j + 1]];
+                if (can_swap(cur, nxt) && !cls(nxt)) std::swap(order[j], order[j + 1]);
+                else break;
+            }
+        }
+    };
+    push_back_class(is_cctrl);
+    push_back_class(is_measurement);
+    return order;
+}
+
+// qengine.hpp:240-345: steps order[pos..] executed reps times, each from
+// the engine state at entry; the statistics count every repetition that
+// measured something; the engine keeps the first repetition's state.
+void repeat_steps(qgpu_engine* e, const std::vector<size_t>& order, size_t pos, uint64_t reps) {
+    Snapshot entry, first;
+    if (reps > 1) entry.copy_from(e);
+    for (uint64_t rep = 0; rep < reps; ++rep) {
+        bool measured = false;
+        for (size_t i = pos; i < order.size(); ++i) {
+            const Step& s = e->circ->steps[order[i]];
+            if (is_measurement(s)) measured = true;
+            run_step(e, s, order[i]);
+        }
+        if (measured) e->stats[e->dits] += 1;
+        if (reps == 1) break;
+        if (rep == 0) {
+            first.take(e);
+            entry.restore_copy(e);
+        } else if (rep + 1 < reps) {
+            entry.restore_copy(e);
+        }
+    }
+    if (reps > 1) first.restore_move(e);
+}
+
+// qengine.hpp:374-481 (no post-selection steps here): the steps from pos on
+// are all projective measurements, so the measurement steps run once (the
+// engine's state and dits) and every further repetition is one full-basis
+// sample of the pre-measurement state, written into the dits that the
+// measurements would fill. The RNG is consumed in qpp's order: one sample,
+// the measurement steps, then one sample per further repetition. Returns
+// false (nothing done) when two classical dits read the same qudit, where
+// qpp's fill loop reads past its sample.
+bool sample_steps(qgpu_engine* e, const std::vector<size_t>& order, size_t pos, uint64_t reps) {
+    std::map<uint64_t, uint64_t> c_q; // dit -> qudit
+    for (size_t i = pos; i < order.size(); ++i) {
+        const Step& s = e->circ->steps[order[i]];
+        for (size_t q = 0; q < s.target.size(); ++q) c_q[s.c_reg + q] = s.target[q];
+    }
+    if (c_q.empty()) return false;
+    std::set<uint64_t> from_set;
+    for (auto& kv : c_q) from_set.insert(kv.second);
+    if (from_set.size() != c_q.size()) return false;
+    std::vector<uint64_t> sample_from(from_set.begin(), from_set.end());
+    qgpu_state* pre = copy_state(e->st);
+    struct Del {
+        qgpu_state* s;
+        ~Del() { free_state(s); }
+    } del{pre};
+    (void)canonical(e->gen); // rep 0's sample (it only checks post-selection)
+    for (size_t i = pos; i < order.size(); ++i) run_step(e, e->circ->steps[order[i]], order[i]);
+    e->stats[e->dits] += 1;
+    if (reps == 1) return true;
+    std::vector<double> us(reps - 1);
+    for (auto& u : us) u = canonical(e->gen);
+    const bool rho = pre->kind == QGPU_RHO;
+    std::vector<uint64_t> idx = prefix_search_many(pre->ctx, pre->prec, pre->data, pre->D, rho, us);
+    std::vector<uint64_t> res;
+    for (uint64_t x : idx) {
+        std::vector<uint64_t> dg = digits_of(x, pre->dims);
+        res = e->dits;
+        size_t i = 0;
+        // qpp fills the dits in increasing dit order from the samples of
+        // the qudits in increasing qudit order
+        for (auto& kv : c_q)
+            if (kv.first < res.size()) res[kv.first] = dg[sample_from[i++]];
+            else ++i;
+        e->stats[res] += 1;
+    }
+    return true;
+}
+
 } // namespace
 } // namespace qgpu
 
@@ -454,14 +668,38 @@ qgpu_status qgpu_engine_set_state(qgpu_engine* e, const qgpu_state* s) {
     return guarded([&] {
         need_handle(e);
         need_handle(s);
-        qgpu::free_state(e->init);
-        e->init = nullptr;
-        e->init = qgpu::new_state(e->ctx, s->kind, e->prec, s->dims, false);
+        // QEngineT::set_state (qengine.hpp:1191-1214): the state must match
+        // the qudits not yet measured destructively
+        const char* W = "qpp::QEngineT::set_state()";
+        qgpu::ensure_state(e);
+        uint64_t n = 0, D = 1;
+        for (char m : e->measured)
+            if (!m) ++n;
+        for (uint64_t i = 0; i < n; ++i) D *= e->circ->d;
+        if (s->kind != e->kind) raise(QGPU_ERR_TYPE_MISMATCH, W, "state");
+        if (s->D != D) raise(QGPU_ERR_DIMS_NOT_EQUAL, W, "state");
+        std::vector<uint64_t> dims(n, e->circ->d);
+        if (dims.empty()) dims.push_back(1);
+        qgpu_state* c = qgpu::new_state(e->ctx, e->kind, e->prec, dims, false);
         if (s->prec == e->prec)
-            QG_CUDA(cudaMemcpyAsync(e->init->data, s->data, s->bytes(),
-                                    cudaMemcpyDeviceToDevice, e->ctx->stream));
+            QG_CUDA(cudaMemcpyAsync(c->data, s->data, s->bytes(), cudaMemcpyDeviceToDevice,
+                                    e->ctx->stream));
         else
-            qgpu::launch_convert(e->ctx, s->data, s->prec, e->init->data, e->prec, s->elems);
+            qgpu::launch_convert(e->ctx, s->data, s->prec, c->data, e->prec, s->elems);
+        qgpu::free_state(e->st);
+        e->st = c;
+    });
+}
+
+qgpu_status qgpu_engine_reset(qgpu_engine* e, int reset_stats) {
+    return guarded([&] {
+        need_handle(e);
+        // QEngineT::reset (qengine.hpp:1251-1260) / QNoisyEngineT::reset
+        qgpu::free_state(e->st);
+        e->st = nullptr;
+        qgpu::clear_registers(e);
+        e->noise_results.assign(e->circ->steps.size(), {});
+        if (reset_stats) e->stats.clear();
     });
 }
 
@@ -479,16 +717,37 @@ qgpu_status qgpu_engine_set_replay(qgpu_engine* e, const uint64_t* outcomes, uin
 qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps) {
     return guarded([&] {
         need_handle(e);
-        if (reps == 0) raise(QGPU_ERR_OUT_OF_RANGE, "qpp::QEngineT::execute()", "reps");
-        e->stats.clear();
+        if (reps == 0)
+            raise(QGPU_ERR_OUT_OF_RANGE,
+                  e->noisy ? "qpp::QNoisyEngineT::execute()" : "qpp::QEngineT::execute()", "reps");
+        qgpu::ensure_state(e);
         e->rec_outcomes.clear();
         e->rec_noise.clear();
         e->fo_pos = e->fn_pos = 0;
-        for (uint64_t rep = 0; rep < reps; ++rep) {
-            qgpu::reset_state(e);
-            for (size_t i = 0; i < e->circ->steps.size(); ++i)
-                qgpu::run_step(e, e->circ->steps[i], i);
-            e->stats[e->dits] += 1;
+        const size_t ns = e->circ->steps.size();
+        if (e->noisy) {
+            // QNoisyEngineT::execute (qnoisy_engine.hpp:129-139): every step,
+            // reps times from the current engine state
+            std::vector<size_t> order(ns);
+            for (size_t i = 0; i < ns; ++i) order[i] = i;
+            qgpu::repeat_steps(e, order, 0, reps);
+        } else {
+            // QEngineT::execute (qengine.hpp:1341-1405)
+            std::vector<uint64_t> full(e->circ->nq, e->circ->d);
+            uint64_t D = 1;
+            for (uint64_t x : full) D *= x;
+            if (e->st->D != D)
+                raise(QGPU_ERR_DIMS_NOT_EQUAL, "qpp::internal::QEngineState::reset()", "state");
+            qgpu::clear_registers(e);
+            std::vector<size_t> order = qgpu::canonical_order(e->circ, reps > 1);
+            size_t pos = 0;
+            while (pos < order.size() && !qgpu::is_measurement(e->circ->steps[order[pos]])) ++pos;
+            for (size_t i = 0; i < pos; ++i) qgpu::run_step(e, e->circ->steps[order[i]], order[i]);
+            bool can_sample = reps > 1 && !e->replay && pos < order.size();
+            for (size_t i = pos; i < order.size() && can_sample; ++i)
+                if (e->circ->steps[order[i]].kind != qgpu::StepKind::Measure) can_sample = false;
+            if (!(can_sample && qgpu::sample_steps(e, order, pos, reps)))
+                qgpu::repeat_steps(e, order, pos, reps);
         }
         QG_CUDA(cudaStreamSynchronize(e->ctx->stream));
     });
@@ -538,6 +797,88 @@ qgpu_status qgpu_engine_get_record(const qgpu_engine* e, uint64_t* n_out, uint64
         if (outcomes) std::copy(e->rec_outcomes.begin(), e->rec_outcomes.end(), outcomes);
         if (n_noise) *n_noise = e->rec_noise.size();
         if (noise) std::copy(e->rec_noise.begin(), e->rec_noise.end(), noise);
+    });
+}
+
+
+namespace {
+bool targets_ok(const std::vector<uint64_t>& t, size_t n) {
+    if (t.size() > n) return false;
+    std::vector<uint64_t> u = t;
+    std::sort(u.begin(), u.end());
+    if (std::adjacent_find(u.begin(), u.end()) != u.end()) return false;
+    for (uint64_t x : t)
+        if (x >= n) return false;
+    return true;
+}
+} // namespace
+
+// qpp::sample(num_samples, A, target, dims) (instruments.hpp:856-940):
+// num_samples full-basis draws of |A_i|^2 (ket) or Re A(i, i) (density
+// matrix), each reported as the digits of `target`.
+qgpu_status qgpu_sample(const qgpu_state* s, const uint64_t* target, uint32_t k,
+                        uint64_t num_samples, uint64_t seed, const double* u,
+                        uint64_t* results) {
+    return guarded([&] {
+        need_handle(s);
+        const char* W = "qpp::sample()";
+        std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
+        if (!targets_ok(tgt, s->dims.size())) raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
+        if (num_samples == 0) raise(QGPU_ERR_OUT_OF_RANGE, W, "num_samples");
+        if (!results && k) raise(QGPU_ERR_INVALID_ARGUMENT, W, "results");
+        std::vector<double> us(num_samples);
+        if (u) {
+            for (uint64_t i = 0; i < num_samples; ++i) {
+                if (!(u[i] >= 0.0 && u[i] < 1.0)) raise(QGPU_ERR_OUT_OF_RANGE, W, "u");
+                us[i] = u[i];
+            }
+        } else {
+            std::mt19937 gen(static_cast<std::mt19937::result_type>(seed));
+            for (auto& x : us) x = qgpu::canonical(gen);
+        }
+        std::vector<uint64_t> idx =
+            qgpu::prefix_search_many(s->ctx, s->prec, s->data, s->D, s->kind == QGPU_RHO, us);
+        for (uint64_t i = 0; i < num_samples; ++i) {
+            std::vector<uint64_t> dg = qgpu::digits_of(idx[i], s->dims);
+            for (uint32_t j = 0; j < k; ++j) results[i * k + j] = dg[tgt[j]];
+        }
+    });
+}
+
+// qpp::measure_seq(A, target, dims, destructive) (instruments.hpp:985-1111)
+// with value semantics: `s` is unchanged, the post-measurement state is a
+// new handle.
+qgpu_status qgpu_measure_seq(const qgpu_state* s, const uint64_t* target, uint32_t k,
+                             int destructive, uint64_t seed, const uint64_t* forced,
+                             uint64_t* results, double* probs, qgpu_state** out) {
+    return guarded([&] {
+        need_handle(s);
+        const char* W = "qpp::measure_seq()";
+        if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "out");
+        std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
+        if (!targets_ok(tgt, s->dims.size())) raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
+        std::vector<uint64_t> res(k);
+        if (forced) {
+            for (uint32_t i = 0; i < k; ++i) {
+                if (forced[i] >= s->dims[tgt[i]]) raise(QGPU_ERR_OUT_OF_RANGE, W, "forced");
+                res[i] = forced[i];
+            }
+        } else if (k) {
+            std::mt19937 gen(static_cast<std::mt19937::result_type>(seed));
+            res = qgpu::sample_once(s, tgt, qgpu::canonical(gen));
+        }
+        qgpu_state* c = qgpu::copy_state(s);
+        std::vector<double> ps;
+        try {
+            qgpu::collapse_seq(c, tgt, destructive != 0, res, ps);
+        } catch (...) {
+            qgpu::free_state(c);
+            throw;
+        }
+        QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        if (results) std::copy(res.begin(), res.end(), results);
+        if (probs) std::copy(ps.begin(), ps.end(), probs);
+        *out = c;
     });
 }
 

@@ -72,6 +72,12 @@ std::vector<double> reduce_marginals(qgpu_ctx* ctx, qgpu_prec prec,
 uint64_t prefix_search(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
                        uint64_t D, bool diag_of_rho, double fraction,
                        double* total_out);
+// The same search for many fractions at once: one pass over the weights
+// (sums of 4096-weight chunks, prefix on the host), then one block per draw
+// scans its chunk.
+std::vector<uint64_t> prefix_search_many(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
+                                         uint64_t D, bool diag_of_rho,
+                                         const std::vector<double>& fractions);
 // Keep the elements whose digit (index / dig_stride) % dig_dim equals
 // dig_val (for rho: in both the row and the column index), scale them by
 // `scale`, zero the rest.

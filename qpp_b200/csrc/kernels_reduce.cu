@@ -155,6 +155,55 @@ __global__ void __launch_bounds__(kRedThreads)
     if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
 }
 
+// Many draws at once: block b scans chunk [lo_b, lo_b + chunk) (clipped to D)
+// for the first index whose running inclusive sum reaches thr[b]; the last
+// index of the chunk holding weight if rounding leaves none.
+template <typename R, bool DIAG>
+__global__ void __launch_bounds__(256)
+    k_chunk_scan_many(const Cplx<R>* __restrict__ x, uint64_t D, uint64_t chunk,
+                      const uint64_t* __restrict__ lo_arr, const double* __restrict__ thr_arr,
+                      unsigned long long* __restrict__ res) {
+    __shared__ double sh[256];
+    __shared__ double run;
+    __shared__ unsigned long long found, last_pos;
+    const uint64_t lo = lo_arr[blockIdx.x], hi = min(D, lo + chunk);
+    const double thr = thr_arr[blockIdx.x];
+    if (threadIdx.x == 0) {
+        run = 0.0;
+        found = ~0ull;
+        last_pos = lo;
+    }
+    __syncthreads();
+    for (uint64_t t0 = lo; t0 < hi; t0 += blockDim.x) {
+        uint64_t i = t0 + threadIdx.x;
+        double w = 0.0;
+        if (i < hi) {
+            if (DIAG) {
+                w = double(x[i * (D + 1)].x);
+            } else {
+                Cplx<R> a = x[i];
+                w = double(a.x) * a.x + double(a.y) * a.y;
+            }
+            if (w > 0) atomicMax(&last_pos, (unsigned long long)i);
+        }
+        sh[threadIdx.x] = w;
+        __syncthreads();
+        for (int s = 1; s < int(blockDim.x); s <<= 1) {
+            double add = threadIdx.x >= unsigned(s) ? sh[threadIdx.x - s] : 0.0;
+            __syncthreads();
+            sh[threadIdx.x] += add;
+            __syncthreads();
+        }
+        double incl = run + sh[threadIdx.x];
+        if (i < hi && incl >= thr) atomicMin(&found, (unsigned long long)i);
+        __syncthreads();
+        if (found != ~0ull) break;
+        if (threadIdx.x == blockDim.x - 1) run = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) res[blockIdx.x] = found == ~0ull ? last_pos : found;
+}
+
 // One block scans [lo, hi) in tiles of blockDim.x and writes the first index
 // whose running inclusive sum reaches `thr` (hi - 1 if none).
 template <typename R, bool DIAG>
@@ -461,6 +510,97 @@ uint64_t prefix_search(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
                             cudaMemcpyDeviceToHost, ctx->stream));
     QG_CUDA(cudaStreamSynchronize(ctx->stream));
     return uint64_t(*pres);
+}
+
+std::vector<uint64_t> prefix_search_many(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
+                                         uint64_t D, bool diag,
+                                         const std::vector<double>& fractions) {
+    std::vector<uint64_t> out(fractions.size());
+    if (fractions.empty()) return out;
+    // fixed chunks of 4096 weights: one pass for the chunk sums, then each
+    // draw scans a single chunk
+    const uint64_t chunk = 4096;
+    const uint64_t nb64 = (D + chunk - 1) / chunk;
+    if (nb64 > (uint64_t(1) << 31)) raise(QGPU_ERR_OUT_OF_RANGE, "prefix_search_many()", "D");
+    const int nb = int(nb64);
+    const size_t m = fractions.size();
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t b_part = al(nb * sizeof(double)), b_lo = al(m * sizeof(uint64_t)),
+                 b_thr = al(m * sizeof(double)), b_res = al(m * sizeof(unsigned long long));
+    unsigned char* buf = nullptr;
+    QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), b_part + b_lo + b_thr + b_res,
+                            ctx->stream));
+    struct Free {
+        qgpu_ctx* c;
+        void* p;
+        ~Free() { cudaFreeAsync(p, c->stream); }
+    } fr{ctx, buf};
+    double* part = reinterpret_cast<double*>(buf);
+    uint64_t* dlo = reinterpret_cast<uint64_t*>(buf + b_part);
+    double* dthr = reinterpret_cast<double*>(buf + b_part + b_lo);
+    unsigned long long* dres =
+        reinterpret_cast<unsigned long long*>(buf + b_part + b_lo + b_thr);
+#define QG_CHUNK(R, T, DG)                                                     \
+    k_chunk_sums<R, DG><<<nb, kRedThreads, 0, ctx->stream>>>(                  \
+        static_cast<const T*>(data), D, chunk, part)
+    if (prec == QGPU_C128) {
+        if (diag) QG_CHUNK(double, double2, true);
+        else QG_CHUNK(double, double2, false);
+    } else {
+        if (diag) QG_CHUNK(float, float2, true);
+        else QG_CHUNK(float, float2, false);
+    }
+#undef QG_CHUNK
+    after_launch(ctx, "k_chunk_sums");
+    std::vector<double> ps(nb);
+    QG_CUDA(cudaMemcpyAsync(ps.data(), part, nb * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    QG_CUDA(cudaStreamSynchronize(ctx->stream));
+    // inclusive chunk prefix (FP64, in order)
+    std::vector<double> cp(nb);
+    double acc = 0;
+    int last = -1;
+    for (int b = 0; b < nb; ++b) {
+        acc += ps[b];
+        cp[b] = acc;
+        if (ps[b] > 0) last = b;
+    }
+    if (last < 0) raise(QGPU_ERR_DIVISION_BY_ZERO, "qpp::sample()", "zero weight");
+    std::vector<uint64_t> lo(m);
+    std::vector<double> thr(m);
+    for (size_t j = 0; j < m; ++j) {
+        const double t = fractions[j] * acc;
+        int b = int(std::lower_bound(cp.begin(), cp.end(), t) - cp.begin());
+        while (b < nb && ps[b] <= 0) ++b; // a chunk that holds weight
+        if (b >= nb) b = last;
+        lo[j] = uint64_t(b) * chunk;
+        thr[j] = t - (b > 0 ? cp[b - 1] : 0.0);
+    }
+    QG_CUDA(cudaMemcpyAsync(dlo, lo.data(), m * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    QG_CUDA(cudaMemcpyAsync(dthr, thr.data(), m * sizeof(double), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    for (size_t j0 = 0; j0 < m; j0 += 65535) {
+        const unsigned g = unsigned(std::min<size_t>(65535, m - j0));
+#define QG_SCAN(R, T, DG)                                                      \
+    k_chunk_scan_many<R, DG><<<g, 256, 0, ctx->stream>>>(                      \
+        static_cast<const T*>(data), D, chunk, dlo + j0, dthr + j0, dres + j0)
+        if (prec == QGPU_C128) {
+            if (diag) QG_SCAN(double, double2, true);
+            else QG_SCAN(double, double2, false);
+        } else {
+            if (diag) QG_SCAN(float, float2, true);
+            else QG_SCAN(float, float2, false);
+        }
+#undef QG_SCAN
+        after_launch(ctx, "k_chunk_scan_many");
+    }
+    std::vector<unsigned long long> r(m);
+    QG_CUDA(cudaMemcpyAsync(r.data(), dres, m * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    QG_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t j = 0; j < m; ++j) out[j] = uint64_t(r[j]);
+    return out;
 }
 
 void launch_project(qgpu_ctx* ctx, qgpu_prec prec, void* data, uint64_t n,

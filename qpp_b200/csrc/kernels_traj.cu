@@ -66,8 +66,8 @@ __global__ void __launch_bounds__(256)
     // registers of up to 2^14 amplitudes live in shared memory; larger ones
     // in this CTA's own slot of a global scratch buffer (L2 / HBM), which
     // __syncthreads makes coherent between the block's threads
-    float2* psi = gscratch ? gscratch + uint64_t(blockIdx.x) * gslot
-                           : reinterpret_cast<float2*>(sm);
+    float2* const base = gscratch ? gscratch + uint64_t(blockIdx.x) * gslot
+                                  : reinterpret_cast<float2*>(sm);
     __shared__ double red[8];
     __shared__ double part[256];
     __shared__ uint32_t xmask_sh, zmask_sh, ny_sh, nev_sh;
@@ -78,7 +78,13 @@ __global__ void __launch_bounds__(256)
         const TWork W = work[w];
         const int n = W.n;
         const uint32_t N = 1u << n;
-        if (W.init)
+        // in place: the CTA works directly on the instance's own state;
+        // an item without a buffer that can hold it is skipped (uniform
+        // across the CTA, before any barrier of this iteration)
+        if (W.inplace ? W.fin == nullptr : (!gscratch && n > kTrajMaxQubits)) continue;
+        float2* const psi = W.inplace ? W.fin : base;
+        if (W.inplace) {
+        } else if (W.init)
             for (uint32_t i = tid; i < N; i += nt) psi[i] = W.init[i];
         else
             for (uint32_t i = tid; i < N; i += nt) psi[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
@@ -187,6 +193,45 @@ __global__ void __launch_bounds__(256)
                     }
                     break;
                 }
+                case kTG4: {
+                    // 16 x 16 on bits (b0, b1, b2, b3) = (b0, b1, cmask & 255,
+                    // cmask >> 8 & 255); row index 8 b0 + 4 b1 + 2 b2 + b3
+                    const float2* m = W.mats + I.mat;
+                    const int bb[4] = {I.b0, I.b1, int(I.cmask & 255u), int((I.cmask >> 8) & 255u)};
+                    int sb[4] = {bb[0], bb[1], bb[2], bb[3]};
+#pragma unroll
+                    for (int x = 0; x < 3; ++x)
+#pragma unroll
+                        for (int y = 0; y < 3 - x; ++y)
+                            if (sb[y] > sb[y + 1]) {
+                                int tmp = sb[y];
+                                sb[y] = sb[y + 1];
+                                sb[y + 1] = tmp;
+                            }
+                    auto off = [&](int r) {
+                        return ((uint32_t(r) >> 3 & 1u) << bb[0]) | ((uint32_t(r) >> 2 & 1u) << bb[1]) |
+                               ((uint32_t(r) >> 1 & 1u) << bb[2]) | ((uint32_t(r) & 1u) << bb[3]);
+                    };
+                    // one output row per thread (16 groups per pass): read
+                    // everything, barrier, then write in place
+                    const int row = tid & 15;
+                    const uint32_t gpp = uint32_t(nt) >> 4;
+                    for (uint32_t g0 = 0; g0 < N / 16; g0 += gpp) {
+                        const uint32_t g = g0 + (uint32_t(tid) >> 4);
+                        const bool valid = g < N / 16;
+                        uint32_t i = 0;
+                        float2 acc = make_float2(0.f, 0.f);
+                        if (valid) {
+                            i = ins0(ins0(ins0(ins0(g, sb[0]), sb[1]), sb[2]), sb[3]);
+#pragma unroll 4
+                            for (int c = 0; c < 16; ++c) acc = c_fma(m[row + 16 * c], psi[i + off(c)], acc);
+                        }
+                        __syncthreads();
+                        if (valid) psi[i + off(row)] = acc;
+                        __syncthreads();
+                    }
+                    break;
+                }
                 case kTMeas: {
                     const uint32_t bit = 1u << I.b0;
                     double p1 = 0, tot = 0;
@@ -222,8 +267,13 @@ __global__ void __launch_bounds__(256)
             }
             __syncthreads();
         }
+        if (W.diag) {
+            // density matrix over n/2 qubits: its diagonal, for the shots
+            const uint32_t Dh = 1u << (n / 2);
+            for (uint32_t i = tid; i < Dh; i += nt) W.diag[i] = double(psi[i * (Dh + 1)].x);
+        }
         // final full-basis sample: FP64 prefix sums over thread chunks
-        {
+        if (!W.diag) {
             const uint32_t chunk = (N + nt - 1) / nt;
             double s = 0;
             const uint32_t lo = tid * chunk, hi = min(N, lo + chunk);
@@ -258,7 +308,7 @@ __global__ void __launch_bounds__(256)
         }
         if (dump)
             for (uint32_t i = tid; i < N; i += nt) dump[size_t(W.out) * N + i] = psi[i];
-        if (W.fin)
+        if (W.fin && !W.inplace)
             for (uint32_t i = tid; i < N; i += nt) W.fin[i] = psi[i];
         __syncthreads();
     }
@@ -280,15 +330,15 @@ int traj_global_grid(qgpu_ctx* ctx, int nwork, int n) {
 
 void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
                  int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
-                 int max_events, float2* gscratch) {
+                 int max_events, float2* gscratch, cudaStream_t stream) {
     if (nwork == 0) return;
+    cudaStream_t st = stream ? stream : ctx->stream;
     if (nmax > kTrajMaxQubits) {
-        if (!gscratch)
-            raise(QGPU_ERR_INVALID_ARGUMENT, "launch_traj()", "registers above 14 qubits need scratch");
-        int grid = traj_global_grid(ctx, nwork, nmax);
-        k_traj<<<grid, 256, 0, ctx->stream>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump,
-                                               devents, max_events, gscratch,
-                                               uint64_t(1) << nmax);
+        // no scratch: the caller promises in-place work items (own states)
+        int grid = gscratch ? traj_global_grid(ctx, nwork, nmax)
+                            : std::min(nwork, ctx->num_sms * 8);
+        k_traj<<<grid, 256, 0, st>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump, devents,
+                                     max_events, gscratch, uint64_t(1) << nmax);
         after_launch(ctx, "k_traj (global)");
         return;
     }
@@ -296,8 +346,8 @@ void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_
     traj_prepare();
     int per_sm = int(std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / (smem + 4096))));
     int grid = std::min(nwork, ctx->num_sms * per_sm);
-    k_traj<<<grid, 256, smem, ctx->stream>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump,
-                                             devents, max_events, nullptr, 0);
+    k_traj<<<grid, 256, smem, st>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump, devents,
+                                    max_events, nullptr, 0);
     after_launch(ctx, "k_traj");
 }
 

@@ -9,15 +9,18 @@
 // lanes, each with its own worker thread and CUDA stream, so small requests
 // never wait behind large ones:
 //
-//   lane 0  kets of <= 14 qubits: trajectories with the state in shared
-//           memory; every request that arrived while the lane's previous
-//           launch ran is admitted (in arrival order, by an estimate of its
-//           HBM footprint against the budget) into the next launch;
+//   lane 0  kets of <= 14 qubits and density matrices of <= 7 qubits (14
+//           virtual qubits, one exact run): trajectories with the state in
+//           shared memory; every request that arrived while the lane's
+//           previous launch ran is admitted (in arrival order, by an estimate
+//           of its HBM footprint against the budget) into the next launch;
 //   lane 1  kets of 15-20 qubits: the same kernel with each CTA on its own
-//           slot of global scratch (L2 / HBM), batched the same way;
-//   lane 2  everything the kernel cannot run (density matrices, > 20 qubits,
-//           wider gates, classical control): the resident engine, one
-//           request at a time.
+//           slot of global scratch (HBM), batched the same way;
+//   lane 2  everything else (larger density matrices, whose single run
+//           would occupy one CTA for seconds; kets above 20 qubits, whose
+//           one-at-a-time engine run keeps the state in L2 and beats an
+//           HBM-bound slot per shot; wider gates, classical control): the
+//           resident engine, one request at a time.
 //   plain mode: every request on lane 2 in complex128, one at a time (the
 //           comparison form: one kernel launch per gate).
 //
@@ -80,11 +83,14 @@ struct qgpu_server {
     uint64_t next_id = 1;
     uint64_t batches = 0, launched_traj = 0, engine_runs = 0;
     double busy_s = 0;
-    std::unordered_map<const qgpu_circuit*, std::pair<bool, qgpu::TProgram>> progs;
+    std::unordered_map<const qgpu_circuit*, std::pair<bool, qgpu::TProgram>> progs, rho_progs;
 };
 
 namespace qgpu {
 namespace {
+
+void sample_diag(const std::vector<double>& diag, uint64_t shots, uint64_t seed,
+                 uint64_t* out);
 
 // Engine path: trajectories one shot at a time on the resident engine; a
 // density matrix evolves once (its noise is in the circuit's channels) and
@@ -116,6 +122,8 @@ void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec) {
     std::vector<uint64_t> dv(nc);
     std::vector<double> pv(nc);
     for (uint64_t s = 0; s < runs; ++s) {
+        // every shot from |0...0> (an engine continues from its last state)
+        if ((st = qgpu_engine_reset(e, 1)) != QGPU_OK) raise(st, "qgpu_server", "reset");
         if ((st = qgpu_engine_execute(e, 1)) != QGPU_OK) raise(st, "qgpu_server", "execute");
         qgpu_engine_get_dits(e, dv.data(), pv.data());
         qgpu_state* fin = nullptr;
@@ -124,28 +132,58 @@ void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec) {
             qgpu_state* s;
             ~DelS() { qgpu_state_destroy(s); }
         } dels{fin};
-        std::uniform_real_distribution<double> U(0.0, 1.0);
-        const uint64_t nsamp = r->kind == QGPU_KET ? 1 : r->shots;
-        for (uint64_t k = 0; k < nsamp; ++k) {
-            uint64_t idx = prefix_search(fin->ctx, fin->prec, fin->data, fin->D,
-                                         fin->kind == QGPU_RHO, U(gen), nullptr);
-            uint64_t slot = r->kind == QGPU_KET ? s : k;
-            r->samples[slot] = idx;
-            for (uint32_t i = 0; i < nc; ++i) r->dits[slot * nc + i] = uint32_t(dv[i]);
+        if (r->kind != QGPU_KET) {
+            // the diagonal once (a strided gather), then the shots on the host
+            qgpu_state* dg = new_state(ctx, QGPU_KET, fin->prec, fin->dims, false);
+            struct DelD {
+                qgpu_state* s;
+                ~DelD() { free_state(s); }
+            } deld{dg};
+            SegPlan m{};
+            m.count = fin->D;
+            m.nseg = 1;
+            m.pow2 = 0;
+            m.size[0] = fin->D;
+            m.stride[0] = fin->D + 1;
+            launch_gather(ctx, fin->prec, fin->data, dg->data, m);
+            std::vector<double> h(2 * fin->D);
+            if (qgpu_state_download_c128(dg, h.data()) != QGPU_OK)
+                raise(QGPU_ERR_CUDA, "qgpu_server", "diagonal");
+            std::vector<double> d(fin->D);
+            for (uint64_t i = 0; i < fin->D; ++i) d[i] = h[2 * i];
+            sample_diag(d, r->shots, r->seed, r->samples.data());
+            for (uint64_t k = 0; k < r->shots; ++k)
+                for (uint32_t i = 0; i < nc; ++i) r->dits[k * nc + i] = uint32_t(dv[i]);
+            continue;
         }
+        std::uniform_real_distribution<double> U(0.0, 1.0);
+        r->samples[s] = prefix_search(fin->ctx, fin->prec, fin->data, fin->D, false, U(gen),
+                                      nullptr);
+        for (uint32_t i = 0; i < nc; ++i) r->dits[s * nc + i] = uint32_t(dv[i]);
     }
 }
 
-// caller holds S->mu
+// caller holds S->mu; kets compile as trajectories, density matrices as one
+// exact run over 2n virtual qubits (keyed separately)
 const TProgram* program_of(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind) {
-    if (kind != QGPU_KET) return nullptr;
-    auto it = S->progs.find(c);
-    if (it == S->progs.end()) {
+    auto& cache = kind == QGPU_KET ? S->progs : S->rho_progs;
+    auto it = cache.find(c);
+    if (it == cache.end()) {
         TProgram P;
-        bool ok = compile_traj(c, P);
-        it = S->progs.emplace(c, std::make_pair(ok, std::move(P))).first;
+        bool ok = kind == QGPU_KET ? compile_traj(c, P) : compile_traj_rho(c, P);
+        it = cache.emplace(c, std::make_pair(ok, std::move(P))).first;
     }
     return it->second.first ? &it->second.second : nullptr;
+}
+
+// `shots` samples of the basis distribution given by the diagonal
+void sample_diag(const std::vector<double>& diag, uint64_t shots, uint64_t seed,
+                 uint64_t* out) {
+    std::vector<double> w(diag.size());
+    for (size_t i = 0; i < diag.size(); ++i) w[i] = std::max(diag[i], 0.0);
+    std::mt19937 gen(uint32_t(seed ^ 0x5eed));
+    std::discrete_distribution<uint64_t> dd(w.begin(), w.end());
+    for (uint64_t s = 0; s < shots; ++s) out[s] = dd(gen);
 }
 
 void finish(qgpu_server* S, Request* r) {
@@ -174,13 +212,16 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         std::vector<TInstr> ins;
         std::vector<float> mats;
         std::vector<std::pair<size_t, size_t>> pofs; // (ins offset, mat offset) per request
+        uint64_t ndiag = 0;
         for (Request* r : rs) {
             const TProgram* P = r->prog;
             pofs.push_back({ins.size(), mats.size() / 2});
             ins.insert(ins.end(), P->ins.begin(), P->ins.end());
             mats.insert(mats.end(), P->mats.begin(), P->mats.end());
             maxcreg = std::max<uint32_t>(maxcreg, std::max<uint32_t>(P->ncreg, 1));
-            nwork += r->shots;
+            // a density matrix is one exact run; its shots sample the diagonal
+            nwork += r->kind == QGPU_KET ? r->shots : 1;
+            if (r->kind != QGPU_KET) ndiag += uint64_t(1) << (n / 2);
         }
         const uint64_t N = uint64_t(1) << n;
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -192,7 +233,9 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         size_t b_g = n > uint32_t(kTrajMaxQubits)
                          ? size_t(traj_global_grid(ctx, int(nwork), int(n))) * N * sizeof(float2)
                          : 0;
-        size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_dits) + al(b_samp) + al(b_g);
+        size_t b_diag = std::max<size_t>(ndiag * sizeof(double), 16);
+        size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_dits) + al(b_samp) + al(b_g) +
+                       al(b_diag);
         unsigned char* buf = nullptr;
         QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), total, ctx->stream));
         unsigned char* p = buf;
@@ -207,21 +250,31 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         auto* ddits = reinterpret_cast<uint32_t*>(take(b_dits));
         auto* dsamp = reinterpret_cast<uint64_t*>(take(b_samp));
         auto* dg = reinterpret_cast<float2*>(b_g ? take(b_g) : nullptr);
+        auto* ddiag = reinterpret_cast<double*>(take(b_diag));
         std::vector<TWork> work;
         work.reserve(nwork);
         uint32_t out = 0;
+        uint64_t doff = 0;
+        std::vector<uint64_t> diag_at(rs.size(), 0);
         for (size_t i = 0; i < rs.size(); ++i) {
             const TProgram* P = rs[i]->prog;
-            for (uint64_t s = 0; s < rs[i]->shots; ++s) {
+            const bool rho = rs[i]->kind != QGPU_KET;
+            const uint64_t nw = rho ? 1 : rs[i]->shots;
+            for (uint64_t s = 0; s < nw; ++s) {
                 TWork w{};
                 w.prog = dins + pofs[i].first;
                 w.mats = dmat + pofs[i].second;
                 w.nins = uint32_t(P->ins.size());
                 w.n = uint8_t(n);
-                w.p_noise = float(rs[i]->p);
+                w.p_noise = rho ? 0.f : float(rs[i]->p);
                 w.shot = uint32_t(s);
                 w.out = out++;
                 w.seed = rs[i]->seed;
+                if (rho) {
+                    w.diag = ddiag + doff;
+                    diag_at[i] = doff;
+                    doff += uint64_t(1) << (n / 2);
+                }
                 work.push_back(w);
             }
         }
@@ -236,18 +289,31 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
                     nullptr, 0, dg);
         std::vector<uint32_t> hd(nwork * maxcreg);
         std::vector<uint64_t> hs(nwork);
+        std::vector<double> hdiag(ndiag);
         QG_CUDA(cudaMemcpyAsync(hd.data(), ddits, b_dits, cudaMemcpyDeviceToHost, ctx->stream));
         QG_CUDA(cudaMemcpyAsync(hs.data(), dsamp, b_samp, cudaMemcpyDeviceToHost, ctx->stream));
+        if (ndiag)
+            QG_CUDA(cudaMemcpyAsync(hdiag.data(), ddiag, ndiag * sizeof(double),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
         QG_CUDA(cudaFreeAsync(buf, ctx->stream));
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
         out = 0;
-        for (Request* r : rs) {
+        for (size_t i = 0; i < rs.size(); ++i) {
+            Request* r = rs[i];
             const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
             r->dits.assign(r->shots * nc, 0);
             r->samples.assign(r->shots, 0);
-            for (uint64_t s = 0; s < r->shots; ++s, ++out) {
-                r->samples[s] = hs[out];
-                for (uint32_t i = 0; i < nc; ++i) r->dits[s * nc + i] = hd[size_t(out) * maxcreg + i];
+            if (r->kind != QGPU_KET) {
+                const uint64_t Dh = uint64_t(1) << (n / 2);
+                std::vector<double> dg(hdiag.begin() + diag_at[i], hdiag.begin() + diag_at[i] + Dh);
+                sample_diag(dg, r->shots, r->seed, r->samples.data());
+                ++out;
+            } else {
+                for (uint64_t s = 0; s < r->shots; ++s, ++out) {
+                    r->samples[s] = hs[out];
+                    for (uint32_t k = 0; k < nc; ++k)
+                        r->dits[s * nc + k] = hd[size_t(out) * maxcreg + k];
+                }
             }
             finish(S, r);
         }
@@ -361,7 +427,12 @@ qgpu_status qgpu_server_submit(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind, 
             int lane = 2;
             if (S->mode == 0) {
                 r->prog = qgpu::program_of(S, c, kind);
-                if (r->prog) lane = r->prog->n > uint32_t(qgpu::kTrajMaxQubits) ? 1 : 0;
+                if (r->prog) {
+                    const uint32_t n = r->prog->n;
+                    if (n <= uint32_t(qgpu::kTrajMaxQubits)) lane = 0;
+                    else if (kind == QGPU_KET && n <= uint32_t(qgpu::kServeMaxSlotQubits)) lane = 1;
+                    else r->prog = nullptr; // one CTA per density matrix is too slow: engine
+                }
             }
             S->lanes[lane].q.push_back(r);
         }

@@ -8,7 +8,8 @@
 
 namespace qgpu {
 
-enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4 };
+// kTG4: 16 x 16 on four bits (b0, b1, cmask & 255, cmask >> 8 & 255)
+enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4, kTG4 = 5 };
 enum : uint8_t { kTNewStep = 1, kTDestructive = 2 };
 
 // One instruction; qubits are bit positions (LSB = 0) of the full register.
@@ -27,7 +28,7 @@ struct TWork {
     const float2* mats;
     uint32_t nins;
     uint8_t n;
-    uint8_t pad0;
+    uint8_t inplace; // 1: run directly in `fin` (== init, HBM), no copies
     uint16_t pad1;
     float p_noise;  // depolarising probability per qubit per step
     uint32_t shot;  // trajectory index inside its request (Philox counter)
@@ -35,6 +36,8 @@ struct TWork {
     uint64_t seed;  // request seed (Philox key)
     const float2* init; // initial register (null: |0...0>)
     float2* fin;        // where the final register goes (null: nowhere)
+    double* diag;       // density-matrix run: Re rho(i, i) of the final state
+                        // (2^(n/2) values; no basis sample is drawn)
 };
 
 // Recorded noise event: before instruction `ins`, Pauli `pauli` (1 X, 2 Y,
@@ -50,6 +53,8 @@ struct TEvent {
 // buffer instead (traj_global_grid(ctx, nwork) slots of 2^n amplitudes).
 constexpr int kTrajMaxQubits = 14;
 constexpr int kTrajMaxGlobalQubits = 22;
+// Largest ket the serving loop sends to the global-slot lane.
+constexpr int kServeMaxSlotQubits = 20;
 // CTAs (= scratch slots) for a launch of nwork trajectories of n qubits:
 // at most 8 per SM and at most 4 GiB of slots.
 int traj_global_grid(qgpu_ctx* ctx, int nwork, int n);
@@ -63,9 +68,12 @@ struct TProgram {
     std::vector<float> mats; // interleaved complex64
 };
 
+// Registers above kTrajMaxQubits run either in a slot of `gscratch` or, when
+// every work item of the launch has `inplace` set (gscratch null), directly
+// in the item's own state. `stream` null: the context's stream.
 void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
                  int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
-                 int max_events, float2* gscratch);
+                 int max_events, float2* gscratch, cudaStream_t stream = nullptr);
 bool compile_traj(const qgpu_circuit* c, TProgram& P);
 // A density-matrix run of `c` as a ket over 2n virtual qubits [column
 // digits, row digits]: 1-qubit gates and 1-qubit channels become 4 x 4

@@ -74,6 +74,26 @@ int main() {
         caught = true;
     }
     EXPECT(caught);
+    // sampling and sequential measurement of the Bell state (|00> + |11>)/sqrt2
+    cmat bell(4, 1);
+    bell(0) = bell(3) = 1 / std::sqrt(2.0);
+    auto counts = sample(200, bell, {0, 1}, {2, 2}, 7);
+    idx total = 0;
+    for (auto& kv : counts) {
+        EXPECT(kv.first.size() == 2 && kv.first[0] == kv.first[1]);
+        total += kv.second;
+    }
+    EXPECT(total == 200 && counts.size() == 2);
+    auto [res, probs, post] = measure_seq(bell, {0}, {2, 2}, true, 3);
+    EXPECT(res.size() == 1 && std::abs(probs[0] - 0.5) < 1e-15);
+    EXPECT(post.rows() == 2 && post.cols() == 1 && std::abs(std::abs(post(res[0])) - 1) < 1e-15);
+    caught = false;
+    try {
+        sample(0, bell, {0}, {2, 2});
+    } catch (const exception::OutOfRange& e) {
+        caught = e.where() == "qpp::sample()" && e.detail() == "num_samples";
+    }
+    EXPECT(caught);
     std::printf(fails ? "shim FAILED (%d)\n" : "shim ok\n", fails);
     return fails ? 1 : 0;
 }

@@ -1,8 +1,10 @@
 """Batched uneven instances: one CUDA-graph launch versus the plain loop.
 
-Kets of 10-16 qubits and density matrices of 4-7 qubits, each with its own
+Kets of 10-16 qubits and density matrices of 4-9 qubits, each with its own
 random layered circuit (density matrices: a depolarising channel p=0.005 on
-every qubit after each layer), complex64. The graph form must agree with the
+every qubit after each layer, and every other one a 16-operator channel on a
+pair), complex64. Registers above 2^14 amplitudes (kets of 15-16 qubits,
+density matrices of 8-9 qubits) run in place in their own states. The graph form must agree with the
 plain per-instance loop on the same inputs within 2e-5 relative (max-norm),
 and a sample of instances with the complex128 oracle within 1e-4.
 """
@@ -15,7 +17,7 @@ from tests.qpp_helpers import depolarizing_kraus, gaussian_ket, haar_unitary, ra
 pytestmark = pytest.mark.gpu
 
 
-def layered(qb, rng, n, depth, rho):
+def layered(qb, rng, n, depth, rho, pair=False):
     c = qb.Circuit(n)
     steps = []
     for _ in range(depth):
@@ -34,6 +36,11 @@ def layered(qb, rng, n, depth, rho):
                 from qpp_b200.serving import c_channel
                 c_channel(c, depolarizing_kraus(0.005), [q])
                 steps.append(("k", depolarizing_kraus(0.005), [q]))
+            if pair:
+                from qpp_b200.serving import c_channel, pair_channel
+                t = [int(x) for x in rng.choice(n, 2, replace=False)]
+                c_channel(c, pair_channel(), t)
+                steps.append(("k", pair_channel(), t))
     return c, steps
 
 
@@ -43,8 +50,8 @@ def test_graph_batch_matches_plain_loop_and_oracle(ctx):
     circuits, inputs, kinds, all_steps = [], [], [], []
     for i in range(40):
         rho = i % 5 == 4
-        n = int(rng.integers(4, 8)) if rho else int(rng.integers(10, 17))
-        c, steps = layered(qb, rng, n, 3, rho)
+        n = int(rng.integers(4, 10)) if rho else int(rng.integers(10, 17))
+        c, steps = layered(qb, rng, n, 3, rho, pair=rho and i % 10 == 9)
         circuits.append(c)
         all_steps.append(steps)
         kinds.append(qb.RHO if rho else qb.KET)
@@ -57,7 +64,9 @@ def test_graph_batch_matches_plain_loop_and_oracle(ctx):
     for i in range(len(circuits)):
         ga, gb = a[i].numpy(), b[i].numpy()
         assert np.max(np.abs(ga - gb)) / np.max(np.abs(gb)) < 2e-5, i
-    for i in (0, 4, 9, 14):
+    big = [i for i in range(len(circuits)) if kinds[i] == qb.RHO and inputs[i].shape[0] >= 256]
+    assert big, "no in-place density matrix in the sample"
+    for i in sorted({0, 4, 9, 14, big[0]}):
         x = inputs[i]
         n = int(round(np.log2(x.shape[0])))
         dims = [2] * n
@@ -65,3 +74,13 @@ def test_graph_batch_matches_plain_loop_and_oracle(ctx):
             x = orc.apply(x, M, t, dims) if kind == "g" else orc.apply_kraus(x, M, t, dims)
         got = a[i].numpy()
         assert np.max(np.abs(got - x)) / np.max(np.abs(x)) < 1e-4, i
+
+
+def test_batch_rejects_a_state_given_twice(ctx):
+    import qpp_b200 as qb
+    c = qb.Circuit(3)
+    c.gate(np.eye(2), [0])
+    s = qb.State(ctx, qb.KET, [2] * 3, qb.C64)
+    with pytest.raises(qb.Duplicates):
+        qb.run_batch(ctx, [c, c], [s, s], qb.FUSED)
+    s.free()
