@@ -369,9 +369,12 @@ qgpu_status qgpu_engine_get_record(const qgpu_engine* e, uint64_t* n_out,
 
 /* ------------------------------------------------ trajectory batches
  * All `shots` stochastic trajectories of a QNoisyEngine request (qubit
- * circuit of at most 14 qubits; 1- and 2-qubit gates, fan gates, controlled
+ * circuit of at most 22 qubits; 1- and 2-qubit gates, fan gates, controlled
  * 1-qubit gates, Z measurements) in one launch, one CTA per trajectory with
- * the state in shared memory. Noise: before every step each non-measured
+ * the state in shared memory (up to 14 qubits) or in a global slot, worked
+ * through in cache-blocked tile passes of the tuned width (15-22 qubits).
+ * No reference counterpart (qpp runs one trajectory per execute). Noise:
+ * before every step each non-measured
  * qubit draws from the depolarising channel {I, X, Y, Z} with probabilities
  * {1 - p, p/3, p/3, p/3} (qnoisy_engine.hpp:105-121, noise.hpp:388-412).
  * Outputs (any may be NULL): samples[shots] = the final full-basis sample of
@@ -384,6 +387,12 @@ qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double p_depol,
                               uint64_t shots, uint64_t seed,
                               uint64_t* samples, uint32_t* dits, double* dump,
                               uint32_t* events, uint32_t max_events);
+/* Tile width of the trajectory kernel for registers of n qubits (15-22) on
+ * this context's device: set_T = -1 queries (timing the candidates {untiled,
+ * 10, 11, 12, 13} once on first use), 0 pins the untiled form, 9..14 (< n)
+ * pins that width, -2 drops the choice so it is timed again. No reference
+ * counterpart. *chosen (if not NULL) receives the width now in force. */
+qgpu_status qgpu_traj_tile_width(qgpu_ctx* ctx, uint32_t n, int set_T, int* chosen);
 
 /* ------------------------------------------------------ batched instances
  * n_inst independent instances, instance i running circuits[i] on

@@ -513,6 +513,16 @@ def apply_tc(state, U, target):
     return state
 
 
+def traj_tile_width(ctx, n, T=None):
+    """Tile width of the trajectory kernel for n-qubit registers (15-22):
+    T=None queries (tuned on first use), 0 pins the untiled form, 9..14
+    pins a width, -2 drops the choice. Returns the width in force."""
+    out = ct.c_int()
+    check(lib().qgpu_traj_tile_width(ctx.h, ct.c_uint32(n), ct.c_int(-1 if T is None else T),
+                                     ct.byref(out)))
+    return out.value
+
+
 def run_batch(ctx, circuits, states, form=FUSED):
     """Independent instances circuits[i] on states[i] (in place): FUSED runs
     every complex64 instance that compiles as one CUDA-graph launch, PLAIN

@@ -28,7 +28,8 @@ import time
 
 import numpy as np
 
-from . import C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, State, run_batch
+from . import (C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, State, run_batch,
+               traj_tile_width)
 from .workloads import haar_unitary, ket_gate_sequence
 
 
@@ -220,13 +221,20 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
 
     res = {"instances": {"kets": n_kets, "rho": n_rho, "depth": depth,
                          "ket_qubits": "10-22", "rho_qubits": "6-11"}}
+    # one instance of every (kind, size) class: the warm-up run that also
+    # lets the tile-width autotuner time each register size once
+    firsts = {}
+    for i, key in enumerate(zip(kinds, sizes)):
+        firsts.setdefault(key, i)
+    warm = sorted(firsts.values())
     for prec, name in ((C64, "c64"), (C128, "c128")):
         st = states(prec)
         ctx.synchronize()
         forms = (("graph", FUSED), ("plain_loop", PLAIN)) if prec == C64 else (("plain_loop", PLAIN),)
         for label, form in forms:
-            if label == "graph":
-                run_batch(ctx, circs[:8], st[:8], form)  # warm-up
+            t0 = time.perf_counter()
+            run_batch(ctx, [circs[i] for i in warm], [st[i] for i in warm], form)  # warm-up
+            res.setdefault("warmup_s", {})[f"{name}_{label}"] = time.perf_counter() - t0
             a, b = _events(torch, stream)
             a.record(stream)
             t0 = time.perf_counter()
@@ -240,6 +248,7 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
         for s in st:
             s.free()
     res["graph_speedup_vs_plain_c64"] = res["c64_plain_loop"]["s"] / res["c64_graph"]["s"]
+    res["tile_widths"] = {n: traj_tile_width(ctx, n) for n in range(15, 23)}
     return res
 
 

@@ -150,6 +150,16 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             else plain.push_back(i);
         }
         if (!prog.empty()) {
+            // registers above shared-memory size: cache-blocked tile passes
+            // at the tuned width of their size class (timed before capture)
+            std::map<uint32_t, int> tile_of;
+            for (auto& pr : prog) {
+                const uint32_t n = pr.second.n;
+                if (n <= uint32_t(qgpu::kTrajMaxQubits)) continue;
+                auto it = tile_of.find(n);
+                if (it == tile_of.end()) it = tile_of.emplace(n, qgpu::tile_width(ctx, int(n))).first;
+                qgpu::plan_tiles(pr.second, it->second);
+            }
             // device copies of all programs, work items grouped by size
             std::map<uint32_t, std::vector<size_t>> by_n;
             std::vector<qgpu::TInstr> ins;
@@ -235,9 +245,11 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 for (size_t g = 0; g < ranges.size(); ++g) {
                     const auto& rg = ranges[g];
                     QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
+                    auto tt = tile_of.find(rg.first);
                     qgpu::launch_traj(ctx, dwork + rg.second.first,
                                       int(rg.second.second - rg.second.first), int(rg.first), ddits, 1,
-                                      dsamp, nullptr, nullptr, 0, nullptr, side[g]);
+                                      dsamp, nullptr, nullptr, 0, nullptr, side[g],
+                                      tt == tile_of.end() ? 0 : tt->second);
                     QG_CUDA(cudaEventRecord(ev[g + 1], side[g]));
                     QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
                 }

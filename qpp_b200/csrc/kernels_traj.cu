@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "common.cuh"
@@ -57,20 +58,258 @@ __device__ double block_sum_d(double v, double* red) {
     return t;
 }
 
-__global__ void __launch_bounds__(256)
+// One gate instruction (G1, CG1, G2, G4) on a register of N amplitudes at
+// psi (shared or global memory); every thread of the CTA calls it.
+__device__ __forceinline__ void tr_gate(const TInstr& I, const float2* __restrict__ mats,
+                                        float2* psi, uint32_t N, int tid, int nt) {
+    switch (I.op) {
+        case kTG1: {
+            const float2* m = mats + I.mat; // column-major 2 x 2
+            const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
+            const uint32_t s = 1u << I.b0;
+            for (uint32_t p = tid; p < N / 2; p += nt) {
+                uint32_t i = ins0(p, I.b0);
+                float2 v0 = psi[i], v1 = psi[i + s];
+                psi[i] = c_fma(a01, v1, c_mul(a00, v0));
+                psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
+            }
+            break;
+        }
+        case kTCG1: {
+            const float2* m = mats + I.mat;
+            const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
+            const uint32_t s = 1u << I.b0;
+            for (uint32_t p = tid; p < N / 2; p += nt) {
+                uint32_t i = ins0(p, I.b0);
+                if ((i & I.cmask) != I.cval) continue;
+                float2 v0 = psi[i], v1 = psi[i + s];
+                psi[i] = c_fma(a01, v1, c_mul(a00, v0));
+                psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
+            }
+            break;
+        }
+        case kTG2: {
+            const float2* m = mats + I.mat; // column-major 4 x 4
+            const int lo = min(I.b0, I.b1), hi = max(I.b0, I.b1);
+            const uint32_t s0 = 1u << I.b0, s1 = 1u << I.b1;
+            for (uint32_t p = tid; p < N / 4; p += nt) {
+                uint32_t i = ins0(ins0(p, lo), hi);
+                float2 v[4] = {psi[i], psi[i + s1], psi[i + s0], psi[i + s0 + s1]};
+                float2 r[4];
+#pragma unroll
+                for (int row = 0; row < 4; ++row) {
+                    float2 acc = c_mul(m[row], v[0]);
+                    acc = c_fma(m[row + 4], v[1], acc);
+                    acc = c_fma(m[row + 8], v[2], acc);
+                    acc = c_fma(m[row + 12], v[3], acc);
+                    r[row] = acc;
+                }
+                psi[i] = r[0];
+                psi[i + s1] = r[1];
+                psi[i + s0] = r[2];
+                psi[i + s0 + s1] = r[3];
+            }
+            break;
+        }
+        case kTG4: {
+            // 16 x 16 on bits (b0, b1, b2, b3) = (b0, b1, cmask & 255,
+            // cmask >> 8 & 255); row index 8 b0 + 4 b1 + 2 b2 + b3
+            const float2* m = mats + I.mat;
+            const int bb[4] = {I.b0, I.b1, int(I.cmask & 255u), int((I.cmask >> 8) & 255u)};
+            int sb[4] = {bb[0], bb[1], bb[2], bb[3]};
+#pragma unroll
+            for (int x = 0; x < 3; ++x)
+#pragma unroll
+                for (int y = 0; y < 3 - x; ++y)
+                    if (sb[y] > sb[y + 1]) {
+                        int tmp = sb[y];
+                        sb[y] = sb[y + 1];
+                        sb[y + 1] = tmp;
+                    }
+            auto off = [&](int r) {
+                return ((uint32_t(r) >> 3 & 1u) << bb[0]) | ((uint32_t(r) >> 2 & 1u) << bb[1]) |
+                       ((uint32_t(r) >> 1 & 1u) << bb[2]) | ((uint32_t(r) & 1u) << bb[3]);
+            };
+            // one output row per thread (16 groups per round): read
+            // everything, barrier, then write in place
+            const int row = tid & 15;
+            const uint32_t gpp = uint32_t(nt) >> 4;
+            for (uint32_t g0 = 0; g0 < N / 16; g0 += gpp) {
+                const uint32_t g = g0 + (uint32_t(tid) >> 4);
+                const bool valid = g < N / 16;
+                uint32_t i = 0;
+                float2 acc = make_float2(0.f, 0.f);
+                if (valid) {
+                    i = ins0(ins0(ins0(ins0(g, sb[0]), sb[1]), sb[2]), sb[3]);
+#pragma unroll 4
+                    for (int c = 0; c < 16; ++c) acc = c_fma(m[row + 16 * c], psi[i + off(c)], acc);
+                }
+                __syncthreads();
+                if (valid) psi[i + off(row)] = acc;
+                __syncthreads();
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// Depolarising draws of one circuit step (counter `ins` = the instruction's
+// index in the untiled program): thread b <-> qubit b. Returns whether any
+// qubit drew a Pauli (uniform over the CTA). With `apply`, the Pauli string is
+// recorded and applied to all N amplitudes at psi.
+__device__ bool tr_noise(const TWork& W, uint32_t ins, int n, uint32_t alive, bool apply,
+                         float2* psi, uint32_t N, TEvent* events, int max_events,
+                         uint32_t* sh /* xm, zm, ny, nev */) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int pk = 0;
+    if (tid < n && ((alive >> tid) & 1u)) {
+        double u0, u1;
+        philox_uniform2(W.seed, W.shot, ins, uint32_t(tid), 0x6e6f6973u, u0, u1);
+        if (u0 < double(W.p_noise)) pk = 1 + min(int(u1 * 3.0), 2); // 1 X, 2 Y, 3 Z
+    }
+    if (!__syncthreads_or(pk != 0)) return false;
+    if (!apply) return true;
+    if (tid == 0) sh[0] = sh[1] = sh[2] = 0;
+    __syncthreads();
+    if (pk) {
+        if (pk != 3) atomicOr(&sh[0], 1u << tid);
+        if (pk != 1) atomicOr(&sh[1], 1u << tid);
+        if (pk == 2) atomicAdd(&sh[2], 1u);
+        if (events) {
+            uint32_t e = atomicAdd(&sh[3], 1u);
+            if (int(e) < max_events)
+                events[size_t(W.out) * max_events + e] = TEvent{ins, uint16_t(tid), uint16_t(pk)};
+        }
+    }
+    __syncthreads();
+    const uint32_t xm = sh[0], zm = sh[1], ny = sh[2];
+    // P|i> = i^ny (-1)^popc(i & zm) |i ^ xm>
+    const float2 gph = ny % 4 == 0 ? make_float2(1, 0)
+                     : ny % 4 == 1 ? make_float2(0, 1)
+                     : ny % 4 == 2 ? make_float2(-1, 0) : make_float2(0, -1);
+    if (xm == 0) {
+        for (uint32_t i = tid; i < N; i += nt) {
+            float2 a = c_mul(gph, psi[i]);
+            if (__popc(i & zm) & 1) a = make_float2(-a.x, -a.y);
+            psi[i] = a;
+        }
+    } else {
+        int hb = 31 - __clz(xm); // pair (i, i ^ xm) with bit hb of i clear
+        for (uint32_t p = tid; p < N / 2; p += nt) {
+            uint32_t i = ins0(p, hb), j = i ^ xm;
+            float2 a = c_mul(gph, psi[i]), b = c_mul(gph, psi[j]);
+            if (__popc(i & zm) & 1) a = make_float2(-a.x, -a.y);
+            if (__popc(j & zm) & 1) b = make_float2(-b.x, -b.y);
+            psi[j] = a;
+            psi[i] = b;
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+// A tile pass (kTTile header H at program position k): the m instructions
+// after it act on the T bits listed at mats + H.mat (bits 0..4 first); each
+// tile of 2^T amplitudes (fixed values of the other n - T bits) is gathered
+// into shared memory, the instructions run there on local bit positions,
+// and the tile is written back. Noise of a step inside the pass splits it:
+// the instructions before run tiled, the Pauli string is applied to the
+// whole register, and the pass resumes. `orig0` = untiled index of the first
+// instruction of the pass.
+__device__ void tr_tile_pass(const TWork& W, uint32_t k, uint32_t orig0, int n, uint32_t alive,
+                             float2* psi, float2* tile, uint32_t* offh, TEvent* events,
+                             int max_events, uint32_t* sh) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const TInstr H = W.prog[k];
+    const int T = H.b0;
+    const uint32_t m = H.cmask;
+    const uint32_t* tb = reinterpret_cast<const uint32_t*>(W.mats + H.mat);
+    const uint32_t NT = 1u << T, NH = NT >> 5;
+    // global offset of local index (lh << 5 | ll) = offh[lh] + ll
+    for (uint32_t lh = tid; lh < NH; lh += nt) {
+        uint32_t o = 0;
+        for (int j = 5; j < T; ++j) o |= ((lh >> (j - 5)) & 1u) << tb[j];
+        offh[lh] = o;
+    }
+    uint32_t tilebits = 0;
+    for (int j = 0; j < T; ++j) tilebits |= 1u << tb[j];
+    const uint32_t rest = (n == 32 ? 0xffffffffu : ((1u << n) - 1)) & ~tilebits;
+    const uint32_t ntiles = 1u << (n - T);
+    __syncthreads();
+    uint32_t start = k + 1;
+    const uint32_t end = k + 1 + m;
+    bool start_done = false; // noise before `start` already applied
+    while (start < end) {
+        uint32_t stop = end;
+        if (W.p_noise > 0.f)
+            for (uint32_t i = start; i < end; ++i) {
+                if (!(W.prog[i].flags & kTNewStep) || (i == start && start_done)) continue;
+                if (tr_noise(W, orig0 + (i - k - 1), n, alive, false, psi, 0, events, max_events, sh)) {
+                    stop = i;
+                    break;
+                }
+            }
+        if (stop > start) {
+            for (uint32_t t = 0; t < ntiles; ++t) {
+                // deposit t into the bits outside the tile
+                uint32_t base = 0, r = rest, tt = t;
+                while (r) {
+                    const uint32_t low = r & (0u - r);
+                    if (tt & 1u) base |= low;
+                    tt >>= 1;
+                    r ^= low;
+                }
+                for (uint32_t l0 = 0; l0 < NT; l0 += 4u * nt) {
+                    float2 v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t l = l0 + u * nt + tid;
+                        v[u] = l < NT ? psi[base + offh[l >> 5] + (l & 31u)] : make_float2(0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t l = l0 + u * nt + tid;
+                        if (l < NT) tile[l] = v[u];
+                    }
+                }
+                __syncthreads();
+                for (uint32_t i = start; i < stop; ++i) {
+                    tr_gate(W.prog[i], W.mats, tile, NT, tid, nt);
+                    __syncthreads();
+                }
+                for (uint32_t l = tid; l < NT; l += nt) psi[base + offh[l >> 5] + (l & 31u)] = tile[l];
+                __syncthreads();
+            }
+        }
+        if (stop < end) {
+            tr_noise(W, orig0 + (stop - k - 1), n, alive, true, psi, 1u << n, events, max_events, sh);
+            start = stop;
+            start_done = true;
+        } else {
+            start = end;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 4)
     k_traj(const TWork* __restrict__ work, int nwork, uint32_t* __restrict__ dits,
            int maxcreg, uint64_t* __restrict__ samples, float2* __restrict__ dump,
            TEvent* __restrict__ events, int max_events, float2* __restrict__ gscratch,
-           uint64_t gslot) {
+           uint64_t gslot, int tile_bits) {
     extern __shared__ __align__(16) unsigned char sm[];
     // registers of up to 2^14 amplitudes live in shared memory; larger ones
-    // in this CTA's own slot of a global scratch buffer (L2 / HBM), which
-    // __syncthreads makes coherent between the block's threads
+    // in this CTA's own slot of a global scratch buffer or in place in their
+    // own state (L2 / HBM), which __syncthreads makes coherent between the
+    // block's threads; their tile passes use the shared memory as the tile
     float2* const base = gscratch ? gscratch + uint64_t(blockIdx.x) * gslot
                                   : reinterpret_cast<float2*>(sm);
+    float2* const tile = reinterpret_cast<float2*>(sm);
+    uint32_t* const offh = reinterpret_cast<uint32_t*>(sm + (size_t(1) << tile_bits) * sizeof(float2));
     __shared__ double red[8];
     __shared__ double part[256];
-    __shared__ uint32_t xmask_sh, zmask_sh, ny_sh, nev_sh;
+    __shared__ uint32_t nsh[4]; // noise: xm, zm, ny, events so far
     __shared__ int outcome_sh;
     const int tid = threadIdx.x, nt = blockDim.x;
 
@@ -89,149 +328,31 @@ __global__ void __launch_bounds__(256)
         else
             for (uint32_t i = tid; i < N; i += nt) psi[i] = make_float2(i == 0 ? 1.f : 0.f, 0.f);
         uint32_t alive = (n == 32) ? 0xffffffffu : ((1u << n) - 1);
-        if (tid == 0) nev_sh = 0;
+        if (tid == 0) nsh[3] = 0;
         __syncthreads();
+        uint32_t nhdr = 0; // tile headers so far: untiled index = k - nhdr
         for (uint32_t k = 0; k < W.nins; ++k) {
             const TInstr I = W.prog[k];
-            if ((I.flags & kTNewStep) && W.p_noise > 0.f) {
-                // one Kraus pick per non-measured qubit (thread b <-> bit b)
-                if (tid == 0) {
-                    xmask_sh = 0;
-                    zmask_sh = 0;
-                    ny_sh = 0;
-                }
+            if (I.op == kTTile) {
+                // headers appear only in programs of registers above 2^14
+                // amplitudes, launched with a tile buffer of 2^tile_bits
+                if (int(I.b0) <= tile_bits && n > kTrajMaxQubits)
+                    tr_tile_pass(W, k, k - nhdr, n, alive, psi, tile, offh, events, max_events, nsh);
+                ++nhdr;
+                k += I.cmask;
                 __syncthreads();
-                if (tid < n && ((alive >> tid) & 1u)) {
-                    double u0, u1;
-                    philox_uniform2(W.seed, W.shot, k, uint32_t(tid), 0x6e6f6973u, u0, u1);
-                    if (u0 < double(W.p_noise)) {
-                        int pk = 1 + min(int(u1 * 3.0), 2); // 1 X, 2 Y, 3 Z
-                        if (pk != 3) atomicOr(&xmask_sh, 1u << tid);
-                        if (pk != 1) atomicOr(&zmask_sh, 1u << tid);
-                        if (pk == 2) atomicAdd(&ny_sh, 1u);
-                        if (events) {
-                            uint32_t e = atomicAdd(&nev_sh, 1u);
-                            if (int(e) < max_events)
-                                events[size_t(W.out) * max_events + e] =
-                                    TEvent{k, uint16_t(tid), uint16_t(pk)};
-                        }
-                    }
-                }
-                __syncthreads();
-                const uint32_t xm = xmask_sh, zm = zmask_sh, ny = ny_sh;
-                if (xm | zm) {
-                    // P|i> = i^ny (-1)^popc(i & zm) |i ^ xm>
-                    float2 gph = ny % 4 == 0 ? make_float2(1, 0)
-                               : ny % 4 == 1 ? make_float2(0, 1)
-                               : ny % 4 == 2 ? make_float2(-1, 0) : make_float2(0, -1);
-                    if (xm == 0) {
-                        for (uint32_t i = tid; i < N; i += nt) {
-                            float2 a = c_mul(gph, psi[i]);
-                            if (__popc(i & zm) & 1) a = make_float2(-a.x, -a.y);
-                            psi[i] = a;
-                        }
-                    } else {
-                        int hb = 31 - __clz(xm); // pair (i, i ^ xm) with bit hb of i clear
-                        for (uint32_t p = tid; p < N / 2; p += nt) {
-                            uint32_t i = ins0(p, hb), j = i ^ xm;
-                            float2 a = c_mul(gph, psi[i]), b = c_mul(gph, psi[j]);
-                            if (__popc(i & zm) & 1) a = make_float2(-a.x, -a.y);
-                            if (__popc(j & zm) & 1) b = make_float2(-b.x, -b.y);
-                            psi[j] = a;
-                            psi[i] = b;
-                        }
-                    }
-                    __syncthreads();
-                }
+                continue;
             }
+            const uint32_t orig = k - nhdr;
+            if ((I.flags & kTNewStep) && W.p_noise > 0.f)
+                tr_noise(W, orig, n, alive, true, psi, N, events, max_events, nsh);
             switch (I.op) {
-                case kTG1: {
-                    const float2* m = W.mats + I.mat; // column-major 2 x 2
-                    const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
-                    const uint32_t s = 1u << I.b0;
-                    for (uint32_t p = tid; p < N / 2; p += nt) {
-                        uint32_t i = ins0(p, I.b0);
-                        float2 v0 = psi[i], v1 = psi[i + s];
-                        psi[i] = c_fma(a01, v1, c_mul(a00, v0));
-                        psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
-                    }
+                case kTG1:
+                case kTCG1:
+                case kTG2:
+                case kTG4:
+                    tr_gate(I, W.mats, psi, N, tid, nt);
                     break;
-                }
-                case kTCG1: {
-                    const float2* m = W.mats + I.mat;
-                    const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
-                    const uint32_t s = 1u << I.b0;
-                    for (uint32_t p = tid; p < N / 2; p += nt) {
-                        uint32_t i = ins0(p, I.b0);
-                        if ((i & I.cmask) != I.cval) continue;
-                        float2 v0 = psi[i], v1 = psi[i + s];
-                        psi[i] = c_fma(a01, v1, c_mul(a00, v0));
-                        psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
-                    }
-                    break;
-                }
-                case kTG2: {
-                    const float2* m = W.mats + I.mat; // column-major 4 x 4
-                    const int lo = min(I.b0, I.b1), hi = max(I.b0, I.b1);
-                    const uint32_t s0 = 1u << I.b0, s1 = 1u << I.b1;
-                    for (uint32_t p = tid; p < N / 4; p += nt) {
-                        uint32_t i = ins0(ins0(p, lo), hi);
-                        float2 v[4] = {psi[i], psi[i + s1], psi[i + s0], psi[i + s0 + s1]};
-                        float2 r[4];
-#pragma unroll
-                        for (int row = 0; row < 4; ++row) {
-                            float2 acc = c_mul(m[row], v[0]);
-                            acc = c_fma(m[row + 4], v[1], acc);
-                            acc = c_fma(m[row + 8], v[2], acc);
-                            acc = c_fma(m[row + 12], v[3], acc);
-                            r[row] = acc;
-                        }
-                        psi[i] = r[0];
-                        psi[i + s1] = r[1];
-                        psi[i + s0] = r[2];
-                        psi[i + s0 + s1] = r[3];
-                    }
-                    break;
-                }
-                case kTG4: {
-                    // 16 x 16 on bits (b0, b1, b2, b3) = (b0, b1, cmask & 255,
-                    // cmask >> 8 & 255); row index 8 b0 + 4 b1 + 2 b2 + b3
-                    const float2* m = W.mats + I.mat;
-                    const int bb[4] = {I.b0, I.b1, int(I.cmask & 255u), int((I.cmask >> 8) & 255u)};
-                    int sb[4] = {bb[0], bb[1], bb[2], bb[3]};
-#pragma unroll
-                    for (int x = 0; x < 3; ++x)
-#pragma unroll
-                        for (int y = 0; y < 3 - x; ++y)
-                            if (sb[y] > sb[y + 1]) {
-                                int tmp = sb[y];
-                                sb[y] = sb[y + 1];
-                                sb[y + 1] = tmp;
-                            }
-                    auto off = [&](int r) {
-                        return ((uint32_t(r) >> 3 & 1u) << bb[0]) | ((uint32_t(r) >> 2 & 1u) << bb[1]) |
-                               ((uint32_t(r) >> 1 & 1u) << bb[2]) | ((uint32_t(r) & 1u) << bb[3]);
-                    };
-                    // one output row per thread (16 groups per pass): read
-                    // everything, barrier, then write in place
-                    const int row = tid & 15;
-                    const uint32_t gpp = uint32_t(nt) >> 4;
-                    for (uint32_t g0 = 0; g0 < N / 16; g0 += gpp) {
-                        const uint32_t g = g0 + (uint32_t(tid) >> 4);
-                        const bool valid = g < N / 16;
-                        uint32_t i = 0;
-                        float2 acc = make_float2(0.f, 0.f);
-                        if (valid) {
-                            i = ins0(ins0(ins0(ins0(g, sb[0]), sb[1]), sb[2]), sb[3]);
-#pragma unroll 4
-                            for (int c = 0; c < 16; ++c) acc = c_fma(m[row + 16 * c], psi[i + off(c)], acc);
-                        }
-                        __syncthreads();
-                        if (valid) psi[i + off(row)] = acc;
-                        __syncthreads();
-                    }
-                    break;
-                }
                 case kTMeas: {
                     const uint32_t bit = 1u << I.b0;
                     double p1 = 0, tot = 0;
@@ -244,7 +365,7 @@ __global__ void __launch_bounds__(256)
                     p1 = block_sum_d(p1, red);
                     if (tid == 0) {
                         double u0, u1;
-                        philox_uniform2(W.seed, W.shot, k, 0xffffu, 0x6d656173u, u0, u1);
+                        philox_uniform2(W.seed, W.shot, orig, 0xffffu, 0x6d656173u, u0, u1);
                         // first outcome whose cumulative probability reaches u
                         outcome_sh = (u0 * tot <= tot - p1 && tot - p1 > 0) ? 0 : 1;
                         if (I.mat < uint32_t(maxcreg))
@@ -317,8 +438,10 @@ __global__ void __launch_bounds__(256)
 void traj_prepare() {
     static std::once_flag once;
     std::call_once(once, [] {
+        // a 2^14-amplitude register, or a tile of up to 2^14 amplitudes with
+        // its offset table
         QG_CUDA(cudaFuncSetAttribute(k_traj, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int((size_t(1) << kTrajMaxQubits) * sizeof(float2))));
+                                     int((size_t(1) << kTrajMaxQubits) * sizeof(float2) + 4096)));
     });
 }
 
@@ -328,26 +451,45 @@ int traj_global_grid(qgpu_ctx* ctx, int nwork, int n) {
     return int(std::min<uint64_t>(std::min<uint64_t>(nwork, uint64_t(ctx->num_sms) * 8), by_mem));
 }
 
+// resident CTAs per SM for a dynamic shared-memory size (cached)
+static int traj_per_sm(size_t smem) {
+    static std::mutex mu;
+    static std::map<size_t, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(smem);
+    if (it != cache.end()) return it->second;
+    int b = 0;
+    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traj, 256, smem));
+    b = std::max(1, std::min(b, 8));
+    cache[smem] = b;
+    return b;
+}
+
 void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
                  int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
-                 int max_events, float2* gscratch, cudaStream_t stream) {
+                 int max_events, float2* gscratch, cudaStream_t stream, int tile_bits) {
     if (nwork == 0) return;
     cudaStream_t st = stream ? stream : ctx->stream;
+    traj_prepare();
     if (nmax > kTrajMaxQubits) {
+        if (tile_bits && (tile_bits < 9 || tile_bits > kTrajMaxQubits))
+            raise(QGPU_ERR_INVALID_ARGUMENT, "launch_traj()", "tile_bits");
+        const size_t smem = tile_bits ? (size_t(1) << tile_bits) * sizeof(float2) +
+                                            (size_t(1) << (tile_bits - 5)) * sizeof(uint32_t)
+                                      : 0;
+        const int cap = ctx->num_sms * traj_per_sm(smem);
         // no scratch: the caller promises in-place work items (own states)
-        int grid = gscratch ? traj_global_grid(ctx, nwork, nmax)
-                            : std::min(nwork, ctx->num_sms * 8);
-        k_traj<<<grid, 256, 0, st>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump, devents,
-                                     max_events, gscratch, uint64_t(1) << nmax);
+        int grid = gscratch ? std::min(traj_global_grid(ctx, nwork, nmax), cap)
+                            : std::min(nwork, cap);
+        k_traj<<<grid, 256, smem, st>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump, devents,
+                                        max_events, gscratch, uint64_t(1) << nmax, tile_bits);
         after_launch(ctx, "k_traj (global)");
         return;
     }
     size_t smem = (size_t(1) << nmax) * sizeof(float2);
-    traj_prepare();
-    int per_sm = int(std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / (smem + 4096))));
-    int grid = std::min(nwork, ctx->num_sms * per_sm);
+    int grid = std::min(nwork, ctx->num_sms * traj_per_sm(smem));
     k_traj<<<grid, 256, smem, st>>>(dwork, nwork, ddits, maxcreg, dsamples, ddump, devents,
-                                    max_events, nullptr, 0);
+                                    max_events, nullptr, 0, 0);
     after_launch(ctx, "k_traj");
 }
 

@@ -213,8 +213,19 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         std::vector<float> mats;
         std::vector<std::pair<size_t, size_t>> pofs; // (ins offset, mat offset) per request
         uint64_t ndiag = 0;
-        for (Request* r : rs) {
-            const TProgram* P = r->prog;
+        // registers above shared-memory size run cache-blocked tile passes
+        const int T = tile_width(ctx, int(n));
+        std::vector<TProgram> tiled;
+        if (T) {
+            tiled.reserve(rs.size());
+            for (Request* r : rs) {
+                tiled.push_back(*r->prog);
+                plan_tiles(tiled.back(), T);
+            }
+        }
+        for (size_t ri = 0; ri < rs.size(); ++ri) {
+            Request* r = rs[ri];
+            const TProgram* P = T ? &tiled[ri] : r->prog;
             pofs.push_back({ins.size(), mats.size() / 2});
             ins.insert(ins.end(), P->ins.begin(), P->ins.end());
             mats.insert(mats.end(), P->mats.begin(), P->mats.end());
@@ -257,7 +268,7 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         uint64_t doff = 0;
         std::vector<uint64_t> diag_at(rs.size(), 0);
         for (size_t i = 0; i < rs.size(); ++i) {
-            const TProgram* P = rs[i]->prog;
+            const TProgram* P = T ? &tiled[i] : rs[i]->prog;
             const bool rho = rs[i]->kind != QGPU_KET;
             const uint64_t nw = rho ? 1 : rs[i]->shots;
             for (uint64_t s = 0; s < nw; ++s) {
@@ -286,7 +297,7 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         QG_CUDA(cudaMemcpyAsync(dwork, work.data(), b_work, cudaMemcpyHostToDevice, ctx->stream));
         QG_CUDA(cudaMemsetAsync(ddits, 0, b_dits, ctx->stream));
         launch_traj(ctx, dwork, int(nwork), int(n), ddits, int(maxcreg), dsamp, nullptr,
-                    nullptr, 0, dg);
+                    nullptr, 0, dg, nullptr, T);
         std::vector<uint32_t> hd(nwork * maxcreg);
         std::vector<uint64_t> hs(nwork);
         std::vector<double> hdiag(ndiag);

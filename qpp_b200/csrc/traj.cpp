@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "capi_common.hpp"
 #include "circuit.hpp"
@@ -100,6 +102,219 @@ bool compile_traj(const qgpu_circuit* c, TProgram& P) {
     return true;
 }
 
+namespace {
+
+bool tileable(const TInstr& I) {
+    return I.op == kTG1 || I.op == kTCG1 || I.op == kTG2 || I.op == kTG4;
+}
+
+// bits an instruction reads or writes (controls included)
+uint32_t ins_bits(const TInstr& I) {
+    switch (I.op) {
+        case kTG1: return 1u << I.b0;
+        case kTCG1: return (1u << I.b0) | I.cmask;
+        case kTG2: return (1u << I.b0) | (1u << I.b1);
+        case kTG4:
+            return (1u << I.b0) | (1u << I.b1) | (1u << (I.cmask & 255u)) |
+                   (1u << ((I.cmask >> 8) & 255u));
+        default: return 0;
+    }
+}
+
+} // namespace
+
+void plan_tiles(TProgram& P, int T) {
+    const int n = int(P.n);
+    if (T < 9 || n <= kTrajMaxQubits || T >= n) return;
+    const uint32_t low = 31u; // bits 0..4: 32 consecutive amplitudes per tile row
+    std::vector<TInstr> out;
+    out.reserve(P.ins.size() + P.ins.size() / 4 + 1);
+    size_t i = 0;
+    while (i < P.ins.size()) {
+        if (!tileable(P.ins[i])) {
+            out.push_back(P.ins[i++]);
+            continue;
+        }
+        // the longest run of gates whose bits outside 0..4 number <= T - 5
+        uint32_t S = 0;
+        size_t j = i;
+        while (j < P.ins.size() && tileable(P.ins[j])) {
+            const uint32_t S2 = S | ins_bits(P.ins[j]);
+            if (__builtin_popcount(S2 & ~low) > T - 5) break;
+            S = S2;
+            ++j;
+        }
+        if (j - i < 2) {
+            out.push_back(P.ins[i++]);
+            continue;
+        }
+        uint32_t tb = S | low;
+        for (int b = 5; b < n && __builtin_popcount(tb) < T; ++b) tb |= 1u << b;
+        int loc[32];
+        std::fill(loc, loc + 32, 0);
+        uint32_t cnt = 0;
+        const uint32_t off = uint32_t(P.mats.size() / 2);
+        for (int b = 0; b < n; ++b)
+            if (tb >> b & 1u) {
+                loc[b] = int(cnt++);
+                const uint32_t w = uint32_t(b);
+                float f;
+                std::memcpy(&f, &w, sizeof f);
+                P.mats.push_back(f);
+            }
+        if (cnt % 2) P.mats.push_back(0.f); // keep whole complex entries
+        TInstr H{};
+        H.op = kTTile;
+        H.b0 = uint8_t(T);
+        H.mat = off;
+        H.cmask = uint32_t(j - i);
+        out.push_back(H);
+        auto remap = [&](uint32_t mask) {
+            uint32_t r = 0;
+            for (int b = 0; b < 32; ++b)
+                if (mask >> b & 1u) r |= 1u << loc[b];
+            return r;
+        };
+        for (size_t k = i; k < j; ++k) {
+            TInstr I = P.ins[k];
+            I.b0 = uint8_t(loc[I.b0]);
+            if (I.op == kTG2 || I.op == kTG4) I.b1 = uint8_t(loc[I.b1]);
+            if (I.op == kTCG1) {
+                I.cmask = remap(I.cmask);
+                I.cval = remap(I.cval);
+            }
+            if (I.op == kTG4)
+                I.cmask = uint32_t(loc[I.cmask & 255u]) | (uint32_t(loc[(I.cmask >> 8) & 255u]) << 8);
+            out.push_back(I);
+        }
+        i = j;
+    }
+    P.ins.swap(out);
+}
+
+namespace {
+std::mutex g_tile_mu;
+std::map<std::pair<int, int>, int> g_tile_chosen; // (device, n) -> T
+} // namespace
+
+void set_tile_width(qgpu_ctx* ctx, int n, int T) {
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    if (T < 0) g_tile_chosen.erase({ctx->device, n});
+    else g_tile_chosen[{ctx->device, n}] = T;
+}
+
+int tile_width(qgpu_ctx* ctx, int n) {
+    if (n <= kTrajMaxQubits) return 0;
+    std::mutex& mu = g_tile_mu;
+    std::map<std::pair<int, int>, int>& chosen = g_tile_chosen;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = chosen.find({ctx->device, n});
+        if (it != chosen.end()) return it->second;
+    }
+    // calibration program: two layers of 1-qubit gates on every qubit and
+    // 2-qubit gates on (0,1), (2,3), ... (matrix values do not change the
+    // time)
+    TProgram P;
+    P.n = uint32_t(n);
+    const float h = 0.70710678f;
+    const float g1[8] = {h, 0, h, 0, h, 0, -h, 0};
+    for (float v : g1) P.mats.push_back(v);
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            P.mats.push_back(r == c ? 1.f : 0.f);
+            P.mats.push_back(0.f);
+        }
+    for (int layer = 0; layer < 2; ++layer) {
+        for (int q = 0; q < n; ++q) {
+            TInstr I{};
+            I.op = kTG1;
+            I.b0 = uint8_t(q);
+            I.flags = q == 0 ? kTNewStep : 0;
+            P.ins.push_back(I);
+        }
+        for (int q = 0; q + 1 < n; q += 2) {
+            TInstr I{};
+            I.op = kTG2;
+            I.b0 = uint8_t(q);
+            I.b1 = uint8_t(q + 1);
+            I.mat = 4;
+            P.ins.push_back(I);
+        }
+    }
+    const uint64_t N = uint64_t(1) << n;
+    const int K = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->num_sms) * 4,
+                                                               (uint64_t(1) << 30) / (N * 8))));
+    const size_t b_state = size_t(K) * N * sizeof(float2);
+    const size_t b_prog = 4096 * sizeof(TInstr), b_mat = 65536, b_work = K * sizeof(TWork);
+    unsigned char* buf = nullptr;
+    QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), b_state + b_prog + b_mat + b_work + 64 * K,
+                            ctx->stream));
+    struct Free {
+        qgpu_ctx* c;
+        void* p;
+        ~Free() { cudaFreeAsync(p, c->stream); }
+    } fr{ctx, buf};
+    auto* dstate = reinterpret_cast<float2*>(buf);
+    auto* dins = reinterpret_cast<TInstr*>(buf + b_state);
+    auto* dmat = reinterpret_cast<float2*>(buf + b_state + b_prog);
+    auto* dwork = reinterpret_cast<TWork*>(buf + b_state + b_prog + b_mat);
+    auto* dsamp = reinterpret_cast<uint64_t*>(buf + b_state + b_prog + b_mat + b_work);
+    QG_CUDA(cudaMemsetAsync(dstate, 0, b_state, ctx->stream));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    QG_CUDA(cudaEventCreate(&e0));
+    QG_CUDA(cudaEventCreate(&e1));
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev{e0, e1};
+    int best = 0;
+    float best_ms = 0;
+    for (int T : {0, 10, 11, 12, 13}) {
+        if (T >= n) continue;
+        TProgram Q = P;
+        plan_tiles(Q, T);
+        if (Q.ins.size() > 4096 || Q.mats.size() * sizeof(float) > b_mat) continue;
+        QG_CUDA(cudaMemcpyAsync(dins, Q.ins.data(), Q.ins.size() * sizeof(TInstr),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        QG_CUDA(cudaMemcpyAsync(dmat, Q.mats.data(), Q.mats.size() * sizeof(float),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<TWork> work(K);
+        for (int k = 0; k < K; ++k) {
+            TWork w{};
+            w.prog = dins;
+            w.mats = dmat;
+            w.nins = uint32_t(Q.ins.size());
+            w.n = uint8_t(n);
+            w.out = uint32_t(k);
+            w.init = dstate + size_t(k) * N;
+            w.fin = dstate + size_t(k) * N;
+            w.inplace = 1;
+            w.diag = nullptr;
+            work[k] = w;
+        }
+        QG_CUDA(cudaMemcpyAsync(dwork, work.data(), K * sizeof(TWork), cudaMemcpyHostToDevice,
+                                ctx->stream));
+        launch_traj(ctx, dwork, K, n, nullptr, 0, dsamp, nullptr, nullptr, 0, nullptr, nullptr, T);
+        QG_CUDA(cudaEventRecord(e0, ctx->stream));
+        launch_traj(ctx, dwork, K, n, nullptr, 0, dsamp, nullptr, nullptr, 0, nullptr, nullptr, T);
+        QG_CUDA(cudaEventRecord(e1, ctx->stream));
+        QG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (T == 0 || ms < best_ms) {
+            best = T;
+            best_ms = ms;
+        }
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    chosen[{ctx->device, n}] = best;
+    return best;
+}
+
 } // namespace qgpu
 
 using qgpu::guarded;
@@ -119,6 +334,8 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
             raise(QGPU_ERR_NOT_SUPPORTED, W,
                   "circuit needs the engine (> 20 qubits, > 2-qubit or classically controlled gates)");
         if (shots == 0) raise(QGPU_ERR_OUT_OF_RANGE, W, "shots");
+        const int T = qgpu::tile_width(ctx, int(P.n));
+        qgpu::plan_tiles(P, T);
         const uint32_t maxcreg = std::max<uint32_t>(P.ncreg, 1);
         const uint64_t N = uint64_t(1) << P.n;
         // device buffers: program, matrices, work, outputs
@@ -173,7 +390,7 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
         QG_CUDA(cudaMemsetAsync(ddits, 0, b_dits, ctx->stream));
         if (dev) QG_CUDA(cudaMemsetAsync(dev, 0xff, b_ev, ctx->stream));
         qgpu::launch_traj(ctx, dwork, int(shots), int(P.n), ddits, int(maxcreg), dsamp, ddump,
-                          dev, int(max_events), dg);
+                          dev, int(max_events), dg, nullptr, T);
         if (samples)
             QG_CUDA(cudaMemcpyAsync(samples, dsamp, b_samp, cudaMemcpyDeviceToHost, ctx->stream));
         if (dits)
@@ -190,5 +407,19 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
         if (dump)
             for (size_t i = 0; i < dumpf.size(); ++i) dump[i] = double(dumpf[i]);
+    });
+}
+
+extern "C" qgpu_status qgpu_traj_tile_width(qgpu_ctx* ctx, uint32_t n, int set_T, int* chosen) {
+    return guarded([&] {
+        need_handle(ctx);
+        const char* W = "qgpu_traj_tile_width()";
+        if (n == 0 || n > uint32_t(qgpu::kTrajMaxGlobalQubits)) raise(QGPU_ERR_OUT_OF_RANGE, W, "n");
+        if (set_T != -1 && set_T != -2 && set_T != 0 && (set_T < 9 || set_T > qgpu::kTrajMaxQubits ||
+                                                         set_T >= int(n)))
+            raise(QGPU_ERR_OUT_OF_RANGE, W, "T");
+        if (set_T >= 0) qgpu::set_tile_width(ctx, int(n), set_T);
+        if (set_T == -2) qgpu::set_tile_width(ctx, int(n), -1);
+        if (chosen) *chosen = qgpu::tile_width(ctx, int(n));
     });
 }

@@ -9,7 +9,11 @@
 namespace qgpu {
 
 // kTG4: 16 x 16 on four bits (b0, b1, cmask & 255, cmask >> 8 & 255)
-enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4, kTG4 = 5 };
+// kTTile: tile-pass header: the next `cmask` instructions act on the b0 = T
+// bits listed (one 32-bit word each, ascending, bits 0..4 first) at float2
+// offset `mat` of the matrix pool, with their bit positions renumbered
+// within that list
+enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4, kTG4 = 5, kTTile = 6 };
 enum : uint8_t { kTNewStep = 1, kTDestructive = 2 };
 
 // One instruction; qubits are bit positions (LSB = 0) of the full register.
@@ -71,9 +75,26 @@ struct TProgram {
 // Registers above kTrajMaxQubits run either in a slot of `gscratch` or, when
 // every work item of the launch has `inplace` set (gscratch null), directly
 // in the item's own state. `stream` null: the context's stream.
+// `tile_bits`: the largest T of the tile passes in the launch's programs
+// (0: none); such a launch reserves a 2^T-amplitude shared-memory tile.
 void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
                  int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
-                 int max_events, float2* gscratch, cudaStream_t stream = nullptr);
+                 int max_events, float2* gscratch, cudaStream_t stream = nullptr,
+                 int tile_bits = 0);
+// Cache blocking for registers above 2^14 amplitudes (no reference
+// counterpart): runs of consecutive gate instructions whose bits outside
+// 0..4 number at most T - 5 become one tile pass (kTTile) of 2^T-amplitude
+// tiles, so the register is read and written once per run instead of once
+// per gate. Noise and measurement draws keep their untiled instruction
+// counters, so a tiled program gives bit-identical results.
+void plan_tiles(TProgram& P, int T);
+// The tile width T (0: untiled) for registers of n qubits on this device,
+// chosen once per (device, n) by timing calibration programs for T in
+// {untiled, 10, 11, 12, 13}; call outside stream capture.
+int tile_width(qgpu_ctx* ctx, int n);
+// Pin the width for (device, n) (T >= 0), or drop the choice (T < 0) so the
+// next tile_width() times it again.
+void set_tile_width(qgpu_ctx* ctx, int n, int T);
 bool compile_traj(const qgpu_circuit* c, TProgram& P);
 // A density-matrix run of `c` as a ket over 2n virtual qubits [column
 // digits, row digits]: 1-qubit gates and 1-qubit channels become 4 x 4

@@ -149,3 +149,31 @@ def test_final_samples_follow_born_rule(ctx):
     counts = np.bincount(samples.astype(np.int64), minlength=8)
     chi2 = float(np.sum((counts - shots * probs) ** 2 / np.maximum(shots * probs, 1e-12)))
     assert chi2 < 24.3  # 7 dof, p = 0.001
+
+
+def test_tiled_registers_match_untiled_and_oracle(ctx):
+    """16-qubit registers run in a global slot; the tile passes (widths 9 and
+    12) must give bit-identical shots, samples, outcomes and noise events to
+    the untiled form, including passes split by noise, and agree with the
+    oracle replay."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(16)
+    nq = 16
+    steps, nc = random_program(rng, nq, 36, destructive=False)
+    c = build(qb, steps, nq, nc)
+    shots, p = 4, 0.02
+    runs = {}
+    try:
+        for T in (0, 9, 12):
+            assert qb.traj_tile_width(ctx, nq, T) == T
+            runs[T] = run_traj(qb, ctx, c, nq, p, shots, seed=7)
+    finally:
+        qb.traj_tile_width(ctx, nq, -2)
+    for T in (9, 12):
+        for a, b in zip(runs[0], runs[T]):
+            assert np.array_equal(a, b), T
+    samples, dits, states, events = runs[0]
+    assert int(np.sum(events[:, :, 0] != 0xffffffff)) > 0
+    for s in range(2):
+        ref, _ = replay(steps, nq, dits[s], events[s])
+        assert np.max(np.abs(states[s] - ref)) / np.max(np.abs(ref)) < 2e-5
