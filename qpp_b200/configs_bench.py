@@ -54,8 +54,21 @@ def config1(ctx, torch, stream, cpu=True):
     D = 2 ** n
     byts = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq)
     out = {"gates": len(seq), "ms": ms, "gates_per_s": len(seq) / (ms / 1e3),
-           "GBps": byts / (ms / 1e3) / 1e9,
+           "GBps": byts / (ms / 1e3) / 1e9, "form": "one Python call per gate",
            "note": "16 MiB state stays in the 126 MB L2: bandwidth is L2, not HBM"}
+    # the same gates as one circuit: one C call, the host loop in C++
+    c = Circuit(n)
+    for U, cs, t in seq:
+        c.CTRL(U, cs, t) if cs else c.gate(U, t)
+    c.run(s, PLAIN)  # warm-up
+    a, b = _events(torch, stream)
+    a.record(stream)
+    c.run(s, PLAIN)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms2 = a.elapsed_time(b)
+    out["circuit"] = {"ms": ms2, "gates_per_s": len(seq) / (ms2 / 1e3),
+                      "GBps": byts / (ms2 / 1e3) / 1e9, "form": "qgpu_run_gates, plain"}
     if cpu:
         from oracle import oracle as orc  # CPU baseline sample only
         psi = s.numpy()

@@ -35,6 +35,28 @@ void launch_apply_generic(qgpu_ctx* ctx, qgpu_prec prec, void* data,
 
 // --- subsystem kernels (kernels_subsys.cu) --------------------------------
 // out[o] = in[map(o)], o over map.count.
+// Tiled bit permutation (see kernels_subsys.cu): when every output digit's
+// dimension is a power of two, out[o] = in[foff + sum_j bit_j(o) *
+// in_stride[j]]; tiles of 2^tb elements are staged in shared memory so that
+// both the reads and the writes are coalesced.
+struct PermPlan {
+    uint64_t in_stride[64];  // input offset of output bit j
+    uint64_t foff;
+    int nb, tb, nrest;
+    uint8_t tbits[12];   // tile bits, ascending (write order)
+    uint8_t tin[12];     // the same bits by ascending input stride (read order)
+    uint8_t tin_pos[12]; // position of tin[j] within tbits
+    uint8_t rest[64];    // output bits outside the tile, ascending
+};
+constexpr int kPermTileBits = 10;
+// false when a dimension is not a power of two or there are <= 10 bits
+bool plan_permute(const std::vector<uint64_t>& out_dims, const std::vector<uint64_t>& src,
+                  uint64_t fixed_off, PermPlan& P);
+// the tiled form of launch_gather(plan_gather(out_dims, src, fixed_off));
+// false (nothing launched) when plan_permute does not apply
+bool launch_permute_tiled(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
+                          const std::vector<uint64_t>& out_dims,
+                          const std::vector<uint64_t>& src, uint64_t fixed_off);
 void launch_gather(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
                    const SegPlan& map);
 // out[o] = in[mapA(o)] * conj(in[mapB(o)]) (ket -> density-matrix forms).

@@ -3,10 +3,12 @@
 //
 // Replaces include/qpp/internal/kernels/qubit/{ptrace,ptranspose,syspermute}.hpp
 // and the generic paths of operations.hpp:1908-2514. ptranspose and
-// syspermute are pure digit permutations of the (virtual) index: the output
-// is written densely and each element gathers its source through a merged
-// segment plan, so the result is bit-exact. ptrace sums diagonal blocks in
-// FP64 whatever the state precision.
+// syspermute are pure digit permutations of the (virtual) index, so the
+// result is bit-exact: on qubit (power-of-two) digits a tiled bit
+// permutation stages 2^10-element tiles in shared memory so reads and writes
+// are both coalesced; otherwise the output is written densely and each
+// element gathers its source through a merged segment plan. ptrace sums
+// diagonal blocks in FP64 whatever the state precision.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -128,6 +130,123 @@ void launch_gather(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
         k_gather<float><<<b, 256, 0, ctx->stream>>>(
             static_cast<const float2*>(in), static_cast<float2*>(out), map);
     after_launch(ctx, "k_gather");
+}
+
+// ------------------------------------------- tiled bit permutation
+// When every digit's dimension is a power of two, a gather is a permutation
+// of index bits: out[o] = in[foff + sum_j bit_j(o) * in_stride[j]]. A plain
+// gather writes densely but reads with the stride of whatever input digit
+// lands on the output's lowest bits. The tiled form moves 2^tb elements per
+// tile through shared memory: the tile's bits are the output's five lowest
+// bits and the five bits with the smallest input strides (then more low
+// output bits), so 32 consecutive elements are read and 32 consecutive
+// elements are written per warp access.
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+    k_permute_tiled(const Cplx<R>* __restrict__ in, Cplx<R>* __restrict__ out,
+                    const __grid_constant__ PermPlan P) {
+    __shared__ Cplx<R> tile[1 << kPermTileBits];
+    __shared__ uint64_t in_off[1 << kPermTileBits];  // by read-order index
+    __shared__ uint64_t out_off[1 << kPermTileBits]; // by write-order index
+    __shared__ uint16_t pos_of[1 << kPermTileBits];  // read-order -> write-order
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t NT = 1u << P.tb;
+    for (uint32_t l = tid; l < NT; l += nt) {
+        uint64_t io = 0, oo = 0;
+        uint32_t lo = 0;
+        for (int j = 0; j < P.tb; ++j)
+            if ((l >> j) & 1u) {
+                io += P.in_stride[P.tin[j]];
+                lo |= 1u << P.tin_pos[j];
+                oo |= uint64_t(1) << P.tbits[j];
+            }
+        in_off[l] = io;
+        out_off[l] = oo;
+        pos_of[l] = uint16_t(lo);
+    }
+    __syncthreads();
+    const uint64_t ntiles = uint64_t(1) << P.nrest;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        uint64_t bo = 0, bi = P.foff;
+        for (int j = 0; j < P.nrest; ++j)
+            if ((t >> j) & 1u) {
+                bo |= uint64_t(1) << P.rest[j];
+                bi += P.in_stride[P.rest[j]];
+            }
+        for (uint32_t l0 = 0; l0 < NT; l0 += 4u * nt) {
+            Cplx<R> v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t l = l0 + u * nt + tid;
+                if (l < NT) v[u] = in[bi + in_off[l]];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t l = l0 + u * nt + tid;
+                if (l < NT) tile[pos_of[l]] = v[u];
+            }
+        }
+        __syncthreads();
+        for (uint32_t l = tid; l < NT; l += nt) out[bo + out_off[l]] = tile[l];
+        __syncthreads();
+    }
+}
+
+bool plan_permute(const std::vector<uint64_t>& out_dims, const std::vector<uint64_t>& src,
+                  uint64_t fixed_off, PermPlan& P) {
+    std::memset(&P, 0, sizeof(P));
+    P.foff = fixed_off;
+    // output bits from the least significant digit up
+    for (size_t v = out_dims.size(); v-- > 0;) {
+        uint64_t d = out_dims[v];
+        if (d == 0 || (d & (d - 1))) return false; // not a power of two
+        for (uint64_t s = src[v]; d > 1; d >>= 1, s <<= 1) {
+            if (P.nb >= 63) return false;
+            P.in_stride[P.nb++] = s;
+        }
+    }
+    if (P.nb < kPermTileBits + 1) return false;
+    P.tb = kPermTileBits;
+    uint64_t mask = 31; // the five lowest output bits
+    std::vector<int> by_in(P.nb);
+    for (int j = 0; j < P.nb; ++j) by_in[j] = j;
+    std::stable_sort(by_in.begin(), by_in.end(),
+                     [&](int a, int b) { return P.in_stride[a] < P.in_stride[b]; });
+    for (int k = 0; k < 5; ++k) mask |= uint64_t(1) << by_in[k];
+    for (int j = 5; j < P.nb && __builtin_popcountll(mask) < P.tb; ++j) mask |= uint64_t(1) << j;
+    int c = 0, r = 0;
+    for (int j = 0; j < P.nb; ++j) {
+        if (mask >> j & 1u) P.tbits[c++] = uint8_t(j);
+        else P.rest[r++] = uint8_t(j);
+    }
+    P.nrest = r;
+    c = 0;
+    for (int j : by_in)
+        if (mask >> j & 1u) {
+            P.tin[c] = uint8_t(j);
+            for (int q = 0; q < P.tb; ++q)
+                if (P.tbits[q] == uint8_t(j)) P.tin_pos[c] = uint8_t(q);
+            ++c;
+        }
+    return true;
+}
+
+bool launch_permute_tiled(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
+                          const std::vector<uint64_t>& out_dims,
+                          const std::vector<uint64_t>& src, uint64_t fixed_off) {
+    PermPlan P;
+    if (!plan_permute(out_dims, src, fixed_off, P)) return false;
+    const uint64_t ntiles = uint64_t(1) << P.nrest;
+    const int b = int(std::min<uint64_t>(ntiles, uint64_t(ctx->num_sms) * 6));
+    if (prec == QGPU_C128)
+        k_permute_tiled<double><<<b, 256, 0, ctx->stream>>>(
+            static_cast<const double2*>(in), static_cast<double2*>(out), P);
+    else
+        k_permute_tiled<float><<<b, 256, 0, ctx->stream>>>(
+            static_cast<const float2*>(in), static_cast<float2*>(out), P);
+    after_launch(ctx, "k_permute_tiled");
+    return true;
 }
 
 void launch_gather_outer(qgpu_ctx* ctx, qgpu_prec prec, const void* in,

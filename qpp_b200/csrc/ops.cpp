@@ -418,8 +418,8 @@ qgpu_state* op_ptranspose(const qgpu_state* s,
                 sa.push_back(inT[q] ? k.strides[q] : k.strides[q] * D);
             for (size_t q = 0; q < n; ++q) // output row digit q
                 sa.push_back(inT[q] ? k.strides[q] * D : k.strides[q]);
-            launch_gather(s->ctx, s->prec, s->data, out->data,
-                          plan_gather(od, sa, 0));
+            if (!launch_permute_tiled(s->ctx, s->prec, s->data, out->data, od, sa, 0))
+                launch_gather(s->ctx, s->prec, s->data, out->data, plan_gather(od, sa, 0));
         } else {
             for (size_t q = 0; q < n; ++q) {
                 sa.push_back(inT[q] ? k.strides[q] : 0);
@@ -458,7 +458,8 @@ qgpu_state* op_syspermute(const qgpu_state* s,
             od.push_back(nd[q]);
             sa.push_back(k.strides[perm[q]]);
         }
-        launch_gather(s->ctx, s->prec, s->data, out->data, plan_gather(od, sa, 0));
+        if (!launch_permute_tiled(s->ctx, s->prec, s->data, out->data, od, sa, 0))
+            launch_gather(s->ctx, s->prec, s->data, out->data, plan_gather(od, sa, 0));
     } catch (...) {
         free_state(out);
         throw;

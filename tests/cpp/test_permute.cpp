@@ -1,0 +1,146 @@
+// CPU check of the tiled bit permutation behind ptranspose / syspermute
+// (qgpu::plan_permute and the addressing of k_permute_tiled): for density
+// matrices of 6-9 qubits with random targets / permutations and for kets of
+// 11-16 qubits, the kernel's tiles must write every output exactly once,
+// read only inside the input, and read for output o the element the plain
+// gather reads (the digit formula sum_v digit_v(o) * src[v]).
+// Built and run by tests/test_permute.py.
+#include <algorithm>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "kernels.hpp"
+
+using namespace qgpu;
+
+static int fails = 0;
+#define EXPECT(c)                                                            \
+    do {                                                                     \
+        if (!(c)) {                                                          \
+            if (fails < 20) std::printf("FAIL %s:%d %s\n", __FILE__, __LINE__, #c); \
+            ++fails;                                                         \
+        }                                                                    \
+    } while (0)
+
+static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& src,
+                  uint64_t in_count) {
+    PermPlan P;
+    EXPECT(plan_permute(od, src, 0, P));
+    uint64_t count = 1;
+    for (uint64_t d : od) count *= d;
+    EXPECT((uint64_t(1) << P.nb) == count);
+    EXPECT(P.tb == kPermTileBits && P.nrest == P.nb - P.tb);
+    const uint32_t NT = 1u << P.tb;
+    std::vector<uint64_t> in_off(NT), out_off(NT);
+    std::vector<uint32_t> pos_of(NT);
+    for (uint32_t l = 0; l < NT; ++l) {
+        uint64_t io = 0, oo = 0;
+        uint32_t lo = 0;
+        for (int j = 0; j < P.tb; ++j)
+            if ((l >> j) & 1u) {
+                io += P.in_stride[P.tin[j]];
+                lo |= 1u << P.tin_pos[j];
+                oo |= uint64_t(1) << P.tbits[j];
+            }
+        in_off[l] = io;
+        out_off[l] = oo;
+        pos_of[l] = lo;
+    }
+    // the low five output bits are in the tile (coalesced writes)
+    for (int j = 0; j < 5; ++j) EXPECT(P.tbits[j] == j);
+    std::vector<uint8_t> written(count, 0);
+    for (uint64_t t = 0; t < (uint64_t(1) << P.nrest); ++t) {
+        uint64_t bo = 0, bi = P.foff;
+        for (int j = 0; j < P.nrest; ++j)
+            if ((t >> j) & 1u) {
+                bo |= uint64_t(1) << P.rest[j];
+                bi += P.in_stride[P.rest[j]];
+            }
+        for (uint32_t l = 0; l < NT; ++l) {
+            const uint64_t ia = bi + in_off[l];
+            const uint64_t oa = bo + out_off[pos_of[l]];
+            EXPECT(ia < in_count && oa < count);
+            if (oa >= count) continue;
+            EXPECT(written[oa] == 0);
+            written[oa] = 1;
+            // the plain gather's source of output oa
+            uint64_t r = oa, want = 0;
+            for (size_t v = od.size(); v-- > 0;) {
+                want += (r % od[v]) * src[v];
+                r /= od[v];
+            }
+            EXPECT(ia == want);
+        }
+    }
+    for (uint64_t o = 0; o < count; ++o) EXPECT(written[o] == 1);
+}
+
+int main() {
+    std::mt19937 rng(7);
+    for (int trial = 0; trial < 12; ++trial) {
+        const int n = 6 + trial % 4; // density matrices of 6..9 qubits
+        const uint64_t D = uint64_t(1) << n;
+        std::vector<uint64_t> strides(n);
+        for (int q = 0; q < n; ++q) strides[q] = uint64_t(1) << (n - 1 - q);
+        // syspermute: out column digits then row digits, permuted
+        std::vector<uint64_t> perm(n);
+        for (int q = 0; q < n; ++q) perm[q] = uint64_t(q);
+        std::shuffle(perm.begin(), perm.end(), rng);
+        std::vector<uint64_t> od, sa;
+        for (int q = 0; q < n; ++q) {
+            od.push_back(2);
+            sa.push_back(strides[perm[q]] * D);
+        }
+        for (int q = 0; q < n; ++q) {
+            od.push_back(2);
+            sa.push_back(strides[perm[q]]);
+        }
+        check(od, sa, D * D);
+        // ptranspose over a random subset
+        std::vector<char> inT(n);
+        for (auto& x : inT) x = char(rng() & 1u);
+        od.clear();
+        sa.clear();
+        for (int q = 0; q < n; ++q) {
+            od.push_back(2);
+            sa.push_back(inT[q] ? strides[q] : strides[q] * D);
+        }
+        for (int q = 0; q < n; ++q) {
+            od.push_back(2);
+            sa.push_back(inT[q] ? strides[q] * D : strides[q]);
+        }
+        check(od, sa, D * D);
+    }
+    for (int n = 11; n <= 16; ++n) { // ket syspermute, mixed power-of-two dims
+        std::vector<uint64_t> dims;
+        int bits = 0;
+        while (bits < n) {
+            const int b = (bits + 2 <= n && (rng() & 1u)) ? 2 : 1;
+            dims.push_back(uint64_t(1) << b);
+            bits += b;
+        }
+        const size_t m = dims.size();
+        std::vector<uint64_t> st(m);
+        uint64_t s = 1;
+        for (size_t q = m; q-- > 0;) {
+            st[q] = s;
+            s *= dims[q];
+        }
+        std::vector<uint64_t> perm(m);
+        for (size_t q = 0; q < m; ++q) perm[q] = q;
+        std::shuffle(perm.begin(), perm.end(), rng);
+        std::vector<uint64_t> od, sa;
+        for (size_t q = 0; q < m; ++q) {
+            od.push_back(dims[perm[q]]);
+            sa.push_back(st[perm[q]]);
+        }
+        check(od, sa, s);
+    }
+    // not applicable: a qutrit, or too few bits
+    PermPlan P;
+    EXPECT(!plan_permute({3, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2}, {1, 3, 6, 12, 24, 48, 96, 192, 384, 768, 1536}, 0, P));
+    EXPECT(!plan_permute({2, 2, 2}, {1, 2, 4}, 0, P));
+    std::printf(fails ? "permute FAILED (%d)\n" : "permute ok\n", fails);
+    return fails ? 1 : 0;
+}
