@@ -388,10 +388,11 @@ qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double p_depol,
                               uint64_t* samples, uint32_t* dits, double* dump,
                               uint32_t* events, uint32_t max_events);
 /* Tile width of the trajectory kernel for registers of n qubits (15-22) on
- * this context's device: set_T = -1 queries (timing the candidates {untiled,
- * 10, 11, 12, 13} once on first use), 0 pins the untiled form, 9..14 (< n)
- * pins that width, -2 drops the choice so it is timed again. No reference
- * counterpart. *chosen (if not NULL) receives the width now in force. */
+ * this context's device: set_T = -1 queries (timing the candidates
+ * {untiled (below 18 qubits), 10, 11, 12, 13} once on first use), 0 pins the
+ * untiled form, 9..14 (< n) pins that width, -2 drops the choice so it is
+ * timed again. No reference counterpart. *chosen (if not NULL) receives the
+ * width now in force. */
 qgpu_status qgpu_traj_tile_width(qgpu_ctx* ctx, uint32_t n, int set_T, int* chosen);
 
 /* ------------------------------------------------------ batched instances
@@ -410,6 +411,12 @@ qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst,
                            qgpu_circuit* const* circuits,
                            qgpu_state* const* states, int form,
                            uint64_t* graph_kernels);
+/* Where the last qgpu_run_batch on ctx spent its time, in milliseconds:
+ * phases_ms[0] compiling and tiling the programs on the host, [1] uploading
+ * them and capturing + instantiating the graph, [2] the graph on the device
+ * (CUDA events), [3] the instances run in the plain form. No reference
+ * counterpart. */
+qgpu_status qgpu_batch_last_phases(qgpu_ctx* ctx, double* phases_ms);
 
 /* ------------------------------------------------------------ serving loop
  * QNoisyEngine requests on one GPU. A worker thread drains the queue.

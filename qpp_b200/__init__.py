@@ -513,6 +513,15 @@ def apply_tc(state, U, target):
     return state
 
 
+def batch_last_phases(ctx):
+    """Milliseconds of the last run_batch on ctx: compile, build (upload +
+    graph capture), graph device time, plain-form instances."""
+    out = (ct.c_double * 4)()
+    check(lib().qgpu_batch_last_phases(ctx.h, out))
+    return {"compile_ms": out[0], "build_ms": out[1], "graph_device_ms": out[2],
+            "plain_ms": out[3]}
+
+
 def traj_tile_width(ctx, n, T=None):
     """Tile width of the trajectory kernel for n-qubit registers (15-22):
     T=None queries (tuned on first use), 0 pins the untiled form, 9..14

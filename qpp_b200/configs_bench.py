@@ -28,8 +28,8 @@ import time
 
 import numpy as np
 
-from . import (C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, State, run_batch,
-               traj_tile_width)
+from . import (C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, State, batch_last_phases,
+               run_batch, traj_tile_width)
 from .workloads import haar_unitary, ket_gate_sequence
 
 
@@ -258,6 +258,8 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
             res[f"{name}_{label}"] = {"s": wall, "device_ms": a.elapsed_time(b),
                                       "instances_per_s": len(circs) / wall,
                                       "graph_kernels": k}
+            if label == "graph":
+                res[f"{name}_{label}"]["phases"] = batch_last_phases(ctx)
         for s in st:
             s.free()
     res["graph_speedup_vs_plain_c64"] = res["c64_plain_loop"]["s"] / res["c64_graph"]["s"]
@@ -266,13 +268,29 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
 
 
 def main():
+    import argparse
+
     import torch
-    cpu = "--no-cpu" not in sys.argv
+    ap = argparse.ArgumentParser(description="configs 1, 2 and 4 on one GPU")
+    ap.add_argument("--only", choices=["config1", "config2", "config4"], action="append",
+                    help="run only these configs (repeatable)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline samples")
+    ap.add_argument("--steps", type=int, default=200, help="config 2 steps")
+    ap.add_argument("--kets", type=int, default=2048, help="config 4 kets")
+    ap.add_argument("--rho", type=int, default=512, help="config 4 density matrices")
+    ap.add_argument("--depth", type=int, default=20, help="config 4 circuit depth")
+    a = ap.parse_args()
+    run = set(a.only or ["config1", "config2", "config4"])
+    cpu = not a.no_cpu
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream())
-    out = {"config1": config1(ctx, torch, stream, cpu),
-           "config2": config2(ctx, torch, stream, cpu),
-           "config4": config4(ctx, torch, stream)}
+    out = {}
+    if "config1" in run:
+        out["config1"] = config1(ctx, torch, stream, cpu)
+    if "config2" in run:
+        out["config2"] = config2(ctx, torch, stream, cpu, steps=max(a.steps, 3))
+    if "config4" in run:
+        out["config4"] = config4(ctx, torch, stream, n_kets=a.kets, n_rho=a.rho, depth=a.depth)
     print(json.dumps(out), flush=True)
 
 

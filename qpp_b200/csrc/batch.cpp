@@ -4,14 +4,18 @@
 // No reference counterpart: Quantum++ runs one state per call. The batched
 // form compiles every instance into a trajectory program (a density matrix
 // as a ket over 2n virtual qubits, see compile_traj_rho), groups instances
-// by register size, and captures one trajectory-kernel launch per size into
-// a single CUDA graph (one parallel branch per size), so the whole batch is
-// one graph launch. One CTA runs one instance: registers of up to 2^14
-// amplitudes are copied into shared memory and back to the instance's own
-// qgpu_state; larger ones are worked on in place in that state (HBM). The
+// by register size, and captures everything into a single CUDA graph, so the
+// whole batch is one graph launch. Registers of up to 2^14 amplitudes: one
+// CTA per instance with the register in shared memory, one trajectory-kernel
+// launch per size on its own graph branch. Larger registers whose programs
+// are all gates: cache-blocked tile passes at the tuned width, run
+// layer-synchronously on one more branch -- graph node k applies pass k of
+// every such register, all tiles in parallel, in place in the instances' own
+// states. Larger registers with measurements keep one CTA per instance. The
 // plain form loops over the instances with one kernel launch per gate
 // (qgpu_run_gates, QGPU_FORM_PLAIN).
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <set>
@@ -30,14 +34,8 @@ bool compile_traj_rho(const qgpu_circuit* c, TProgram& P) {
     P.n = uint32_t(nv);
     P.ncreg = c->nc;
     auto vbit = [&](int v) { return uint8_t(nv - 1 - v); };
-    auto add_mat = [&](const std::vector<cd>& U) {
-        uint32_t off = uint32_t(P.mats.size() / 2);
-        for (const cd& z : U) {
-            P.mats.push_back(float(z.real()));
-            P.mats.push_back(float(z.imag()));
-        }
-        return off;
-    };
+    MatPool pool(P);
+    auto add_mat = [&](const std::vector<cd>& U) { return pool.add(U); };
     auto super1 = [&](int t, const std::vector<cd>& S, uint8_t flags) {
         TInstr I{};
         I.op = kTG2;
@@ -139,6 +137,12 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 if (d != circuits[i]->d) raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, W, "state/circuit");
         }
         if (graph_kernels) *graph_kernels = 0;
+        using clk = std::chrono::steady_clock;
+        auto ms_since = [](clk::time_point t) {
+            return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+        };
+        for (double& x : ctx->batch_ms) x = 0;
+        auto t_compile = clk::now();
         std::vector<uint32_t> plain;
         std::vector<std::pair<uint32_t, qgpu::TProgram>> prog;
         for (uint32_t i = 0; i < n_inst; ++i) {
@@ -146,21 +150,48 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             bool ok = form == 1 && states[i]->prec == QGPU_C64 &&
                       (states[i]->kind == QGPU_KET ? qgpu::compile_traj(circuits[i], P)
                                                    : qgpu::compile_traj_rho(circuits[i], P));
-            if (ok) prog.emplace_back(i, std::move(P));
-            else plain.push_back(i);
+            if (ok) {
+                qgpu::fold_1q_gates(P); // batch programs carry no noise
+                prog.emplace_back(i, std::move(P));
+            } else {
+                plain.push_back(i);
+            }
         }
         if (!prog.empty()) {
-            // registers above shared-memory size: cache-blocked tile passes
-            // at the tuned width of their size class (timed before capture)
+            // Registers above shared-memory size whose programs are all gates
+            // run layer-synchronously: every gate belongs to a tile pass of
+            // the tuned width, and launch k runs pass k of every such
+            // register, all tiles in parallel. Programs with measurements keep
+            // one CTA per register (tile passes inside k_traj).
+            auto all_gates = [](const qgpu::TProgram& P) {
+                for (const auto& I : P.ins)
+                    if (I.op != qgpu::kTG1 && I.op != qgpu::kTCG1 && I.op != qgpu::kTG2 &&
+                        I.op != qgpu::kTG4)
+                        return false;
+                return true;
+            };
             std::map<uint32_t, int> tile_of;
-            for (auto& pr : prog) {
-                const uint32_t n = pr.second.n;
+            std::vector<char> layered(prog.size(), 0);
+            int layer_bits = 0;
+            for (size_t k = 0; k < prog.size(); ++k) {
+                qgpu::TProgram& P = prog[k].second;
+                const uint32_t n = P.n;
                 if (n <= uint32_t(qgpu::kTrajMaxQubits)) continue;
                 auto it = tile_of.find(n);
                 if (it == tile_of.end()) it = tile_of.emplace(n, qgpu::tile_width(ctx, int(n))).first;
-                qgpu::plan_tiles(pr.second, it->second);
+                if (all_gates(P) && !P.ins.empty()) {
+                    // two 2^T tiles per CTA: T = 12 keeps three CTAs per SM
+                    const int T = std::min(it->second ? it->second : 12, 12);
+                    qgpu::plan_tiles(P, T, 1);
+                    layered[k] = 1;
+                    layer_bits = std::max(layer_bits, T);
+                } else {
+                    qgpu::plan_tiles(P, it->second);
+                }
             }
-            // device copies of all programs, work items grouped by size
+            ctx->batch_ms[0] = ms_since(t_compile);
+            auto t_build = clk::now();
+            // device copies of all programs, per-CTA work items grouped by size
             std::map<uint32_t, std::vector<size_t>> by_n;
             std::vector<qgpu::TInstr> ins;
             std::vector<float> mats;
@@ -169,14 +200,35 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 ofs[k] = {ins.size(), mats.size() / 2};
                 ins.insert(ins.end(), prog[k].second.ins.begin(), prog[k].second.ins.end());
                 mats.insert(mats.end(), prog[k].second.mats.begin(), prog[k].second.mats.end());
-                by_n[prog[k].second.n].push_back(k);
+                if (!layered[k]) by_n[prog[k].second.n].push_back(k);
+            }
+            // the passes of each layered register, in program order
+            struct Pass {
+                uint32_t pos, nins, tb_off;
+                uint8_t T;
+            };
+            std::vector<std::vector<Pass>> passes(prog.size());
+            size_t kmax = 0;
+            for (size_t k = 0; k < prog.size(); ++k) {
+                if (!layered[k]) continue;
+                const auto& P = prog[k].second;
+                for (size_t i = 0; i < P.ins.size(); ++i)
+                    if (P.ins[i].op == qgpu::kTTile) {
+                        passes[k].push_back({uint32_t(i + 1), P.ins[i].cmask, P.ins[i].mat,
+                                             P.ins[i].b0});
+                        i += P.ins[i].cmask;
+                    }
+                kmax = std::max(kmax, passes[k].size());
             }
             auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+            size_t npass_total = 0;
+            for (auto& v : passes) npass_total += v.size();
             size_t b_ins = std::max<size_t>(ins.size() * sizeof(qgpu::TInstr), 16);
             size_t b_mat = std::max<size_t>(mats.size() * sizeof(float), 16);
-            size_t b_work = prog.size() * sizeof(qgpu::TWork);
+            size_t b_work = std::max<size_t>(prog.size() * sizeof(qgpu::TWork), 16);
+            size_t b_pass = std::max<size_t>(npass_total * sizeof(qgpu::PassInst), 16);
             size_t b_out = prog.size() * (sizeof(uint64_t) + sizeof(uint32_t) * 8);
-            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_out);
+            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_out);
             unsigned char* buf = nullptr;
             QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), total, ctx->stream));
             unsigned char* p = buf;
@@ -188,6 +240,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             auto* dins = reinterpret_cast<qgpu::TInstr*>(take(b_ins));
             auto* dmat = reinterpret_cast<float2*>(take(b_mat));
             auto* dwork = reinterpret_cast<qgpu::TWork*>(take(b_work));
+            auto* dpass = reinterpret_cast<qgpu::PassInst*>(take(b_pass));
             auto* dsamp = reinterpret_cast<uint64_t*>(take(prog.size() * sizeof(uint64_t)));
             auto* ddits = reinterpret_cast<uint32_t*>(take(prog.size() * sizeof(uint32_t) * 8));
             std::vector<qgpu::TWork> work;
@@ -212,21 +265,59 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 }
                 ranges.push_back({kv.first, {lo, work.size()}});
             }
+            // launch k: pass k of every layered register; an item is 2^15
+            // amplitudes of one register (equal work per item)
+            std::vector<qgpu::PassInst> pinst;
+            pinst.reserve(npass_total);
+            std::vector<std::pair<size_t, std::pair<int, uint32_t>>> launches; // offset, (count, items)
+            for (size_t kk = 0; kk < kmax; ++kk) {
+                const size_t off = pinst.size();
+                uint32_t items = 0;
+                for (size_t k = 0; k < prog.size(); ++k) {
+                    if (!layered[k] || kk >= passes[k].size()) continue;
+                    const Pass& ps = passes[k][kk];
+                    const uint32_t n = prog[k].second.n;
+                    const uint32_t ntiles = 1u << (n - ps.T);
+                    const uint32_t tpi =
+                        std::min<uint32_t>(ntiles, std::max<uint32_t>(1, (1u << 15) >> ps.T));
+                    qgpu::PassInst q{};
+                    q.psi = static_cast<float2*>(states[prog[k].first]->data);
+                    if (reinterpret_cast<uintptr_t>(q.psi) % 16)
+                        raise(QGPU_ERR_INVALID_ARGUMENT, W, "state not 16-byte aligned");
+                    q.mats = dmat + ofs[k].second;
+                    q.ins = dins + ofs[k].first + ps.pos;
+                    q.nins = ps.nins;
+                    q.tb_off = ps.tb_off;
+                    q.first_item = items;
+                    q.tiles_per_item = tpi;
+                    q.n = uint8_t(n);
+                    q.T = ps.T;
+                    pinst.push_back(q);
+                    items += (ntiles + tpi - 1) / tpi;
+                }
+                launches.push_back({off, {int(pinst.size() - off), items}});
+            }
             QG_CUDA(cudaMemcpyAsync(dins, ins.data(), ins.size() * sizeof(qgpu::TInstr),
                                     cudaMemcpyHostToDevice, ctx->stream));
             if (!mats.empty())
                 QG_CUDA(cudaMemcpyAsync(dmat, mats.data(), mats.size() * sizeof(float),
                                         cudaMemcpyHostToDevice, ctx->stream));
-            QG_CUDA(cudaMemcpyAsync(dwork, work.data(), b_work, cudaMemcpyHostToDevice,
-                                    ctx->stream));
-            // one graph: a launch per register size, each on its own branch
-            // (the groups touch disjoint states), so the small-register
-            // launches fill the SMs that the few large instances leave idle
+            if (!work.empty())
+                QG_CUDA(cudaMemcpyAsync(dwork, work.data(), work.size() * sizeof(qgpu::TWork),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+            if (!pinst.empty())
+                QG_CUDA(cudaMemcpyAsync(dpass, pinst.data(), pinst.size() * sizeof(qgpu::PassInst),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+            int* dflag = launches.empty() ? nullptr : qgpu::ctx_error_flag(ctx);
+            // one graph: a k_traj launch per register size on its own branch,
+            // and the chain of layer launches on one more branch (all touch
+            // disjoint states)
             qgpu::traj_prepare();
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
-            std::vector<cudaStream_t> side(ranges.size(), nullptr);
-            std::vector<cudaEvent_t> ev(ranges.size() + 1, nullptr);
+            const size_t nbr = ranges.size() + (launches.empty() ? 0 : 1);
+            std::vector<cudaStream_t> side(nbr, nullptr);
+            std::vector<cudaEvent_t> ev(nbr + 1, nullptr);
             struct Rel {
                 std::vector<cudaStream_t>& s;
                 std::vector<cudaEvent_t>& e;
@@ -242,8 +333,17 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             QG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
             try {
                 QG_CUDA(cudaEventRecord(ev[0], ctx->stream));
-                for (size_t g = 0; g < ranges.size(); ++g) {
-                    const auto& rg = ranges[g];
+                size_t g = 0;
+                if (!launches.empty()) { // longest chain first
+                    QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
+                    for (auto& L : launches)
+                        qgpu::launch_pass_batch(ctx, dpass + L.first, L.second.first,
+                                                L.second.second, layer_bits, dflag, side[g]);
+                    QG_CUDA(cudaEventRecord(ev[g + 1], side[g]));
+                    QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
+                    ++g;
+                }
+                for (const auto& rg : ranges) {
                     QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
                     auto tt = tile_of.find(rg.first);
                     qgpu::launch_traj(ctx, dwork + rg.second.first,
@@ -252,6 +352,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                                       tt == tile_of.end() ? 0 : tt->second);
                     QG_CUDA(cudaEventRecord(ev[g + 1], side[g]));
                     QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
+                    ++g;
                 }
             } catch (...) {
                 cudaStreamEndCapture(ctx->stream, &graph);
@@ -260,14 +361,43 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             }
             QG_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
             QG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+            QG_CUDA(cudaStreamSynchronize(ctx->stream)); // uploads done
+            ctx->batch_ms[1] = ms_since(t_build);
+            // the graph's device time, on timing events of its own
+            cudaEvent_t g0 = nullptr, g1 = nullptr;
+            QG_CUDA(cudaEventCreate(&g0));
+            QG_CUDA(cudaEventCreate(&g1));
+            struct DelEv {
+                cudaEvent_t a, b;
+                ~DelEv() {
+                    cudaEventDestroy(a);
+                    cudaEventDestroy(b);
+                }
+            } delev{g0, g1};
+            QG_CUDA(cudaEventRecord(g0, ctx->stream));
             QG_CUDA(cudaGraphLaunch(exec, ctx->stream));
+            QG_CUDA(cudaEventRecord(g1, ctx->stream));
             QG_CUDA(cudaFreeAsync(buf, ctx->stream));
             QG_CUDA(cudaStreamSynchronize(ctx->stream));
+            float gms = 0;
+            QG_CUDA(cudaEventElapsedTime(&gms, g0, g1));
+            ctx->batch_ms[2] = gms;
             cudaGraphExecDestroy(exec);
             cudaGraphDestroy(graph);
-            if (graph_kernels) *graph_kernels = ranges.size();
+            if (dflag && qgpu::fused_error(ctx))
+                raise(QGPU_ERR_TIMEOUT, W, "a bounded wait of the layer kernel gave up");
+            if (graph_kernels) *graph_kernels = ranges.size() + launches.size();
         }
+        auto t_plain = clk::now();
         for (uint32_t i : plain) qgpu::run_gates(states[i], circuits[i], 0, 0, circuits[i]->steps.size());
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->batch_ms[3] = ms_since(t_plain);
+    });
+}
+
+extern "C" qgpu_status qgpu_batch_last_phases(qgpu_ctx* ctx, double* phases_ms) {
+    return guarded([&] {
+        need_handle(ctx);
+        if (phases_ms) std::copy(ctx->batch_ms, ctx->batch_ms + 4, phases_ms);
     });
 }

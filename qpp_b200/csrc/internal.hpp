@@ -31,6 +31,10 @@ struct qgpu_ctx {
     // context is torn down only when the last of them is freed.
     std::atomic<int64_t> live_states{0};
     std::atomic<bool> closing{false};
+    // phases of the last qgpu_run_batch (milliseconds): programs compiled and
+    // tiled on the host, buffers uploaded and the graph captured and
+    // instantiated, the graph's device time, the plain-form instances
+    double batch_ms[4] = {0, 0, 0, 0};
 };
 
 struct qgpu_state {

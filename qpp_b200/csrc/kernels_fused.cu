@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(512, 1)
 }
 
 // ------------------------------------------------------------- launcher
-static int* fused_err_flag(qgpu_ctx* ctx) {
+int* ctx_error_flag(qgpu_ctx* ctx) {
     if (!ctx->dev_flag) {
         QG_CUDA(cudaMalloc(&ctx->dev_flag, sizeof(int)));
         QG_CUDA(cudaMemset(ctx->dev_flag, 0, sizeof(int)));
@@ -318,7 +318,7 @@ void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
         p.off[m] = o;
     }
     p.B = dB;
-    p.err = fused_err_flag(ctx);
+    p.err = ctx_error_flag(ctx);
     size_t smem = 2 * 65536 + 1024;
     static bool attr = false;
     if (!attr) {
@@ -333,7 +333,7 @@ void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
 
 int fused_error(qgpu_ctx* ctx) {
     int h = 0;
-    int* f = fused_err_flag(ctx);
+    int* f = ctx_error_flag(ctx);
     QG_CUDA(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     QG_CUDA(cudaStreamSynchronize(ctx->stream));
     if (h) QG_CUDA(cudaMemsetAsync(f, 0, sizeof(int), ctx->stream));

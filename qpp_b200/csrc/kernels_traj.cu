@@ -435,6 +435,257 @@ __global__ void __launch_bounds__(256, 4)
     }
 }
 
+// One tile pass of many registers at once (layer-synchronous batches): the
+// launch covers pass k of every register that has one. A CTA takes a
+// contiguous range of items; an item is tiles_per_item consecutive tiles of
+// one register. Tiles move by bulk copies (the copy engine, untiled
+// cp.async.bulk; rows = runs of >= 32 consecutive amplitudes, 16-byte
+// aligned): warp 0 loads tile i + 1 into the second buffer (completion
+// counted on an mbarrier) while all warps apply tile i's gates in shared
+// memory, and writes tile i back with bulk stores. Every mbarrier wait is
+// bounded; a timeout sets *err, waits once more (bounded) for the copies in
+// flight and ends the CTA. Registers are independent, and the kernel
+// boundary orders pass k before pass k + 1.
+constexpr uint32_t kPassSpinLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool pass_mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (uint32_t it = 0; it < kPassSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+struct PassCursor {
+    int j;          // register (PassInst) index
+    uint32_t it;    // item
+    uint32_t t, t1; // tile and end of the item's tiles
+};
+
+__device__ __forceinline__ void cursor_item(const PassInst* insts, PassCursor& c) {
+    const PassInst& P = insts[c.j];
+    c.t = (c.it - P.first_item) * P.tiles_per_item;
+    c.t1 = min(c.t + P.tiles_per_item, 1u << (P.n - P.T));
+}
+
+// false when the CTA's range is exhausted
+__device__ __forceinline__ bool cursor_next(const PassInst* insts, int ninst, uint32_t it1,
+                                            PassCursor& c) {
+    if (++c.t < c.t1) return true;
+    if (++c.it >= it1) return false;
+    while (c.j + 1 < ninst && insts[c.j + 1].first_item <= c.it) ++c.j;
+    cursor_item(insts, c);
+    return true;
+}
+
+// Geometry of one register's tile pass, cached in shared memory by the CTA
+// while it works on that register: row offsets (rows = runs of 2^crow
+// consecutive amplitudes) and the bits outside the tile.
+struct PassGeom {
+    uint32_t nrows, rowbytes, rest;
+    int j; // register the table belongs to (-1: none)
+};
+
+// every thread fills rows; thread 0 writes the header (call between
+// barriers)
+__device__ void pass_geom(const PassInst& P, int j, PassGeom* g, uint32_t* rowoff) {
+    const uint32_t* tb = reinterpret_cast<const uint32_t*>(P.mats + P.tb_off);
+    const int T = P.T, n = P.n;
+    int crow = 0;
+    while (crow < T && tb[crow] == uint32_t(crow)) ++crow;
+    const uint32_t nrows = 1u << (T - crow);
+    if (threadIdx.x == 0) {
+        uint32_t tilebits = 0;
+        for (int q = 0; q < T; ++q) tilebits |= 1u << tb[q];
+        g->rest = (n == 32 ? 0xffffffffu : ((1u << n) - 1)) & ~tilebits;
+        g->nrows = nrows;
+        g->rowbytes = (1u << crow) * uint32_t(sizeof(float2));
+        g->j = j;
+    }
+    for (uint32_t row = threadIdx.x; row < nrows; row += blockDim.x) {
+        uint32_t off = 0;
+        for (int q = crow; q < T; ++q) off |= ((row >> (q - crow)) & 1u) << tb[q];
+        rowoff[row] = off;
+    }
+}
+
+__device__ __forceinline__ uint32_t tile_base(uint32_t rest, uint32_t t) {
+    uint32_t base = 0;
+    while (rest) {
+        const uint32_t low = rest & (0u - rest);
+        if (t & 1u) base |= low;
+        t >>= 1;
+        rest ^= low;
+    }
+    return base;
+}
+
+// warp 0: bulk-load tile t into buf, completion on mbar
+__device__ __forceinline__ void pass_issue_load(const PassInst& P, const PassGeom& g,
+                                                const uint32_t* rowoff, uint32_t t, float2* buf,
+                                                uint32_t mbar, int lane) {
+    const float2* src = P.psi + tile_base(g.rest, t);
+    if (lane == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+                     "r"(g.nrows * g.rowbytes)
+                     : "memory");
+    __syncwarp();
+    const uint32_t rowlen = g.rowbytes / uint32_t(sizeof(float2));
+    for (uint32_t row = lane; row < g.nrows; row += 32)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                "r"(smem_addr(buf + row * rowlen)),
+            "l"(src + rowoff[row]), "r"(g.rowbytes), "r"(mbar)
+            : "memory");
+}
+
+// warp 0: bulk-store tile t from buf back into its register
+__device__ __forceinline__ void pass_issue_store(const PassInst& P, const PassGeom& g,
+                                                 const uint32_t* rowoff, uint32_t t,
+                                                 const float2* buf, int lane) {
+    float2* dst = P.psi + tile_base(g.rest, t);
+    const uint32_t rowlen = g.rowbytes / uint32_t(sizeof(float2));
+    for (uint32_t row = lane; row < g.nrows; row += 32)
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(
+                         dst + rowoff[row]),
+                     "r"(smem_addr(buf + row * rowlen)), "r"(g.rowbytes)
+                     : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(256, 3)
+    k_pass_batch(const PassInst* __restrict__ insts, int ninst, uint32_t nitems, int tile_bits,
+                 int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    float2* const buf0 = reinterpret_cast<float2*>(sm);
+    float2* const buf1 = reinterpret_cast<float2*>(sm + (size_t(1) << tile_bits) * sizeof(float2));
+    // row tables of the registers of the current and the next tile (at
+    // most 2^(tile_bits - 5) rows each)
+    uint32_t* const rows0 = reinterpret_cast<uint32_t*>(sm + (size_t(2) << tile_bits) * sizeof(float2));
+    uint32_t* const rows1 = rows0 + (size_t(1) << (tile_bits - 5));
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ int abort_sh;
+    __shared__ PassGeom geom[2];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t per = (nitems + gridDim.x - 1) / gridDim.x;
+    const uint32_t it0 = blockIdx.x * per, it1 = min(nitems, it0 + per);
+    if (it0 >= it1) return; // uniform across the CTA
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        abort_sh = 0;
+        geom[0].j = geom[1].j = -1;
+    }
+    PassCursor cur;
+    {
+        int lo = 0, hi = ninst - 1; // last register with first_item <= it0
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (insts[mid].first_item <= it0) lo = mid;
+            else hi = mid - 1;
+        }
+        cur.j = lo;
+        cur.it = it0;
+        cursor_item(insts, cur);
+    }
+    __syncthreads();
+    // geometry slot x belongs to buffer x
+    pass_geom(insts[cur.j], cur.j, &geom[0], rows0);
+    __syncthreads();
+    uint32_t parity[2] = {0u, 0u};
+    bool pending[2] = {true, false}; // a load in flight into buffer x
+    int b = 0;
+    if (warp == 0)
+        pass_issue_load(insts[cur.j], geom[0], rows0, cur.t, buf0, smem_addr(&mbar[0]), lane);
+    bool more = true;
+    while (more) {
+        float2* const bc = b ? buf1 : buf0;
+        float2* const bn = b ? buf0 : buf1;
+        uint32_t* const rc = b ? rows1 : rows0;
+        uint32_t* const rn = b ? rows0 : rows1;
+        PassCursor nxt = cur;
+        more = cursor_next(insts, ninst, it1, nxt);
+        if (more) {
+            // rebuilt only when the register changes; nothing writes the
+            // slot before the first barrier, so every thread takes the
+            // same branch
+            if (geom[b ^ 1].j != nxt.j) {
+                __syncthreads();
+                pass_geom(insts[nxt.j], nxt.j, &geom[b ^ 1], rn);
+                __syncthreads();
+            }
+            if (warp == 0) {
+                // the other buffer's last bulk store must have read it
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                __syncwarp();
+                pass_issue_load(insts[nxt.j], geom[b ^ 1], rn, nxt.t, bn, smem_addr(&mbar[b ^ 1]),
+                                lane);
+            }
+            pending[b ^ 1] = true;
+        }
+        if (pass_mbar_wait(smem_addr(&mbar[b]), parity[b])) {
+            parity[b] ^= 1u;
+            pending[b] = false;
+        } else {
+            atomicExch(err, 1);
+            abort_sh = 1;
+        }
+        __syncthreads();
+        if (abort_sh) break;
+        const PassInst& P = insts[cur.j];
+        const uint32_t NT = 1u << P.T;
+        for (uint32_t i = 0; i < P.nins; ++i) {
+            tr_gate(P.ins[i], P.mats, bc, NT, tid, nt);
+            __syncthreads();
+        }
+        // the threads' shared-memory writes, visible to the bulk stores
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (warp == 0) pass_issue_store(P, geom[b], rc, cur.t, bc, lane);
+        cur = nxt;
+        b ^= 1;
+    }
+    // after a timeout: wait once more (bounded) for the loads in flight
+    for (int x = 0; x < 2; ++x)
+        if (pending[x]) pass_mbar_wait(smem_addr(&mbar[x]), parity[x]);
+    if (warp == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+void launch_pass_batch(qgpu_ctx* ctx, const PassInst* dinsts, int ninst, uint32_t nitems,
+                       int tile_bits, int* err, cudaStream_t stream) {
+    if (ninst == 0 || nitems == 0) return;
+    if (tile_bits < 9 || tile_bits > 13)
+        raise(QGPU_ERR_INVALID_ARGUMENT, "launch_pass_batch()", "tile_bits");
+    static std::once_flag once;
+    std::call_once(once, [] {
+        QG_CUDA(cudaFuncSetAttribute(k_pass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int((size_t(2) << 13) * sizeof(float2) +
+                                         (size_t(2) << 8) * sizeof(uint32_t))));
+    });
+    // two tile buffers and two row tables
+    const size_t smem = (size_t(2) << tile_bits) * sizeof(float2) +
+                        (size_t(2) << (tile_bits - 5)) * sizeof(uint32_t);
+    int per_sm = 0;
+    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass_batch, 256, smem));
+    per_sm = std::max(1, per_sm);
+    const uint32_t grid = std::min<uint32_t>(nitems, uint32_t(ctx->num_sms) * uint32_t(per_sm));
+    k_pass_batch<<<grid, 256, smem, stream ? stream : ctx->stream>>>(dinsts, ninst, nitems,
+                                                                      tile_bits, err);
+    after_launch(ctx, "k_pass_batch");
+}
+
 void traj_prepare() {
     static std::once_flag once;
     std::call_once(once, [] {

@@ -3,14 +3,31 @@
 #include "traj.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 
 #include "capi_common.hpp"
 #include "circuit.hpp"
 
 namespace qgpu {
+
+uint32_t MatPool::add(const std::vector<cd>& U) {
+    std::string key(U.size() * 2 * sizeof(float), '\0');
+    float* k = reinterpret_cast<float*>(&key[0]);
+    for (size_t i = 0; i < U.size(); ++i) {
+        k[2 * i] = float(U[i].real());
+        k[2 * i + 1] = float(U[i].imag());
+    }
+    auto it = seen.find(key);
+    if (it != seen.end()) return it->second;
+    const uint32_t off = uint32_t(P.mats.size() / 2);
+    P.mats.insert(P.mats.end(), k, k + 2 * U.size());
+    seen.emplace(std::move(key), off);
+    return off;
+}
 
 // false when the circuit needs a step the kernel does not execute (gates on
 // more than two qubits, controlled multi-qubit gates, classical control) or
@@ -22,14 +39,8 @@ bool compile_traj(const qgpu_circuit* c, TProgram& P) {
     P.ncreg = c->nc;
     const int n = int(c->nq);
     auto bit = [&](uint64_t q) { return uint8_t(n - 1 - int(q)); };
-    auto add_mat = [&](const std::vector<cd>& U) {
-        uint32_t off = uint32_t(P.mats.size() / 2);
-        for (const cd& z : U) {
-            P.mats.push_back(float(z.real()));
-            P.mats.push_back(float(z.imag()));
-        }
-        return off;
-    };
+    MatPool pool(P);
+    auto add_mat = [&](const std::vector<cd>& U) { return pool.add(U); };
     for (const Step& s : c->steps) {
         uint8_t first = kTNewStep;
         switch (s.kind) {
@@ -123,7 +134,88 @@ uint32_t ins_bits(const TInstr& I) {
 
 } // namespace
 
-void plan_tiles(TProgram& P, int T) {
+void fold_1q_gates(TProgram& P) {
+    using C = std::complex<double>;
+    using M2 = std::array<C, 4>;
+    using M4 = std::array<C, 16>;
+    auto ld = [&](uint32_t off, C* m, int count) {
+        for (int i = 0; i < count; ++i)
+            m[i] = C(P.mats[2 * (size_t(off) + i)], P.mats[2 * (size_t(off) + i) + 1]);
+    };
+    MatPool pool(P);
+    auto store = [&](const C* m, int count) {
+        return pool.add(std::vector<C>(m, m + count));
+    };
+    std::vector<TInstr> out;
+    out.reserve(P.ins.size());
+    M2 g1[32];
+    int pending[32];
+    std::fill(pending, pending + 32, -1);
+    auto flush = [&](uint32_t bits) {
+        for (int b = 0; b < 32; ++b)
+            if ((bits >> b & 1u) && pending[b] >= 0) {
+                out[pending[b]].mat = store(g1[b].data(), 4);
+                pending[b] = -1;
+            }
+    };
+    for (const TInstr& I : P.ins) {
+        if (I.op == kTG1) {
+            const int b = I.b0;
+            M2 G;
+            ld(I.mat, G.data(), 4);
+            if (pending[b] >= 0) { // the later gate acts second: G * g1
+                const M2 A = g1[b];
+                for (int r = 0; r < 2; ++r)
+                    for (int c = 0; c < 2; ++c)
+                        g1[b][r + 2 * c] = G[r] * A[2 * c] + G[r + 2] * A[1 + 2 * c];
+            } else {
+                pending[b] = int(out.size());
+                g1[b] = G;
+                out.push_back(I);
+            }
+        } else if (I.op == kTG2) {
+            M4 M;
+            ld(I.mat, M.data(), 16);
+            for (int side = 0; side < 2; ++side) {
+                const int b = side == 0 ? I.b0 : I.b1;
+                if (pending[b] < 0) continue;
+                // M * (G on the row index's high bit (side 0) or low bit)
+                const M2& G = g1[b];
+                M4 R;
+                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c) {
+                        C acc = 0.0;
+                        for (int k = 0; k < 4; ++k) {
+                            const bool hi = side == 0;
+                            const int kh = k >> 1, kl = k & 1, ch = c >> 1, cl = c & 1;
+                            C lk = hi ? (kl == cl ? G[kh + 2 * ch] : C(0.0))
+                                      : (kh == ch ? G[kl + 2 * cl] : C(0.0));
+                            acc += M[r + 4 * k] * lk;
+                        }
+                        R[r + 4 * c] = acc;
+                    }
+                M = R;
+                out[pending[b]].op = 0; // folded into this gate
+                pending[b] = -1;
+            }
+            TInstr J = I;
+            J.mat = store(M.data(), 16);
+            out.push_back(J);
+        } else {
+            flush(ins_bits(I) | (I.op == kTMeas ? (1u << I.b0) : 0u) |
+                  (I.op == kTTile ? 0xffffffffu : 0u));
+            out.push_back(I);
+        }
+    }
+    flush(0xffffffffu);
+    std::vector<TInstr> kept;
+    kept.reserve(out.size());
+    for (const TInstr& I : out)
+        if (I.op != 0) kept.push_back(I);
+    P.ins.swap(kept);
+}
+
+void plan_tiles(TProgram& P, int T, size_t min_run) {
     const int n = int(P.n);
     if (T < 9 || n <= kTrajMaxQubits || T >= n) return;
     const uint32_t low = 31u; // bits 0..4: 32 consecutive amplitudes per tile row
@@ -144,7 +236,7 @@ void plan_tiles(TProgram& P, int T) {
             S = S2;
             ++j;
         }
-        if (j - i < 2) {
+        if (j - i < std::max<size_t>(min_run, 1)) {
             out.push_back(P.ins[i++]);
             continue;
         }
@@ -212,7 +304,7 @@ int tile_width(qgpu_ctx* ctx, int n) {
         auto it = chosen.find({ctx->device, n});
         if (it != chosen.end()) return it->second;
     }
-    // calibration program: two layers of 1-qubit gates on every qubit and
+    // calibration program: one layer of 1-qubit gates on every qubit and
     // 2-qubit gates on (0,1), (2,3), ... (matrix values do not change the
     // time)
     TProgram P;
@@ -225,7 +317,7 @@ int tile_width(qgpu_ctx* ctx, int n) {
             P.mats.push_back(r == c ? 1.f : 0.f);
             P.mats.push_back(0.f);
         }
-    for (int layer = 0; layer < 2; ++layer) {
+    for (int layer = 0; layer < 1; ++layer) {
         for (int q = 0; q < n; ++q) {
             TInstr I{};
             I.op = kTG1;
@@ -243,8 +335,8 @@ int tile_width(qgpu_ctx* ctx, int n) {
         }
     }
     const uint64_t N = uint64_t(1) << n;
-    const int K = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->num_sms) * 4,
-                                                               (uint64_t(1) << 30) / (N * 8))));
+    const int K = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->num_sms) * 2,
+                                                               (uint64_t(1) << 28) / (N * 8))));
     const size_t b_state = size_t(K) * N * sizeof(float2);
     const size_t b_prog = 4096 * sizeof(TInstr), b_mat = 65536, b_work = K * sizeof(TWork);
     unsigned char* buf = nullptr;
@@ -274,7 +366,9 @@ int tile_width(qgpu_ctx* ctx, int n) {
     int best = 0;
     float best_ms = 0;
     for (int T : {0, 10, 11, 12, 13}) {
-        if (T >= n) continue;
+        // from 18 qubits on the untiled form (one register pass per gate)
+        // is never competitive and the slowest to time
+        if (T >= n || (T == 0 && n >= 18)) continue;
         TProgram Q = P;
         plan_tiles(Q, T);
         if (Q.ins.size() > 4096 || Q.mats.size() * sizeof(float) > b_mat) continue;
@@ -305,7 +399,7 @@ int tile_width(qgpu_ctx* ctx, int n) {
         QG_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (T == 0 || ms < best_ms) {
+        if (best_ms == 0 || ms < best_ms) {
             best = T;
             best_ms = ms;
         }

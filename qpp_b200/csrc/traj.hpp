@@ -1,7 +1,10 @@
 // traj.hpp -- compiled trajectory programs for the shared-memory kernel.
 #pragma once
 
+#include <complex>
 #include <cstdint>
+#include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "internal.hpp"
@@ -72,6 +75,16 @@ struct TProgram {
     std::vector<float> mats; // interleaved complex64
 };
 
+// Appends complex64 copies of gate matrices to a program's pool, each
+// distinct matrix once (a layered circuit drawn from a gate bank stores the
+// bank, not one copy per gate); returns the float2 offset.
+struct MatPool {
+    explicit MatPool(TProgram& p) : P(p) {}
+    uint32_t add(const std::vector<std::complex<double>>& U);
+    TProgram& P;
+    std::unordered_map<std::string, uint32_t> seen;
+};
+
 // Registers above kTrajMaxQubits run either in a slot of `gscratch` or, when
 // every work item of the launch has `inplace` set (gscratch null), directly
 // in the item's own state. `stream` null: the context's stream.
@@ -87,10 +100,47 @@ void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_
 // tiles, so the register is read and written once per run instead of once
 // per gate. Noise and measurement draws keep their untiled instruction
 // counters, so a tiled program gives bit-identical results.
-void plan_tiles(TProgram& P, int T);
+// Noiseless programs only (folding moves gates across step boundaries, where
+// noise would be drawn): every 1-qubit gate is folded into the next gate on
+// its qubit when that gate is a 1- or 2-qubit gate (it commutes past the
+// gates in between, which act on other qubits); products in FP64, rounded
+// to complex64 once. No reference counterpart.
+void fold_1q_gates(TProgram& P);
+// min_run: the shortest run that becomes a pass (2 by default; 1 turns
+// every gate into a pass, as the layer-synchronous batches need).
+void plan_tiles(TProgram& P, int T, size_t min_run = 2);
+
+// One register's tile pass in a layer-synchronous launch: items
+// [first_item, first_item + ceil(2^(n-T) / tiles_per_item)) of the launch
+// run tiles_per_item tiles each; `ins` = the pass's nins gate instructions
+// (bits renumbered within the tile), tile bits at float2 offset tb_off of
+// `mats` (one 32-bit word each).
+struct PassInst {
+    float2* psi;
+    const float2* mats;
+    const TInstr* ins;
+    uint32_t nins;
+    uint32_t tb_off;
+    uint32_t first_item;
+    uint32_t tiles_per_item;
+    uint8_t n, T;
+    uint16_t pad;
+};
+// One launch of k_pass_batch over `ninst` registers (sorted by first_item,
+// nitems items in total) with two 2^tile_bits-amplitude tile buffers
+// (tile_bits >= every T, <= 13). Every register must start on a 16-byte
+// boundary. A bounded wait that gives up sets *err (the context's device
+// error word).
+void launch_pass_batch(qgpu_ctx* ctx, const PassInst* dinsts, int ninst, uint32_t nitems,
+                       int tile_bits, int* err, cudaStream_t stream);
+// The context's device error word (allocated on first use: call outside
+// stream capture), and whether a kernel set it (reading clears it).
+int* ctx_error_flag(qgpu_ctx* ctx);
+int fused_error(qgpu_ctx* ctx);
 // The tile width T (0: untiled) for registers of n qubits on this device,
 // chosen once per (device, n) by timing calibration programs for T in
-// {untiled, 10, 11, 12, 13}; call outside stream capture.
+// {untiled (below 18 qubits), 10, 11, 12, 13} on a one-layer program;
+// call outside stream capture.
 int tile_width(qgpu_ctx* ctx, int n);
 // Pin the width for (device, n) (T >= 0), or drop the choice (T < 0) so the
 // next tile_width() times it again.

@@ -173,8 +173,63 @@ static void run(const TProgram& P, std::vector<f2>& psi) {
     }
 }
 
+// The layer kernel's traversal (k_pass_batch: contiguous item ranges per
+// CTA, a cursor over (register, item, tile)) with the launch layout of the
+// batch runner (items of 2^15 amplitudes): every tile of every register of
+// the launch is visited exactly once, whatever the grid.
+static void check_layer_cursor(std::mt19937& rng) {
+    for (int trial = 0; trial < 50; ++trial) {
+        const int ninst = 1 + int(rng() % 40);
+        std::vector<PassInst> insts(ninst);
+        uint32_t items = 0;
+        for (int j = 0; j < ninst; ++j) {
+            PassInst& q = insts[j];
+            q.n = uint8_t(15 + rng() % 8);
+            q.T = uint8_t(rng() & 1 ? 12 : 13);
+            const uint32_t ntiles = 1u << (q.n - q.T);
+            q.tiles_per_item = std::min<uint32_t>(ntiles, std::max<uint32_t>(1, (1u << 15) >> q.T));
+            q.first_item = items;
+            items += (ntiles + q.tiles_per_item - 1) / q.tiles_per_item;
+        }
+        std::vector<std::vector<int>> seen(ninst);
+        for (int j = 0; j < ninst; ++j) seen[j].assign(1u << (insts[j].n - insts[j].T), 0);
+        const uint32_t grid = 1 + rng() % 300;
+        const uint32_t per = (items + grid - 1) / grid;
+        for (uint32_t bx = 0; bx < grid; ++bx) {
+            const uint32_t it0 = bx * per, it1 = std::min(items, it0 + per);
+            if (it0 >= it1) continue;
+            int lo = 0, hi = ninst - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (insts[mid].first_item <= it0) lo = mid;
+                else hi = mid - 1;
+            }
+            int j = lo;
+            uint32_t it = it0;
+            auto item = [&](uint32_t& t, uint32_t& t1) {
+                const PassInst& P = insts[j];
+                t = (it - P.first_item) * P.tiles_per_item;
+                t1 = std::min(t + P.tiles_per_item, 1u << (P.n - P.T));
+            };
+            uint32_t t, t1;
+            item(t, t1);
+            for (;;) {
+                EXPECT(t < seen[j].size());
+                if (t < seen[j].size()) ++seen[j][t];
+                if (++t < t1) continue;
+                if (++it >= it1) break;
+                while (j + 1 < ninst && insts[j + 1].first_item <= it) ++j;
+                item(t, t1);
+            }
+        }
+        for (int j = 0; j < ninst; ++j)
+            for (int c : seen[j]) EXPECT(c == 1);
+    }
+}
+
 int main() {
     std::mt19937 rng(12345);
+    check_layer_cursor(rng);
     std::normal_distribution<float> g(0.f, 1.f);
     for (int trial = 0; trial < 8; ++trial) {
         const int n = 15 + trial % 4; // 15..18
@@ -228,24 +283,49 @@ int main() {
         }
         // measurements split the runs; the interpreter skips them
         const TProgram U = P;
+        {
+            // folding 1-qubit gates into their next gate: same result up to
+            // complex64 rounding, no more instructions than before
+            TProgram F = U;
+            fold_1q_gates(F);
+            EXPECT(F.ins.size() <= U.ins.size());
+            const uint32_t N = 1u << n;
+            std::vector<f2> a(N), c(N);
+            for (uint32_t i = 0; i < N; ++i) a[i] = c[i] = f2(g(rng), g(rng));
+            run(U, a);
+            run(F, c);
+            double num = 0, den = 0;
+            for (uint32_t i = 0; i < N; ++i) {
+                num = std::max(num, double(std::abs(a[i] - c[i])));
+                den = std::max(den, double(std::abs(a[i])));
+            }
+            EXPECT(num <= 1e-4 * den);
+        }
         const uint32_t N = 1u << n;
         std::vector<f2> x0(N);
         for (auto& v : x0) v = f2(g(rng), g(rng));
         std::vector<f2> ref = x0;
         run(U, ref);
-        for (int T : {9, 12, 14}) {
+        for (int mode = 0; mode < 4; ++mode) {
+            const int T = mode == 3 ? 12 : (mode == 0 ? 9 : (mode == 1 ? 12 : 14));
+            const size_t min_run = mode == 3 ? 1 : 2; // 1: every gate in a pass
             if (T >= n) continue;
             TProgram Q = U;
-            plan_tiles(Q, T);
+            plan_tiles(Q, T, min_run);
             size_t headers = 0, inner = 0;
             for (size_t k = 0; k < Q.ins.size(); ++k)
                 if (Q.ins[k].op == kTTile) {
                     ++headers;
                     inner += Q.ins[k].cmask;
-                    EXPECT(Q.ins[k].cmask >= 2);
+                    EXPECT(Q.ins[k].cmask >= min_run);
                 }
             EXPECT(Q.ins.size() == U.ins.size() + headers);
             EXPECT(headers > 0);
+            if (min_run == 1) { // every gate inside a pass
+                size_t gates = 0;
+                for (const auto& I : U.ins) gates += I.op != kTMeas;
+                EXPECT(inner == gates);
+            }
             std::vector<f2> got = x0;
             run(Q, got);
             EXPECT(std::memcmp(got.data(), ref.data(), N * sizeof(f2)) == 0);
