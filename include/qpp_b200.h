@@ -411,11 +411,12 @@ qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst,
                            qgpu_circuit* const* circuits,
                            qgpu_state* const* states, int form,
                            uint64_t* graph_kernels);
-/* Where the last qgpu_run_batch on ctx spent its time, in milliseconds:
- * phases_ms[0] compiling and tiling the programs on the host, [1] uploading
- * them and capturing + instantiating the graph, [2] the graph on the device
- * (CUDA events), [3] the instances run in the plain form. No reference
- * counterpart. */
+/* Where the last qgpu_run_batch on ctx spent its time, in milliseconds
+ * (phases_ms holds 6 values): [0] compiling and tiling the programs on the
+ * host, [1] uploading them and capturing + instantiating the graph, [2] the
+ * graph on the device (CUDA events), [3] the instances run in the plain
+ * form, [4] the argument checks, [5] releasing the graph after it ran. No
+ * reference counterpart. */
 qgpu_status qgpu_batch_last_phases(qgpu_ctx* ctx, double* phases_ms);
 
 /* ------------------------------------------------------------ serving loop

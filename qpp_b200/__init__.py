@@ -516,10 +516,10 @@ def apply_tc(state, U, target):
 def batch_last_phases(ctx):
     """Milliseconds of the last run_batch on ctx: compile, build (upload +
     graph capture), graph device time, plain-form instances."""
-    out = (ct.c_double * 4)()
+    out = (ct.c_double * 6)()
     check(lib().qgpu_batch_last_phases(ctx.h, out))
     return {"compile_ms": out[0], "build_ms": out[1], "graph_device_ms": out[2],
-            "plain_ms": out[3]}
+            "plain_ms": out[3], "check_ms": out[4], "teardown_ms": out[5]}
 
 
 def traj_tile_width(ctx, n, T=None):

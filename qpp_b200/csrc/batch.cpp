@@ -15,10 +15,15 @@
 // plain form loops over the instances with one kernel launch per gate
 // (qgpu_run_gates, QGPU_FORM_PLAIN).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
+#include <exception>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <set>
+#include <thread>
 
 #include "capi_common.hpp"
 #include "circuit.hpp"
@@ -123,6 +128,12 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
     return guarded([&] {
         need_handle(ctx);
         const char* W = "qgpu_run_batch()";
+        using clk = std::chrono::steady_clock;
+        auto ms_since = [](clk::time_point t) {
+            return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+        };
+        for (double& x : ctx->batch_ms) x = 0;
+        auto t_check = clk::now();
         if (n_inst && (!circuits || !states)) raise(QGPU_ERR_INVALID_ARGUMENT, W, "arrays");
         std::set<const qgpu_state*> seen;
         for (uint32_t i = 0; i < n_inst; ++i) {
@@ -137,25 +148,45 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 if (d != circuits[i]->d) raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, W, "state/circuit");
         }
         if (graph_kernels) *graph_kernels = 0;
-        using clk = std::chrono::steady_clock;
-        auto ms_since = [](clk::time_point t) {
-            return std::chrono::duration<double, std::milli>(clk::now() - t).count();
-        };
-        for (double& x : ctx->batch_ms) x = 0;
+        ctx->batch_ms[4] = ms_since(t_check);
         auto t_compile = clk::now();
         std::vector<uint32_t> plain;
         std::vector<std::pair<uint32_t, qgpu::TProgram>> prog;
+        // compile (and fold, tile, stage) every instance; the programs are
+        // independent, so host threads share the work
+        auto pfor = [](size_t count, const std::function<void(size_t)>& fn) {
+            const size_t nth = std::min<size_t>(
+                std::max(1u, std::thread::hardware_concurrency()), std::max<size_t>(1, count / 16));
+            std::atomic<size_t> next{0};
+            std::exception_ptr first;
+            std::mutex emu;
+            auto body = [&] {
+                try {
+                    for (size_t i; (i = next.fetch_add(1)) < count;) fn(i);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lock(emu);
+                    if (!first) first = std::current_exception();
+                    next = count;
+                }
+            };
+            std::vector<std::thread> th;
+            for (size_t t = 1; t < nth; ++t) th.emplace_back(body);
+            body();
+            for (auto& t : th) t.join();
+            if (first) std::rethrow_exception(first);
+        };
+        std::vector<qgpu::TProgram> progs(n_inst);
+        std::vector<char> ok(n_inst, 0);
+        pfor(n_inst, [&](size_t i) {
+            qgpu::TProgram& P = progs[i];
+            ok[i] = form == 1 && states[i]->prec == QGPU_C64 &&
+                    (states[i]->kind == QGPU_KET ? qgpu::compile_traj(circuits[i], P)
+                                                 : qgpu::compile_traj_rho(circuits[i], P));
+            if (ok[i]) qgpu::fold_1q_gates(P); // batch programs carry no noise
+        });
         for (uint32_t i = 0; i < n_inst; ++i) {
-            qgpu::TProgram P;
-            bool ok = form == 1 && states[i]->prec == QGPU_C64 &&
-                      (states[i]->kind == QGPU_KET ? qgpu::compile_traj(circuits[i], P)
-                                                   : qgpu::compile_traj_rho(circuits[i], P));
-            if (ok) {
-                qgpu::fold_1q_gates(P); // batch programs carry no noise
-                prog.emplace_back(i, std::move(P));
-            } else {
-                plain.push_back(i);
-            }
+            if (ok[i]) prog.emplace_back(i, std::move(progs[i]));
+            else plain.push_back(i);
         }
         if (!prog.empty()) {
             // Registers above shared-memory size whose programs are all gates
@@ -170,25 +201,30 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                         return false;
                 return true;
             };
-            std::map<uint32_t, int> tile_of;
+            std::map<uint32_t, int> tile_of; // tuned serially (it times on the GPU)
+            for (auto& pr : prog) {
+                const uint32_t n = pr.second.n;
+                if (n > uint32_t(qgpu::kTrajMaxQubits) && !tile_of.count(n))
+                    tile_of.emplace(n, qgpu::tile_width(ctx, int(n)));
+            }
             std::vector<char> layered(prog.size(), 0);
-            int layer_bits = 0;
-            for (size_t k = 0; k < prog.size(); ++k) {
+            pfor(prog.size(), [&](size_t k) {
                 qgpu::TProgram& P = prog[k].second;
                 const uint32_t n = P.n;
-                if (n <= uint32_t(qgpu::kTrajMaxQubits)) continue;
-                auto it = tile_of.find(n);
-                if (it == tile_of.end()) it = tile_of.emplace(n, qgpu::tile_width(ctx, int(n))).first;
-                if (all_gates(P) && !P.ins.empty()) {
-                    // two 2^T tiles per CTA: T = 12 keeps three CTAs per SM
-                    const int T = std::min(it->second ? it->second : 12, 12);
-                    qgpu::plan_tiles(P, T, 1);
-                    layered[k] = 1;
-                    layer_bits = std::max(layer_bits, T);
-                } else {
-                    qgpu::plan_tiles(P, it->second);
+                if (n > uint32_t(qgpu::kTrajMaxQubits)) {
+                    const int tw = tile_of.at(n);
+                    if (all_gates(P) && !P.ins.empty()) {
+                        // two 2^T tiles per CTA: T = 12 keeps three CTAs per SM
+                        qgpu::plan_tiles(P, std::min(tw ? tw : 12, 12), 1);
+                        layered[k] = 1;
+                    } else {
+                        qgpu::plan_tiles(P, tw);
+                    }
                 }
-            }
+            });
+            int layer_bits = 0;
+            for (size_t k = 0; k < prog.size(); ++k)
+                if (layered[k]) layer_bits = std::max(layer_bits, std::min(tile_of.at(prog[k].second.n) ? tile_of.at(prog[k].second.n) : 12, 12));
             ctx->batch_ms[0] = ms_since(t_compile);
             auto t_build = clk::now();
             // device copies of all programs, per-CTA work items grouped by size
@@ -382,10 +418,12 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             float gms = 0;
             QG_CUDA(cudaEventElapsedTime(&gms, g0, g1));
             ctx->batch_ms[2] = gms;
+            auto t_tear = clk::now();
             cudaGraphExecDestroy(exec);
             cudaGraphDestroy(graph);
             if (dflag && qgpu::fused_error(ctx))
                 raise(QGPU_ERR_TIMEOUT, W, "a bounded wait of the layer kernel gave up");
+            ctx->batch_ms[5] = ms_since(t_tear);
             if (graph_kernels) *graph_kernels = ranges.size() + launches.size();
         }
         auto t_plain = clk::now();
@@ -398,6 +436,6 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
 extern "C" qgpu_status qgpu_batch_last_phases(qgpu_ctx* ctx, double* phases_ms) {
     return guarded([&] {
         need_handle(ctx);
-        if (phases_ms) std::copy(ctx->batch_ms, ctx->batch_ms + 4, phases_ms);
+        if (phases_ms) std::copy(ctx->batch_ms, ctx->batch_ms + 6, phases_ms);
     });
 }

@@ -33,8 +33,9 @@ struct qgpu_ctx {
     std::atomic<bool> closing{false};
     // phases of the last qgpu_run_batch (milliseconds): programs compiled and
     // tiled on the host, buffers uploaded and the graph captured and
-    // instantiated, the graph's device time, the plain-form instances
-    double batch_ms[4] = {0, 0, 0, 0};
+    // instantiated, the graph's device time, the plain-form instances, the
+    // argument checks, the teardown after the graph
+    double batch_ms[6] = {0, 0, 0, 0, 0, 0};
 };
 
 struct qgpu_state {
