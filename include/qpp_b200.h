@@ -207,6 +207,37 @@ qgpu_status qgpu_sample(const qgpu_state* s, const uint64_t* target, uint32_t k,
 qgpu_status qgpu_measure_seq(const qgpu_state* s, const uint64_t* target, uint32_t k,
                              int destructive, uint64_t seed, const uint64_t* forced,
                              uint64_t* results, double* probs, qgpu_state** out);
+/* Replaces qpp::measure(A, Ks, target, dims, destructive)
+ * (instruments.hpp:371-494): each of the nK Kraus operators (DK x DK,
+ * consecutive, column-major, DK = the targets' dimension) is applied on the
+ * targets (K psi, or K rho K^dagger); probs[i] = ||K psi||^2 or |tr|, outs[i]
+ * = the normalised post-measurement state (a new handle; the targets traced
+ * out when destructive, which makes a ket's result a density matrix; NULL
+ * where probs[i] == 0); *result = one std::discrete_distribution draw of a
+ * std::mt19937 seeded with `seed`. outs may be NULL. All probabilities zero:
+ * QGPU_ERR_DIVISION_BY_ZERO. */
+qgpu_status qgpu_measure_kraus(const qgpu_state* s, const double* Ks, uint32_t nK,
+                               uint64_t DK, const uint64_t* target, uint32_t k,
+                               int destructive, uint64_t seed, uint64_t* result,
+                               double* probs, qgpu_state** outs);
+/* Replaces qpp::measure(A, V, target, dims, destructive)
+ * (instruments.hpp:587-712): the M columns of V (rows x M, rows = the
+ * targets' dimension) as rank-1 projectors; a ket measured destructively
+ * keeps <v_i|psi> over the targets (a ket of the other subsystems). Outputs
+ * as qgpu_measure_kraus. */
+qgpu_status qgpu_measure_basis(const qgpu_state* s, const double* V, uint64_t rows,
+                               uint64_t M, const uint64_t* target, uint32_t k,
+                               int destructive, uint64_t seed, uint64_t* result,
+                               double* probs, qgpu_state** outs);
+/* Replaces qpp::reset(A, target, dims) (instruments.hpp:1148-1206): a seeded
+ * non-destructive measure_seq, then Xd^(d - result_i) on each target, with
+ * d = dims[i] (qpp indexes dims by the target's position). New handle. */
+qgpu_status qgpu_reset(const qgpu_state* s, const uint64_t* target, uint32_t k,
+                       uint64_t seed, qgpu_state** out);
+/* Replaces qpp::discard(A, target, dims) (instruments.hpp:1243-1292): a seeded
+ * destructive measure_seq; the post-measurement state as a new handle. */
+qgpu_status qgpu_discard(const qgpu_state* s, const uint64_t* target, uint32_t k,
+                         uint64_t seed, qgpu_state** out);
 
 /* ------------------------------------- value-semantics entry points (host)
  * These mirror qpp's free functions exactly: the state is a host array with
@@ -389,7 +420,7 @@ qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double p_depol,
                               uint32_t* events, uint32_t max_events);
 /* Tile width of the trajectory kernel for registers of n qubits (15-22) on
  * this context's device: set_T = -1 queries (timing the candidates
- * {untiled (below 18 qubits), 10, 11, 12, 13} once on first use), 0 pins the
+ * {untiled (below 17 qubits), 10, 11, 12, 13} once on first use), 0 pins the
  * untiled form, 9..14 (< n) pins that width, -2 drops the choice so it is
  * timed again. No reference counterpart. *chosen (if not NULL) receives the
  * width now in force. */

@@ -14,6 +14,8 @@
 //   qpp_b200::syspermute(A, perm, dims)                     operations.hpp:2386
 //   qpp_b200::sample(num_samples, A, target, dims, seed)    instruments.hpp:856
 //   qpp_b200::measure_seq(A, target, dims, destructive, seed) instruments.hpp:985
+//   qpp_b200::measure(A, Ks | V, target, dims, destructive, seed) instruments.hpp:371, :587
+//   qpp_b200::reset(A, target, dims, seed), discard(...)    instruments.hpp:1148, :1243
 //
 // Matrices are qpp_b200::cmat (column-major std::complex<double>, rows x
 // cols; a ket is D x 1). When Eigen is available the same functions accept
@@ -347,6 +349,93 @@ measure_seq(const cmat& A, const std::vector<idx>& target, const std::vector<idx
     detail::check(qgpu_state_download_c128(o.s, out.raw()));
     return {std::vector<idx>(res.begin(), res.begin() + t.size()),
             std::vector<double>(ps.begin(), ps.begin() + t.size()), out};
+}
+
+namespace detail {
+inline cmat download(qgpu_state* s) {
+    qgpu_kind kind = QGPU_KET;
+    uint64_t D = 0;
+    check(qgpu_state_info(s, &kind, nullptr, nullptr, nullptr, &D));
+    cmat out(D, kind == QGPU_KET ? 1 : D);
+    check(qgpu_state_download_c128(s, out.raw()));
+    return out;
+}
+inline std::tuple<idx, std::vector<double>, std::vector<cmat>>
+collect(uint64_t r, const std::vector<double>& probs, std::vector<qgpu_state*>& outs) {
+    std::vector<cmat> states(outs.size());
+    for (size_t i = 0; i < outs.size(); ++i)
+        if (outs[i]) {
+            StateHolder h;
+            h.s = outs[i];
+            states[i] = download(outs[i]);
+        }
+    return {idx(r), probs, states};
+}
+} // namespace detail
+
+// qpp::measure(A, Ks, target, dims, destructive) (instruments.hpp:371-494):
+// (result, probabilities, post-measurement states; empty where a probability
+// is 0), the result drawn from a std::mt19937 seeded with `seed`.
+inline std::tuple<idx, std::vector<double>, std::vector<cmat>>
+measure(const cmat& A, const std::vector<cmat>& Ks, const std::vector<idx>& target,
+        const std::vector<idx>& dims, bool destructive = true, uint64_t seed = 0) {
+    detail::StateHolder h;
+    detail::upload_checked(A, dims, "qpp::measure()", h);
+    auto t = detail::u64(target);
+    const idx DK = Ks.empty() ? 0 : Ks[0].rows();
+    std::vector<cplx> packed;
+    for (const cmat& K : Ks) {
+        if (K.rows() != DK || K.cols() != DK)
+            throw exception::DimsNotEqual("qpp::measure()", "K");
+        packed.insert(packed.end(), K.data_.begin(), K.data_.end());
+    }
+    std::vector<double> probs(Ks.size() + 1);
+    std::vector<qgpu_state*> outs(Ks.size() + 1, nullptr);
+    uint64_t r = 0;
+    detail::check(qgpu_measure_kraus(h.s, reinterpret_cast<const double*>(packed.data()),
+                                     uint32_t(Ks.size()), DK, detail::ptr(t), uint32_t(t.size()),
+                                     destructive ? 1 : 0, seed, &r, probs.data(), outs.data()));
+    probs.resize(Ks.size());
+    outs.resize(Ks.size());
+    return detail::collect(r, probs, outs);
+}
+
+// qpp::measure(A, V, target, dims, destructive) (instruments.hpp:587-712).
+inline std::tuple<idx, std::vector<double>, std::vector<cmat>>
+measure(const cmat& A, const cmat& V, const std::vector<idx>& target,
+        const std::vector<idx>& dims, bool destructive = true, uint64_t seed = 0) {
+    detail::StateHolder h;
+    detail::upload_checked(A, dims, "qpp::measure()", h);
+    auto t = detail::u64(target);
+    std::vector<double> probs(V.cols() + 1);
+    std::vector<qgpu_state*> outs(V.cols() + 1, nullptr);
+    uint64_t r = 0;
+    detail::check(qgpu_measure_basis(h.s, V.raw(), V.rows(), V.cols(), detail::ptr(t),
+                                     uint32_t(t.size()), destructive ? 1 : 0, seed, &r,
+                                     probs.data(), outs.data()));
+    probs.resize(V.cols());
+    outs.resize(V.cols());
+    return detail::collect(r, probs, outs);
+}
+
+// qpp::reset(A, target, dims) (instruments.hpp:1148-1206), seeded.
+inline cmat reset(const cmat& A, const std::vector<idx>& target, const std::vector<idx>& dims,
+                  uint64_t seed = 0) {
+    detail::StateHolder h, o;
+    detail::upload_checked(A, dims, "qpp::reset()", h);
+    auto t = detail::u64(target);
+    detail::check(qgpu_reset(h.s, detail::ptr(t), uint32_t(t.size()), seed, &o.s));
+    return detail::download(o.s);
+}
+
+// qpp::discard(A, target, dims) (instruments.hpp:1243-1292), seeded.
+inline cmat discard(const cmat& A, const std::vector<idx>& target, const std::vector<idx>& dims,
+                    uint64_t seed = 0) {
+    detail::StateHolder h, o;
+    detail::upload_checked(A, dims, "qpp::discard()", h);
+    auto t = detail::u64(target);
+    detail::check(qgpu_discard(h.s, detail::ptr(t), uint32_t(t.size()), seed, &o.s));
+    return detail::download(o.s);
 }
 
 #ifdef QPP_B200_HAS_EIGEN

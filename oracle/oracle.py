@@ -230,3 +230,100 @@ def sample(state, target, dims, num_samples, seed=0):
                                ct.c_uint64(num_samples), ct.c_uint64(seed),
                                out.ctypes.data_as(u64p)))
     return out[: num_samples * k].reshape(num_samples, k).astype(np.int64)
+
+
+def discrete_draw(weights, seed=0):
+    """One std::discrete_distribution draw from std::mt19937(seed)."""
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+    L = lib()
+    L.oracle_discrete_draw.restype = ct.c_uint64
+    return int(L.oracle_discrete_draw(_dp(w), ct.c_uint64(w.size), ct.c_uint64(seed)))
+
+
+def _is_ket(a):
+    a = np.asarray(a)
+    return a.ndim == 1 or a.shape[1] == 1
+
+
+def measure_kraus(state, Ks, target, dims, destructive=True, seed=0):
+    """qpp::measure(A, Ks, target, dims, destructive), instruments.hpp:371-494:
+    every Kraus operator applied on the targets (K psi, or K rho K^dagger),
+    its probability, the normalised post-measurement state (targets traced
+    out when destructive: a density matrix even for a ket), then one draw.
+    Returns (result, probs, states with None where the probability is 0)."""
+    ket = _is_ket(state)
+    probs, outs = [], []
+    for K in Ks:
+        tmp = apply(state, K, target, dims)
+        if ket:
+            p = float(np.linalg.norm(tmp)) ** 2
+            out = None
+            if p > 0:
+                tmp = tmp / np.sqrt(p)
+                out = ptrace(tmp, target, dims) if destructive else tmp
+        else:
+            if destructive:
+                tmp = ptrace(tmp, target, dims)
+            p = abs(np.trace(tmp))
+            out = tmp / p if p > 0 else None
+        probs.append(p)
+        outs.append(out)
+    return discrete_draw(probs, seed), probs, outs
+
+
+def _ip(v, psi, target, dims):
+    """qpp::ip(phi, psi, subsys, dims): sum over the target digits of
+    conj(phi) psi, the other digits kept in their order."""
+    n = len(dims)
+    x = np.asarray(psi).reshape([int(d) for d in dims])
+    vv = np.conj(np.asarray(v).reshape([int(dims[t]) for t in target]))
+    rest = [q for q in range(n) if q not in target]
+    x = np.transpose(x, list(target) + rest)
+    out = np.tensordot(vv, x, axes=(list(range(len(target))), list(range(len(target)))))
+    return out.reshape(-1)
+
+
+def measure_basis(state, V, target, dims, destructive=True, seed=0):
+    """qpp::measure(A, V, target, dims, destructive), instruments.hpp:587-712:
+    the columns of V as rank-1 projectors; a ket measured destructively keeps
+    <v_i| psi> over the targets (a ket), otherwise prj(v_i) is applied; a
+    density matrix goes through measure_kraus with K_i = v_i v_i^dagger."""
+    V = np.asarray(V, dtype=np.complex128)
+    if not _is_ket(state):
+        return measure_kraus(state, [np.outer(V[:, i], V[:, i].conj()) for i in range(V.shape[1])],
+                             target, dims, destructive, seed)
+    psi = np.asarray(state).reshape(-1)
+    probs, outs = [], []
+    for i in range(V.shape[1]):
+        v = V[:, i]
+        o = _ip(v, psi, target, dims) if destructive else \
+            apply(psi, np.outer(v, v.conj()), target, dims)
+        nrm = float(np.linalg.norm(o))
+        p = nrm * nrm
+        probs.append(p)
+        outs.append(o / nrm if p > 0 else None)
+    return discrete_draw(probs, seed), probs, outs
+
+
+def _xd_power(d, k):
+    X = np.zeros((d, d), dtype=np.complex128)
+    for j in range(d):
+        X[(j + 1) % d, j] = 1
+    return np.linalg.matrix_power(X, k)
+
+
+def reset(state, target, dims, seed=0):
+    """qpp::reset(A, target, dims), instruments.hpp:1148-1206: measure_seq
+    without destruction, then Xd^(d - result) on each target; d is dims[i]
+    for the i-th target (qpp indexes dims by the target's position)."""
+    res, _, out, nd = measure_seq(state, target, dims, destructive=False, seed=seed)
+    for i, t in enumerate(target):
+        d = int(dims[i])
+        out = apply(out, _xd_power(d, d - res[i]), [t], dims)
+    return out
+
+
+def discard(state, target, dims, seed=0):
+    """qpp::discard(A, target, dims), instruments.hpp:1243-1292: measure_seq
+    with destruction, the post-measurement state only."""
+    return measure_seq(state, target, dims, destructive=True, seed=seed)[2]

@@ -971,6 +971,14 @@ int oracle_sample(const double* state, idx rows, idx cols, const uint64_t* targe
 // Philox4x32-10 (Salmon et al., SC'11) + Box-Muller, the same counter-based
 // stream the product uses for qgpu_state_fill_gaussian, so the CPU baseline
 // and the GPU start from the same seeded input. Not normalised here.
+// One std::discrete_distribution draw over w[0..n) from std::mt19937(seed):
+// the sampling step of qpp::measure (instruments.hpp:289-292, :488-491).
+extern "C" uint64_t oracle_discrete_draw(const double* w, uint64_t n, uint64_t seed) {
+    std::mt19937 gen(static_cast<uint32_t>(seed));
+    std::discrete_distribution<uint64_t> dd(w, w + n);
+    return dd(gen);
+}
+
 extern "C" void oracle_fill_gaussian(double* out, uint64_t n, uint64_t seed) {
 #pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < n; ++i) {

@@ -298,6 +298,47 @@ class State:
             res[key] = res.get(key, 0) + 1
         return res
 
+    def _measure_out(self, fn, n, *args):
+        res = ct.c_uint64()
+        probs = np.zeros(max(n, 1), dtype=np.float64)
+        outs = (vp * max(n, 1))()
+        check(fn(*args, ct.byref(res), _dp(probs), outs))
+        states = [State(self.ctx, KET, None, handle=vp(outs[i])) if outs[i] else None
+                  for i in range(n)]
+        return int(res.value), [float(x) for x in probs[:n]], states
+
+    def measure_kraus(self, Ks, target, destructive=True, seed=0):
+        """qpp::measure(A, Ks, target, dims, destructive): (result, probs,
+        post-measurement States, None where the probability is 0)."""
+        packed, DA = _pack_kraus(Ks)
+        t, tp, nt = _u64(target)
+        return self._measure_out(lib().qgpu_measure_kraus, len(Ks), self.h, _dp(packed),
+                                 ct.c_uint32(len(Ks)), ct.c_uint64(DA), tp, ct.c_uint32(nt),
+                                 ct.c_int(1 if destructive else 0), ct.c_uint64(seed))
+
+    def measure_basis(self, V, target, destructive=True, seed=0):
+        """qpp::measure(A, V, target, dims, destructive) with the columns of V."""
+        V = _mat(V)
+        t, tp, nt = _u64(target)
+        return self._measure_out(lib().qgpu_measure_basis, V.shape[1], self.h, _dp(V),
+                                 ct.c_uint64(V.shape[0]), ct.c_uint64(V.shape[1]), tp,
+                                 ct.c_uint32(nt), ct.c_int(1 if destructive else 0),
+                                 ct.c_uint64(seed))
+
+    def reset(self, target, seed=0):
+        """qpp::reset(A, target, dims): a new State."""
+        t, tp, nt = _u64(target)
+        h = vp()
+        check(lib().qgpu_reset(self.h, tp, ct.c_uint32(nt), ct.c_uint64(seed), ct.byref(h)))
+        return State(self.ctx, self.kind, None, handle=h)
+
+    def discard(self, target, seed=0):
+        """qpp::discard(A, target, dims): a new State."""
+        t, tp, nt = _u64(target)
+        h = vp()
+        check(lib().qgpu_discard(self.h, tp, ct.c_uint32(nt), ct.c_uint64(seed), ct.byref(h)))
+        return State(self.ctx, self.kind, None, handle=h)
+
     def measure_seq(self, target, destructive=True, seed=0, forced=None):
         """qpp::measure_seq(A, target, dims, destructive): (results, probs,
         post-measurement State); this state is unchanged."""

@@ -882,4 +882,237 @@ qgpu_status qgpu_measure_seq(const qgpu_state* s, const uint64_t* target, uint32
     });
 }
 
+
+namespace {
+
+// one std::discrete_distribution draw from std::mt19937(seed)
+uint64_t draw_seeded(const std::vector<double>& w, uint64_t seed) {
+    std::mt19937 gen(static_cast<std::mt19937::result_type>(seed));
+    return qgpu::draw(gen, w);
+}
+
+void scale_state(qgpu_state* s, double f) {
+    qgpu::launch_scale(s->ctx, s->prec, s->data, s->elems, qgpu::cd(f, 0.0));
+}
+
+const char* kMeasure = "qpp::measure()";
+
+void check_kraus_shape(const qgpu_state* s, const std::vector<uint64_t>& tgt, uint32_t nK,
+                       uint64_t DK) {
+    if (!targets_ok(tgt, s->dims.size()))
+        raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, kMeasure, "dims/target");
+    uint64_t Dsub = 1;
+    for (uint64_t t : tgt) Dsub *= s->dims[t];
+    if (nK == 0) raise(QGPU_ERR_ZERO_SIZE, kMeasure, "Ks");
+    if (DK != Dsub) raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, kMeasure, "Ks[0]");
+}
+
+// instruments.hpp:429-486 for operators Ks (nK consecutive DK x DK)
+void measure_ops(const qgpu_state* s, const qgpu::cd* Ks, uint32_t nK, uint64_t DK,
+                 const std::vector<uint64_t>& tgt, bool destructive, std::vector<double>& probs,
+                 std::vector<qgpu_state*>& outs) {
+    probs.assign(nK, 0.0);
+    outs.assign(nK, nullptr);
+    try {
+        for (uint32_t i = 0; i < nK; ++i) {
+            qgpu_state* c = qgpu::copy_state(s);
+            qgpu::op_apply(c, Ks + size_t(i) * DK * DK, DK, tgt);
+            if (s->kind == QGPU_KET) {
+                const double p = qgpu::op_norm2(c);
+                probs[i] = p;
+                if (p > 0) {
+                    scale_state(c, 1.0 / std::sqrt(p));
+                    if (destructive) {
+                        qgpu_state* r = qgpu::op_ptrace(c, tgt);
+                        qgpu::free_state(c);
+                        c = r;
+                    }
+                    outs[i] = c;
+                } else {
+                    qgpu::free_state(c);
+                }
+            } else {
+                if (destructive) {
+                    qgpu_state* r = qgpu::op_ptrace(c, tgt);
+                    qgpu::free_state(c);
+                    c = r;
+                }
+                const double p = std::abs(qgpu::op_trace(c));
+                probs[i] = p;
+                if (p > 0) {
+                    scale_state(c, 1.0 / p);
+                    outs[i] = c;
+                } else {
+                    qgpu::free_state(c);
+                }
+            }
+        }
+    } catch (...) {
+        for (auto*& o : outs) qgpu::free_state(o);
+        throw;
+    }
+}
+
+void finish_measure(const std::vector<double>& probs, std::vector<qgpu_state*>& outs,
+                    uint64_t seed, uint64_t* result, double* probs_out, qgpu_state** outs_out) {
+    bool any = false;
+    for (double p : probs) any = any || p > 0;
+    if (!any) {
+        for (auto*& o : outs) qgpu::free_state(o);
+        raise(QGPU_ERR_DIVISION_BY_ZERO, kMeasure, "all outcome probabilities are zero");
+    }
+    const uint64_t r = draw_seeded(probs, seed);
+    if (result) *result = r;
+    if (probs_out) std::copy(probs.begin(), probs.end(), probs_out);
+    for (size_t i = 0; i < outs.size(); ++i) {
+        if (outs_out) outs_out[i] = outs[i];
+        else qgpu::free_state(outs[i]);
+    }
+}
+
+} // namespace
+
+// qpp::measure(A, Ks, target, dims, destructive) (instruments.hpp:371-494).
+qgpu_status qgpu_measure_kraus(const qgpu_state* s, const double* Ks, uint32_t nK, uint64_t DK,
+                               const uint64_t* target, uint32_t k, int destructive,
+                               uint64_t seed, uint64_t* result, double* probs,
+                               qgpu_state** outs) {
+    return guarded([&] {
+        need_handle(s);
+        std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
+        check_kraus_shape(s, tgt, nK, DK);
+        if (!Ks) raise(QGPU_ERR_INVALID_ARGUMENT, kMeasure, "Ks");
+        std::vector<double> pr;
+        std::vector<qgpu_state*> os;
+        measure_ops(s, reinterpret_cast<const qgpu::cd*>(Ks), nK, DK, tgt, destructive != 0, pr,
+                    os);
+        QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        finish_measure(pr, os, seed, result, probs, outs);
+    });
+}
+
+// qpp::measure(A, V, target, dims, destructive) (instruments.hpp:587-712):
+// the M columns of V (Dsub x M, column-major) as rank-1 projectors.
+qgpu_status qgpu_measure_basis(const qgpu_state* s, const double* V, uint64_t rows, uint64_t M,
+                               const uint64_t* target, uint32_t k, int destructive,
+                               uint64_t seed, uint64_t* result, double* probs,
+                               qgpu_state** outs) {
+    return guarded([&] {
+        need_handle(s);
+        std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
+        if (!targets_ok(tgt, s->dims.size()))
+            raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, kMeasure, "dims/target");
+        uint64_t Dsub = 1;
+        for (uint64_t t : tgt) Dsub *= s->dims[t];
+        if (rows * M == 0 || !V) raise(QGPU_ERR_ZERO_SIZE, kMeasure, "V");
+        if (rows != Dsub) raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, kMeasure, "V");
+        const qgpu::cd* v = reinterpret_cast<const qgpu::cd*>(V);
+        std::vector<qgpu::cd> Ks(size_t(M) * Dsub * Dsub);
+        for (uint64_t i = 0; i < M; ++i) // K_i = v_i v_i^dagger
+            for (uint64_t c = 0; c < Dsub; ++c)
+                for (uint64_t r = 0; r < Dsub; ++r)
+                    Ks[i * Dsub * Dsub + r + c * Dsub] = v[i * Dsub + r] * std::conj(v[i * Dsub + c]);
+        std::vector<double> pr;
+        std::vector<qgpu_state*> os;
+        if (s->kind == QGPU_KET && destructive) {
+            // <v_i| psi> over the targets (qpp::ip): E = |0><v_i| on the
+            // targets, then the targets dropped at digit 0 -- a ket
+            pr.assign(M, 0.0);
+            os.assign(M, nullptr);
+            try {
+                std::vector<uint64_t> zeros(tgt.size(), 0);
+                for (uint64_t i = 0; i < M; ++i) {
+                    std::vector<qgpu::cd> E(Dsub * Dsub, 0.0);
+                    for (uint64_t c = 0; c < Dsub; ++c) E[0 + c * Dsub] = std::conj(v[i * Dsub + c]);
+                    qgpu_state* c0 = qgpu::copy_state(s);
+                    qgpu::op_apply(c0, E.data(), Dsub, tgt);
+                    qgpu_state* o = qgpu::drop(c0, tgt, zeros);
+                    qgpu::free_state(c0);
+                    const double p = qgpu::op_norm2(o);
+                    pr[i] = p;
+                    if (p > 0) {
+                        scale_state(o, 1.0 / std::sqrt(p));
+                        os[i] = o;
+                    } else {
+                        qgpu::free_state(o);
+                    }
+                }
+            } catch (...) {
+                for (auto*& o : os) qgpu::free_state(o);
+                throw;
+            }
+        } else {
+            measure_ops(s, Ks.data(), uint32_t(M), Dsub, tgt, destructive != 0, pr, os);
+        }
+        QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        finish_measure(pr, os, seed, result, probs, outs);
+    });
+}
+
+// qpp::reset(A, target, dims) (instruments.hpp:1148-1206): measure_seq
+// without destruction, then Xd^(d - result) on each target, d = dims[i] for
+// the i-th target as qpp indexes it.
+qgpu_status qgpu_reset(const qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t seed,
+                       qgpu_state** out) {
+    return guarded([&] {
+        need_handle(s);
+        const char* W = "qpp::reset()";
+        if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "out");
+        std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
+        if (!targets_ok(tgt, s->dims.size())) raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
+        std::vector<uint64_t> res;
+        if (k) {
+            std::mt19937 gen(static_cast<std::mt19937::result_type>(seed));
+            res = qgpu::sample_once(s, tgt, qgpu::canonical(gen));
+        }
+        qgpu_state* c = qgpu::copy_state(s);
+        try {
+            std::vector<double> ps;
+            qgpu::collapse_seq(c, tgt, false, res, ps);
+            for (uint32_t i = 0; i < k; ++i) {
+                const uint64_t d = s->dims[i];
+                if (d != s->dims[tgt[i]])
+                    raise(QGPU_ERR_MATRIX_MISMATCH_SUBSYS, "qpp::apply()", "A/dims/target");
+                // Xd^(d - r): |j> -> |j + d - r mod d>
+                std::vector<qgpu::cd> X(d * d, 0.0);
+                for (uint64_t j = 0; j < d; ++j) X[((j + d - res[i]) % d) + j * d] = 1.0;
+                qgpu::op_apply(c, X.data(), d, {tgt[i]});
+            }
+        } catch (...) {
+            qgpu::free_state(c);
+            throw;
+        }
+        QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        *out = c;
+    });
+}
+
+// qpp::discard(A, target, dims) (instruments.hpp:1243-1292): measure_seq
+// with destruction, keeping only the post-measurement state.
+qgpu_status qgpu_discard(const qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t seed,
+                         qgpu_state** out) {
+    return guarded([&] {
+        need_handle(s);
+        const char* W = "qpp::discard()";
+        if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "out");
+        std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
+        if (!targets_ok(tgt, s->dims.size())) raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
+        std::vector<uint64_t> res;
+        if (k) {
+            std::mt19937 gen(static_cast<std::mt19937::result_type>(seed));
+            res = qgpu::sample_once(s, tgt, qgpu::canonical(gen));
+        }
+        qgpu_state* c = qgpu::copy_state(s);
+        try {
+            std::vector<double> ps;
+            qgpu::collapse_seq(c, tgt, true, res, ps);
+        } catch (...) {
+            qgpu::free_state(c);
+            throw;
+        }
+        QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        *out = c;
+    });
+}
+
 } // extern "C"

@@ -304,9 +304,9 @@ int tile_width(qgpu_ctx* ctx, int n) {
         auto it = chosen.find({ctx->device, n});
         if (it != chosen.end()) return it->second;
     }
-    // calibration program: one layer of 1-qubit gates on every qubit and
+    // calibration program: two layers of 1-qubit gates on every qubit and
     // 2-qubit gates on (0,1), (2,3), ... (matrix values do not change the
-    // time)
+    // time; one layer under-rates the narrower tiles)
     TProgram P;
     P.n = uint32_t(n);
     const float h = 0.70710678f;
@@ -317,7 +317,7 @@ int tile_width(qgpu_ctx* ctx, int n) {
             P.mats.push_back(r == c ? 1.f : 0.f);
             P.mats.push_back(0.f);
         }
-    for (int layer = 0; layer < 1; ++layer) {
+    for (int layer = 0; layer < 2; ++layer) {
         for (int q = 0; q < n; ++q) {
             TInstr I{};
             I.op = kTG1;
@@ -335,8 +335,8 @@ int tile_width(qgpu_ctx* ctx, int n) {
         }
     }
     const uint64_t N = uint64_t(1) << n;
-    const int K = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->num_sms) * 2,
-                                                               (uint64_t(1) << 28) / (N * 8))));
+    const int K = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->num_sms) * 4,
+                                                               (uint64_t(1) << 29) / (N * 8))));
     const size_t b_state = size_t(K) * N * sizeof(float2);
     const size_t b_prog = 4096 * sizeof(TInstr), b_mat = 65536, b_work = K * sizeof(TWork);
     unsigned char* buf = nullptr;
@@ -366,9 +366,9 @@ int tile_width(qgpu_ctx* ctx, int n) {
     int best = 0;
     float best_ms = 0;
     for (int T : {0, 10, 11, 12, 13}) {
-        // from 18 qubits on the untiled form (one register pass per gate)
+        // from 17 qubits on the untiled form (one register pass per gate)
         // is never competitive and the slowest to time
-        if (T >= n || (T == 0 && n >= 18)) continue;
+        if (T >= n || (T == 0 && n >= 17)) continue;
         TProgram Q = P;
         plan_tiles(Q, T);
         if (Q.ins.size() > 4096 || Q.mats.size() * sizeof(float) > b_mat) continue;

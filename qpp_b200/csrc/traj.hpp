@@ -139,7 +139,7 @@ int* ctx_error_flag(qgpu_ctx* ctx);
 int fused_error(qgpu_ctx* ctx);
 // The tile width T (0: untiled) for registers of n qubits on this device,
 // chosen once per (device, n) by timing calibration programs for T in
-// {untiled (below 18 qubits), 10, 11, 12, 13} on a one-layer program;
+// {untiled (below 17 qubits), 10, 11, 12, 13} on a two-layer program;
 // call outside stream capture.
 int tile_width(qgpu_ctx* ctx, int n);
 // Pin the width for (device, n) (T >= 0), or drop the choice (T < 0) so the

@@ -94,6 +94,21 @@ int main() {
         caught = e.where() == "qpp::sample()" && e.detail() == "num_samples";
     }
     EXPECT(caught);
+    // measuring the first qubit of the Bell state with projectors / a basis
+    cmat P0(2, 2), P1(2, 2);
+    P0(0, 0) = 1;
+    P1(1, 1) = 1;
+    auto [mr, mp, ms] = measure(bell, std::vector<cmat>{P0, P1}, {0}, {2, 2}, true, 5);
+    EXPECT(mp.size() == 2 && std::abs(mp[0] - 0.5) < 1e-15 && std::abs(mp[1] - 0.5) < 1e-15);
+    EXPECT(ms[mr].rows() == 2 && ms[mr].cols() == 2 && std::abs(ms[mr](mr, mr) - 1.0) < 1e-15);
+    cmat I2(2, 2);
+    I2(0, 0) = I2(1, 1) = 1;
+    auto [br, bp, bs] = measure(bell, I2, {1}, {2, 2}, true, 5);
+    EXPECT(bs[br].rows() == 2 && bs[br].cols() == 1 && std::abs(std::abs(bs[br](br)) - 1.0) < 1e-15);
+    cmat z = reset(bell, {0, 1}, {2, 2}, 9);
+    EXPECT(std::abs(std::abs(z(0)) - 1.0) < 1e-15);
+    cmat dsc = discard(bell, {0}, {2, 2}, 9);
+    EXPECT(dsc.rows() == 2 && dsc.cols() == 1);
     std::printf(fails ? "shim FAILED (%d)\n" : "shim ok\n", fails);
     return fails ? 1 : 0;
 }

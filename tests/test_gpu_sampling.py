@@ -13,7 +13,10 @@ execute(reps) semantics.
   after the canonical reordering; otherwise the steps after the first
   measurement repeat from the same point and the engine keeps the first
   repetition; execute continues from the engine's current state; statistics
-  accumulate until reset; set_state checks the size.
+  accumulate until reset; set_state checks the size;
+* qpp::measure with Kraus operators or a basis (instruments.hpp:371-712),
+  reset and discard (:1148-1292) agree with the oracle: the same seeded
+  outcome, probabilities and post-measurement states within 1e-12.
 """
 import numpy as np
 import pytest
@@ -201,3 +204,83 @@ def test_set_state_checks_size_and_kind(ctx):
         e.set_state(qb.State(ctx, qb.KET, [2, 2]))
     with pytest.raises(qb.TypeMismatch):
         e.set_state(qb.State(ctx, qb.RHO, [2, 2, 2]))
+
+
+# ------------------------------------------- general measurements
+def _close(got, want, tol=1e-12):
+    got, want = np.asarray(got), np.asarray(want)
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) <= tol * max(1.0, np.max(np.abs(want)))
+
+
+@pytest.mark.parametrize("kind,destructive", [("ket", True), ("ket", False), ("rho", True),
+                                              ("rho", False)])
+def test_measure_kraus_matches_oracle(ctx, kind, destructive):
+    import qpp_b200 as qb
+    from tests.qpp_helpers import depolarizing_kraus
+    rng = np.random.default_rng(11)
+    dims = [2] * 7
+    x = gaussian_ket(rng, 128) if kind == "ket" else random_rho(rng, 128, 4)
+    Ks = [np.kron(a, b) for a in depolarizing_kraus(0.3) for b in depolarizing_kraus(0.2)]
+    Ks = Ks[:5] + [np.zeros((4, 4))]  # a zero-probability outcome too
+    s = qb.State.from_numpy(ctx, x, dims)
+    r, p, outs = s.measure_kraus(Ks, [5, 2], destructive=destructive, seed=4)
+    orr, op_, oouts = orc.measure_kraus(x, Ks, [5, 2], dims, destructive=destructive, seed=4)
+    assert r == orr
+    assert np.allclose(p, op_, rtol=1e-12, atol=1e-15)
+    for g, w in zip(outs, oouts):
+        assert (g is None) == (w is None)
+        if g is not None:
+            _close(g.numpy(), w)
+            g.free()
+    s.free()
+
+
+@pytest.mark.parametrize("kind,destructive", [("ket", True), ("ket", False), ("rho", True)])
+def test_measure_basis_matches_oracle(ctx, kind, destructive):
+    import qpp_b200 as qb
+    rng = np.random.default_rng(12)
+    dims = [2, 3, 2, 2]
+    D = 24
+    x = gaussian_ket(rng, D) if kind == "ket" else random_rho(rng, D, 3)
+    V = haar_unitary(rng, 6)[:, :4]  # 4 of 6 basis vectors of the (1, 2) targets
+    s = qb.State.from_numpy(ctx, x, dims)
+    r, p, outs = s.measure_basis(V, [1, 2], destructive=destructive, seed=9)
+    orr, op_, oouts = orc.measure_basis(x, V, [1, 2], dims, destructive=destructive, seed=9)
+    assert r == orr
+    assert np.allclose(p, op_, rtol=1e-12, atol=1e-15)
+    for g, w in zip(outs, oouts):
+        if g is not None:
+            _close(g.numpy().reshape(np.asarray(w).shape), w)
+            g.free()
+    s.free()
+
+
+@pytest.mark.parametrize("kind", ["ket", "rho"])
+def test_reset_and_discard_match_oracle(ctx, kind):
+    import qpp_b200 as qb
+    rng = np.random.default_rng(13)
+    dims = [2] * 6
+    x = gaussian_ket(rng, 64) if kind == "ket" else random_rho(rng, 64, 4)
+    s = qb.State.from_numpy(ctx, x, dims)
+    for seed in (1, 2, 3):
+        g = s.reset([4, 1], seed=seed)
+        _close(g.numpy(), orc.reset(x, [4, 1], dims, seed=seed))
+        g.free()
+        g = s.discard([4, 1], seed=seed)
+        _close(g.numpy(), orc.discard(x, [4, 1], dims, seed=seed))
+        assert g.dims == [2] * 4
+        g.free()
+    s.free()
+
+
+def test_general_measurement_errors(ctx):
+    import qpp_b200 as qb
+    s = qb.State(ctx, qb.KET, [2, 2], qb.C128)
+    with pytest.raises(qb.MatrixMismatchSubsys):
+        s.measure_kraus([np.eye(2)], [0, 1])
+    with pytest.raises(qb.SubsysMismatchDims):
+        s.measure_basis(np.eye(2), [2])
+    with pytest.raises(qb.SubsysMismatchDims):
+        s.reset([0, 0])
+    s.free()
