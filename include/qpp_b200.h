@@ -312,6 +312,25 @@ qgpu_status qgpu_circuit_cctrl(qgpu_circuit* c, const double* U, uint64_t DU,
  * the first outcome goes to classical dit c_reg. */
 qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target,
                                  uint32_t k, uint64_t c_reg, int destructive);
+/* QCircuit::reset / reset_many: RESET steps; an engine applies qpp::reset
+ * (instruments.hpp:1148-1206) on them with its own generator. */
+qgpu_status qgpu_circuit_reset(qgpu_circuit* c, const uint64_t* target, uint32_t k);
+/* QCircuit::cond_if / cond_end: the steps added between the two run only
+ * when the classical dits (dits[0] the least significant bit) spell `value`
+ * (a runtime IF, qengine.hpp:837-861; a false IF skips its block and its
+ * END). Not nested. Circuits with conditionals run on engines only. */
+qgpu_status qgpu_circuit_cond_if(qgpu_circuit* c, const uint64_t* dits, uint32_t n,
+                                 uint64_t value);
+qgpu_status qgpu_circuit_cond_end(qgpu_circuit* c);
+/* OpenQASM 2.0 reader (replaces qpp::qasm::read_from_string /
+ * read_from_file, qasm/qasm.hpp:781-820): registers in declaration order,
+ * non-destructive measurements, resets, runtime conditionals for `if`, and
+ * qelib1.inc's gates as single steps with qpp's matrices (u3/u2/u1 as U; the
+ * gates qpp expands into several U/CX steps -- cu1, cu3, crx, cry, cswap,
+ * rxx, rzz, sx, ... -- as one step with the same matrix). Parse errors are
+ * QGPU_ERR_INVALID_ARGUMENT with "line L, column C: ..." in the message. */
+qgpu_status qgpu_qasm_read(const char* source, qgpu_circuit** out);
+qgpu_status qgpu_qasm_read_file(const char* path, qgpu_circuit** out);
 /* A Kraus channel sum_i K_i . K_i^+ on `target` (nK consecutive DK x DK
  * operators). No QCircuit counterpart: density-matrix engines apply it
  * exactly (qpp::apply(rho, Ks, target, dims), operations.hpp:476-560); ket
@@ -321,6 +340,8 @@ qgpu_status qgpu_circuit_channel(qgpu_circuit* c, const double* Ks,
                                  const uint64_t* target, uint32_t k);
 qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq,
                               uint64_t* n_steps);
+/* Qudits, their dimension and the classical dits of a circuit. */
+qgpu_status qgpu_circuit_shape(const qgpu_circuit* c, uint32_t* nq, uint64_t* d, uint32_t* nc);
 /* Number of state passes of the fused plan with blocks of <= max_k qubits
  * (host-side planning only). */
 qgpu_status qgpu_circuit_fuse(qgpu_circuit* c, uint32_t max_k,

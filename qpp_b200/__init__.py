@@ -516,6 +516,45 @@ class Circuit:
                                        ct.c_int(1 if fan else 0)))
         return self
 
+    @classmethod
+    def from_qasm(cls, source):
+        """qpp::qasm::read_from_string: an OpenQASM 2.0 program as a Circuit."""
+        h = vp()
+        check(lib().qgpu_qasm_read(source.encode(), ct.byref(h)))
+        return cls._wrap(h)
+
+    @classmethod
+    def from_qasm_file(cls, path):
+        """qpp::qasm::read_from_file."""
+        h = vp()
+        check(lib().qgpu_qasm_read_file(str(path).encode(), ct.byref(h)))
+        return cls._wrap(h)
+
+    @classmethod
+    def _wrap(cls, h):
+        c = cls.__new__(cls)
+        c.h = h
+        nq, d, nc = ct.c_uint32(), ct.c_uint64(), ct.c_uint32()
+        check(lib().qgpu_circuit_shape(h, ct.byref(nq), ct.byref(d), ct.byref(nc)))
+        c.nq, c.d, c.nc = nq.value, d.value, nc.value
+        return c
+
+    def reset(self, target):
+        t, tp, nt = _u64(target if isinstance(target, (list, tuple)) else [target])
+        check(lib().qgpu_circuit_reset(self.h, tp, ct.c_uint32(nt)))
+        return self
+
+    def cond_if(self, dits, value):
+        """Steps until cond_end() run only when the dits (dits[0] the least
+        significant bit) spell `value`."""
+        d, dp_, nd = _u64(dits)
+        check(lib().qgpu_circuit_cond_if(self.h, dp_, ct.c_uint32(nd), ct.c_uint64(value)))
+        return self
+
+    def cond_end(self):
+        check(lib().qgpu_circuit_cond_end(self.h))
+        return self
+
     def measure(self, target, c_reg=0, destructive=True):
         t, tp, nt = _u64(target if isinstance(target, (list, tuple)) else [target])
         check(lib().qgpu_circuit_measure(self.h, tp, ct.c_uint32(nt), ct.c_uint64(c_reg),

@@ -196,6 +196,64 @@ qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target, uint32
     });
 }
 
+// QCircuit::reset (qcircuit.hpp): RESET / RESET_MANY measurement steps.
+qgpu_status qgpu_circuit_reset(qgpu_circuit* c, const uint64_t* target, uint32_t k) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = k > 1 ? "qpp::QCircuit::reset_many()" : "qpp::QCircuit::reset()";
+        auto t = vec_of(target, k);
+        check_targets(c, W, t, "target", measured_of(c));
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::Reset;
+        s.target = t;
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+// QCircuit::cond_if / cond_end: the steps added in between run only when
+// the dits (dits[0] the least significant bit) spell `value`.
+qgpu_status qgpu_circuit_cond_if(qgpu_circuit* c, const uint64_t* dits, uint32_t n,
+                                 uint64_t value) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = "qpp::QCircuit::cond_if()";
+        for (const auto& st : c->steps)
+            if (st.kind == qgpu::StepKind::CondIf && st.nK == 0)
+                raise(QGPU_ERR_INVALID_ARGUMENT, W, "nested conditionals are not supported");
+        auto d = vec_of(dits, n);
+        if (d.empty() || d.size() > 63) raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + "dits");
+        for (uint64_t x : d)
+            if (x >= c->nc) raise(QGPU_ERR_OUT_OF_RANGE, W, ctx_of(c) + "dits");
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::CondIf;
+        s.ctrl = d;
+        s.c_reg = value;
+        s.nK = 0; // open
+        c->steps.push_back(std::move(s));
+        c->plan_k = 0;
+    });
+}
+
+qgpu_status qgpu_circuit_cond_end(qgpu_circuit* c) {
+    return guarded([&] {
+        need_handle(c);
+        size_t open = c->steps.size();
+        for (size_t i = c->steps.size(); i-- > 0;)
+            if (c->steps[i].kind == qgpu::StepKind::CondIf && c->steps[i].nK == 0) {
+                open = i;
+                break;
+            }
+        if (open == c->steps.size())
+            raise(QGPU_ERR_INVALID_ARGUMENT, "qpp::QCircuit::cond_end()", "no open cond_if");
+        qgpu::Step s;
+        s.kind = qgpu::StepKind::CondEnd;
+        c->steps.push_back(std::move(s));
+        c->steps[open].nK = uint32_t(c->steps.size() - 1 - open); // the block and the END
+        c->plan_k = 0;
+    });
+}
+
 qgpu_status qgpu_circuit_channel(qgpu_circuit* c, const double* Ks, uint32_t nK, uint64_t DK,
                                  const uint64_t* target, uint32_t k) {
     return guarded([&] {
@@ -222,6 +280,15 @@ qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq, uint64_t* n_s
         need_handle(c);
         if (nq) *nq = c->nq;
         if (n_steps) *n_steps = c->steps.size();
+    });
+}
+
+qgpu_status qgpu_circuit_shape(const qgpu_circuit* c, uint32_t* nq, uint64_t* d, uint32_t* nc) {
+    return guarded([&] {
+        need_handle(c);
+        if (nq) *nq = c->nq;
+        if (d) *d = c->d;
+        if (nc) *nc = c->nc;
     });
 }
 

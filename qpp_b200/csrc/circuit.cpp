@@ -277,6 +277,10 @@ static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
 }
 
 void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_t count) {
+    for (const Step& st : c->steps)
+        if (st.kind == StepKind::CondIf)
+            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
+                  "classical conditionals need an engine (qgpu_engine_execute)");
     if (form == 0) {
         for (uint64_t i = first; i < first + count && i < c->steps.size(); ++i)
             apply_step(s, c->steps[i]);

@@ -36,6 +36,10 @@ enum class StepKind {
     Reset,     // reset targets to |0>
     Channel,   // Kraus channel sum_i K_i . K_i^+ on the targets (no QCircuit step:
                // exact on density matrices, one sampled branch on kets)
+    CondIf,    // runtime IF (qengine.hpp:837-861): ctrl = the dits (LSB first),
+               // c_reg = the value they must spell; nK = the steps to skip when
+               // false (the block and its CondEnd)
+    CondEnd,   // runtime ENDIF
     Nop
 };
 

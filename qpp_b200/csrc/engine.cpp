@@ -343,7 +343,9 @@ void apply_noise(qgpu_engine* e, size_t step_idx) {
     }
 }
 
-void run_step(qgpu_engine* e, const Step& st, size_t idx) {
+// Executes one step; returns how many following steps to skip (a runtime IF
+// that is false jumps past its block and its END, qengine.hpp:853-861).
+uint32_t run_step(qgpu_engine* e, const Step& st, size_t idx) {
     if (e->noisy) apply_noise(e, idx);
     auto relv = [&](const std::vector<uint64_t>& v) {
         std::vector<uint64_t> r;
@@ -371,8 +373,8 @@ void run_step(qgpu_engine* e, const Step& st, size_t idx) {
             };
             uint64_t first = val(0);
             for (size_t m = 1; m < st.ctrl.size(); ++m)
-                if (val(m) != first) return;
-            if (first == 0) return; // U^0 = identity
+                if (val(m) != first) return 0;
+            if (first == 0) return 0; // U^0 = identity
             std::vector<cd> Up = mat_pow(st.U, st.DU, first);
             auto t = relv(st.target);
             if (st.kind == StepKind::CCtrlFan) {
@@ -415,6 +417,30 @@ void run_step(qgpu_engine* e, const Step& st, size_t idx) {
                 raise(QGPU_ERR_DIVISION_BY_ZERO, "qpp::normalize()", "Division by zero!");
             break;
         }
+        case StepKind::CondIf: {
+            uint64_t v = 0;
+            for (size_t i = 0; i < st.ctrl.size(); ++i)
+                v |= (e->dits[st.ctrl[i]] & 1u) << i;
+            return v == st.c_reg ? 0u : st.nK;
+        }
+        case StepKind::CondEnd:
+            break;
+        case StepKind::Reset: {
+            // qpp::reset (instruments.hpp:1148-1206) on the relative
+            // positions: measure_seq without destruction (one draw), then
+            // Xd^(d - r) on each target
+            const std::vector<uint64_t> rel = relv(st.target);
+            std::vector<uint64_t> res;
+            std::vector<double> ps;
+            measure_seq(e, rel, false, res, ps);
+            const uint64_t d = e->circ->d;
+            for (size_t i = 0; i < rel.size(); ++i) {
+                std::vector<cd> X(d * d, 0.0);
+                for (uint64_t j = 0; j < d; ++j) X[((j + d - res[i]) % d) + j * d] = 1.0;
+                op_apply(e->st, X.data(), d, {rel[i]});
+            }
+            break;
+        }
         case StepKind::Measure: {
             std::vector<uint64_t> res;
             std::vector<double> ps;
@@ -430,6 +456,7 @@ void run_step(qgpu_engine* e, const Step& st, size_t idx) {
         default:
             break;
     }
+    return 0;
 }
 
 int classify(const std::vector<cd>& K, uint64_t d, std::vector<cd>& unit) {
@@ -460,6 +487,7 @@ int classify(const std::vector<cd>& K, uint64_t d, std::vector<cd>& unit) {
 }
 
 bool is_measurement(const Step& s) { return s.kind == StepKind::Measure || s.kind == StepKind::Reset; }
+bool is_runtime(const Step& s) { return s.kind == StepKind::CondIf || s.kind == StepKind::CondEnd; }
 bool is_cctrl(const Step& s) { return s.kind == StepKind::CCtrl || s.kind == StepKind::CCtrlFan; }
 
 // (ctrl, target, c_reg) of a step as qpp's
@@ -510,6 +538,8 @@ std::vector<size_t> canonical_order(const qgpu_circuit* c, bool canonical) {
     std::vector<size_t> order(ns);
     for (size_t i = 0; i < ns; ++i) order[i] = i;
     if (!canonical) return order;
+    for (const Step& s : c->steps) // runtime steps: the circuit as it is
+        if (is_runtime(s)) return order;
     size_t first = 0;
     while (first < ns && !is_measurement(c->steps[first])) ++first;
     auto push_back_class = [&](bool (*cls)(const Step&)) {
@@ -539,7 +569,7 @@ void repeat_steps(qgpu_engine* e, const std::vector<size_t>& order, size_t pos, 
         for (size_t i = pos; i < order.size(); ++i) {
             const Step& s = e->circ->steps[order[i]];
             if (is_measurement(s)) measured = true;
-            run_step(e, s, order[i]);
+            i += run_step(e, s, order[i]); // a false IF skips its block
         }
         if (measured) e->stats[e->dits] += 1;
         if (reps == 1) break;
@@ -740,8 +770,10 @@ qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps) {
                 raise(QGPU_ERR_DIMS_NOT_EQUAL, "qpp::internal::QEngineState::reset()", "state");
             qgpu::clear_registers(e);
             std::vector<size_t> order = qgpu::canonical_order(e->circ, reps > 1);
-            size_t pos = 0;
-            while (pos < order.size() && !qgpu::is_measurement(e->circ->steps[order[pos]])) ++pos;
+            size_t pos = 0; // the first measurement, reset or runtime step
+            while (pos < order.size() && !qgpu::is_measurement(e->circ->steps[order[pos]]) &&
+                   !qgpu::is_runtime(e->circ->steps[order[pos]]))
+                ++pos;
             for (size_t i = 0; i < pos; ++i) qgpu::run_step(e, e->circ->steps[order[i]], order[i]);
             bool can_sample = reps > 1 && !e->replay && pos < order.size();
             for (size_t i = pos; i < order.size() && can_sample; ++i)
