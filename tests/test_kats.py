@@ -41,6 +41,10 @@ class _OracleBackend:
     def syspermute(self, s, p, dims):
         return self.m.syspermute(s, p, dims)
 
+    def measure_seq(self, s, t, dims, destructive):
+        res, probs, out, _ = self.m.measure_seq(s, t, dims, destructive=destructive)
+        return res, probs, out
+
 
 class _GpuBackend:
     def __init__(self, ctx):
@@ -67,6 +71,14 @@ class _GpuBackend:
 
     def syspermute(self, s, p, dims):
         return self.qb.syspermute(s, p, dims, ctx=self.ctx)
+
+    def measure_seq(self, s, t, dims, destructive):
+        st = self.qb.State.from_numpy(self.ctx, s, dims)
+        res, probs, out = st.measure_seq(t, destructive=destructive)
+        x = out.numpy()
+        out.free()
+        st.free()
+        return res, probs, x
 
 
 @pytest.fixture(params=BACKENDS)
@@ -276,3 +288,25 @@ def test_kraus_channel_trace_and_dense(be):
     assert abs(np.trace(out) - 1) < 1e-12
     ref = sum(dense_gate(K, [2, 0], dims) @ rho @ dense_gate(K, [2, 0], dims).conj().T for K in Ks)
     assert np.max(np.abs(out - ref)) < 1e-12
+
+
+# unit_tests/tests/instruments.cpp:102-160 (qpp_measure_seq, Qudits)
+def test_measure_seq_qudits(be):
+    dims = [2, 2, 3, 2, 3, 2]
+    mask = [0, 1, 2, 1, 2, 0]
+    psi, rho = mket(mask, dims), mprj(mask, dims)
+    ms, ps, out = be.measure_seq(psi, [4, 2, 3, 0], dims, True)
+    assert ms == [2, 2, 1, 0] and ps == [1, 1, 1, 1]
+    assert _norm(np.asarray(out).reshape(-1) - mket([1, 0], [2, 2])) < 1e-5
+    ms, ps, out = be.measure_seq(rho, [4, 2, 3, 0], dims, True)
+    assert ms == [2, 2, 1, 0] and ps == [1, 1, 1, 1]
+    assert _norm(out - mprj([1, 0], [2, 2])) < 1e-5
+    ms, ps, out = be.measure_seq(psi, [4, 2, 3, 0], dims, False)
+    assert ms == [2, 2, 1, 0] and ps == [1, 1, 1, 1]
+    assert _norm(np.asarray(out).reshape(-1) - psi) < 1e-5
+    ms, ps, out = be.measure_seq(psi, [3, 0, 4, 2], dims, False)
+    assert ms == [1, 0, 2, 2] and ps == [1, 1, 1, 1]
+    assert _norm(np.asarray(out).reshape(-1) - psi) < 1e-5
+    ms, ps, out = be.measure_seq(rho, [3, 0, 4, 2], dims, False)
+    assert ms == [1, 0, 2, 2] and ps == [1, 1, 1, 1]
+    assert _norm(out - rho) < 1e-5
