@@ -155,6 +155,25 @@ qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
  * perm[i] moves to position i; writes a new state of the same kind. */
 qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
                             uint32_t n, qgpu_state** out);
+/* qpp::applyQFT(A, target, d, swap) (inverse = 0, operations.hpp:2565-2676)
+ * and qpp::applyTFQ (inverse = 1, :2680-2787), in place: the qudit quantum
+ * Fourier transform (or its adjoint) on the targets of the state viewed as
+ * n = round(log2 D / log2 d) qudits of dimension d (a density matrix gets
+ * U rho U^dagger). target[0] is the most significant digit of the
+ * transformed register; swap reverses the targets at the end (QFT) or the
+ * start (TFQ), as qpp's SWAP gates do. The steps of up to 8 consecutive
+ * targets run as one pass over the state in shared memory, so the transform
+ * costs ceil(k / 8) passes (qubits; fewer targets per pass for d > 2)
+ * instead of qpp's k (k + 1) / 2 gate passes; with swap the reversal rides
+ * on the last pass, which writes a new buffer (the state's device pointer
+ * changes). Results match qpp's gate sequence to rounding (the butterflies
+ * sum the same terms). d above 16 runs qpp's gate sequence on the gate
+ * kernels. */
+qgpu_status qgpu_apply_qft(qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t d,
+                           int swap, int inverse);
+/* qpp::QFT(A, d, swap) / qpp::TFQ (operations.hpp:2792-2899): every digit
+ * is a target, in order. */
+qgpu_status qgpu_qft(qgpu_state* s, uint64_t d, int swap, int inverse);
 /* Partial trace that allocates nothing. No counterpart in the reference:
  * Quantum++ always returns a freshly allocated matrix. This entry point is
  * for callers that cannot allocate device memory when they need the trace --
@@ -282,6 +301,15 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* dims, uint32_t n,
                                  double* result);
 
+/* qpp::applyQFT / applyTFQ (inverse = 1) on a host array; result has the
+ * input's shape. */
+qgpu_status qgpu_host_apply_qft(qgpu_ctx* ctx, const double* state, uint64_t rows,
+                                uint64_t cols, const uint64_t* target, uint32_t k,
+                                uint64_t d, int swap, int inverse, double* result);
+/* qpp::QFT / TFQ (inverse = 1) on a host array. */
+qgpu_status qgpu_host_qft(qgpu_ctx* ctx, const double* state, uint64_t rows, uint64_t cols,
+                          uint64_t d, int swap, int inverse, double* result);
+
 /* --------------------------------------------------------------- circuits
  * The step list of qpp::QCircuit (include/qpp/classes/qcircuit.hpp) over nq
  * qudits of dimension d with nc classical dits. Step checks follow
@@ -322,6 +350,14 @@ qgpu_status qgpu_circuit_reset(qgpu_circuit* c, const uint64_t* target, uint32_t
 qgpu_status qgpu_circuit_cond_if(qgpu_circuit* c, const uint64_t* dits, uint32_t n,
                                  uint64_t value);
 qgpu_status qgpu_circuit_cond_end(qgpu_circuit* c);
+/* QCircuit::QFT(target, swap) (inverse = 0, qcircuit.hpp:1514-1617) and
+ * QCircuit::TFQ (inverse = 1, :1628-1732): appends qpp's gate sequence as
+ * steps (H or Fd on target i followed by CTRL R_j from target i + j - 1,
+ * then the SWAPs; the adjoint sequence in reverse for TFQ). target == NULL
+ * takes every qudit not measured so far. Noiseless engines run the appended
+ * block as one transform (qgpu_apply_qft); noisy engines step through it. */
+qgpu_status qgpu_circuit_qft(qgpu_circuit* c, const uint64_t* target, uint32_t k, int swap,
+                             int inverse);
 /* OpenQASM 2.0 reader (replaces qpp::qasm::read_from_string /
  * read_from_file, qasm/qasm.hpp:781-820): registers in declaration order,
  * non-destructive measurements, resets, runtime conditionals for `if`, and

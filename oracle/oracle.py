@@ -327,3 +327,117 @@ def discard(state, target, dims, seed=0):
     """qpp::discard(A, target, dims), instruments.hpp:1243-1292: measure_seq
     with destruction, the post-measurement state only."""
     return measure_seq(state, target, dims, destructive=True, seed=seed)[2]
+
+
+# ------------------------------------------------------- Fourier transforms
+def _fd(d):
+    """qpp::Gates::Fd(d), gates.hpp:260-285: H for d = 2, else
+    F(i, j) = omega^(i j) / sqrt(d) with omega = exp(2 pi i / d)."""
+    if d == 2:
+        h = 1.0 / np.sqrt(2.0)
+        return np.array([[h, h], [h, -h]], dtype=np.complex128)
+    om = np.exp(2.0 * np.pi * 1j / d)
+    F = np.empty((d, d), dtype=np.complex128)
+    for j in range(d):
+        for i in range(d):
+            F[i, j] = 1.0 / np.sqrt(d) * om ** (i * j)
+    return F
+
+
+def _swapd(d):
+    """qpp::Gates::SWAPd(d): |a b> -> |b a>."""
+    S = np.zeros((d * d, d * d), dtype=np.complex128)
+    for a in range(d):
+        for b in range(d):
+            S[b * d + a, a * d + b] = 1
+    return S
+
+
+def _rj(d, j, sign):
+    """R_j = diag(exp(sign 2 pi i m / d^j)), operations.hpp:2616-2618, :2641-2646."""
+    return np.diag([np.exp(sign * 2.0 * np.pi * m * 1j / float(d) ** j) for m in range(d)])
+
+
+_QFT_CODES = dict(ZeroSize=1, MatrixNotSquareNorCvector=3, DimsInvalid=5,
+                  DimsMismatchMatrix=7, DimsMismatchCvector=8, SubsysMismatchDims=9)
+
+
+def _check_qft(where, a, target, d, whole):
+    """The checks of applyQFT / applyTFQ (operations.hpp:2569-2605,
+    :2684-2720) and of QFT / TFQ (:2793-2826, :2845-2878, whose dims checks
+    both name qpp::QFT()), in qpp's order. Returns dims = n x d."""
+    def err(kind, w, what):
+        raise OracleError(_QFT_CODES[kind], w, what)
+    rows = a.shape[0]
+    cols = 1 if a.ndim == 1 else a.shape[1]
+    if rows * cols == 0:
+        err("ZeroSize", where, "A")
+    if d < 2:
+        err("DimsInvalid", where, "d")
+    n = int(np.rint(np.log2(rows) / np.log2(d)))  # get_num_subsys, util.hpp:389-397
+    dims = [d] * n
+    if not whole:
+        if len(target) > n or len(set(target)) != len(target) or any(t >= n for t in target):
+            err("SubsysMismatchDims", where, "dims/target")
+    wd = "qpp::QFT()" if whole else where
+    if cols == 1:
+        if n == 0 or d ** n != rows:
+            err("DimsMismatchCvector", wd, "A/dims")
+    elif rows == cols:
+        if n == 0 or d ** n != rows:
+            err("DimsMismatchMatrix", wd, "A/dims")
+    else:
+        err("MatrixNotSquareNorCvector", wd, "A")
+    return dims
+
+
+def applyQFT(state, target, d=2, swap=True, _where="qpp::applyQFT()", _whole=False):
+    """qpp::applyQFT(A, target, d, swap), operations.hpp:2565-2676: for each
+    target i, Fd (H for qubits) on it, then controlled R_j (control
+    target[i + j - 1], j = 2..k-i) on it; with swap, SWAPs reverse the
+    targets at the end. Every gate goes through this oracle's apply /
+    applyCTRL."""
+    a = _cplx(state)
+    dims = _check_qft(_where, a, list(target), d, _whole)
+    if _whole:
+        target = list(range(len(dims)))
+    out = a
+    k = len(target)
+    for i in range(k):
+        out = apply(out, _fd(d), [target[i]], dims)
+        for j in range(2, k - i + 1):
+            out = applyCTRL(out, _rj(d, j, 1.0), [target[i + j - 1]], [target[i]], dims)
+    if swap:
+        for i in range(k // 2):
+            out = apply(out, _swapd(d), [target[i], target[k - i - 1]], dims)
+    return out
+
+
+def applyTFQ(state, target, d=2, swap=True, _where="qpp::applyTFQ()", _whole=False):
+    """qpp::applyTFQ(A, target, d, swap), operations.hpp:2680-2787: the
+    adjoint of applyQFT, gate by gate in the reverse order (SWAPs first)."""
+    a = _cplx(state)
+    dims = _check_qft(_where, a, list(target), d, _whole)
+    if _whole:
+        target = list(range(len(dims)))
+    out = a
+    k = len(target)
+    if swap:
+        for i in reversed(range(k // 2)):
+            out = apply(out, _swapd(d), [target[i], target[k - i - 1]], dims)
+    for i in reversed(range(k)):
+        for j in reversed(range(2, k - i + 1)):
+            out = applyCTRL(out, _rj(d, j, -1.0), [target[i + j - 1]], [target[i]], dims)
+        out = apply(out, _fd(d).conj().T, [target[i]], dims)
+    return out
+
+
+def QFT(state, d=2, swap=True):
+    """qpp::QFT(A, d, swap), operations.hpp:2792-2826: applyQFT on every
+    subsystem in order."""
+    return applyQFT(state, [], d, swap, _where="qpp::QFT()", _whole=True)
+
+
+def TFQ(state, d=2, swap=True):
+    """qpp::TFQ(A, d, swap), operations.hpp:2844-2878."""
+    return applyTFQ(state, [], d, swap, _where="qpp::TFQ()", _whole=True)

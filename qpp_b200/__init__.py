@@ -252,6 +252,26 @@ class State:
         check(lib().qgpu_syspermute(self.h, pp, ct.c_uint32(npm), ct.byref(h)))
         return State(self.ctx, self.kind, None, handle=h)
 
+    def apply_qft(self, target, d=2, swap=True):
+        """qpp::applyQFT on the resident state, in place."""
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_apply_qft(self.h, tp, ct.c_uint32(nt), ct.c_uint64(d),
+                                   ct.c_int(int(swap)), ct.c_int(0)))
+        return self
+
+    def apply_tfq(self, target, d=2, swap=True):
+        """qpp::applyTFQ on the resident state, in place."""
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_apply_qft(self.h, tp, ct.c_uint32(nt), ct.c_uint64(d),
+                                   ct.c_int(int(swap)), ct.c_int(1)))
+        return self
+
+    def qft(self, d=2, swap=True, inverse=False):
+        """qpp::QFT / TFQ (inverse) on every subsystem of the resident state."""
+        check(lib().qgpu_qft(self.h, ct.c_uint64(d), ct.c_int(int(swap)),
+                             ct.c_int(int(inverse))))
+        return self
+
     def norm2(self):
         v = ct.c_double()
         check(lib().qgpu_norm2(self.h, ct.byref(v)))
@@ -470,6 +490,42 @@ def syspermute(state, perm, dims, ctx=None):
     return out
 
 
+def _host_qft(state, target, d, swap, inverse, ctx):
+    ctx = ctx or default_context()
+    s, rows, cols, one_d = _host_state(state)
+    out = np.zeros(s.shape, dtype=np.complex128, order="F")
+    if target is None:
+        check(lib().qgpu_host_qft(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols),
+                                  ct.c_uint64(d), ct.c_int(int(swap)), ct.c_int(int(inverse)),
+                                  _dp(out)))
+    else:
+        t, tp, nt = _u64(target)
+        check(lib().qgpu_host_apply_qft(ctx.h, _dp(s), ct.c_uint64(rows), ct.c_uint64(cols), tp,
+                                        ct.c_uint32(nt), ct.c_uint64(d), ct.c_int(int(swap)),
+                                        ct.c_int(int(inverse)), _dp(out)))
+    return out
+
+
+def applyQFT(state, target, d=2, swap=True, ctx=None):
+    """qpp::applyQFT(A, target, d, swap) (operations.hpp:2565-2676)."""
+    return _host_qft(state, target, d, swap, False, ctx)
+
+
+def applyTFQ(state, target, d=2, swap=True, ctx=None):
+    """qpp::applyTFQ(A, target, d, swap) (operations.hpp:2680-2787)."""
+    return _host_qft(state, target, d, swap, True, ctx)
+
+
+def QFT(state, d=2, swap=True, ctx=None):
+    """qpp::QFT(A, d, swap) (operations.hpp:2792-2826)."""
+    return _host_qft(state, None, d, swap, False, ctx)
+
+
+def TFQ(state, d=2, swap=True, ctx=None):
+    """qpp::TFQ(A, d, swap) (operations.hpp:2844-2878)."""
+    return _host_qft(state, None, d, swap, True, ctx)
+
+
 # ------------------------------------------------------------------ circuits
 PLAIN, FUSED = 0, 1
 
@@ -549,6 +605,28 @@ class Circuit:
         significant bit) spell `value`."""
         d, dp_, nd = _u64(dits)
         check(lib().qgpu_circuit_cond_if(self.h, dp_, ct.c_uint32(nd), ct.c_uint64(value)))
+        return self
+
+    def QFT(self, target=None, swap=True):
+        """QCircuit::QFT(target, swap); target None = every qudit not yet measured."""
+        if target is None:
+            check(lib().qgpu_circuit_qft(self.h, None, ct.c_uint32(0), ct.c_int(int(swap)),
+                                         ct.c_int(0)))
+        else:
+            t, tp, nt = _u64(target)
+            check(lib().qgpu_circuit_qft(self.h, tp, ct.c_uint32(nt), ct.c_int(int(swap)),
+                                         ct.c_int(0)))
+        return self
+
+    def TFQ(self, target=None, swap=True):
+        """QCircuit::TFQ(target, swap)."""
+        if target is None:
+            check(lib().qgpu_circuit_qft(self.h, None, ct.c_uint32(0), ct.c_int(int(swap)),
+                                         ct.c_int(1)))
+        else:
+            t, tp, nt = _u64(target)
+            check(lib().qgpu_circuit_qft(self.h, tp, ct.c_uint32(nt), ct.c_int(int(swap)),
+                                         ct.c_int(1)))
         return self
 
     def cond_end(self):

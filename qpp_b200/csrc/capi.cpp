@@ -240,6 +240,31 @@ void check_perm(uint64_t rows, uint64_t cols, const std::vector<uint64_t>& perm,
     state_shape(rows, cols, dims, W, "A/dims", "A/dims", "A");
 }
 
+// qpp::applyQFT / applyTFQ (operations.hpp:2569-2605, :2684-2720) on A
+// viewed as n = get_num_subsys(D, d) qudits of dimension d (util.hpp:389-397);
+// `whole` = QFT / TFQ (:2793-2826, :2845-2878), which check no target and
+// name qpp::QFT() in the dims checks of both.
+void check_qft(const char* W, bool whole, uint64_t rows, uint64_t cols,
+               const std::vector<uint64_t>& target, uint64_t d) {
+    if (rows * cols == 0) raise(QGPU_ERR_ZERO_SIZE, W, "A");
+    if (d < 2) raise(QGPU_ERR_DIMS_INVALID, W, "d");
+    const uint64_t n = uint64_t(std::llround(std::log2(double(rows)) / std::log2(double(d))));
+    std::vector<uint64_t> dims(n, d);
+    if (!whole && !subsys_ok(target, dims))
+        raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
+    // prod(dims) with overflow saturating to 0 (never equal to rows then)
+    uint64_t p = 1;
+    for (uint64_t i = 0; i < n && p; ++i) p = p > UINT64_MAX / d ? 0 : p * d;
+    const char* Wd = whole ? "qpp::QFT()" : W;
+    if (cols == 1) {
+        if (dims.empty() || p != rows) raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, Wd, "A/dims");
+    } else if (rows == cols) {
+        if (dims.empty() || p != rows) raise(QGPU_ERR_DIMS_MISMATCH_MATRIX, Wd, "A/dims");
+    } else {
+        raise(QGPU_ERR_MATRIX_NOT_SQUARE_NOR_CVECTOR, Wd, "A");
+    }
+}
+
 void shape_of(const qgpu_state* s, uint64_t& rows, uint64_t& cols) {
     rows = s->D;
     cols = s->kind == QGPU_KET ? 1 : s->D;
@@ -739,6 +764,62 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
         o.s = qgpu::op_syspermute(s.s, p);
         download_c128(o.s, result);
     });
+}
+
+// ------------------------------------------------------- Fourier transforms
+qgpu_status qgpu_apply_qft(qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t d,
+                           int swap, int inverse) {
+    return guard([&] {
+        check_handle(s);
+        uint64_t r, c;
+        shape_of(s, r, c);
+        std::vector<uint64_t> t = vec(target, k);
+        check_qft(inverse ? "qpp::applyTFQ()" : "qpp::applyQFT()", false, r, c, t, d);
+        qgpu::op_apply_qft(s, t, d, swap != 0, inverse != 0);
+    });
+}
+
+qgpu_status qgpu_qft(qgpu_state* s, uint64_t d, int swap, int inverse) {
+    return guard([&] {
+        check_handle(s);
+        uint64_t r, c;
+        shape_of(s, r, c);
+        check_qft(inverse ? "qpp::TFQ()" : "qpp::QFT()", true, r, c, {}, d);
+        std::vector<uint64_t> t;
+        for (uint64_t x = 1; x < r; x *= d) t.push_back(t.size());
+        qgpu::op_apply_qft(s, t, d, swap != 0, inverse != 0);
+    });
+}
+
+static qgpu_status host_qft(qgpu_ctx* ctx, const double* state, uint64_t rows,
+                            uint64_t cols, const uint64_t* target, uint32_t k, bool whole,
+                            uint64_t d, int swap, int inverse, double* result) {
+    return guard([&] {
+        check_handle(ctx);
+        std::vector<uint64_t> t = vec(target, k);
+        const char* W = whole ? (inverse ? "qpp::TFQ()" : "qpp::QFT()")
+                              : (inverse ? "qpp::applyTFQ()" : "qpp::applyQFT()");
+        check_qft(W, whole, rows, cols, t, d);
+        std::vector<uint64_t> dims;
+        for (uint64_t x = 1; x < rows; x *= d) dims.push_back(d);
+        if (whole)
+            for (size_t i = 0; i < dims.size(); ++i) t.push_back(i);
+        Tmp s;
+        s.s = host_state(ctx, state, rows, cols, dims);
+        qgpu::op_apply_qft(s.s, t, d, swap != 0, inverse != 0);
+        download_c128(s.s, result);
+    });
+}
+
+qgpu_status qgpu_host_apply_qft(qgpu_ctx* ctx, const double* state, uint64_t rows,
+                                uint64_t cols, const uint64_t* target, uint32_t k,
+                                uint64_t d, int swap, int inverse, double* result) {
+    return host_qft(ctx, state, rows, cols, target, k, false, d, swap, inverse, result);
+}
+
+qgpu_status qgpu_host_qft(qgpu_ctx* ctx, const double* state, uint64_t rows, uint64_t cols,
+                          uint64_t d, int swap, int inverse, double* result) {
+    return host_qft(ctx, state, rows, cols, nullptr, 0, true, d, swap, inverse, result);
 }
 
 } // extern "C"

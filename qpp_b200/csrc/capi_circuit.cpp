@@ -235,6 +235,76 @@ qgpu_status qgpu_circuit_cond_if(qgpu_circuit* c, const uint64_t* dits, uint32_t
     });
 }
 
+// QCircuit::QFT / TFQ (qcircuit.hpp:1514-1617, :1628-1732): qpp's gate
+// sequence as steps (H or Fd on target i, CTRL R_j from target i + j - 1,
+// SWAP / SWAPd; the adjoint sequence in the reverse order for TFQ);
+// target == NULL takes every qudit not yet measured (QFT(bool swap)).
+qgpu_status qgpu_circuit_qft(qgpu_circuit* c, const uint64_t* target, uint32_t k, int swap,
+                             int inverse) {
+    return guarded([&] {
+        need_handle(c);
+        const char* W = inverse ? "qpp::QCircuit::TFQ()" : "qpp::QCircuit::QFT()";
+        auto meas = measured_of(c);
+        std::vector<uint64_t> t;
+        if (target) {
+            t = vec_of(target, k);
+        } else {
+            for (uint64_t q = 0; q < c->nq; ++q)
+                if (!meas[q]) t.push_back(q);
+        }
+        check_targets(c, W, t, "target", meas);
+        const uint64_t d = c->d;
+        const size_t n = t.size();
+        std::vector<cd> F = qgpu::fourier_gate(d);
+        if (inverse) {
+            std::vector<cd> Fa(d * d);
+            for (uint64_t i = 0; i < d; ++i)
+                for (uint64_t j = 0; j < d; ++j) Fa[i + j * d] = std::conj(F[j + i * d]);
+            F = Fa;
+        }
+        const std::vector<cd> SW = qgpu::swap_gate(d);
+        const size_t first = c->steps.size();
+        auto gate = [&](const std::vector<cd>& U, uint64_t DU, std::vector<uint64_t> tg) {
+            qgpu::Step s;
+            s.kind = qgpu::StepKind::Gate;
+            s.U = U;
+            s.DU = DU;
+            s.target = std::move(tg);
+            c->steps.push_back(std::move(s));
+        };
+        auto ctrl = [&](size_t i, size_t j) {
+            qgpu::Step s;
+            s.kind = qgpu::StepKind::Ctrl;
+            s.U = qgpu::qft_phase(d, j, inverse != 0);
+            s.DU = d;
+            s.ctrl = {t[i + j - 1]};
+            s.target = {t[i]};
+            c->steps.push_back(std::move(s));
+        };
+        if (!inverse) {
+            for (size_t i = 0; i < n; ++i) {
+                gate(F, d, {t[i]});
+                for (size_t j = 2; j <= n - i; ++j) ctrl(i, j);
+            }
+            if (swap)
+                for (size_t i = 0; i < n / 2; ++i) gate(SW, d * d, {t[i], t[n - i - 1]});
+        } else {
+            if (swap)
+                for (size_t i = n / 2; i-- > 0;) gate(SW, d * d, {t[i], t[n - i - 1]});
+            for (size_t i = n; i-- > 0;) {
+                for (size_t j = n - i + 1; j-- > 2;) ctrl(i, j);
+                gate(F, d, {t[i]});
+            }
+        }
+        qgpu::Step& b = c->steps[first];
+        b.block_len = uint32_t(c->steps.size() - first);
+        b.block_inverse = inverse != 0;
+        b.block_swap = swap != 0;
+        b.block_target = t;
+        c->plan_k = 0;
+    });
+}
+
 qgpu_status qgpu_circuit_cond_end(qgpu_circuit* c) {
     return guarded([&] {
         need_handle(c);

@@ -52,6 +52,12 @@ struct Step {
     bool has_shift = false;
     uint64_t c_reg = 0;
     bool destructive = true;
+    // first step of a QCircuit::QFT / TFQ block: the block's step count, its
+    // targets and flags, so that noiseless engines can run the block as one
+    // transform (the steps themselves are qpp's gate sequence)
+    uint32_t block_len = 0;
+    bool block_inverse = false, block_swap = false;
+    std::vector<uint64_t> block_target;
 };
 
 struct Block {

@@ -558,6 +558,23 @@ std::vector<size_t> canonical_order(const qgpu_circuit* c, bool canonical) {
     return order;
 }
 
+// A QCircuit::QFT / TFQ block met in its own step order by a noiseless
+// engine runs as one transform (op_apply_qft) instead of its k(k+1)/2 gate
+// steps; returns the steps consumed, 0 when the block does not apply.
+size_t run_block(qgpu_engine* e, const std::vector<size_t>& order, size_t i) {
+    const Step& st = e->circ->steps[order[i]];
+    if (e->noisy || st.block_len < 2 || i + st.block_len > order.size()) return 0;
+    for (size_t m = 1; m < st.block_len; ++m)
+        if (order[i + m] != order[i] + m) return 0;
+    std::vector<uint64_t> rel;
+    for (uint64_t q : st.block_target) {
+        if (e->measured[q]) return 0;
+        rel.push_back(rel_pos(e, q));
+    }
+    op_apply_qft(e->st, rel, e->circ->d, st.block_swap, st.block_inverse);
+    return st.block_len;
+}
+
 // qengine.hpp:240-345: steps order[pos..] executed reps times, each from
 // the engine state at entry; the statistics count every repetition that
 // measured something; the engine keeps the first repetition's state.
@@ -569,6 +586,10 @@ void repeat_steps(qgpu_engine* e, const std::vector<size_t>& order, size_t pos, 
         for (size_t i = pos; i < order.size(); ++i) {
             const Step& s = e->circ->steps[order[i]];
             if (is_measurement(s)) measured = true;
+            if (size_t b = run_block(e, order, i)) {
+                i += b - 1;
+                continue;
+            }
             i += run_step(e, s, order[i]); // a false IF skips its block
         }
         if (measured) e->stats[e->dits] += 1;
@@ -774,7 +795,13 @@ qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps) {
             while (pos < order.size() && !qgpu::is_measurement(e->circ->steps[order[pos]]) &&
                    !qgpu::is_runtime(e->circ->steps[order[pos]]))
                 ++pos;
-            for (size_t i = 0; i < pos; ++i) qgpu::run_step(e, e->circ->steps[order[i]], order[i]);
+            for (size_t i = 0; i < pos; ++i) {
+                if (size_t b = qgpu::run_block(e, order, i)) {
+                    i += b - 1;
+                    continue;
+                }
+                qgpu::run_step(e, e->circ->steps[order[i]], order[i]);
+            }
             bool can_sample = reps > 1 && !e->replay && pos < order.size();
             for (size_t i = pos; i < order.size() && can_sample; ++i)
                 if (e->circ->steps[order[i]].kind != qgpu::StepKind::Measure) can_sample = false;

@@ -70,6 +70,17 @@ qgpu_state* op_ptranspose(const qgpu_state* s,
                           const std::vector<uint64_t>& target);
 qgpu_state* op_syspermute(const qgpu_state* s,
                           const std::vector<uint64_t>& perm);
+// The gates of qpp's QFT circuits, column-major: Fd(d) as qpp::Gates::Fd
+// builds it (gates.hpp:260-285: H for d = 2, else pow(omega, i j) / sqrt(d),
+// omega = exp(2 pi i / d)); R_j = diag(exp(+-2 pi i m / d^j))
+// (operations.hpp:2616-2618, :2641-2646); SWAPd |a b> -> |b a>.
+std::vector<cd> fourier_gate(uint64_t d);
+std::vector<cd> qft_phase(uint64_t d, size_t j, bool inverse);
+std::vector<cd> swap_gate(uint64_t d);
+// qpp::applyQFT (inverse = false) / applyTFQ (true) on the state viewed as
+// qudits of dimension d; in place (the state's buffer may be replaced).
+void op_apply_qft(qgpu_state* s, const std::vector<uint64_t>& target, uint64_t d, bool swap,
+                  bool inverse);
 double op_norm2(const qgpu_state* s);
 cd op_trace(const qgpu_state* s);
 // qpp::normalize: ket / norm, rho / trace; returns false on a zero divisor.

@@ -1,0 +1,333 @@
+// CPU check of the QFT pass plans behind qgpu_apply_qft (qgpu::plan_qft) and
+// of the arithmetic of k_qft_pass: a host model of the kernel (same tables,
+// tile loop, step order and phases, in FP64) runs every pass of the plan,
+// and the result must equal the transform's definition within 1e-12:
+//   QFT with swap = the DFT on the register spelled by the targets
+//   (target[0] most significant): out[y] = sum_x w^(x y) in[x] / sqrt(N),
+//   w = exp(2 pi i / N), N = d^k; without swap the output digits are then
+//   reversed; TFQ is the adjoint. A density matrix gets U rho U^dagger.
+// It also checks that each pass reads and writes inside the state and writes
+// every element exactly once, and that the shared memory fits.
+// Built and run by tests/test_qft_plan.py.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "kernels.hpp"
+#include "ops.hpp"
+
+using namespace qgpu;
+using cdd = std::complex<double>;
+
+static int fails = 0;
+#define EXPECT(c)                                                                     \
+    do {                                                                              \
+        if (!(c)) {                                                                   \
+            if (fails < 20) std::printf("FAIL %s:%d %s\n", __FILE__, __LINE__, #c); \
+            ++fails;                                                                  \
+        }                                                                             \
+    } while (0)
+
+static uint64_t tile_sum(const QftPlan& p, uint32_t idx, bool write_order, int what) {
+    uint64_t acc = 0;
+    for (int q = 0; q < p.ntd; ++q) {
+        const int td = write_order ? p.wperm[q] : q;
+        const uint32_t pitch = write_order ? p.fpitch[q] : p.tpitch[q];
+        const uint32_t dg = (idx / pitch) % p.tdim[td];
+        const uint64_t w = what == 0 ? p.trs[td] : what == 1 ? p.tws[td] : p.tpitch[td];
+        acc += uint64_t(dg) * w;
+    }
+    return acc;
+}
+
+// Host model of one k_qft_pass launch (kernels_qft.cu), FP64.
+static size_t max_smem = 0;
+
+static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& W,
+                     const std::vector<cdd>& F, const std::vector<cdd>& in,
+                     std::vector<cdd>& out) {
+    const bool QB = p.d == 2;
+    EXPECT(p.E / p.Elo <= 256 && p.Elo <= 256 && p.E / p.Flo <= 256 && p.Flo <= 256);
+    EXPECT(p.E * eb <= 32768);
+    max_smem = std::max(max_smem, qft_smem_bytes(p, eb));
+    EXPECT(qft_smem_bytes(p, eb) <= 64 * 1024);
+    std::vector<uint64_t> rlo(p.Elo), rhi(p.E / p.Elo), wlo(p.Flo), whi(p.E / p.Flo);
+    std::vector<uint32_t> elo(p.Flo), ehi(p.E / p.Flo);
+    for (uint32_t i = 0; i < p.Elo; ++i) rlo[i] = tile_sum(p, i, false, 0);
+    for (uint32_t i = 0; i < p.E / p.Elo; ++i) rhi[i] = tile_sum(p, i * p.Elo, false, 0);
+    for (uint32_t i = 0; i < p.Flo; ++i) {
+        wlo[i] = tile_sum(p, i, true, 1);
+        elo[i] = uint32_t(tile_sum(p, i, true, 2));
+    }
+    for (uint32_t i = 0; i < p.E / p.Flo; ++i) {
+        whi[i] = tile_sum(p, i * p.Flo, true, 1);
+        ehi[i] = uint32_t(tile_sum(p, i * p.Flo, true, 2));
+    }
+    std::vector<int> written(out.size(), 0);
+    std::vector<cdd> tile(p.E), cst(size_t(p.M) * p.d * p.CZ);
+    const int M = p.M, d = p.d;
+    for (uint64_t t = 0; t < p.ntiles; ++t) {
+        uint64_t rb = 0, wb = 0, z = 0;
+        for (int q = 0; q < p.nod; ++q) {
+            const uint64_t dg = p.pow2 ? (t >> p.oshift[q]) & (p.odim[q] - 1)
+                                       : (t / p.opitch[q]) % p.odim[q];
+            rb += dg * p.ors[q];
+            wb += dg * p.ows[q];
+            z += dg * p.ozw[q];
+        }
+        for (int i = 0; i < M * d * int(p.CZ); ++i) {
+            const int c = i % int(p.CZ), jr = i / int(p.CZ);
+            const int j = jr / d, r = jr % d;
+            uint64_t zz = z;
+            for (int q = 0, cc = c; q < p.nzr; ++q, cc /= d) zz += uint64_t(cc % d) * p.zrw[q];
+            const uint64_t N = p.dpow[p.k - p.a - j];
+            EXPECT(uint64_t(r) * zz < N || r == 0);
+            const double x = 2.0 * (double(uint64_t(r) * zz) / double(N));
+            cst[size_t(i)] = cdd(std::cos(M_PI * x), p.sigma * std::sin(M_PI * x));
+        }
+        for (uint32_t e = 0; e < p.E; ++e) {
+            const uint32_t lo = QB ? (e & (p.Elo - 1)) : e % p.Elo;
+            const uint32_t hi = QB ? (e >> p.elo_shift) : e / p.Elo;
+            const uint64_t a = rb + rlo[lo] + rhi[hi];
+            EXPECT(a < in.size());
+            tile[e] = a < in.size() ? in[a] : 0.0;
+        }
+        for (int s = 0; s < M; ++s) {
+            const int j = p.inverse ? M - 1 - s : s;
+            if (QB) {
+                const int g = p.gpos[j];
+                const uint32_t lm = (1u << g) - 1;
+                const cdd* cj = cst.data() + (size_t(j) * 2 + 1) * p.CZ;
+                for (uint32_t pr = 0; pr < p.E / 2; ++pr) {
+                    const uint32_t e0 = ((pr & ~lm) << 1) | (pr & lm);
+                    const uint32_t e1 = e0 | (1u << g);
+                    uint32_t L = 0, c = 0;
+                    for (int l = j + 1; l < M; ++l) L = (L << 1) | ((e0 >> p.gpos[l]) & 1u);
+                    for (int q = 0; q < p.nzr; ++q) c |= ((e0 >> p.zpos[q]) & 1u) << q;
+                    const uint64_t wi = uint64_t(L << j) * p.wmul;
+                    EXPECT(wi < W.size());
+                    cdd w = W[wi];
+                    if (p.sigma < 0) w = std::conj(w);
+                    const cdd ph = w * cj[c];
+                    const cdd x = tile[e0];
+                    cdd y = tile[e1];
+                    if (!p.inverse) {
+                        tile[e0] = x + y;
+                        tile[e1] = (x - y) * ph;
+                    } else {
+                        y *= ph;
+                        tile[e0] = x + y;
+                        tile[e1] = x - y;
+                    }
+                }
+            } else {
+                const uint32_t pj = p.tpitch[p.gpos[j]];
+                const uint64_t dj = p.dpow[j];
+                for (uint32_t fb = 0; fb < p.E / d; ++fb) {
+                    const uint32_t hi = fb / pj, lo = fb - hi * pj;
+                    const uint32_t e0 = hi * pj * d + lo;
+                    uint64_t L = 0;
+                    uint32_t c = 0;
+                    for (int l = j + 1; l < M; ++l) L = L * d + (e0 / p.tpitch[p.gpos[l]]) % d;
+                    for (int q = p.nzr; q-- > 0;) c = c * d + (e0 / p.tpitch[p.zpos[q]]) % d;
+                    cdd v[kQftMaxD], o[kQftMaxD];
+                    for (int r = 0; r < d; ++r) v[r] = tile[e0 + r * pj];
+                    auto phase = [&](int r) {
+                        const uint64_t wi = (uint64_t(r) * L * dj) * p.wmul;
+                        EXPECT(wi < W.size());
+                        cdd w = W[wi];
+                        if (p.sigma < 0) w = std::conj(w);
+                        return w * cst[(size_t(j) * d + r) * p.CZ + c];
+                    };
+                    if (p.inverse)
+                        for (int r = 1; r < d; ++r) v[r] *= phase(r);
+                    for (int x = 0; x < d; ++x) {
+                        cdd acc = 0;
+                        for (int y = 0; y < d; ++y) acc += F[x + y * d] * v[y];
+                        o[x] = acc;
+                    }
+                    if (!p.inverse)
+                        for (int r = 1; r < d; ++r) o[r] *= phase(r);
+                    for (int r = 0; r < d; ++r) tile[e0 + r * pj] = o[r];
+                }
+            }
+        }
+        for (uint32_t f = 0; f < p.E; ++f) {
+            const uint32_t lo = QB ? (f & (p.Flo - 1)) : f % p.Flo;
+            const uint32_t hi = QB ? (f >> p.flo_shift) : f / p.Flo;
+            const uint32_t e = elo[lo] + ehi[hi];
+            EXPECT(e < p.E);
+            const uint64_t a = wb + wlo[lo] + whi[hi];
+            EXPECT(a < out.size());
+            if (a < out.size() && e < p.E) {
+                out[a] = tile[e] * (QB ? p.scale : 1.0);
+                written[a]++;
+            }
+        }
+    }
+    for (int w : written) EXPECT(w == 1);
+}
+
+// The transform's definition on virtual digits vt (all of dimension d) of a
+// vector over nv digits; conj_u applies conj(U) instead of U.
+static void reference(std::vector<cdd>& v, size_t nv, uint64_t d, const std::vector<size_t>& vt,
+                      bool swap, bool inverse, bool conj_u) {
+    const size_t k = vt.size();
+    uint64_t N = 1;
+    for (size_t i = 0; i < k; ++i) N *= d;
+    std::vector<uint64_t> stride(nv);
+    uint64_t s = 1;
+    for (size_t q = nv; q-- > 0;) {
+        stride[q] = s;
+        s *= d;
+    }
+    std::vector<char> is_t(nv, 0);
+    for (size_t t : vt) is_t[t] = 1;
+    auto reg_off = [&](uint64_t x) { // offset of register value x
+        uint64_t o = 0;
+        for (size_t a = k; a-- > 0;) {
+            o += (x % d) * stride[vt[a]];
+            x /= d;
+        }
+        return o;
+    };
+    auto rev = [&](uint64_t x) {
+        uint64_t r = 0;
+        for (size_t a = 0; a < k; ++a) {
+            r = r * d + x % d;
+            x /= d;
+        }
+        return r;
+    };
+    const double sgn = (inverse ? -1.0 : 1.0) * (conj_u ? -1.0 : 1.0);
+    std::vector<cdd> root(N);
+    for (uint64_t e = 0; e < N; ++e) root[e] = std::polar(1.0, sgn * 2.0 * M_PI * double(e) / double(N));
+    std::vector<cdd> reg(N), res(N);
+    for (uint64_t base = 0; base < v.size(); ++base) {
+        bool zero = true; // bases with every target digit 0
+        for (size_t q = 0; q < nv; ++q)
+            if (is_t[q] && (base / stride[q]) % d) zero = false;
+        if (!zero) continue;
+        for (uint64_t x = 0; x < N; ++x) reg[x] = v[base + reg_off(x)];
+        if (inverse && !swap) {
+            std::vector<cdd> t(N);
+            for (uint64_t x = 0; x < N; ++x) t[rev(x)] = reg[x];
+            reg = t;
+        }
+        for (uint64_t y = 0; y < N; ++y) {
+            cdd acc = 0;
+            for (uint64_t x = 0; x < N; ++x) {
+                acc += root[(x * y) % N] * reg[x];
+            }
+            res[y] = acc / std::sqrt(double(N));
+        }
+        if (!inverse && !swap) {
+            std::vector<cdd> t(N);
+            for (uint64_t x = 0; x < N; ++x) t[rev(x)] = res[x];
+            res = t;
+        }
+        for (uint64_t y = 0; y < N; ++y) v[base + reg_off(y)] = res[y];
+    }
+}
+
+static double check_case(bool rho, size_t n, uint64_t d, const std::vector<uint64_t>& target,
+                         bool swap, bool inverse, size_t eb, std::mt19937_64& rng) {
+    uint64_t D = 1;
+    for (size_t i = 0; i < n; ++i) D *= d;
+    const uint64_t elems = rho ? D * D : D;
+    std::normal_distribution<double> g;
+    std::vector<cdd> v(elems);
+    for (auto& x : v) x = cdd(g(rng), g(rng));
+    std::vector<cdd> ref = v;
+    if (!rho) {
+        std::vector<size_t> vt(target.begin(), target.end());
+        reference(ref, n, d, vt, swap, inverse, false);
+    } else {
+        std::vector<size_t> rows, cols;
+        for (uint64_t t : target) {
+            rows.push_back(n + t);
+            cols.push_back(t);
+        }
+        reference(ref, 2 * n, d, rows, swap, inverse, false);
+        reference(ref, 2 * n, d, cols, swap, inverse, true);
+    }
+    const bool rev = swap && target.size() >= 2;
+    QftSchedule S;
+    const bool ok = plan_qft(rho, D, d, eb, target, inverse, rev, S);
+    EXPECT(ok);
+    if (!ok) return 1e300;
+    int nfold = 0;
+    for (char f : S.fold) nfold += f;
+    EXPECT(nfold == (rev ? 1 : 0));
+    const std::vector<cdd> W = qft_roots(S.nW);
+    const std::vector<cdd> Fd = fourier_gate(d);
+    std::vector<cdd> Fc(Fd.size());
+    for (size_t i = 0; i < Fd.size(); ++i) Fc[i] = std::conj(Fd[i]);
+    std::vector<cdd> cur = v, other(elems);
+    for (size_t i = 0; i < S.plans.size(); ++i) {
+        const QftPlan& p = S.plans[i];
+        EXPECT(p.ntiles * p.E == elems);
+        const std::vector<cdd>& F = p.sigma > 0 ? Fd : Fc;
+        if (S.fold[i]) {
+            run_pass(p, eb, W, F, cur, other);
+            std::swap(cur, other);
+        } else {
+            std::vector<cdd> tmp(elems);
+            run_pass(p, eb, W, F, cur, tmp);
+            cur.swap(tmp);
+        }
+    }
+    double num = 0, den = 0;
+    for (uint64_t i = 0; i < elems; ++i) {
+        num = std::max(num, std::abs(cur[i] - ref[i]));
+        den = std::max(den, std::abs(ref[i]));
+    }
+    return num / den;
+}
+
+int main() {
+    std::mt19937_64 rng(12345);
+    int cases = 0;
+    double worst = 0;
+    struct Cfg {
+        bool rho;
+        size_t n;
+        uint64_t d;
+    };
+    std::vector<Cfg> cfgs = {{false, 1, 2},  {false, 2, 2}, {false, 5, 2},  {false, 9, 2},
+                             {false, 12, 2}, {false, 14, 2}, {false, 3, 3}, {false, 6, 3},
+                             {false, 4, 4},  {false, 3, 5}, {false, 2, 16}, {true, 1, 2},
+                             {true, 3, 2},   {true, 5, 2},  {true, 6, 2},   {true, 2, 3},
+                             {true, 3, 3}};
+    for (const Cfg& c : cfgs) {
+        for (int rep = 0; rep < 6; ++rep) {
+            // random target subset in random order (all digits on rep 0)
+            std::vector<uint64_t> all(c.n);
+            for (size_t i = 0; i < c.n; ++i) all[i] = i;
+            std::shuffle(all.begin(), all.end(), rng);
+            size_t k = rep == 0 ? c.n : 1 + rng() % c.n;
+            if (rep == 0) std::sort(all.begin(), all.end());
+            std::vector<uint64_t> t(all.begin(), all.begin() + long(k));
+            const bool swap = rep % 3 != 2, inverse = rep % 2 == 1;
+            for (size_t eb : {size_t(16), size_t(8)}) {
+                double e = check_case(c.rho, c.n, c.d, t, swap, inverse, eb, rng);
+                worst = std::max(worst, e);
+                if (e > 1e-12 && fails < 20) {
+                    std::printf("FAIL rho=%d n=%zu d=%llu k=%zu swap=%d inv=%d eb=%zu err=%g\n",
+                                int(c.rho), c.n, (unsigned long long)c.d, k, int(swap),
+                                int(inverse), eb, e);
+                    ++fails;
+                }
+                ++cases;
+            }
+        }
+    }
+    std::printf("%d cases, worst relative error %.3g, shared memory up to %zu B\n", cases,
+                worst, max_smem);
+    if (fails) return 1;
+    std::printf("qft plans ok\n");
+    return 0;
+}
