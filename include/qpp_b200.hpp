@@ -16,6 +16,8 @@
 //   qpp_b200::measure_seq(A, target, dims, destructive, seed) instruments.hpp:985
 //   qpp_b200::measure(A, Ks | V, target, dims, destructive, seed) instruments.hpp:371, :587
 //   qpp_b200::reset(A, target, dims, seed), discard(...)    instruments.hpp:1148, :1243
+//   qpp_b200::applyQFT / applyTFQ(A, target, d, swap)       operations.hpp:2565, :2680
+//   qpp_b200::QFT / TFQ(A, d, swap)                         operations.hpp:2792, :2844
 //
 // Matrices are qpp_b200::cmat (column-major std::complex<double>, rows x
 // cols; a ket is D x 1). When Eigen is available the same functions accept
@@ -349,6 +351,39 @@ measure_seq(const cmat& A, const std::vector<idx>& target, const std::vector<idx
     detail::check(qgpu_state_download_c128(o.s, out.raw()));
     return {std::vector<idx>(res.begin(), res.begin() + t.size()),
             std::vector<double>(ps.begin(), ps.begin() + t.size()), out};
+}
+
+// qpp::applyQFT / applyTFQ (operations.hpp:2565-2787), qpp::QFT / TFQ
+// (:2792-2899): A viewed as qudits of dimension d.
+inline cmat applyQFT(const cmat& A, const std::vector<idx>& target, idx d = 2,
+                     bool swap = true) {
+    auto t = detail::u64(target);
+    cmat out(A.rows(), A.cols());
+    detail::check(qgpu_host_apply_qft(detail::ctx(), A.raw(), A.rows(), A.cols(),
+                                      detail::ptr(t), uint32_t(t.size()), d, swap ? 1 : 0, 0,
+                                      out.raw()));
+    return out;
+}
+inline cmat applyTFQ(const cmat& A, const std::vector<idx>& target, idx d = 2,
+                     bool swap = true) {
+    auto t = detail::u64(target);
+    cmat out(A.rows(), A.cols());
+    detail::check(qgpu_host_apply_qft(detail::ctx(), A.raw(), A.rows(), A.cols(),
+                                      detail::ptr(t), uint32_t(t.size()), d, swap ? 1 : 0, 1,
+                                      out.raw()));
+    return out;
+}
+inline cmat QFT(const cmat& A, idx d = 2, bool swap = true) {
+    cmat out(A.rows(), A.cols());
+    detail::check(qgpu_host_qft(detail::ctx(), A.raw(), A.rows(), A.cols(), d, swap ? 1 : 0, 0,
+                                out.raw()));
+    return out;
+}
+inline cmat TFQ(const cmat& A, idx d = 2, bool swap = true) {
+    cmat out(A.rows(), A.cols());
+    detail::check(qgpu_host_qft(detail::ctx(), A.raw(), A.rows(), A.cols(), d, swap ? 1 : 0, 1,
+                                out.raw()));
+    return out;
 }
 
 namespace detail {

@@ -109,6 +109,27 @@ int main() {
     EXPECT(std::abs(std::abs(z(0)) - 1.0) < 1e-15);
     cmat dsc = discard(bell, {0}, {2, 2}, 9);
     EXPECT(dsc.rows() == 2 && dsc.cols() == 1);
+    // QFT of |1> on 3 qubits: amplitudes exp(2 pi i y / 8) / sqrt(8); TFQ
+    // brings it back; applyQFT on one qubit is H
+    cmat one(8, 1);
+    one(1) = 1;
+    cmat f = QFT(one);
+    double qerr = 0;
+    for (idx y = 0; y < 8; ++y)
+        qerr = std::max(qerr, std::abs(f(y) - std::polar(1.0 / std::sqrt(8.0), 2 * M_PI * y / 8.0)));
+    EXPECT(qerr < 1e-15);
+    EXPECT(dist(TFQ(f), one) < 1e-15);
+    cmat H(2, 2);
+    H(0, 0) = H(0, 1) = H(1, 0) = 1 / std::sqrt(2.0);
+    H(1, 1) = -1 / std::sqrt(2.0);
+    EXPECT(dist(applyQFT(one, {2}), apply(one, H, {2}, {2, 2, 2})) < 1e-15);
+    caught = false;
+    try {
+        applyQFT(one, {3});
+    } catch (const exception::SubsysMismatchDims& e) {
+        caught = e.where() == "qpp::applyQFT()" && e.detail() == "dims/target";
+    }
+    EXPECT(caught);
     std::printf(fails ? "shim FAILED (%d)\n" : "shim ok\n", fails);
     return fails ? 1 : 0;
 }
