@@ -13,6 +13,12 @@
            layer), complex64: one CUDA-graph launch versus the plain loop of
            per-instance launches (and that loop in complex128).
 
+  qft      QCircuit::QFT on n qubits executed by QEngine, as the reference's
+           benchmarks/src/qft_bench.cpp and tfq_bench.cpp time it (engine
+           reset, then execute); n = 20, 26, 30 in complex128 and n = 30 in
+           complex64, against the same circuit run gate by gate (one pass per
+           qpp gate) on the GPU.
+
 Device times are CUDA events on the library's stream. The CPU figures time
 the oracle (the CPU restatement of qpp, all host cores) on a bounded sample
 of the same work; the oracle is test infrastructure and is imported only
@@ -28,7 +34,8 @@ import time
 
 import numpy as np
 
-from . import (C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, State, batch_last_phases,
+from . import (C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, Engine, State,
+               batch_last_phases,
                run_batch, traj_tile_width)
 from .workloads import haar_unitary, ket_gate_sequence
 
@@ -81,6 +88,64 @@ def config1(ctx, torch, stream, cpu=True):
         out["cpu"] = {"gates_per_s": 200 / cpu_s, "GBps": cb / cpu_s / 1e9,
                       "cores": os.cpu_count(), "sample": "first 200 gates", "kind": "port"}
     s.free()
+    return out
+
+
+def qft(ctx, torch, stream, sizes=(20, 26, 30), cpu=True):
+    """QCircuit::QFT / TFQ on every qubit, QEngine reset + execute per
+    iteration (benchmarks/src/qft_bench.cpp, tfq_bench.cpp). The engine runs
+    the QFT block as ceil(n / 8) shared-memory passes; the bytes per
+    iteration are that many reads and writes of the state."""
+    rows = []
+    for n in sizes:
+        for prec, eb in ((C128, 16), (C64, 8)):
+            if prec == C64 and n != max(sizes):
+                continue
+            for inverse in (False, True):
+                c = Circuit(n)
+                c.TFQ() if inverse else c.QFT()
+                e = Engine(ctx, c, KET, prec)
+                e.reset().execute()  # warm-up: state allocation
+                ts, tx = [], []
+                for _ in range(5):
+                    a, m, b = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+                    a.record(stream)
+                    e.reset()
+                    m.record(stream)
+                    e.execute()
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    ts.append(a.elapsed_time(b))
+                    tx.append(m.elapsed_time(b))
+                ms, mx = float(np.median(ts)), float(np.median(tx))
+                passes = -(-n // 8)
+                byts = passes * 2 * eb * 2 ** n
+                row = {"n": n, "prec": "c128" if prec == C128 else "c64",
+                       "op": "TFQ" if inverse else "QFT", "steps": c.steps(),
+                       "ms_reset_execute": ms, "ms_execute": mx, "passes": passes,
+                       "GBps_execute": byts / (mx / 1e3) / 1e9}
+                if n <= 26 and prec == C128:
+                    s = State(ctx, KET, [2] * n, C128).fill_gaussian(1)
+                    c.run(s, PLAIN)
+                    a, b = _events(torch, stream)
+                    a.record(stream)
+                    c.run(s, PLAIN)
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    row["gate_by_gate_ms"] = a.elapsed_time(b)
+                    s.free()
+                del e
+                rows.append(row)
+    out = {"rows": rows}
+    if cpu:
+        from oracle import oracle as orc  # CPU baseline sample only
+        n = 18
+        psi = np.zeros(2 ** n, dtype=np.complex128)
+        psi[0] = 1
+        t0 = time.perf_counter()
+        orc.QFT(psi)
+        out["cpu"] = {"n": n, "ms": (time.perf_counter() - t0) * 1e3, "cores": os.cpu_count(),
+                      "kind": "port", "sample": "qpp's QFT gate sequence on 18 qubits"}
     return out
 
 
@@ -271,16 +336,18 @@ def main():
     import argparse
 
     import torch
-    ap = argparse.ArgumentParser(description="configs 1, 2 and 4 on one GPU")
-    ap.add_argument("--only", choices=["config1", "config2", "config4"], action="append",
+    ap = argparse.ArgumentParser(description="configs 1, 2 and 4 and the QFT benchmark on one GPU")
+    ap.add_argument("--only", choices=["config1", "config2", "config4", "qft"], action="append",
                     help="run only these configs (repeatable)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline samples")
     ap.add_argument("--steps", type=int, default=200, help="config 2 steps")
     ap.add_argument("--kets", type=int, default=2048, help="config 4 kets")
     ap.add_argument("--rho", type=int, default=512, help="config 4 density matrices")
     ap.add_argument("--depth", type=int, default=20, help="config 4 circuit depth")
+    ap.add_argument("--qft-n", type=int, action="append",
+                    help="QFT benchmark qubit counts (repeatable; default 20, 26, 30)")
     a = ap.parse_args()
-    run = set(a.only or ["config1", "config2", "config4"])
+    run = set(a.only or ["config1", "config2", "config4", "qft"])
     cpu = not a.no_cpu
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -289,6 +356,8 @@ def main():
         out["config1"] = config1(ctx, torch, stream, cpu)
     if "config2" in run:
         out["config2"] = config2(ctx, torch, stream, cpu, steps=max(a.steps, 3))
+    if "qft" in run:
+        out["qft"] = qft(ctx, torch, stream, sizes=tuple(a.qft_n or (20, 26, 30)), cpu=cpu)
     if "config4" in run:
         out["config4"] = config4(ctx, torch, stream, n_kets=a.kets, n_rho=a.rho, depth=a.depth)
     print(json.dumps(out), flush=True)

@@ -86,7 +86,7 @@ void clear_registers(qgpu_engine* e) {
 
 // materialise |0...0> (ket) or |0...0><0...0| when the engine has no state
 void ensure_state(qgpu_engine* e) {
-    if (e->dits.size() != e->circ->nc) clear_registers(e);
+    if (e->dits.size() != e->circ->nc || e->measured.size() != e->circ->nq) clear_registers(e);
     if (e->noise_results.size() != e->circ->steps.size())
         e->noise_results.resize(e->circ->steps.size());
     if (e->st) return;
