@@ -22,16 +22,26 @@ using qgpu::raise;
 
 namespace qgpu {
 
-thread_local std::string t_where, t_what;
+// Plain character arrays: trivially destructible, so that a library call made
+// while the thread is being torn down (a caller's thread_local holder
+// destroying its context after this file's thread_locals are gone) still
+// writes valid memory.
+thread_local char t_where[256], t_what[1024];
+
+static void copy_msg(char* dst, size_t cap, const std::string& src) {
+    const size_t n = std::min(cap - 1, src.size());
+    std::memcpy(dst, src.data(), n);
+    dst[n] = '\0';
+}
 
 void record_error(qgpu_status, const std::string& where,
                   const std::string& what) {
-    t_where = where;
-    t_what = what;
+    copy_msg(t_where, sizeof(t_where), where);
+    copy_msg(t_what, sizeof(t_what), what);
 }
 void clear_error() {
-    t_where.clear();
-    t_what.clear();
+    t_where[0] = '\0';
+    t_what[0] = '\0';
 }
 
 void after_launch(qgpu_ctx* ctx, const char* name) {
@@ -347,8 +357,8 @@ qgpu_state* host_state(qgpu_ctx* ctx, const double* state, uint64_t rows,
 
 extern "C" {
 
-const char* qgpu_last_error_where(void) { return qgpu::t_where.c_str(); }
-const char* qgpu_last_error_what(void) { return qgpu::t_what.c_str(); }
+const char* qgpu_last_error_where(void) { return qgpu::t_where; }
+const char* qgpu_last_error_what(void) { return qgpu::t_what; }
 const char* qgpu_version(void) { return "qpp_b200 0.1.0 (sm_100a)"; }
 
 const char* qgpu_status_name(qgpu_status s) {
