@@ -70,16 +70,15 @@ void launch_ptrace(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
 
 // --- quantum Fourier transform passes (kernels_qft.cu) --------------------
 // One pass applies the QFT (or TFQ) steps of targets [a, a + M) of a k-target
-// transform to every tile. Tile digits are listed by ascending read stride
-// (tile index e = sum digit * tpitch); `wperm` lists them by ascending write
-// stride (store index f = sum digit * fpitch). Outer digits enumerate the
-// tiles (tile number = sum digit * opitch); ozw is a digit's weight in the
-// integer Z spelled by the targets after the group (0 for other digits).
-// Later targets that sit in the tile (the low digits that make the runs
-// contiguous) are the tile's phase digits: zpos (tile digit; tile bit for
-// qubits) and zrw (weight in Z); the per-tile step constants are tabulated
-// over their d^nzr values.
-constexpr int kQftMaxPhaseDigits = 4;
+// transform to every tile. The tile index is mixed radix over the tile
+// digits in tile order: first the nr run digits (the lowest other digits in
+// memory, Rsize values together), then the group digits with step M - 1
+// lowest and step 0 highest, so that a step's phase index is a plain shift
+// and mask of the tile index. Loads and stores walk the tile in memory order
+// (rperm / wperm: tile digits by ascending read / write stride, with pitches
+// rpitch / wpitch in that order). Outer digits enumerate the tiles (tile
+// number = sum digit * opitch); ozw / tzw are a digit's weight in the integer
+// spelled by the targets after the group (0 for other digits).
 constexpr int kQftMaxTile = 16;
 constexpr int kQftMaxOuter = 64;
 constexpr int kQftMaxD = 16;
@@ -88,17 +87,13 @@ struct QftPlan {
     uint64_t dpow[65]; // d^e for e <= k
     uint64_t odim[kQftMaxOuter], opitch[kQftMaxOuter];
     uint64_t ors[kQftMaxOuter], ows[kQftMaxOuter], ozw[kQftMaxOuter];
-    uint64_t trs[kQftMaxTile], tws[kQftMaxTile];
-    uint32_t tdim[kQftMaxTile], tpitch[kQftMaxTile], fpitch[kQftMaxTile];
-    int wperm[kQftMaxTile];
-    int gpos[kQftMaxTile]; // tile digit of group step j
-    uint64_t zrw[kQftMaxPhaseDigits];
-    int zpos[kQftMaxPhaseDigits];
-    int nzr;
-    uint32_t CZ; // d^nzr
+    uint64_t trs[kQftMaxTile], tws[kQftMaxTile], tzw[kQftMaxTile];
+    uint32_t tdim[kQftMaxTile], tpitch[kQftMaxTile];
+    int rperm[kQftMaxTile], wperm[kQftMaxTile];
+    uint32_t rpitch[kQftMaxTile], wpitch[kQftMaxTile];
     uint8_t oshift[kQftMaxOuter];
-    uint32_t E, Elo, Flo, wmul;
-    int ntd, nod, M, a, k, d, sigma, inverse, pow2, elo_shift, flo_shift;
+    uint32_t E, Rsize, Glo, Flo, wmul, nW;
+    int ntd, nr, nod, M, a, k, d, sigma, inverse, pow2, glo_shift, flo_shift;
     double scale; // qubit passes: 2^(-M/2)
 };
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes);
@@ -117,7 +112,7 @@ bool plan_qft(bool rho, uint64_t D, uint64_t d, size_t elem_bytes,
               const std::vector<uint64_t>& target, bool inverse, bool fold, QftSchedule& S);
 // exp(2 pi i e / nW), e < nW
 std::vector<std::complex<double>> qft_roots(uint64_t nW);
-// W: exp(2 pi i e / d^Mmax), e < d^Mmax (state precision; p.wmul = d^(Mmax-M));
+// W: exp(2 pi i e / nW), e < nW = d^Mmax (state precision; p.wmul = d^(Mmax-M));
 // F: the d x d Fourier matrix of the pass, column-major (qudits only).
 void launch_qft_pass(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
                      const QftPlan& p, const void* W, const void* F);

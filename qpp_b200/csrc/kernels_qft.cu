@@ -13,9 +13,12 @@
 // A pass applies the steps of M consecutive targets [a, a + M) to tiles that
 // hold every value of those M digits, plus the lowest other digits in memory
 // order so that reads and writes run over >= 128 contiguous bytes, staged in
-// shared memory. The part of each step's phase that depends on digits
-// outside the group is one constant per tile, step and value of the later
-// targets inside the tile (at most 4 of them). A pass reads and
+// shared memory. In the tile index the run digits come first and the group
+// digits follow with step M - 1 lowest, so the phase of step j splits into
+// W[L << j] (L = the group digits after j: a shift and mask of the index),
+// a constant per tile for the later targets outside the tile, and a factor
+// for the later targets among the run digits (the low index bits): the last
+// two are tabulated per tile over the run digits' values. A pass reads and
 // writes every amplitude once, so a k-digit transform costs ceil(k / M)
 // passes over the state instead of the k(k+1)/2 gate passes of the gate
 // sequence. The pass that also reverses the targets reads one buffer and
@@ -40,14 +43,13 @@ __device__ __forceinline__ C csub(C a, C b) {
     return {a.x - b.x, a.y - b.y};
 }
 
-// Tile offsets of index e (tile digits in read order) or of store index f
-// (tile digits in write order): sum over the digits of digit * stride.
-__device__ inline uint64_t tile_sum(const QftPlan& p, uint32_t idx, bool write_order,
-                                    int what) {
+// Memory offset (what = 0 read, 1 write) or tile index (what = 2) of the
+// element at position idx of the read (write_order = false) or write order.
+__device__ inline uint64_t order_sum(const QftPlan& p, uint32_t idx, bool write_order, int what) {
     uint64_t acc = 0;
     for (int q = 0; q < p.ntd; ++q) {
-        const int td = write_order ? p.wperm[q] : q;
-        const uint32_t pitch = write_order ? p.fpitch[q] : p.tpitch[q];
+        const int td = write_order ? p.wperm[q] : p.rperm[q];
+        const uint32_t pitch = write_order ? p.wpitch[q] : p.rpitch[q];
         const uint32_t dg = (idx / pitch) % p.tdim[td];
         const uint64_t w = what == 0 ? p.trs[td] : what == 1 ? p.tws[td] : p.tpitch[td];
         acc += uint64_t(dg) * w;
@@ -58,40 +60,56 @@ __device__ inline uint64_t tile_sum(const QftPlan& p, uint32_t idx, bool write_o
 } // namespace
 
 // One CTA per tile (grid-stride over tiles). Dynamic shared memory: the tile
-// (E amplitudes), the per-tile step constants (M * d * d^nzr), and the read /
-// write offset tables split into a low and a high half.
+// (E amplitudes), the per-tile step constants (M * d * Rsize), the roots of
+// unity W (nW, conjugated for s = -1), and the offset / tile-index tables of
+// the read and write orders split into a low and a high half.
 template <typename R, bool QB>
 __global__ void __launch_bounds__(256, 4)
     k_qft_pass(const Cplx<R>* in, Cplx<R>* out, const __grid_constant__ QftPlan p,
-               const Cplx<R>* __restrict__ W, const Cplx<R>* __restrict__ F) {
+               const Cplx<R>* __restrict__ Wg, const Cplx<R>* __restrict__ F) {
     using C = Cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int M = p.M, d = p.d;
+    const uint32_t ncst = uint32_t(M) * d * p.Rsize;
     C* tile = reinterpret_cast<C*>(smem_raw);
     C* cst = tile + p.E;
-    uint64_t* rlo = reinterpret_cast<uint64_t*>(cst + p.M * p.d * p.CZ);
-    uint64_t* rhi = rlo + p.Elo;
-    uint64_t* wlo = rhi + p.E / p.Elo;
-    uint64_t* whi = wlo + p.Flo;
-    uint32_t* elo = reinterpret_cast<uint32_t*>(whi + p.E / p.Flo);
-    uint32_t* ehi = elo + p.Flo;
+    C* W = cst + ncst;
+    uint64_t* goff_lo = reinterpret_cast<uint64_t*>(W + p.nW);
+    uint64_t* goff_hi = goff_lo + p.Glo;
+    uint64_t* woff_lo = goff_hi + p.E / p.Glo;
+    uint64_t* woff_hi = woff_lo + p.Flo;
+    uint32_t* ge_lo = reinterpret_cast<uint32_t*>(woff_hi + p.E / p.Flo);
+    uint32_t* ge_hi = ge_lo + p.Glo;
+    uint32_t* we_lo = ge_hi + p.E / p.Glo;
+    uint32_t* we_hi = we_lo + p.Flo;
 
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (uint32_t i = tid; i < p.Elo; i += nt) rlo[i] = tile_sum(p, i, false, 0);
-    for (uint32_t i = tid; i < p.E / p.Elo; i += nt) rhi[i] = tile_sum(p, i * p.Elo, false, 0);
+    for (uint32_t i = tid; i < p.Glo; i += nt) {
+        goff_lo[i] = order_sum(p, i, false, 0);
+        ge_lo[i] = uint32_t(order_sum(p, i, false, 2));
+    }
+    for (uint32_t i = tid; i < p.E / p.Glo; i += nt) {
+        goff_hi[i] = order_sum(p, i * p.Glo, false, 0);
+        ge_hi[i] = uint32_t(order_sum(p, i * p.Glo, false, 2));
+    }
     for (uint32_t i = tid; i < p.Flo; i += nt) {
-        wlo[i] = tile_sum(p, i, true, 1);
-        elo[i] = uint32_t(tile_sum(p, i, true, 2));
+        woff_lo[i] = order_sum(p, i, true, 1);
+        we_lo[i] = uint32_t(order_sum(p, i, true, 2));
     }
     for (uint32_t i = tid; i < p.E / p.Flo; i += nt) {
-        whi[i] = tile_sum(p, i * p.Flo, true, 1);
-        ehi[i] = uint32_t(tile_sum(p, i * p.Flo, true, 2));
+        woff_hi[i] = order_sum(p, i * p.Flo, true, 1);
+        we_hi[i] = uint32_t(order_sum(p, i * p.Flo, true, 2));
+    }
+    for (uint32_t i = tid; i < p.nW; i += nt) {
+        C w = Wg[i];
+        w.y *= R(p.sigma);
+        W[i] = w;
     }
     __syncthreads();
 
-    const int M = p.M, d = p.d;
-    const R sg = R(p.sigma);
+    const uint32_t Rs = p.Rsize;
     for (uint64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
-        // base offsets and Z (the value of the later targets outside the tile)
+        // base offsets and Z (the later targets outside the tile)
         uint64_t rb = 0, wb = 0, z = 0;
         for (int q = 0; q < p.nod; ++q) {
             const uint64_t dg = p.pow2 ? (t >> p.oshift[q]) & (p.odim[q] - 1)
@@ -101,39 +119,37 @@ __global__ void __launch_bounds__(256, 4)
             z += dg * p.ozw[q];
         }
         // step constants exp(s 2 pi i r (Z + Zr(c)) / d^(k-i)), i = a + j, for
-        // every value c of the phase digits; r (Z + Zr) < d^(k-i)
-        for (int i = tid; i < M * d * int(p.CZ); i += nt) {
-            const int c = i % int(p.CZ), jr = i / int(p.CZ);
-            const int j = jr / d, r = jr % d;
+        // every value c of the run digits (Zr: the later targets among them);
+        // r (Z + Zr) < d^(k-i)
+        for (uint32_t i = tid; i < ncst; i += nt) {
+            const uint32_t c = i % Rs, jr = i / Rs;
+            const int j = int(jr) / d, r = int(jr) % d;
             uint64_t zz = z;
-            for (int q = 0, cc = c; q < p.nzr; ++q, cc /= d) zz += uint64_t(cc % d) * p.zrw[q];
+            for (int q = 0; q < p.nr; ++q) zz += uint64_t((c / p.tpitch[q]) % p.tdim[q]) * p.tzw[q];
             const uint64_t N = p.dpow[p.k - p.a - j];
             double sn, cs;
             sincospi(2.0 * (double(uint64_t(r) * zz) / double(N)), &sn, &cs);
             cst[i] = C{R(cs), R(p.sigma * sn)};
         }
-        for (uint32_t e = tid; e < p.E; e += nt) {
-            const uint32_t lo = QB ? (e & (p.Elo - 1)) : e % p.Elo;
-            const uint32_t hi = QB ? (e >> p.elo_shift) : e / p.Elo;
-            tile[e] = in[rb + rlo[lo] + rhi[hi]];
+        for (uint32_t g = tid; g < p.E; g += nt) {
+            const uint32_t lo = QB ? (g & (p.Glo - 1)) : g % p.Glo;
+            const uint32_t hi = QB ? (g >> p.glo_shift) : g / p.Glo;
+            tile[ge_lo[lo] + ge_hi[hi]] = in[rb + goff_lo[lo] + goff_hi[hi]];
         }
         __syncthreads();
 
         for (int s = 0; s < M; ++s) {
             const int j = p.inverse ? M - 1 - s : s;
             if constexpr (QB) {
-                const int g = p.gpos[j]; // tile bit of digit j
+                const int g = p.nr + M - 1 - j; // tile bit of step j
                 const uint32_t lm = (1u << g) - 1;
-                const C* cj = cst + (j * 2 + 1) * p.CZ;
+                const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
+                const C* cj = cst + (j * 2 + 1) * Rs;
                 for (uint32_t pr = tid; pr < p.E / 2; pr += nt) {
                     const uint32_t e0 = ((pr & ~lm) << 1) | (pr & lm);
                     const uint32_t e1 = e0 | (1u << g);
-                    uint32_t L = 0, c = 0;
-                    for (int l = j + 1; l < M; ++l) L = (L << 1) | ((e0 >> p.gpos[l]) & 1u);
-                    for (int q = 0; q < p.nzr; ++q) c |= ((e0 >> p.zpos[q]) & 1u) << q;
-                    C w = W[(L << j) * p.wmul];
-                    w.y *= sg;
-                    const C ph = cmul(w, cj[c]);
+                    const uint32_t L = (e0 >> p.nr) & Lmask;
+                    const C ph = cmul(W[(L << j) * p.wmul], cj[e0 & (Rs - 1)]);
                     const C x = tile[e0];
                     C y = tile[e1];
                     if (!p.inverse) {
@@ -146,22 +162,18 @@ __global__ void __launch_bounds__(256, 4)
                     }
                 }
             } else {
-                const uint32_t pj = p.tpitch[p.gpos[j]];
-                const uint64_t dj = p.dpow[j];
+                const uint32_t pj = Rs * uint32_t(p.dpow[M - 1 - j]);
+                const uint64_t Ld = p.dpow[M - 1 - j], dj = p.dpow[j];
                 for (uint32_t fb = tid; fb < p.E / d; fb += nt) {
                     const uint32_t hi = fb / pj, lo = fb - hi * pj;
                     const uint32_t e0 = hi * pj * d + lo;
-                    uint64_t L = 0;
-                    uint32_t c = 0;
-                    for (int l = j + 1; l < M; ++l)
-                        L = L * d + (e0 / p.tpitch[p.gpos[l]]) % d;
-                    for (int q = p.nzr; q-- > 0;) c = c * d + (e0 / p.tpitch[p.zpos[q]]) % d;
+                    const uint64_t L = (e0 / Rs) % Ld;
+                    const uint32_t c = e0 % Rs;
                     C v[kQftMaxD], o[kQftMaxD];
                     for (int r = 0; r < d; ++r) v[r] = tile[e0 + r * pj];
                     auto phase = [&](int r) {
-                        C w = W[(uint64_t(r) * L * dj) * p.wmul]; // r L d^j < d^M
-                        w.y *= sg;
-                        return cmul(w, cst[(j * d + r) * p.CZ + c]);
+                        return cmul(W[(uint64_t(r) * L * dj) * p.wmul], // r L d^j < d^M
+                                    cst[(j * d + r) * Rs + c]);
                     };
                     if (p.inverse)
                         for (int r = 1; r < d; ++r) v[r] = cmul(v[r], phase(r));
@@ -182,21 +194,20 @@ __global__ void __launch_bounds__(256, 4)
         for (uint32_t f = tid; f < p.E; f += nt) {
             const uint32_t lo = QB ? (f & (p.Flo - 1)) : f % p.Flo;
             const uint32_t hi = QB ? (f >> p.flo_shift) : f / p.Flo;
-            C v = tile[elo[lo] + ehi[hi]];
+            C v = tile[we_lo[lo] + we_hi[hi]];
             if (QB) {
                 v.x *= sc;
                 v.y *= sc;
             }
-            out[wb + wlo[lo] + whi[hi]] = v;
+            out[wb + woff_lo[lo] + woff_hi[hi]] = v;
         }
         __syncthreads();
     }
 }
 
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes) {
-    return p.E * elem_bytes + size_t(p.M) * p.d * p.CZ * elem_bytes +
-           (p.Elo + p.E / p.Elo + p.Flo + p.E / p.Flo) * sizeof(uint64_t) +
-           (p.Flo + p.E / p.Flo) * sizeof(uint32_t);
+    return (p.E + size_t(p.M) * p.d * p.Rsize + p.nW) * elem_bytes +
+           (p.Glo + p.E / p.Glo + p.Flo + p.E / p.Flo) * (sizeof(uint64_t) + sizeof(uint32_t));
 }
 
 template <typename R>

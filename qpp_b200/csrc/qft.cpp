@@ -112,9 +112,10 @@ struct PassSpec {
     bool fold = false;
 };
 
-// Largest prefix product p of dims (in order) with p <= 256 and E / p <= 256.
+// The prefix product p of dims (in order) with p <= 256 and E / p <= 256
+// closest to sqrt(E); 0 when there is none.
 uint32_t split_prefix(const std::vector<uint32_t>& dims, uint32_t E) {
-    uint32_t p = 1, best = 1;
+    uint32_t p = 1, best = 0;
     double bestd = 1e300;
     for (size_t i = 0; i <= dims.size(); ++i) {
         if (p <= 256 && E / p <= 256) {
@@ -136,10 +137,10 @@ int log2u(uint64_t x) {
 }
 
 // Builds the launch plan of one pass; false when it does not fit the kernel's
-// limits (too many tile or outer digits, or offset tables too large).
+// limits (too many tile or outer digits, or tables too large).
 bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
                 const std::vector<uint64_t>& rs, const std::vector<uint64_t>& ws,
-                uint32_t Emax, uint32_t Rt, int Mmax, QftPlan& P) {
+                uint32_t Emax, uint32_t Rt, int Mmax, uint64_t nW, QftPlan& P) {
     std::memset(&P, 0, sizeof(P));
     const size_t N = vs.dims.size();
     std::vector<char> in_tile(N, 0);
@@ -148,45 +149,29 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
         in_tile[size_t(v)] = 1;
         E *= vs.dims[size_t(v)];
     }
+    // run digits: the lowest digits in read order, then in write order, until
+    // each order's contiguous run reaches Rt elements
+    std::vector<int> run;
     auto add_run = [&](const std::vector<uint64_t>& st) {
         std::vector<int> order(N);
         std::iota(order.begin(), order.end(), 0);
         std::sort(order.begin(), order.end(), [&](int x, int y) { return st[x] < st[y]; });
-        uint64_t run = 1;
+        uint64_t len = 1;
         for (int v : order) {
-            if (run >= Rt || st[size_t(v)] != run) break;
+            if (len >= Rt || st[size_t(v)] != len) break;
             if (!in_tile[size_t(v)]) {
                 if (E * vs.dims[size_t(v)] > Emax) break;
                 in_tile[size_t(v)] = 1;
                 E *= vs.dims[size_t(v)];
+                run.push_back(v);
             }
-            run *= vs.dims[size_t(v)];
+            len *= vs.dims[size_t(v)];
         }
     };
     add_run(rs);
     add_run(ws);
+    std::sort(run.begin(), run.end(), [&](int x, int y) { return rs[x] < rs[y]; });
 
-    std::vector<int> tdig;
-    for (size_t v = 0; v < N; ++v)
-        if (in_tile[v]) tdig.push_back(int(v));
-    std::sort(tdig.begin(), tdig.end(), [&](int x, int y) { return rs[x] < rs[y]; });
-    if (tdig.size() > size_t(kQftMaxTile)) return false;
-    P.ntd = int(tdig.size());
-    P.E = uint32_t(E);
-    std::vector<uint32_t> tdims;
-    uint32_t pitch = 1;
-    for (int q = 0; q < P.ntd; ++q) {
-        const size_t v = size_t(tdig[size_t(q)]);
-        P.tdim[q] = uint32_t(vs.dims[v]);
-        P.tpitch[q] = pitch;
-        pitch *= P.tdim[q];
-        P.trs[q] = rs[v];
-        P.tws[q] = ws[v];
-        tdims.push_back(P.tdim[q]);
-    }
-    for (int j = 0; j < ps.M; ++j)
-        P.gpos[j] = int(std::find(tdig.begin(), tdig.end(), ps.group[size_t(j)]) - tdig.begin());
-    // phase digits: later targets inside the tile
     std::vector<int> qidx(N, -1); // QFT index of this half's targets
     for (size_t l = 0; l < ps.half->size(); ++l) qidx[size_t((*ps.half)[l])] = int(l);
     const int b = ps.a + ps.M;
@@ -195,35 +180,46 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
         for (size_t e = 0; e + 1 + size_t(l) < k; ++e) w *= d; // d^(k-1-l)
         return w;
     };
-    P.nzr = 0;
-    P.CZ = 1;
+
+    // tile order: run digits, then group steps M - 1 .. 0
+    std::vector<int> tdig = run;
+    for (int j = ps.M; j-- > 0;) tdig.push_back(ps.group[size_t(j)]);
+    if (tdig.size() > size_t(kQftMaxTile)) return false;
+    P.ntd = int(tdig.size());
+    P.nr = int(run.size());
+    P.E = uint32_t(E);
+    uint32_t pitch = 1;
     for (int q = 0; q < P.ntd; ++q) {
-        const int l = qidx[size_t(tdig[size_t(q)])];
-        if (l < b) continue;
-        if (P.nzr >= kQftMaxPhaseDigits) return false;
-        P.zpos[P.nzr] = d == 2 ? log2u(P.tpitch[q]) : q;
-        P.zrw[P.nzr] = zweight(l);
-        ++P.nzr;
-        P.CZ *= uint32_t(d);
+        const size_t v = size_t(tdig[size_t(q)]);
+        P.tdim[q] = uint32_t(vs.dims[v]);
+        P.tpitch[q] = pitch;
+        pitch *= P.tdim[q];
+        P.trs[q] = rs[v];
+        P.tws[q] = ws[v];
+        const int l = qidx[v];
+        P.tzw[q] = (q < P.nr && l >= b) ? zweight(l) : 0;
     }
-    if (size_t(ps.M) * d * P.CZ > 1024) return false;
-    if (d == 2)
-        for (int j = 0; j < ps.M; ++j) P.gpos[j] = log2u(P.tpitch[P.gpos[j]]); // tile bit
-    std::vector<int> wp(size_t(P.ntd));
-    std::iota(wp.begin(), wp.end(), 0);
-    std::sort(wp.begin(), wp.end(), [&](int x, int y) { return P.tws[x] < P.tws[y]; });
-    std::vector<uint32_t> wdims;
-    pitch = 1;
-    for (int q = 0; q < P.ntd; ++q) {
-        P.wperm[q] = wp[size_t(q)];
-        P.fpitch[q] = pitch;
-        pitch *= P.tdim[wp[size_t(q)]];
-        wdims.push_back(P.tdim[wp[size_t(q)]]);
-    }
-    P.Elo = split_prefix(tdims, P.E);
-    P.Flo = split_prefix(wdims, P.E);
-    if (P.E / P.Elo > 256 || P.E / P.Flo > 256 || P.Elo > 256 || P.Flo > 256) return false;
-    P.elo_shift = log2u(P.Elo);
+    P.Rsize = P.nr > 0 ? P.tpitch[P.nr - 1] * P.tdim[P.nr - 1] : 1;
+    if (size_t(ps.M) * d * P.Rsize > 1024) return false;
+    // memory orders of the tile digits
+    auto order_of = [&](const uint64_t* st, int* perm, uint32_t* mp) {
+        std::vector<int> o(size_t(P.ntd));
+        std::iota(o.begin(), o.end(), 0);
+        std::sort(o.begin(), o.end(), [&](int x, int y) { return st[x] < st[y]; });
+        std::vector<uint32_t> dims;
+        uint32_t pp = 1;
+        for (int q = 0; q < P.ntd; ++q) {
+            perm[q] = o[size_t(q)];
+            mp[q] = pp;
+            pp *= P.tdim[o[size_t(q)]];
+            dims.push_back(P.tdim[o[size_t(q)]]);
+        }
+        return split_prefix(dims, P.E);
+    };
+    P.Glo = order_of(P.trs, P.rperm, P.rpitch);
+    P.Flo = order_of(P.tws, P.wperm, P.wpitch);
+    if (P.Glo == 0 || P.Flo == 0) return false;
+    P.glo_shift = log2u(P.Glo);
     P.flo_shift = log2u(P.Flo);
 
     // outer digits by ascending read stride, merged where read stride, write
@@ -269,6 +265,7 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
     P.sigma = ps.sigma;
     P.wmul = 1;
     for (int e = ps.M; e < Mmax; ++e) P.wmul *= uint32_t(d);
+    P.nW = uint32_t(nW);
     P.scale = d == 2 ? std::ldexp(1.0, -(ps.M / 2)) * ((ps.M & 1) ? 1.0 / std::sqrt(2.0) : 1.0)
                      : 1.0;
     return true;
@@ -343,7 +340,7 @@ bool plan_qft(bool rho, uint64_t D, uint64_t d, size_t elem_bytes,
         const PassSpec& ps = passes[i];
         const std::vector<uint64_t>& rs = (ps.fold && inverse) ? perm : nat;
         const std::vector<uint64_t>& ws = (ps.fold && !inverse) ? perm : nat;
-        if (!build_pass(vs, ps, d, k, rs, ws, Emax, Rt, Mmax, S.plans[i])) return false;
+        if (!build_pass(vs, ps, d, k, rs, ws, Emax, Rt, Mmax, S.nW, S.plans[i])) return false;
         S.plans[i].inverse = inverse ? 1 : 0;
         S.fold.push_back(ps.fold ? 1 : 0);
     }

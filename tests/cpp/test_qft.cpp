@@ -31,11 +31,11 @@ static int fails = 0;
         }                                                                             \
     } while (0)
 
-static uint64_t tile_sum(const QftPlan& p, uint32_t idx, bool write_order, int what) {
+static uint64_t order_sum(const QftPlan& p, uint32_t idx, bool write_order, int what) {
     uint64_t acc = 0;
     for (int q = 0; q < p.ntd; ++q) {
-        const int td = write_order ? p.wperm[q] : q;
-        const uint32_t pitch = write_order ? p.fpitch[q] : p.tpitch[q];
+        const int td = write_order ? p.wperm[q] : p.rperm[q];
+        const uint32_t pitch = write_order ? p.wpitch[q] : p.rpitch[q];
         const uint32_t dg = (idx / pitch) % p.tdim[td];
         const uint64_t w = what == 0 ? p.trs[td] : what == 1 ? p.tws[td] : p.tpitch[td];
         acc += uint64_t(dg) * w;
@@ -43,32 +43,44 @@ static uint64_t tile_sum(const QftPlan& p, uint32_t idx, bool write_order, int w
     return acc;
 }
 
-// Host model of one k_qft_pass launch (kernels_qft.cu), FP64.
 static size_t max_smem = 0;
 
-static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& W,
+// Host model of one k_qft_pass launch (kernels_qft.cu), FP64.
+static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
                      const std::vector<cdd>& F, const std::vector<cdd>& in,
                      std::vector<cdd>& out) {
     const bool QB = p.d == 2;
-    EXPECT(p.E / p.Elo <= 256 && p.Elo <= 256 && p.E / p.Flo <= 256 && p.Flo <= 256);
+    EXPECT(p.Glo && p.Flo && p.E / p.Glo <= 256 && p.Glo <= 256 && p.E / p.Flo <= 256 &&
+           p.Flo <= 256);
     EXPECT(p.E * eb <= 32768);
+    EXPECT(p.nW == Wg.size());
     max_smem = std::max(max_smem, qft_smem_bytes(p, eb));
     EXPECT(qft_smem_bytes(p, eb) <= 64 * 1024);
-    std::vector<uint64_t> rlo(p.Elo), rhi(p.E / p.Elo), wlo(p.Flo), whi(p.E / p.Flo);
-    std::vector<uint32_t> elo(p.Flo), ehi(p.E / p.Flo);
-    for (uint32_t i = 0; i < p.Elo; ++i) rlo[i] = tile_sum(p, i, false, 0);
-    for (uint32_t i = 0; i < p.E / p.Elo; ++i) rhi[i] = tile_sum(p, i * p.Elo, false, 0);
-    for (uint32_t i = 0; i < p.Flo; ++i) {
-        wlo[i] = tile_sum(p, i, true, 1);
-        elo[i] = uint32_t(tile_sum(p, i, true, 2));
+    const uint32_t Glo = p.Glo, Flo = p.Flo;
+    std::vector<uint64_t> goff_lo(Glo), goff_hi(p.E / Glo), woff_lo(Flo), woff_hi(p.E / Flo);
+    std::vector<uint32_t> ge_lo(Glo), ge_hi(p.E / Glo), we_lo(Flo), we_hi(p.E / Flo);
+    for (uint32_t i = 0; i < Glo; ++i) {
+        goff_lo[i] = order_sum(p, i, false, 0);
+        ge_lo[i] = uint32_t(order_sum(p, i, false, 2));
     }
-    for (uint32_t i = 0; i < p.E / p.Flo; ++i) {
-        whi[i] = tile_sum(p, i * p.Flo, true, 1);
-        ehi[i] = uint32_t(tile_sum(p, i * p.Flo, true, 2));
+    for (uint32_t i = 0; i < p.E / Glo; ++i) {
+        goff_hi[i] = order_sum(p, i * Glo, false, 0);
+        ge_hi[i] = uint32_t(order_sum(p, i * Glo, false, 2));
     }
-    std::vector<int> written(out.size(), 0);
-    std::vector<cdd> tile(p.E), cst(size_t(p.M) * p.d * p.CZ);
+    for (uint32_t i = 0; i < Flo; ++i) {
+        woff_lo[i] = order_sum(p, i, true, 1);
+        we_lo[i] = uint32_t(order_sum(p, i, true, 2));
+    }
+    for (uint32_t i = 0; i < p.E / Flo; ++i) {
+        woff_hi[i] = order_sum(p, i * Flo, true, 1);
+        we_hi[i] = uint32_t(order_sum(p, i * Flo, true, 2));
+    }
+    std::vector<cdd> W(p.nW);
+    for (uint32_t i = 0; i < p.nW; ++i) W[i] = p.sigma < 0 ? std::conj(Wg[i]) : Wg[i];
+    std::vector<int> written(out.size(), 0), loaded(p.E);
     const int M = p.M, d = p.d;
+    const uint32_t Rs = p.Rsize, ncst = uint32_t(M) * d * Rs;
+    std::vector<cdd> tile(p.E), cst(ncst);
     for (uint64_t t = 0; t < p.ntiles; ++t) {
         uint64_t rb = 0, wb = 0, z = 0;
         for (int q = 0; q < p.nod; ++q) {
@@ -78,40 +90,43 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& W,
             wb += dg * p.ows[q];
             z += dg * p.ozw[q];
         }
-        for (int i = 0; i < M * d * int(p.CZ); ++i) {
-            const int c = i % int(p.CZ), jr = i / int(p.CZ);
-            const int j = jr / d, r = jr % d;
+        for (uint32_t i = 0; i < ncst; ++i) {
+            const uint32_t c = i % Rs, jr = i / Rs;
+            const int j = int(jr) / d, r = int(jr) % d;
             uint64_t zz = z;
-            for (int q = 0, cc = c; q < p.nzr; ++q, cc /= d) zz += uint64_t(cc % d) * p.zrw[q];
+            for (int q = 0; q < p.nr; ++q) zz += uint64_t((c / p.tpitch[q]) % p.tdim[q]) * p.tzw[q];
             const uint64_t N = p.dpow[p.k - p.a - j];
             EXPECT(uint64_t(r) * zz < N || r == 0);
             const double x = 2.0 * (double(uint64_t(r) * zz) / double(N));
-            cst[size_t(i)] = cdd(std::cos(M_PI * x), p.sigma * std::sin(M_PI * x));
+            cst[i] = cdd(std::cos(M_PI * x), p.sigma * std::sin(M_PI * x));
         }
-        for (uint32_t e = 0; e < p.E; ++e) {
-            const uint32_t lo = QB ? (e & (p.Elo - 1)) : e % p.Elo;
-            const uint32_t hi = QB ? (e >> p.elo_shift) : e / p.Elo;
-            const uint64_t a = rb + rlo[lo] + rhi[hi];
-            EXPECT(a < in.size());
-            tile[e] = a < in.size() ? in[a] : 0.0;
+        std::fill(loaded.begin(), loaded.end(), 0);
+        for (uint32_t g = 0; g < p.E; ++g) {
+            const uint32_t lo = QB ? (g & (Glo - 1)) : g % Glo;
+            const uint32_t hi = QB ? (g >> p.glo_shift) : g / Glo;
+            const uint32_t e = ge_lo[lo] + ge_hi[hi];
+            const uint64_t a = rb + goff_lo[lo] + goff_hi[hi];
+            EXPECT(a < in.size() && e < p.E);
+            if (a < in.size() && e < p.E) {
+                tile[e] = in[a];
+                loaded[e]++;
+            }
         }
+        for (int x : loaded) EXPECT(x == 1);
         for (int s = 0; s < M; ++s) {
             const int j = p.inverse ? M - 1 - s : s;
             if (QB) {
-                const int g = p.gpos[j];
+                const int g = p.nr + M - 1 - j;
                 const uint32_t lm = (1u << g) - 1;
-                const cdd* cj = cst.data() + (size_t(j) * 2 + 1) * p.CZ;
+                const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
+                const cdd* cj = cst.data() + size_t(j * 2 + 1) * Rs;
                 for (uint32_t pr = 0; pr < p.E / 2; ++pr) {
                     const uint32_t e0 = ((pr & ~lm) << 1) | (pr & lm);
                     const uint32_t e1 = e0 | (1u << g);
-                    uint32_t L = 0, c = 0;
-                    for (int l = j + 1; l < M; ++l) L = (L << 1) | ((e0 >> p.gpos[l]) & 1u);
-                    for (int q = 0; q < p.nzr; ++q) c |= ((e0 >> p.zpos[q]) & 1u) << q;
+                    const uint32_t L = (e0 >> p.nr) & Lmask;
                     const uint64_t wi = uint64_t(L << j) * p.wmul;
                     EXPECT(wi < W.size());
-                    cdd w = W[wi];
-                    if (p.sigma < 0) w = std::conj(w);
-                    const cdd ph = w * cj[c];
+                    const cdd ph = W[wi] * cj[e0 & (Rs - 1)];
                     const cdd x = tile[e0];
                     cdd y = tile[e1];
                     if (!p.inverse) {
@@ -124,23 +139,19 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& W,
                     }
                 }
             } else {
-                const uint32_t pj = p.tpitch[p.gpos[j]];
-                const uint64_t dj = p.dpow[j];
+                const uint32_t pj = Rs * uint32_t(p.dpow[M - 1 - j]);
+                const uint64_t Ld = p.dpow[M - 1 - j], dj = p.dpow[j];
                 for (uint32_t fb = 0; fb < p.E / d; ++fb) {
                     const uint32_t hi = fb / pj, lo = fb - hi * pj;
                     const uint32_t e0 = hi * pj * d + lo;
-                    uint64_t L = 0;
-                    uint32_t c = 0;
-                    for (int l = j + 1; l < M; ++l) L = L * d + (e0 / p.tpitch[p.gpos[l]]) % d;
-                    for (int q = p.nzr; q-- > 0;) c = c * d + (e0 / p.tpitch[p.zpos[q]]) % d;
+                    const uint64_t L = (e0 / Rs) % Ld;
+                    const uint32_t c = e0 % Rs;
                     cdd v[kQftMaxD], o[kQftMaxD];
                     for (int r = 0; r < d; ++r) v[r] = tile[e0 + r * pj];
                     auto phase = [&](int r) {
                         const uint64_t wi = (uint64_t(r) * L * dj) * p.wmul;
                         EXPECT(wi < W.size());
-                        cdd w = W[wi];
-                        if (p.sigma < 0) w = std::conj(w);
-                        return w * cst[(size_t(j) * d + r) * p.CZ + c];
+                        return W[wi] * cst[(size_t(j) * d + r) * Rs + c];
                     };
                     if (p.inverse)
                         for (int r = 1; r < d; ++r) v[r] *= phase(r);
@@ -156,11 +167,11 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& W,
             }
         }
         for (uint32_t f = 0; f < p.E; ++f) {
-            const uint32_t lo = QB ? (f & (p.Flo - 1)) : f % p.Flo;
-            const uint32_t hi = QB ? (f >> p.flo_shift) : f / p.Flo;
-            const uint32_t e = elo[lo] + ehi[hi];
+            const uint32_t lo = QB ? (f & (Flo - 1)) : f % Flo;
+            const uint32_t hi = QB ? (f >> p.flo_shift) : f / Flo;
+            const uint32_t e = we_lo[lo] + we_hi[hi];
             EXPECT(e < p.E);
-            const uint64_t a = wb + wlo[lo] + whi[hi];
+            const uint64_t a = wb + woff_lo[lo] + woff_hi[hi];
             EXPECT(a < out.size());
             if (a < out.size() && e < p.E) {
                 out[a] = tile[e] * (QB ? p.scale : 1.0);
