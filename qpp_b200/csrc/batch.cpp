@@ -266,7 +266,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             size_t b_out = prog.size() * (sizeof(uint64_t) + sizeof(uint32_t) * 8);
             size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_out);
             unsigned char* buf = nullptr;
-            QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), total, ctx->stream));
+            QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf), total));
             unsigned char* p = buf;
             auto take = [&](size_t b) {
                 unsigned char* q = p;

@@ -65,6 +65,17 @@ void* ctx_scratch(qgpu_ctx* ctx, size_t bytes) {
     return ctx->scratch;
 }
 
+cudaError_t ctx_malloc(qgpu_ctx* ctx, void** p, size_t bytes) {
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+    if (e == cudaSuccess) return e;
+    cudaGetLastError();
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->pool, 0);
+    e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+    if (e != cudaSuccess) cudaGetLastError();
+    return e;
+}
+
 void destroy_ctx(qgpu_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
@@ -72,6 +83,7 @@ void destroy_ctx(qgpu_ctx* ctx) {
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->dev_flag) cudaFree(ctx->dev_flag);
     cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
 
@@ -310,7 +322,7 @@ void upload_c128(qgpu_state* s, const double* host) {
                                 s->ctx->stream));
     } else {
         void* tmp = nullptr;
-        QG_CUDA(cudaMallocAsync(&tmp, s->elems * 16, s->ctx->stream));
+        QG_CUDA(qgpu::ctx_malloc(s->ctx, &tmp, s->elems * 16));
         QG_CUDA(cudaMemcpyAsync(tmp, host, s->elems * 16, cudaMemcpyHostToDevice,
                                 s->ctx->stream));
         qgpu::launch_convert(s->ctx, tmp, QGPU_C128, s->data, QGPU_C64, s->elems);
@@ -324,7 +336,7 @@ void download_c128(const qgpu_state* s, double* host) {
                                 s->ctx->stream));
     } else {
         void* tmp = nullptr;
-        QG_CUDA(cudaMallocAsync(&tmp, s->elems * 16, s->ctx->stream));
+        QG_CUDA(qgpu::ctx_malloc(s->ctx, &tmp, s->elems * 16));
         qgpu::launch_convert(s->ctx, s->data, QGPU_C64, tmp, QGPU_C128, s->elems);
         QG_CUDA(cudaMemcpyAsync(host, tmp, s->elems * 16, cudaMemcpyDeviceToHost,
                                 s->ctx->stream));
@@ -412,6 +424,15 @@ qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out) {
         }
         c->num_sms = prop.multiProcessorCount;
         QG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        cudaMemPoolProps pp;
+        std::memset(&pp, 0, sizeof(pp));
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        QG_CUDA(cudaMemPoolCreate(&c->pool, &pp));
+        // keep up to a quarter of the device's memory reserved between uses
+        uint64_t keep = uint64_t(prop.totalGlobalMem) / 4;
+        QG_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));
         *out = c;
     });
 }
@@ -439,6 +460,11 @@ qgpu_status qgpu_ctx_mem_info(qgpu_ctx* ctx, uint64_t* free_b, uint64_t* total_b
         size_t f = 0, t = 0;
         QG_CUDA(cudaSetDevice(ctx->device));
         QG_CUDA(cudaMemGetInfo(&f, &t));
+        // the pool's idle reserve is free for this context's allocations
+        uint64_t reserved = 0, used = 0;
+        QG_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+        QG_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        if (reserved > used) f += size_t(reserved - used);
         if (free_b) *free_b = f;
         if (total_b) *total_b = t;
     });

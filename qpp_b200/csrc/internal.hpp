@@ -27,6 +27,11 @@ struct qgpu_ctx {
     size_t pinned_bytes = 0;
     // Device word where kernels with bounded waits record a timeout.
     int* dev_flag = nullptr;
+    // Stream-ordered pool of every device buffer the context allocates
+    // (states, transform buffers, batch arenas): freed blocks stay reserved
+    // up to a threshold, so repeated large allocations skip the driver's
+    // mapping work.
+    cudaMemPool_t pool = nullptr;
     // States created on this context that are still alive; a destroyed
     // context is torn down only when the last of them is freed.
     std::atomic<int64_t> live_states{0};
@@ -83,6 +88,10 @@ void after_launch(qgpu_ctx* ctx, const char* name);
 
 // Frees the context's stream, buffers and the context itself.
 void destroy_ctx(qgpu_ctx* ctx);
+
+// Stream-ordered allocation from the context pool on the context stream; on
+// failure the pool's idle reserve is released and the allocation retried.
+cudaError_t ctx_malloc(qgpu_ctx* ctx, void** p, size_t bytes);
 
 // Context scratch of at least `bytes` (stream-ordered reuse).
 void* ctx_scratch(qgpu_ctx* ctx, size_t bytes);

@@ -74,7 +74,9 @@ void launch_ptrace(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
 // digits in tile order: first the nr run digits (the lowest other digits in
 // memory, Rsize values together), then the group digits with step M - 1
 // lowest and step 0 highest, so that a step's phase index is a plain shift
-// and mask of the tile index. Loads and stores walk the tile in memory order
+// and mask of the tile index. The run digits that are later targets (nz of
+// them, CZ values) come first: the per-tile step constants are tabulated over
+// their values. Loads and stores walk the tile in memory order
 // (rperm / wperm: tile digits by ascending read / write stride, with pitches
 // rpitch / wpitch in that order). Outer digits enumerate the tiles (tile
 // number = sum digit * opitch); ozw / tzw are a digit's weight in the integer
@@ -92,8 +94,8 @@ struct QftPlan {
     int rperm[kQftMaxTile], wperm[kQftMaxTile];
     uint32_t rpitch[kQftMaxTile], wpitch[kQftMaxTile];
     uint8_t oshift[kQftMaxOuter];
-    uint32_t E, Rsize, Glo, Flo, wmul, nW;
-    int ntd, nr, nod, M, a, k, d, sigma, inverse, pow2, glo_shift, flo_shift;
+    uint32_t E, Rsize, CZ, Glo, Flo, wmul, nW;
+    int ntd, nr, nz, nod, M, a, k, d, sigma, inverse, pow2, glo_shift, flo_shift;
     double scale; // qubit passes: 2^(-M/2)
 };
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes);

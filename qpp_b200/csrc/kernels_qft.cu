@@ -57,20 +57,68 @@ __device__ inline uint64_t order_sum(const QftPlan& p, uint32_t idx, bool write_
     return acc;
 }
 
+// G consecutive qubit steps starting at step jf (forward: jf, jf + 1, ...;
+// inverse: jf, jf - 1, ...) on every base of the tile, in registers. Step j
+// sits on tile bit nr + M - 1 - j: the round's bits are [lo, lo + G) and step
+// u of the round (u = 0 first) is on bit lo + G - 1 - u (forward) or lo + u
+// (inverse).
+template <typename R, int G, bool INV>
+__device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
+                                            const Cplx<R>* cst, const Cplx<R>* W, int jf) {
+    using C = Cplx<R>;
+    const int M = p.M;
+    const uint32_t CZ = p.CZ;
+    const int jlow = INV ? jf : jf + G - 1; // the step on the lowest bit
+    const int lo = p.nr + M - 1 - jlow;
+    const uint32_t lom = (1u << lo) - 1;
+    for (uint32_t q = threadIdx.x; q < (p.E >> G); q += blockDim.x) {
+        const uint32_t eb = ((q & ~lom) << G) | (q & lom);
+        const C* cc = cst + (eb & (CZ - 1));
+        C v[1 << G];
+#pragma unroll
+        for (int m = 0; m < (1 << G); ++m) v[m] = tile[eb | (uint32_t(m) << lo)];
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+            const int j = INV ? jf - u : jf + u;
+            const int rel = INV ? u : G - 1 - u;
+            const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
+            const C cj = cc[(j * 2 + 1) * CZ];
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) {
+                if ((m >> rel) & 1) continue;
+                const int m1 = m | (1 << rel);
+                const uint32_t L = ((eb | (uint32_t(m) << lo)) >> p.nr) & Lmask;
+                const C ph = cmul(W[(L << j) * p.wmul], cj);
+                if (!INV) {
+                    const C x = v[m], y = v[m1];
+                    v[m] = cadd(x, y);
+                    v[m1] = cmul(csub(x, y), ph);
+                } else {
+                    const C x = v[m], y = cmul(v[m1], ph);
+                    v[m] = cadd(x, y);
+                    v[m1] = csub(x, y);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < (1 << G); ++m) tile[eb | (uint32_t(m) << lo)] = v[m];
+    }
+}
+
 } // namespace
 
 // One CTA per tile (grid-stride over tiles). Dynamic shared memory: the tile
-// (E amplitudes), the per-tile step constants (M * d * Rsize), the roots of
+// (E amplitudes), the per-tile step constants (M * d * CZ), the roots of
 // unity W (nW, conjugated for s = -1), and the offset / tile-index tables of
 // the read and write orders split into a low and a high half.
 template <typename R, bool QB>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
     k_qft_pass(const Cplx<R>* in, Cplx<R>* out, const __grid_constant__ QftPlan p,
                const Cplx<R>* __restrict__ Wg, const Cplx<R>* __restrict__ F) {
     using C = Cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int M = p.M, d = p.d;
-    const uint32_t ncst = uint32_t(M) * d * p.Rsize;
+    const uint32_t ncst = uint32_t(M) * d * p.CZ;
     C* tile = reinterpret_cast<C*>(smem_raw);
     C* cst = tile + p.E;
     C* W = cst + ncst;
@@ -107,7 +155,7 @@ __global__ void __launch_bounds__(256, 4)
     }
     __syncthreads();
 
-    const uint32_t Rs = p.Rsize;
+    const uint32_t Rs = p.Rsize, CZ = p.CZ;
     for (uint64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
         // base offsets and Z (the later targets outside the tile)
         uint64_t rb = 0, wb = 0, z = 0;
@@ -122,10 +170,10 @@ __global__ void __launch_bounds__(256, 4)
         // every value c of the run digits (Zr: the later targets among them);
         // r (Z + Zr) < d^(k-i)
         for (uint32_t i = tid; i < ncst; i += nt) {
-            const uint32_t c = i % Rs, jr = i / Rs;
+            const uint32_t c = i % CZ, jr = i / CZ;
             const int j = int(jr) / d, r = int(jr) % d;
             uint64_t zz = z;
-            for (int q = 0; q < p.nr; ++q) zz += uint64_t((c / p.tpitch[q]) % p.tdim[q]) * p.tzw[q];
+            for (int q = 0; q < p.nz; ++q) zz += uint64_t((c / p.tpitch[q]) % p.tdim[q]) * p.tzw[q];
             const uint64_t N = p.dpow[p.k - p.a - j];
             double sn, cs;
             sincospi(2.0 * (double(uint64_t(r) * zz) / double(N)), &sn, &cs);
@@ -138,42 +186,40 @@ __global__ void __launch_bounds__(256, 4)
         }
         __syncthreads();
 
+        if constexpr (QB) {
+            // up to three consecutive steps per round in registers: step j
+            // sits on tile bit nr + M - 1 - j, so the round's bits are
+            // contiguous; each thread takes the 2^G amplitudes of a base
+            for (int s0 = 0; s0 < M; s0 += 3) {
+                const int G = M - s0 < 3 ? M - s0 : 3;
+                const int jf = p.inverse ? M - 1 - s0 : s0;
+                if (p.inverse) {
+                    if (G == 3) qubit_round<R, 3, true>(p, tile, cst, W, jf);
+                    else if (G == 2) qubit_round<R, 2, true>(p, tile, cst, W, jf);
+                    else qubit_round<R, 1, true>(p, tile, cst, W, jf);
+                } else {
+                    if (G == 3) qubit_round<R, 3, false>(p, tile, cst, W, jf);
+                    else if (G == 2) qubit_round<R, 2, false>(p, tile, cst, W, jf);
+                    else qubit_round<R, 1, false>(p, tile, cst, W, jf);
+                }
+                __syncthreads();
+            }
+        } else {
         for (int s = 0; s < M; ++s) {
             const int j = p.inverse ? M - 1 - s : s;
-            if constexpr (QB) {
-                const int g = p.nr + M - 1 - j; // tile bit of step j
-                const uint32_t lm = (1u << g) - 1;
-                const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
-                const C* cj = cst + (j * 2 + 1) * Rs;
-                for (uint32_t pr = tid; pr < p.E / 2; pr += nt) {
-                    const uint32_t e0 = ((pr & ~lm) << 1) | (pr & lm);
-                    const uint32_t e1 = e0 | (1u << g);
-                    const uint32_t L = (e0 >> p.nr) & Lmask;
-                    const C ph = cmul(W[(L << j) * p.wmul], cj[e0 & (Rs - 1)]);
-                    const C x = tile[e0];
-                    C y = tile[e1];
-                    if (!p.inverse) {
-                        tile[e0] = cadd(x, y);
-                        tile[e1] = cmul(csub(x, y), ph);
-                    } else {
-                        y = cmul(y, ph);
-                        tile[e0] = cadd(x, y);
-                        tile[e1] = csub(x, y);
-                    }
-                }
-            } else {
+            {
                 const uint32_t pj = Rs * uint32_t(p.dpow[M - 1 - j]);
                 const uint64_t Ld = p.dpow[M - 1 - j], dj = p.dpow[j];
                 for (uint32_t fb = tid; fb < p.E / d; fb += nt) {
                     const uint32_t hi = fb / pj, lo = fb - hi * pj;
                     const uint32_t e0 = hi * pj * d + lo;
                     const uint64_t L = (e0 / Rs) % Ld;
-                    const uint32_t c = e0 % Rs;
+                    const uint32_t c = e0 % CZ;
                     C v[kQftMaxD], o[kQftMaxD];
                     for (int r = 0; r < d; ++r) v[r] = tile[e0 + r * pj];
                     auto phase = [&](int r) {
                         return cmul(W[(uint64_t(r) * L * dj) * p.wmul], // r L d^j < d^M
-                                    cst[(j * d + r) * Rs + c]);
+                                    cst[(j * d + r) * CZ + c]);
                     };
                     if (p.inverse)
                         for (int r = 1; r < d; ++r) v[r] = cmul(v[r], phase(r));
@@ -188,6 +234,7 @@ __global__ void __launch_bounds__(256, 4)
                 }
             }
             __syncthreads();
+        }
         }
 
         const R sc = R(p.scale);
@@ -206,7 +253,7 @@ __global__ void __launch_bounds__(256, 4)
 }
 
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes) {
-    return (p.E + size_t(p.M) * p.d * p.Rsize + p.nW) * elem_bytes +
+    return (p.E + size_t(p.M) * p.d * p.CZ + p.nW) * elem_bytes +
            (p.Glo + p.E / p.Glo + p.Flo + p.E / p.Flo) * (sizeof(uint64_t) + sizeof(uint32_t));
 }
 
@@ -215,7 +262,7 @@ static void qft_launch(qgpu_ctx* ctx, const void* in, void* out, const QftPlan& 
                        const void* W, const void* F) {
     using C = Cplx<R>;
     const size_t sm = qft_smem_bytes(p, sizeof(C));
-    uint64_t blocks = uint64_t(grid_blocks(ctx, 4));
+    uint64_t blocks = uint64_t(grid_blocks(ctx, sizeof(R) == 8 ? 3 : 4));
     if (p.ntiles < blocks) blocks = p.ntiles;
     if (p.d == 2) {
         if (sm > 48 * 1024)

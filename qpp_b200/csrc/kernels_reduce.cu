@@ -528,8 +528,7 @@ std::vector<uint64_t> prefix_search_many(qgpu_ctx* ctx, qgpu_prec prec, const vo
     const size_t b_part = al(nb * sizeof(double)), b_lo = al(m * sizeof(uint64_t)),
                  b_thr = al(m * sizeof(double)), b_res = al(m * sizeof(unsigned long long));
     unsigned char* buf = nullptr;
-    QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), b_part + b_lo + b_thr + b_res,
-                            ctx->stream));
+    QG_CUDA(ctx_malloc(ctx, reinterpret_cast<void**>(&buf), b_part + b_lo + b_thr + b_res));
     struct Free {
         qgpu_ctx* c;
         void* p;

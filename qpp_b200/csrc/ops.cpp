@@ -181,7 +181,7 @@ qgpu_state* new_state(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
     s->D = 1;
     for (uint64_t d : dims) s->D *= d;
     s->elems = kind == QGPU_KET ? s->D : s->D * s->D;
-    cudaError_t e = cudaMallocAsync(&s->data, s->bytes(), ctx->stream);
+    cudaError_t e = ctx_malloc(ctx, &s->data, s->bytes());
     if (e != cudaSuccess) {
         cudaGetLastError();
         delete s;

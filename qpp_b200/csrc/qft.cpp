@@ -170,11 +170,39 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
     };
     add_run(rs);
     add_run(ws);
-    std::sort(run.begin(), run.end(), [&](int x, int y) { return rs[x] < rs[y]; });
-
     std::vector<int> qidx(N, -1); // QFT index of this half's targets
     for (size_t l = 0; l < ps.half->size(); ++l) qidx[size_t((*ps.half)[l])] = int(l);
     const int b = ps.a + ps.M;
+    // the step constants are tabulated over the values of the later targets
+    // among the run digits (CZ of them): M * d * CZ entries at most 1024
+    uint64_t CZ = 1;
+    for (int v : run)
+        if (qidx[size_t(v)] >= b) CZ *= vs.dims[size_t(v)];
+    // then the next lowest digits in read order while the tile fits: larger
+    // tiles spread the per-tile work over more amplitudes
+    {
+        std::vector<int> order(N);
+        std::iota(order.begin(), order.end(), 0);
+        std::sort(order.begin(), order.end(), [&](int x, int y) { return rs[x] < rs[y]; });
+        for (int v : order) {
+            if (in_tile[size_t(v)]) continue;
+            const uint64_t dim = vs.dims[size_t(v)];
+            if (E * dim > Emax) break;
+            const bool later = qidx[size_t(v)] >= b;
+            if (later && uint64_t(ps.M) * d * CZ * dim > 1024) break;
+            if (later) CZ *= dim;
+            in_tile[size_t(v)] = 1;
+            E *= dim;
+            run.push_back(v);
+        }
+    }
+    // run digits: the later targets first (lowest tile index digits), each
+    // part by read stride
+    std::sort(run.begin(), run.end(), [&](int x, int y) {
+        const bool lx = qidx[size_t(x)] >= b, ly = qidx[size_t(y)] >= b;
+        if (lx != ly) return lx;
+        return rs[x] < rs[y];
+    });
     auto zweight = [&](int l) {
         uint64_t w = 1;
         for (size_t e = 0; e + 1 + size_t(l) < k; ++e) w *= d; // d^(k-1-l)
@@ -198,9 +226,11 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
         P.tws[q] = ws[v];
         const int l = qidx[v];
         P.tzw[q] = (q < P.nr && l >= b) ? zweight(l) : 0;
+        if (P.tzw[q]) ++P.nz;
     }
     P.Rsize = P.nr > 0 ? P.tpitch[P.nr - 1] * P.tdim[P.nr - 1] : 1;
-    if (size_t(ps.M) * d * P.Rsize > 1024) return false;
+    P.CZ = P.nz > 0 ? P.tpitch[P.nz - 1] * P.tdim[P.nz - 1] : 1;
+    if (size_t(ps.M) * d * P.CZ > 1024) return false;
     // memory orders of the tile digits
     auto order_of = [&](const uint64_t* st, int* perm, uint32_t* mp) {
         std::vector<int> o(size_t(P.ntd));
@@ -373,7 +403,7 @@ void op_apply_qft(qgpu_state* s, const std::vector<uint64_t>& target, uint64_t d
     // the reversal rides on one pass, which needs a second buffer
     void* other = nullptr;
     if (rev) {
-        if (cudaMallocAsync(&other, s->bytes(), s->ctx->stream) == cudaSuccess) {
+        if (ctx_malloc(s->ctx, &other, s->bytes()) == cudaSuccess) {
             if (!plan_qft(rho, s->D, d, eb, target, inverse, true, S)) {
                 cudaFreeAsync(other, s->ctx->stream);
                 qft_gate_sequence(s, target, d, swap, inverse, true, true);

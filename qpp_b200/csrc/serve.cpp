@@ -248,7 +248,7 @@ void run_batch(qgpu_server* S, qgpu_ctx* ctx, std::vector<Request*>& batch) {
         size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_dits) + al(b_samp) + al(b_g) +
                        al(b_diag);
         unsigned char* buf = nullptr;
-        QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), total, ctx->stream));
+        QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf), total));
         unsigned char* p = buf;
         auto take = [&](size_t b) {
             unsigned char* q = p;

@@ -340,8 +340,8 @@ int tile_width(qgpu_ctx* ctx, int n) {
     const size_t b_state = size_t(K) * N * sizeof(float2);
     const size_t b_prog = 4096 * sizeof(TInstr), b_mat = 65536, b_work = K * sizeof(TWork);
     unsigned char* buf = nullptr;
-    QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), b_state + b_prog + b_mat + b_work + 64 * K,
-                            ctx->stream));
+    QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf),
+                             b_state + b_prog + b_mat + b_work + 64 * K));
     struct Free {
         qgpu_ctx* c;
         void* p;
@@ -448,7 +448,7 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
         size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_dits) + al(b_samp) + al(b_dump) +
                        al(b_ev) + al(b_g);
         unsigned char* buf = nullptr;
-        QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&buf), total, ctx->stream));
+        QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf), total));
         unsigned char* p = buf;
         auto take = [&](size_t b) {
             unsigned char* r = p;

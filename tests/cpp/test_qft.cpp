@@ -54,6 +54,7 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
            p.Flo <= 256);
     EXPECT(p.E * eb <= 32768);
     EXPECT(p.nW == Wg.size());
+    for (int q = 0; q < p.nr; ++q) EXPECT((p.tzw[q] != 0) == (q < p.nz));
     max_smem = std::max(max_smem, qft_smem_bytes(p, eb));
     EXPECT(qft_smem_bytes(p, eb) <= 64 * 1024);
     const uint32_t Glo = p.Glo, Flo = p.Flo;
@@ -79,7 +80,7 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
     for (uint32_t i = 0; i < p.nW; ++i) W[i] = p.sigma < 0 ? std::conj(Wg[i]) : Wg[i];
     std::vector<int> written(out.size(), 0), loaded(p.E);
     const int M = p.M, d = p.d;
-    const uint32_t Rs = p.Rsize, ncst = uint32_t(M) * d * Rs;
+    const uint32_t Rs = p.Rsize, CZ = p.CZ, ncst = uint32_t(M) * d * CZ;
     std::vector<cdd> tile(p.E), cst(ncst);
     for (uint64_t t = 0; t < p.ntiles; ++t) {
         uint64_t rb = 0, wb = 0, z = 0;
@@ -91,10 +92,10 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
             z += dg * p.ozw[q];
         }
         for (uint32_t i = 0; i < ncst; ++i) {
-            const uint32_t c = i % Rs, jr = i / Rs;
+            const uint32_t c = i % CZ, jr = i / CZ;
             const int j = int(jr) / d, r = int(jr) % d;
             uint64_t zz = z;
-            for (int q = 0; q < p.nr; ++q) zz += uint64_t((c / p.tpitch[q]) % p.tdim[q]) * p.tzw[q];
+            for (int q = 0; q < p.nz; ++q) zz += uint64_t((c / p.tpitch[q]) % p.tdim[q]) * p.tzw[q];
             const uint64_t N = p.dpow[p.k - p.a - j];
             EXPECT(uint64_t(r) * zz < N || r == 0);
             const double x = 2.0 * (double(uint64_t(r) * zz) / double(N));
@@ -113,45 +114,71 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
             }
         }
         for (int x : loaded) EXPECT(x == 1);
+        if (QB) {
+            // the kernel's rounds of up to three steps (qubit_round)
+            for (int s0 = 0; s0 < M; s0 += 3) {
+                const int G = M - s0 < 3 ? M - s0 : 3;
+                const bool INV = p.inverse;
+                const int jf = INV ? M - 1 - s0 : s0;
+                const int jlow = INV ? jf : jf + G - 1;
+                const int lo = p.nr + M - 1 - jlow;
+                const uint32_t lom = (1u << lo) - 1;
+                std::vector<int> touched(p.E, 0);
+                for (uint32_t q = 0; q < (p.E >> G); ++q) {
+                    const uint32_t eb = ((q & ~lom) << G) | (q & lom);
+                    const cdd* cc = cst.data() + (eb & (CZ - 1));
+                    cdd v[8];
+                    for (int m = 0; m < (1 << G); ++m) {
+                        const uint32_t e = eb | (uint32_t(m) << lo);
+                        EXPECT(e < p.E);
+                        v[m] = tile[e];
+                        touched[e]++;
+                    }
+                    for (int u = 0; u < G; ++u) {
+                        const int j = INV ? jf - u : jf + u;
+                        const int rel = INV ? u : G - 1 - u;
+                        EXPECT(p.nr + M - 1 - j == lo + rel);
+                        const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
+                        const cdd cj = cc[size_t(j * 2 + 1) * CZ];
+                        for (int m = 0; m < (1 << G); ++m) {
+                            if ((m >> rel) & 1) continue;
+                            const int m1 = m | (1 << rel);
+                            const uint32_t L = ((eb | (uint32_t(m) << lo)) >> p.nr) & Lmask;
+                            const uint64_t wi = uint64_t(L << j) * p.wmul;
+                            EXPECT(wi < W.size());
+                            const cdd ph = W[wi] * cj;
+                            if (!INV) {
+                                const cdd x = v[m], y = v[m1];
+                                v[m] = x + y;
+                                v[m1] = (x - y) * ph;
+                            } else {
+                                const cdd x = v[m], y = v[m1] * ph;
+                                v[m] = x + y;
+                                v[m1] = x - y;
+                            }
+                        }
+                    }
+                    for (int m = 0; m < (1 << G); ++m) tile[eb | (uint32_t(m) << lo)] = v[m];
+                }
+                for (int x : touched) EXPECT(x == 1);
+            }
+        } else {
         for (int s = 0; s < M; ++s) {
             const int j = p.inverse ? M - 1 - s : s;
-            if (QB) {
-                const int g = p.nr + M - 1 - j;
-                const uint32_t lm = (1u << g) - 1;
-                const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
-                const cdd* cj = cst.data() + size_t(j * 2 + 1) * Rs;
-                for (uint32_t pr = 0; pr < p.E / 2; ++pr) {
-                    const uint32_t e0 = ((pr & ~lm) << 1) | (pr & lm);
-                    const uint32_t e1 = e0 | (1u << g);
-                    const uint32_t L = (e0 >> p.nr) & Lmask;
-                    const uint64_t wi = uint64_t(L << j) * p.wmul;
-                    EXPECT(wi < W.size());
-                    const cdd ph = W[wi] * cj[e0 & (Rs - 1)];
-                    const cdd x = tile[e0];
-                    cdd y = tile[e1];
-                    if (!p.inverse) {
-                        tile[e0] = x + y;
-                        tile[e1] = (x - y) * ph;
-                    } else {
-                        y *= ph;
-                        tile[e0] = x + y;
-                        tile[e1] = x - y;
-                    }
-                }
-            } else {
+            {
                 const uint32_t pj = Rs * uint32_t(p.dpow[M - 1 - j]);
                 const uint64_t Ld = p.dpow[M - 1 - j], dj = p.dpow[j];
                 for (uint32_t fb = 0; fb < p.E / d; ++fb) {
                     const uint32_t hi = fb / pj, lo = fb - hi * pj;
                     const uint32_t e0 = hi * pj * d + lo;
                     const uint64_t L = (e0 / Rs) % Ld;
-                    const uint32_t c = e0 % Rs;
+                    const uint32_t c = e0 % CZ;
                     cdd v[kQftMaxD], o[kQftMaxD];
                     for (int r = 0; r < d; ++r) v[r] = tile[e0 + r * pj];
                     auto phase = [&](int r) {
                         const uint64_t wi = (uint64_t(r) * L * dj) * p.wmul;
                         EXPECT(wi < W.size());
-                        return W[wi] * cst[(size_t(j) * d + r) * Rs + c];
+                        return W[wi] * cst[(size_t(j) * d + r) * CZ + c];
                     };
                     if (p.inverse)
                         for (int r = 1; r < d; ++r) v[r] *= phase(r);
@@ -165,6 +192,7 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
                     for (int r = 0; r < d; ++r) tile[e0 + r * pj] = o[r];
                 }
             }
+        }
         }
         for (uint32_t f = 0; f < p.E; ++f) {
             const uint32_t lo = QB ? (f & (Flo - 1)) : f % Flo;
