@@ -57,6 +57,24 @@ __device__ inline uint64_t order_sum(const QftPlan& p, uint32_t idx, bool write_
     return acc;
 }
 
+// Asynchronous global -> shared copies of one amplitude (16 B for complex128
+// through L2 only, 8 B for complex64) and their group fences.
+template <typename C>
+__device__ __forceinline__ void cp_async_elem(C* dst, const C* src) {
+    const uint32_t a = uint32_t(__cvta_generic_to_shared(dst));
+    if constexpr (sizeof(C) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // G consecutive qubit steps starting at step jf (forward: jf, jf + 1, ...;
 // inverse: jf, jf - 1, ...) on every base of the tile, in registers. Step j
 // sits on tile bit nr + M - 1 - j: the round's bits are [lo, lo + G) and step
@@ -83,18 +101,24 @@ __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
             const int rel = INV ? u : G - 1 - u;
             const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
             const C cj = cc[(j * 2 + 1) * CZ];
+            // the phase depends on the round bits below the step's bit only
+            C ph[1 << (G - 1)];
+#pragma unroll
+            for (int lb = 0; lb < (1 << rel); ++lb) {
+                const uint32_t L = ((eb >> p.nr) + (uint32_t(lb) << (lo - p.nr))) & Lmask;
+                ph[lb] = cmul(W[(L << j) * p.wmul], cj);
+            }
 #pragma unroll
             for (int m = 0; m < (1 << G); ++m) {
                 if ((m >> rel) & 1) continue;
                 const int m1 = m | (1 << rel);
-                const uint32_t L = ((eb | (uint32_t(m) << lo)) >> p.nr) & Lmask;
-                const C ph = cmul(W[(L << j) * p.wmul], cj);
+                const C phm = ph[m & ((1 << rel) - 1)];
                 if (!INV) {
                     const C x = v[m], y = v[m1];
                     v[m] = cadd(x, y);
-                    v[m1] = cmul(csub(x, y), ph);
+                    v[m1] = cmul(csub(x, y), phm);
                 } else {
-                    const C x = v[m], y = cmul(v[m1], ph);
+                    const C x = v[m], y = cmul(v[m1], phm);
                     v[m] = cadd(x, y);
                     v[m1] = csub(x, y);
                 }
@@ -107,20 +131,22 @@ __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
 
 } // namespace
 
-// One CTA per tile (grid-stride over tiles). Dynamic shared memory: the tile
-// (E amplitudes), the per-tile step constants (M * d * CZ), the roots of
-// unity W (nW, conjugated for s = -1), and the offset / tile-index tables of
-// the read and write orders split into a low and a high half.
+// One CTA per tile (grid-stride over tiles); the next tile's amplitudes are
+// copied into the second tile buffer while the current one is transformed.
+// Dynamic shared memory: two tile buffers (E amplitudes each), the per-tile
+// step constants (M * d * CZ), the roots of unity W (nW, conjugated for
+// s = -1), and the offset / tile-index tables of the read and write orders
+// split into a low and a high half.
 template <typename R, bool QB>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
     k_qft_pass(const Cplx<R>* in, Cplx<R>* out, const __grid_constant__ QftPlan p,
                const Cplx<R>* __restrict__ Wg, const Cplx<R>* __restrict__ F) {
     using C = Cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int M = p.M, d = p.d;
     const uint32_t ncst = uint32_t(M) * d * p.CZ;
-    C* tile = reinterpret_cast<C*>(smem_raw);
-    C* cst = tile + p.E;
+    C* bufs = reinterpret_cast<C*>(smem_raw);
+    C* cst = bufs + 2 * p.E;
     C* W = cst + ncst;
     uint64_t* goff_lo = reinterpret_cast<uint64_t*>(W + p.nW);
     uint64_t* goff_hi = goff_lo + p.Glo;
@@ -155,10 +181,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
     }
     __syncthreads();
 
-    const uint32_t Rs = p.Rsize, CZ = p.CZ;
-    for (uint64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
-        // base offsets and Z (the later targets outside the tile)
-        uint64_t rb = 0, wb = 0, z = 0;
+    // base offsets and Z (the later targets outside the tile) of tile t
+    auto tile_base = [&](uint64_t t, uint64_t& rb, uint64_t& wb, uint64_t& z) {
+        rb = wb = z = 0;
         for (int q = 0; q < p.nod; ++q) {
             const uint64_t dg = p.pow2 ? (t >> p.oshift[q]) & (p.odim[q] - 1)
                                        : (t / p.opitch[q]) % p.odim[q];
@@ -166,9 +191,28 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
             wb += dg * p.ows[q];
             z += dg * p.ozw[q];
         }
+    };
+    // async copies of a tile's amplitudes, walked in read order
+    auto issue_loads = [&](uint64_t rb, C* dst) {
+        for (uint32_t g = tid; g < p.E; g += nt) {
+            const uint32_t lo = QB ? (g & (p.Glo - 1)) : g % p.Glo;
+            const uint32_t hi = QB ? (g >> p.glo_shift) : g / p.Glo;
+            cp_async_elem(dst + ge_lo[lo] + ge_hi[hi], in + rb + goff_lo[lo] + goff_hi[hi]);
+        }
+        cp_async_commit();
+    };
+
+    const uint32_t Rs = p.Rsize, CZ = p.CZ;
+    uint64_t t = blockIdx.x;
+    if (t >= p.ntiles) return;
+    uint64_t rb, wb, z;
+    tile_base(t, rb, wb, z);
+    issue_loads(rb, bufs);
+    for (int it = 0; t < p.ntiles; t += gridDim.x, ++it) {
+        C* tile = bufs + (it & 1) * p.E;
         // step constants exp(s 2 pi i r (Z + Zr(c)) / d^(k-i)), i = a + j, for
-        // every value c of the run digits (Zr: the later targets among them);
-        // r (Z + Zr) < d^(k-i)
+        // every value c of the later targets among the run digits (Zr: their
+        // value); r (Z + Zr) < d^(k-i)
         for (uint32_t i = tid; i < ncst; i += nt) {
             const uint32_t c = i % CZ, jr = i / CZ;
             const int j = int(jr) / d, r = int(jr) % d;
@@ -179,10 +223,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
             sincospi(2.0 * (double(uint64_t(r) * zz) / double(N)), &sn, &cs);
             cst[i] = C{R(cs), R(p.sigma * sn)};
         }
-        for (uint32_t g = tid; g < p.E; g += nt) {
-            const uint32_t lo = QB ? (g & (p.Glo - 1)) : g % p.Glo;
-            const uint32_t hi = QB ? (g >> p.glo_shift) : g / p.Glo;
-            tile[ge_lo[lo] + ge_hi[hi]] = in[rb + goff_lo[lo] + goff_hi[hi]];
+        const uint64_t tn = t + gridDim.x;
+        uint64_t rbn = 0, wbn = 0, zn = 0;
+        if (tn < p.ntiles) {
+            tile_base(tn, rbn, wbn, zn);
+            issue_loads(rbn, bufs + ((it + 1) & 1) * p.E);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
 
@@ -205,9 +253,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
                 __syncthreads();
             }
         } else {
-        for (int s = 0; s < M; ++s) {
-            const int j = p.inverse ? M - 1 - s : s;
-            {
+            for (int s = 0; s < M; ++s) {
+                const int j = p.inverse ? M - 1 - s : s;
                 const uint32_t pj = Rs * uint32_t(p.dpow[M - 1 - j]);
                 const uint64_t Ld = p.dpow[M - 1 - j], dj = p.dpow[j];
                 for (uint32_t fb = tid; fb < p.E / d; fb += nt) {
@@ -232,9 +279,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
                         for (int r = 1; r < d; ++r) o[r] = cmul(o[r], phase(r));
                     for (int r = 0; r < d; ++r) tile[e0 + r * pj] = o[r];
                 }
+                __syncthreads();
             }
-            __syncthreads();
-        }
         }
 
         const R sc = R(p.scale);
@@ -249,11 +295,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 3 : 4)
             out[wb + woff_lo[lo] + woff_hi[hi]] = v;
         }
         __syncthreads();
+        wb = wbn;
+        z = zn;
     }
 }
 
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes) {
-    return (p.E + size_t(p.M) * p.d * p.CZ + p.nW) * elem_bytes +
+    return (2 * size_t(p.E) + size_t(p.M) * p.d * p.CZ + p.nW) * elem_bytes +
            (p.Glo + p.E / p.Glo + p.Flo + p.E / p.Flo) * (sizeof(uint64_t) + sizeof(uint32_t));
 }
 
@@ -262,7 +310,7 @@ static void qft_launch(qgpu_ctx* ctx, const void* in, void* out, const QftPlan& 
                        const void* W, const void* F) {
     using C = Cplx<R>;
     const size_t sm = qft_smem_bytes(p, sizeof(C));
-    uint64_t blocks = uint64_t(grid_blocks(ctx, sizeof(R) == 8 ? 3 : 4));
+    uint64_t blocks = uint64_t(grid_blocks(ctx, sizeof(R) == 8 ? 2 : 3));
     if (p.ntiles < blocks) blocks = p.ntiles;
     if (p.d == 2) {
         if (sm > 48 * 1024)

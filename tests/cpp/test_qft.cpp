@@ -56,7 +56,7 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
     EXPECT(p.nW == Wg.size());
     for (int q = 0; q < p.nr; ++q) EXPECT((p.tzw[q] != 0) == (q < p.nz));
     max_smem = std::max(max_smem, qft_smem_bytes(p, eb));
-    EXPECT(qft_smem_bytes(p, eb) <= 64 * 1024);
+    EXPECT(qft_smem_bytes(p, eb) <= 75 * 1024); // two or three CTAs per SM
     const uint32_t Glo = p.Glo, Flo = p.Flo;
     std::vector<uint64_t> goff_lo(Glo), goff_hi(p.E / Glo), woff_lo(Flo), woff_hi(p.E / Flo);
     std::vector<uint32_t> ge_lo(Glo), ge_hi(p.E / Glo), we_lo(Flo), we_hi(p.E / Flo);
@@ -143,7 +143,10 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
                         for (int m = 0; m < (1 << G); ++m) {
                             if ((m >> rel) & 1) continue;
                             const int m1 = m | (1 << rel);
-                            const uint32_t L = ((eb | (uint32_t(m) << lo)) >> p.nr) & Lmask;
+                            // the kernel's per-round phase: round bits below rel
+                            const uint32_t lb = uint32_t(m) & ((1u << rel) - 1);
+                            const uint32_t L = ((eb >> p.nr) + (lb << (lo - p.nr))) & Lmask;
+                            EXPECT(L == (((eb | (uint32_t(m) << lo)) >> p.nr) & Lmask));
                             const uint64_t wi = uint64_t(L << j) * p.wmul;
                             EXPECT(wi < W.size());
                             const cdd ph = W[wi] * cj;
