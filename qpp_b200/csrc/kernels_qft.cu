@@ -192,12 +192,22 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
             z += dg * p.ozw[q];
         }
     };
+    // qubit tiles split their orders at the block size: a thread's low
+    // table entries are the same for every element it moves
+    const bool fixed_lo = QB && p.Glo == uint32_t(nt) && p.Flo == uint32_t(nt);
     // async copies of a tile's amplitudes, walked in read order
     auto issue_loads = [&](uint64_t rb, C* dst) {
-        for (uint32_t g = tid; g < p.E; g += nt) {
-            const uint32_t lo = QB ? (g & (p.Glo - 1)) : g % p.Glo;
-            const uint32_t hi = QB ? (g >> p.glo_shift) : g / p.Glo;
-            cp_async_elem(dst + ge_lo[lo] + ge_hi[hi], in + rb + goff_lo[lo] + goff_hi[hi]);
+        if (fixed_lo) {
+            const C* src = in + rb + goff_lo[tid];
+            C* d0 = dst + ge_lo[tid];
+            for (uint32_t h = 0; h < p.E / uint32_t(nt); ++h)
+                cp_async_elem(d0 + ge_hi[h], src + goff_hi[h]);
+        } else {
+            for (uint32_t g = tid; g < p.E; g += nt) {
+                const uint32_t lo = QB ? (g & (p.Glo - 1)) : g % p.Glo;
+                const uint32_t hi = QB ? (g >> p.glo_shift) : g / p.Glo;
+                cp_async_elem(dst + ge_lo[lo] + ge_hi[hi], in + rb + goff_lo[lo] + goff_hi[hi]);
+            }
         }
         cp_async_commit();
     };
@@ -284,15 +294,26 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
         }
 
         const R sc = R(p.scale);
-        for (uint32_t f = tid; f < p.E; f += nt) {
-            const uint32_t lo = QB ? (f & (p.Flo - 1)) : f % p.Flo;
-            const uint32_t hi = QB ? (f >> p.flo_shift) : f / p.Flo;
-            C v = tile[we_lo[lo] + we_hi[hi]];
-            if (QB) {
+        if (fixed_lo) {
+            C* dst = out + wb + woff_lo[tid];
+            const C* t0 = tile + we_lo[tid];
+            for (uint32_t h = 0; h < p.E / uint32_t(nt); ++h) {
+                C v = t0[we_hi[h]];
                 v.x *= sc;
                 v.y *= sc;
+                dst[woff_hi[h]] = v;
             }
-            out[wb + woff_lo[lo] + woff_hi[hi]] = v;
+        } else {
+            for (uint32_t f = tid; f < p.E; f += nt) {
+                const uint32_t lo = QB ? (f & (p.Flo - 1)) : f % p.Flo;
+                const uint32_t hi = QB ? (f >> p.flo_shift) : f / p.Flo;
+                C v = tile[we_lo[lo] + we_hi[hi]];
+                if (QB) {
+                    v.x *= sc;
+                    v.y *= sc;
+                }
+                out[wb + woff_lo[lo] + woff_hi[hi]] = v;
+            }
         }
         __syncthreads();
         wb = wbn;

@@ -174,7 +174,8 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
     for (size_t l = 0; l < ps.half->size(); ++l) qidx[size_t((*ps.half)[l])] = int(l);
     const int b = ps.a + ps.M;
     // the step constants are tabulated over the values of the later targets
-    // among the run digits (CZ of them): M * d * CZ entries at most 1024
+    // among the run digits (CZ of them): M * d * CZ entries; tile filling
+    // keeps that at most 256
     uint64_t CZ = 1;
     for (int v : run)
         if (qidx[size_t(v)] >= b) CZ *= vs.dims[size_t(v)];
@@ -189,7 +190,7 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
             const uint64_t dim = vs.dims[size_t(v)];
             if (E * dim > Emax) break;
             const bool later = qidx[size_t(v)] >= b;
-            if (later && uint64_t(ps.M) * d * CZ * dim > 1024) break;
+            if (later && uint64_t(ps.M) * d * CZ * dim > 256) break;
             if (later) CZ *= dim;
             in_tile[size_t(v)] = 1;
             E *= dim;
@@ -230,7 +231,7 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
     }
     P.Rsize = P.nr > 0 ? P.tpitch[P.nr - 1] * P.tdim[P.nr - 1] : 1;
     P.CZ = P.nz > 0 ? P.tpitch[P.nz - 1] * P.tdim[P.nz - 1] : 1;
-    if (size_t(ps.M) * d * P.CZ > 1024) return false;
+    if (size_t(ps.M) * d * P.CZ > 1024) return false; // the run digits alone stay within this
     // memory orders of the tile digits
     auto order_of = [&](const uint64_t* st, int* perm, uint32_t* mp) {
         std::vector<int> o(size_t(P.ntd));
@@ -248,6 +249,9 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
     };
     P.Glo = order_of(P.trs, P.rperm, P.rpitch);
     P.Flo = order_of(P.tws, P.wperm, P.wpitch);
+    // qubit tiles of 256 to 65536 amplitudes split both orders at the kernel's
+    // block size (256 threads): each thread's low table entries stay fixed
+    if (d == 2 && P.E >= 256 && P.E / 256 <= 256) P.Glo = P.Flo = 256;
     if (P.Glo == 0 || P.Flo == 0) return false;
     P.glo_shift = log2u(P.Glo);
     P.flo_shift = log2u(P.Flo);
