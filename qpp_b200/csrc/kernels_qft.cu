@@ -82,7 +82,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // (inverse).
 template <typename R, int G, bool INV>
 __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
-                                            const Cplx<R>* cst, const Cplx<R>* W, int jf) {
+                                            const Cplx<R>* T, const Cplx<R>* B, const Cplx<R>* W,
+                                            int jf) {
     using C = Cplx<R>;
     const int M = p.M;
     const uint32_t CZ = p.CZ;
@@ -91,7 +92,7 @@ __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
     const uint32_t lom = (1u << lo) - 1;
     for (uint32_t q = threadIdx.x; q < (p.E >> G); q += blockDim.x) {
         const uint32_t eb = ((q & ~lom) << G) | (q & lom);
-        const C* cc = cst + (eb & (CZ - 1));
+        const C* cc = T + (eb & (CZ - 1));
         C v[1 << G];
 #pragma unroll
         for (int m = 0; m < (1 << G); ++m) v[m] = tile[eb | (uint32_t(m) << lo)];
@@ -100,7 +101,7 @@ __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
             const int j = INV ? jf - u : jf + u;
             const int rel = INV ? u : G - 1 - u;
             const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
-            const C cj = cc[(j * 2 + 1) * CZ];
+            const C cj = cmul(B[j], cc[j * CZ]);
             // the phase depends on the round bits below the step's bit only
             C ph[1 << (G - 1)];
 #pragma unroll
@@ -146,8 +147,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
     const int M = p.M, d = p.d;
     const uint32_t ncst = uint32_t(M) * d * p.CZ;
     C* bufs = reinterpret_cast<C*>(smem_raw);
-    C* cst = bufs + 2 * p.E;
-    C* W = cst + ncst;
+    C* cst = bufs + 2 * p.E; // qubits: T (M x CZ), then B (M); qudits: M x d x CZ
+    C* W = cst + ncst + M;
     uint64_t* goff_lo = reinterpret_cast<uint64_t*>(W + p.nW);
     uint64_t* goff_hi = goff_lo + p.Glo;
     uint64_t* woff_lo = goff_hi + p.E / p.Glo;
@@ -178,6 +179,19 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
         C w = Wg[i];
         w.y *= R(p.sigma);
         W[i] = w;
+    }
+    if constexpr (QB) {
+        // T[j][c] = exp(s 2 pi i Zr(c) / 2^(k-i)), i = a + j: the later
+        // targets among the run digits (value c); the same for every tile
+        for (uint32_t i = tid; i < uint32_t(M) * p.CZ; i += nt) {
+            const uint32_t c = i % p.CZ;
+            const int j = int(i / p.CZ);
+            uint64_t zz = 0;
+            for (int q = 0; q < p.nz; ++q) zz += uint64_t((c >> q) & 1u) * p.tzw[q];
+            double sn, cs;
+            sincospi(ldexp(double(zz), 1 - (p.k - p.a - j)), &sn, &cs);
+            cst[i] = C{R(cs), R(p.sigma * sn)};
+        }
     }
     __syncthreads();
 
@@ -223,6 +237,15 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
         // step constants exp(s 2 pi i r (Z + Zr(c)) / d^(k-i)), i = a + j, for
         // every value c of the later targets among the run digits (Zr: their
         // value); r (Z + Zr) < d^(k-i)
+        if constexpr (QB) {
+            // B[j] = exp(s 2 pi i Z / 2^(k-i)); the step constant of run
+            // value c is B[j] T[j][c]
+            if (tid < M) {
+                double sn, cs;
+                sincospi(ldexp(double(z), 1 - (p.k - p.a - tid)), &sn, &cs);
+                cst[uint32_t(M) * CZ + tid] = C{R(cs), R(p.sigma * sn)};
+            }
+        } else
         for (uint32_t i = tid; i < ncst; i += nt) {
             const uint32_t c = i % CZ, jr = i / CZ;
             const int j = int(jr) / d, r = int(jr) % d;
@@ -252,13 +275,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
                 const int G = M - s0 < 3 ? M - s0 : 3;
                 const int jf = p.inverse ? M - 1 - s0 : s0;
                 if (p.inverse) {
-                    if (G == 3) qubit_round<R, 3, true>(p, tile, cst, W, jf);
-                    else if (G == 2) qubit_round<R, 2, true>(p, tile, cst, W, jf);
-                    else qubit_round<R, 1, true>(p, tile, cst, W, jf);
+                    if (G == 3) qubit_round<R, 3, true>(p, tile, cst, cst + M * CZ, W, jf);
+                    else if (G == 2) qubit_round<R, 2, true>(p, tile, cst, cst + M * CZ, W, jf);
+                    else qubit_round<R, 1, true>(p, tile, cst, cst + M * CZ, W, jf);
                 } else {
-                    if (G == 3) qubit_round<R, 3, false>(p, tile, cst, W, jf);
-                    else if (G == 2) qubit_round<R, 2, false>(p, tile, cst, W, jf);
-                    else qubit_round<R, 1, false>(p, tile, cst, W, jf);
+                    if (G == 3) qubit_round<R, 3, false>(p, tile, cst, cst + M * CZ, W, jf);
+                    else if (G == 2) qubit_round<R, 2, false>(p, tile, cst, cst + M * CZ, W, jf);
+                    else qubit_round<R, 1, false>(p, tile, cst, cst + M * CZ, W, jf);
                 }
                 __syncthreads();
             }
@@ -322,7 +345,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
 }
 
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes) {
-    return (2 * size_t(p.E) + size_t(p.M) * p.d * p.CZ + p.nW) * elem_bytes +
+    return (2 * size_t(p.E) + size_t(p.M) * p.d * p.CZ + p.M + p.nW) * elem_bytes +
            (p.Glo + p.E / p.Glo + p.Flo + p.E / p.Flo) * (sizeof(uint64_t) + sizeof(uint32_t));
 }
 

@@ -83,6 +83,17 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
     const int M = p.M, d = p.d;
     const uint32_t Rs = p.Rsize, CZ = p.CZ, ncst = uint32_t(M) * d * CZ;
     std::vector<cdd> tile(p.E), cst(ncst);
+    // qubits: the kernel's per-block table T[j][c] and per-tile bases B[j]
+    std::vector<cdd> Tq(size_t(M) * CZ), Bq(static_cast<size_t>(M));
+    if (QB)
+        for (uint32_t i = 0; i < uint32_t(M) * CZ; ++i) {
+            const uint32_t c = i % CZ;
+            const int j = int(i / CZ);
+            uint64_t zz = 0;
+            for (int q = 0; q < p.nz; ++q) zz += uint64_t((c >> q) & 1u) * p.tzw[q];
+            const double x = std::ldexp(double(zz), 1 - (p.k - p.a - j));
+            Tq[i] = cdd(std::cos(M_PI * x), p.sigma * std::sin(M_PI * x));
+        }
     for (uint64_t t = 0; t < p.ntiles; ++t) {
         uint64_t rb = 0, wb = 0, z = 0;
         for (int q = 0; q < p.nod; ++q) {
@@ -102,6 +113,11 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
             const double x = 2.0 * (double(uint64_t(r) * zz) / double(N));
             cst[i] = cdd(std::cos(M_PI * x), p.sigma * std::sin(M_PI * x));
         }
+        if (QB)
+            for (int j = 0; j < M; ++j) {
+                const double x = std::ldexp(double(z), 1 - (p.k - p.a - j));
+                Bq[size_t(j)] = cdd(std::cos(M_PI * x), p.sigma * std::sin(M_PI * x));
+            }
         std::fill(loaded.begin(), loaded.end(), 0);
         for (uint32_t g = 0; g < p.E; ++g) {
             const uint32_t lo = QB ? (g & (Glo - 1)) : g % Glo;
@@ -127,7 +143,7 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
                 std::vector<int> touched(p.E, 0);
                 for (uint32_t q = 0; q < (p.E >> G); ++q) {
                     const uint32_t eb = ((q & ~lom) << G) | (q & lom);
-                    const cdd* cc = cst.data() + (eb & (CZ - 1));
+                    const cdd* cc = Tq.data() + (eb & (CZ - 1));
                     cdd v[8];
                     for (int m = 0; m < (1 << G); ++m) {
                         const uint32_t e = eb | (uint32_t(m) << lo);
@@ -140,7 +156,8 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
                         const int rel = INV ? u : G - 1 - u;
                         EXPECT(p.nr + M - 1 - j == lo + rel);
                         const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
-                        const cdd cj = cc[size_t(j * 2 + 1) * CZ];
+                        const cdd cj = Bq[size_t(j)] * cc[size_t(j) * CZ];
+                        EXPECT(std::abs(cj - cst[size_t(j * 2 + 1) * CZ + (eb & (CZ - 1))]) < 1e-14);
                         for (int m = 0; m < (1 << G); ++m) {
                             if ((m >> rel) & 1) continue;
                             const int m1 = m | (1 << rel);
