@@ -201,7 +201,8 @@ qgpu_status qgpu_trace(const qgpu_state* s, double* re, double* im);
 /* qpp::normalize(A), functions.hpp:304-333, in place (ket / norm,
  * rho / trace). */
 qgpu_status qgpu_normalize(qgpu_state* s);
-/* <a|b> for two kets over the same dims (FP64 accumulation). */
+/* <a|b> for two kets over the same dims, or tr(A^dagger B) for two density
+ * matrices (FP64 accumulation; no qpp counterpart). */
 qgpu_status qgpu_inner(const qgpu_state* a, const qgpu_state* b, double* re,
                        double* im);
 

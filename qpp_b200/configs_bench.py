@@ -270,6 +270,31 @@ def _layered(rng, n, depth, rho, bank1, bank2, chan):
     return c
 
 
+def _config4_accuracy(ctx, circs, states):
+    """The chosen form (complex64, one graph) against the plain complex128 form from the
+    same initial states: per ket the infidelity 1 - |<a|b>|^2 / (<a|a><b|b>), per density
+    matrix the relative Hilbert-Schmidt distance ||A - B|| / ||B||; on the device (the
+    complex64 result widened to complex128)."""
+    s64, s128 = states(C64), states(C128)
+    run_batch(ctx, circs, s64, FUSED)
+    run_batch(ctx, circs, s128, PLAIN)
+    ket_inf, rho_err = [], []
+    for a64, b in zip(s64, s128):
+        a = State(ctx, b.kind, b.dims, C128).convert_from(a64)
+        ab, aa, bb = a.inner(b), a.inner(a).real, b.inner(b).real
+        if b.kind == KET:
+            ket_inf.append(max(0.0, 1.0 - abs(ab) ** 2 / (aa * bb)))
+        else:
+            rho_err.append(math.sqrt(max(0.0, aa + bb - 2 * ab.real) / bb))
+        a.free()
+    for s in s64 + s128:
+        s.free()
+    return {"kets_max_infidelity": max(ket_inf), "kets_median_infidelity": float(np.median(ket_inf)),
+            "rho_max_rel_hs_error": max(rho_err),
+            "rho_median_rel_hs_error": float(np.median(rho_err)),
+            "compared": len(ket_inf) + len(rho_err)}
+
+
 def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
     from .serving import _depol
     rng = np.random.default_rng(4)
@@ -328,6 +353,7 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
         for s in st:
             s.free()
     res["graph_speedup_vs_plain_c64"] = res["c64_plain_loop"]["s"] / res["c64_graph"]["s"]
+    res["accuracy_vs_plain_c128"] = _config4_accuracy(ctx, circs, states)
     res["tile_widths"] = {n: traj_tile_width(ctx, n) for n in range(15, 23)}
     return res
 

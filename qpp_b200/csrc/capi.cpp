@@ -697,8 +697,7 @@ qgpu_status qgpu_inner(const qgpu_state* a, const qgpu_state* b, double* re,
     return guard([&] {
         check_handle(a);
         check_handle(b);
-        if (a->kind != QGPU_KET || b->kind != QGPU_KET || a->dims != b->dims ||
-            a->prec != b->prec)
+        if (a->kind != b->kind || a->dims != b->dims || a->prec != b->prec)
             raise(QGPU_ERR_DIMS_NOT_EQUAL, "qgpu_inner()", "a/b");
         cd v = qgpu::reduce_inner(a->ctx, a->prec, a->data, b->data, a->elems);
         if (re) *re = v.real();
