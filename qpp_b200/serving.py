@@ -100,11 +100,14 @@ def pair_channel():
 
 
 class Request:
-    __slots__ = ("circuit", "kind", "n", "p", "shots", "nc")
+    """A request template; `steps` lists its circuit as ("gate", U, targets),
+    ("channel", Ks, targets) and ("measure", [q], dit, destructive) tuples."""
+    __slots__ = ("circuit", "kind", "n", "p", "shots", "nc", "steps")
 
-    def __init__(self, circuit, kind, n, p, shots, nc):
+    def __init__(self, circuit, kind, n, p, shots, nc, steps=None):
         self.circuit, self.kind, self.n, self.p, self.shots, self.nc = \
             circuit, kind, n, p, shots, nc
+        self.steps = steps if steps is not None else []
 
 
 def request_pool(count, seed=2025, max_ket_qubits=28, max_rho_qubits=13):
@@ -126,24 +129,31 @@ def request_pool(count, seed=2025, max_ket_qubits=28, max_rho_qubits=13):
             if measure else set()
         nc = 6 if measure else 1
         c = Circuit(n, 2, nc)
+        steps = []
         creg = 0
         for layer in range(depth):
             for q in range(n):
-                c.gate(bank1[int(rng.integers(128))], [q])
+                U = bank1[int(rng.integers(128))]
+                c.gate(U, [q])
+                steps.append(("gate", U, [q]))
             perm = rng.permutation(n)
             for i in range(n // 2):
                 a, b = int(perm[2 * i]), int(perm[2 * i + 1])
-                c.gate(bank2[int(rng.integers(128))], [a, b])
+                U = bank2[int(rng.integers(128))]
+                c.gate(U, [a, b])
+                steps.append(("gate", U, [a, b]))
                 if kind == RHO:
                     c_channel(c, chan, [a, b])
+                    steps.append(("channel", chan, [a, b]))
             if layer in meas_layers:
                 k = int(rng.integers(1, 4))
                 for q in rng.choice(n, size=k, replace=False):
                     if creg < nc:
                         c.measure([int(q)], creg, destructive=False)
+                        steps.append(("measure", [int(q)], creg, False))
                         creg += 1
         shots = int(round(math.exp(rng.uniform(0, math.log(1000)))))
-        pool.append(Request(c, kind, n, 1e-3 if kind == KET else 0.0, max(shots, 1), nc))
+        pool.append(Request(c, kind, n, 1e-3 if kind == KET else 0.0, max(shots, 1), nc, steps))
     return pool
 
 
