@@ -291,7 +291,7 @@ void plan_pass_segments(const TInstr* ins, uint32_t nins, int T, std::vector<uin
         if (!open || end == first) return;
         uint32_t wb = 0;
         int k = 0;
-        for (int b = T - 1; b >= 5 && k < 3; --b) // the three highest free bits
+        for (int b = T - 1; b >= 0 && k < 3; --b) // the three highest free bits
             if (!(used >> b & 1u)) wb |= uint32_t(b) << (8 * k++);
         out.push_back(first | ((end - first) << 16));
         out.push_back(wb);
@@ -311,17 +311,8 @@ void plan_pass_segments(const TInstr* ins, uint32_t nins, int T, std::vector<uin
             out.push_back(kSegBlock);
             continue;
         }
-        // the warp bits come from tile bits 5.. (above the 32-amplitude rows):
-        // with low warp bits a warp's lanes would stride across shared-memory
-        // banks
-        const uint32_t high = ((1u << T) - 1) & ~31u;
-        if (open && __builtin_popcount(high & ~(used | bits)) < 3) close_warp(i);
+        if (open && __builtin_popcount(used | bits) > T - 3) close_warp(i);
         if (!open) {
-            if (__builtin_popcount(high & ~bits) < 3) { // cannot own a warp segment
-                out.push_back(i | (1u << 16));
-                out.push_back(kSegBlock);
-                continue;
-            }
             open = true;
             first = i;
             used = 0;

@@ -129,9 +129,8 @@ struct PassInst {
     uint16_t pad;
 };
 // Segments of a tile pass's gates (no reference counterpart): consecutive
-// gates whose target bits leave at least 3 of the tile bits 5..T-1 untouched
-// form one warp segment. Those 3 bits (the highest free ones) select the
-// warp, so
+// gates whose target bits leave at least 3 of the T tile bits untouched form
+// one warp segment. Those 3 bits (the highest free ones) select the warp, so
 // each of the 8 warps owns 1/8 of the tile for the whole segment and needs
 // only warp-level synchronisation between gates; one block barrier separates
 // segments. Two words per segment: first | count << 16, then the three warp

@@ -123,8 +123,7 @@ static void segmented(const std::vector<TInstr>& prog, const float* mats, size_t
             continue;
         }
         const int wb[3] = {int(w1 & 255u), int((w1 >> 8) & 255u), int((w1 >> 16) & 255u)};
-        EXPECT(wb[0] < T && wb[1] < T && wb[2] < T && wb[0] >= 5 && wb[1] >= 5 && wb[2] >= 5 &&
-               wb[0] != wb[1] && wb[1] != wb[2] &&
+        EXPECT(wb[0] < T && wb[1] < T && wb[2] < T && wb[0] != wb[1] && wb[1] != wb[2] &&
                wb[0] != wb[2]);
         for (uint32_t i = i0; i < i0 + cnt; ++i) {
             const TInstr& I = prog[k + 1 + i];
