@@ -263,19 +263,8 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             size_t b_mat = std::max<size_t>(mats.size() * sizeof(float), 16);
             size_t b_work = std::max<size_t>(prog.size() * sizeof(qgpu::TWork), 16);
             size_t b_pass = std::max<size_t>(npass_total * sizeof(qgpu::PassInst), 16);
-            // the warp segments of every pass (two words each)
-            std::vector<uint32_t> segs;
-            std::vector<std::vector<std::pair<uint32_t, uint32_t>>> seg_of(prog.size());
-            for (size_t k = 0; k < prog.size(); ++k)
-                for (const Pass& ps : passes[k]) {
-                    const uint32_t at = uint32_t(segs.size());
-                    qgpu::plan_pass_segments(prog[k].second.ins.data() + ps.pos, ps.nins, ps.T,
-                                             segs);
-                    seg_of[k].push_back({at, uint32_t(segs.size() - at) / 2});
-                }
-            size_t b_seg = std::max<size_t>(segs.size() * sizeof(uint32_t), 16);
             size_t b_out = prog.size() * (sizeof(uint64_t) + sizeof(uint32_t) * 8);
-            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_seg) + al(b_out);
+            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_out);
             unsigned char* buf = nullptr;
             QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf), total));
             unsigned char* p = buf;
@@ -288,7 +277,6 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             auto* dmat = reinterpret_cast<float2*>(take(b_mat));
             auto* dwork = reinterpret_cast<qgpu::TWork*>(take(b_work));
             auto* dpass = reinterpret_cast<qgpu::PassInst*>(take(b_pass));
-            auto* dseg = reinterpret_cast<uint32_t*>(take(b_seg));
             auto* dsamp = reinterpret_cast<uint64_t*>(take(prog.size() * sizeof(uint64_t)));
             auto* ddits = reinterpret_cast<uint32_t*>(take(prog.size() * sizeof(uint32_t) * 8));
             std::vector<qgpu::TWork> work;
@@ -335,8 +323,6 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     q.mats = dmat + ofs[k].second;
                     q.ins = dins + ofs[k].first + ps.pos;
                     q.nins = ps.nins;
-                    q.seg = dseg + seg_of[k][kk].first;
-                    q.nseg = seg_of[k][kk].second;
                     q.tb_off = ps.tb_off;
                     q.first_item = items;
                     q.tiles_per_item = tpi;
@@ -357,9 +343,6 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                                         cudaMemcpyHostToDevice, ctx->stream));
             if (!pinst.empty())
                 QG_CUDA(cudaMemcpyAsync(dpass, pinst.data(), pinst.size() * sizeof(qgpu::PassInst),
-                                        cudaMemcpyHostToDevice, ctx->stream));
-            if (!segs.empty())
-                QG_CUDA(cudaMemcpyAsync(dseg, segs.data(), segs.size() * sizeof(uint32_t),
                                         cudaMemcpyHostToDevice, ctx->stream));
             int* dflag = launches.empty() ? nullptr : qgpu::ctx_error_flag(ctx);
             // one graph: a k_traj launch per register size on its own branch,

@@ -564,71 +564,6 @@ __device__ __forceinline__ void pass_issue_store(const PassInst& P, const PassGe
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
 
-// Inserts a zero bit at each of the k ascending positions pos[] of x.
-template <int K>
-__device__ __forceinline__ uint32_t deposit_zeros(uint32_t x, const int (&pos)[K]) {
-#pragma unroll
-    for (int i = 0; i < K; ++i) x = ins0(x, pos[i]);
-    return x;
-}
-template <int K>
-__device__ __forceinline__ void sort_small(int (&a)[K]) {
-#pragma unroll
-    for (int i = 1; i < K; ++i)
-#pragma unroll
-        for (int j = i; j > 0; --j)
-            if (a[j - 1] > a[j]) {
-                const int t = a[j];
-                a[j] = a[j - 1];
-                a[j - 1] = t;
-            }
-}
-
-// One 1- or 2-qubit gate (G1, CG1, G2) on the amplitudes of a tile of N whose
-// three warp bits wb[] spell this warp's number (wval: those bits set); the
-// 32 lanes of the warp share the work, no other warp touches these amplitudes.
-__device__ __forceinline__ void warp_gate(const TInstr& I, const float2* __restrict__ mats,
-                                          float2* psi, uint32_t N, const int (&wb)[3],
-                                          uint32_t wval, int lane) {
-    if (I.op == kTG2) {
-        const float2* m = mats + I.mat; // column-major 4 x 4
-        int pos[5] = {wb[0], wb[1], wb[2], int(I.b0), int(I.b1)};
-        sort_small(pos);
-        const uint32_t s0 = 1u << I.b0, s1 = 1u << I.b1;
-        for (uint32_t p = lane; p < (N >> 5); p += 32) {
-            const uint32_t i = deposit_zeros(p, pos) | wval;
-            float2 v[4] = {psi[i], psi[i + s1], psi[i + s0], psi[i + s0 + s1]};
-            float2 r[4];
-#pragma unroll
-            for (int row = 0; row < 4; ++row) {
-                float2 acc = c_mul(m[row], v[0]);
-                acc = c_fma(m[row + 4], v[1], acc);
-                acc = c_fma(m[row + 8], v[2], acc);
-                acc = c_fma(m[row + 12], v[3], acc);
-                r[row] = acc;
-            }
-            psi[i] = r[0];
-            psi[i + s1] = r[1];
-            psi[i + s0] = r[2];
-            psi[i + s0 + s1] = r[3];
-        }
-    } else { // kTG1 / kTCG1 (controls only filter the pairs)
-        const float2* m = mats + I.mat;
-        const float2 a00 = m[0], a10 = m[1], a01 = m[2], a11 = m[3];
-        int pos[4] = {wb[0], wb[1], wb[2], int(I.b0)};
-        sort_small(pos);
-        const uint32_t s = 1u << I.b0;
-        const bool ctl = I.op == kTCG1;
-        for (uint32_t p = lane; p < (N >> 4); p += 32) {
-            const uint32_t i = deposit_zeros(p, pos) | wval;
-            if (ctl && (i & I.cmask) != I.cval) continue;
-            const float2 v0 = psi[i], v1 = psi[i + s];
-            psi[i] = c_fma(a01, v1, c_mul(a00, v0));
-            psi[i + s] = c_fma(a11, v1, c_mul(a10, v0));
-        }
-    }
-}
-
 __global__ void __launch_bounds__(256, 3)
     k_pass_batch(const PassInst* __restrict__ insts, int ninst, uint32_t nitems, int tile_bits,
                  int* __restrict__ err) {
@@ -711,27 +646,9 @@ __global__ void __launch_bounds__(256, 3)
         if (abort_sh) break;
         const PassInst& P = insts[cur.j];
         const uint32_t NT = 1u << P.T;
-        for (uint32_t sg = 0; sg < P.nseg; ++sg) {
-            const uint32_t w0 = P.seg[2 * sg], w1 = P.seg[2 * sg + 1];
-            const uint32_t i0 = w0 & 0xffffu, i1 = i0 + (w0 >> 16);
-            if (w1 == kSegBlock) {
-                for (uint32_t i = i0; i < i1; ++i) {
-                    tr_gate(P.ins[i], P.mats, bc, NT, tid, nt);
-                    __syncthreads();
-                }
-            } else {
-                // each warp owns the amplitudes whose three warp bits spell
-                // its number: warp-level syncs between the segment's gates
-                const int wb[3] = {int(w1 & 255u), int((w1 >> 8) & 255u), int((w1 >> 16) & 255u)};
-                const uint32_t wval = (uint32_t(warp & 1) << wb[0]) |
-                                      (uint32_t((warp >> 1) & 1) << wb[1]) |
-                                      (uint32_t((warp >> 2) & 1) << wb[2]);
-                for (uint32_t i = i0; i < i1; ++i) {
-                    warp_gate(P.ins[i], P.mats, bc, NT, wb, wval, lane);
-                    __syncwarp();
-                }
-                __syncthreads();
-            }
+        for (uint32_t i = 0; i < P.nins; ++i) {
+            tr_gate(P.ins[i], P.mats, bc, NT, tid, nt);
+            __syncthreads();
         }
         // the threads' shared-memory writes, visible to the bulk stores
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

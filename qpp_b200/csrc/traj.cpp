@@ -284,44 +284,6 @@ void plan_tiles(TProgram& P, int T, size_t min_run) {
     P.ins.swap(out);
 }
 
-void plan_pass_segments(const TInstr* ins, uint32_t nins, int T, std::vector<uint32_t>& out) {
-    uint32_t first = 0, used = 0;
-    bool open = false;
-    auto close_warp = [&](uint32_t end) {
-        if (!open || end == first) return;
-        uint32_t wb = 0;
-        int k = 0;
-        for (int b = T - 1; b >= 0 && k < 3; --b) // the three highest free bits
-            if (!(used >> b & 1u)) wb |= uint32_t(b) << (8 * k++);
-        out.push_back(first | ((end - first) << 16));
-        out.push_back(wb);
-        open = false;
-    };
-    for (uint32_t i = 0; i < nins; ++i) {
-        const TInstr& I = ins[i];
-        uint32_t bits = 0;
-        switch (I.op) {
-            case kTG1: case kTCG1: bits = 1u << I.b0; break; // controls only filter
-            case kTG2: bits = (1u << I.b0) | (1u << I.b1); break;
-            default: bits = ~0u; // G4 and anything else: block mode
-        }
-        if (bits == ~0u) {
-            close_warp(i);
-            out.push_back(i | (1u << 16));
-            out.push_back(kSegBlock);
-            continue;
-        }
-        if (open && __builtin_popcount(used | bits) > T - 3) close_warp(i);
-        if (!open) {
-            open = true;
-            first = i;
-            used = 0;
-        }
-        used |= bits;
-    }
-    close_warp(nins);
-}
-
 namespace {
 std::mutex g_tile_mu;
 std::map<std::pair<int, int>, int> g_tile_chosen; // (device, n) -> T

@@ -119,25 +119,13 @@ struct PassInst {
     float2* psi;
     const float2* mats;
     const TInstr* ins;
-    const uint32_t* seg; // nseg segments of the pass (plan_pass_segments)
     uint32_t nins;
-    uint32_t nseg;
     uint32_t tb_off;
     uint32_t first_item;
     uint32_t tiles_per_item;
     uint8_t n, T;
     uint16_t pad;
 };
-// Segments of a tile pass's gates (no reference counterpart): consecutive
-// gates whose target bits leave at least 3 of the T tile bits untouched form
-// one warp segment. Those 3 bits (the highest free ones) select the warp, so
-// each of the 8 warps owns 1/8 of the tile for the whole segment and needs
-// only warp-level synchronisation between gates; one block barrier separates
-// segments. Two words per segment: first | count << 16, then the three warp
-// bits (bits 0-7, 8-15, 16-23), or kSegBlock for gates run with block
-// barriers (4-bit gates).
-constexpr uint32_t kSegBlock = 0xff000000u;
-void plan_pass_segments(const TInstr* ins, uint32_t nins, int T, std::vector<uint32_t>& out);
 // One launch of k_pass_batch over `ninst` registers (sorted by first_item,
 // nitems items in total) with two 2^tile_bits-amplitude tile buffers
 // (tile_bits >= every T, <= 13). Every register must start on a 16-byte

@@ -103,73 +103,6 @@ static void gate(const TInstr& I, const float* mats, f2* psi, uint32_t N) {
     }
 }
 
-// k_pass_batch's warp segments on one tile: each segment's gates run warp by
-// warp on the amplitudes whose three warp bits spell the warp's number
-// (warp_gate: zero bits deposited at the sorted target and warp positions),
-// block segments gate by gate; also checks the segment list itself.
-static void segmented(const std::vector<TInstr>& prog, const float* mats, size_t k, int T,
-                      f2* tile) {
-    const uint32_t m = prog[k].cmask, NT = 1u << T;
-    std::vector<uint32_t> seg;
-    plan_pass_segments(prog.data() + k + 1, m, T, seg);
-    EXPECT(seg.size() % 2 == 0);
-    uint32_t next = 0;
-    for (size_t sgi = 0; sgi < seg.size(); sgi += 2) {
-        const uint32_t i0 = seg[sgi] & 0xffffu, cnt = seg[sgi] >> 16, w1 = seg[sgi + 1];
-        EXPECT(i0 == next && cnt > 0);
-        next = i0 + cnt;
-        if (w1 == kSegBlock) {
-            for (uint32_t i = i0; i < i0 + cnt; ++i) gate(prog[k + 1 + i], mats, tile, NT);
-            continue;
-        }
-        const int wb[3] = {int(w1 & 255u), int((w1 >> 8) & 255u), int((w1 >> 16) & 255u)};
-        EXPECT(wb[0] < T && wb[1] < T && wb[2] < T && wb[0] != wb[1] && wb[1] != wb[2] &&
-               wb[0] != wb[2]);
-        for (uint32_t i = i0; i < i0 + cnt; ++i) {
-            const TInstr& I = prog[k + 1 + i];
-            EXPECT(I.op == kTG1 || I.op == kTCG1 || I.op == kTG2);
-            for (int x : wb) EXPECT(x != I.b0 && (I.op != kTG2 || x != I.b1));
-        }
-        for (int w = 0; w < 8; ++w) {
-            const uint32_t wval = (uint32_t(w & 1) << wb[0]) | (uint32_t((w >> 1) & 1) << wb[1]) |
-                                  (uint32_t((w >> 2) & 1) << wb[2]);
-            for (uint32_t i = i0; i < i0 + cnt; ++i) {
-                const TInstr& I = prog[k + 1 + i];
-                std::vector<int> pos = {wb[0], wb[1], wb[2], int(I.b0)};
-                if (I.op == kTG2) pos.push_back(int(I.b1));
-                std::sort(pos.begin(), pos.end());
-                const uint32_t groups = NT >> pos.size();
-                const f2* mm = reinterpret_cast<const f2*>(mats) + I.mat;
-                for (uint32_t q = 0; q < groups; ++q) {
-                    uint32_t e = q;
-                    for (int ps : pos) e = ((e & ~((1u << ps) - 1)) << 1) | (e & ((1u << ps) - 1));
-                    e |= wval;
-                    EXPECT(e < NT);
-                    if (I.op == kTG2) {
-                        const uint32_t s0 = 1u << I.b0, s1 = 1u << I.b1;
-                        const uint32_t idx[4] = {e, e + s1, e + s0, e + s0 + s1};
-                        f2 v[4], r[4];
-                        for (int c = 0; c < 4; ++c) v[c] = tile[idx[c]];
-                        for (int row = 0; row < 4; ++row) {
-                            f2 acc = cmul(mm[row], v[0]);
-                            for (int c = 1; c < 4; ++c) acc = cfma(mm[row + 4 * c], v[c], acc);
-                            r[row] = acc;
-                        }
-                        for (int c = 0; c < 4; ++c) tile[idx[c]] = r[c];
-                    } else {
-                        if (I.op == kTCG1 && (e & I.cmask) != I.cval) continue;
-                        const uint32_t sb = 1u << I.b0;
-                        const f2 v0 = tile[e], v1 = tile[e + sb];
-                        tile[e] = cfma(mm[2], v1, cmul(mm[0], v0));
-                        tile[e + sb] = cfma(mm[3], v1, cmul(mm[1], v0));
-                    }
-                }
-            }
-        }
-    }
-    EXPECT(next == m);
-}
-
 // The kernel's tile pass (no noise): offset table, deposit, gather, local
 // gates, scatter.
 static void tile_pass(const std::vector<TInstr>& prog, const float* mats, size_t k, int n,
@@ -211,7 +144,6 @@ static void tile_pass(const std::vector<TInstr>& prog, const float* mats, size_t
                 tile[l] = psi[a];
             }
         }
-        std::vector<f2> seg_tile = tile;
         for (uint32_t i = k + 1; i < k + 1 + m; ++i) {
             const TInstr& I = prog[i];
             // local bits inside the tile
@@ -220,8 +152,6 @@ static void tile_pass(const std::vector<TInstr>& prog, const float* mats, size_t
             if (I.op == kTCG1) EXPECT((I.cmask >> T) == 0);
             gate(I, mats, tile.data(), NT);
         }
-        segmented(prog, mats, k, T, seg_tile.data());
-        EXPECT(std::memcmp(seg_tile.data(), tile.data(), NT * sizeof(f2)) == 0);
         for (uint32_t l = 0; l < NT; ++l) {
             const uint32_t a = base + offh[l >> 5] + (l & 31u);
             if (a < N) psi[a] = tile[l];
