@@ -16,18 +16,19 @@
 // shared memory. In the tile index the run digits come first and the group
 // digits follow with step M - 1 lowest, so the phase of step j splits into
 // W[L << j] (L = the group digits after j: a shift and mask of the index),
-// a constant per tile for the later targets outside the tile, and a factor
-// for the later targets among the run digits (the low index bits): the last
-// two are tabulated per tile over the run digits' values. A pass reads and
-// writes every amplitude once, so a k-digit transform costs ceil(k / M)
-// passes over the state instead of the k(k+1)/2 gate passes of the gate
-// sequence. The pass that also reverses the targets reads one buffer and
-// writes another with permuted digit strides.
+// a constant per tile and step for the later targets outside the tile, and a
+// factor for the later targets among the run digits (the lowest index
+// digits). For qubits the last two are a per-block table over the run
+// digits' values times one base per tile and step; for qudits they are
+// tabulated per tile. A pass reads and writes every amplitude once, so a
+// k-digit transform costs ceil(k / M) passes over the state instead of the
+// k(k+1)/2 gate passes of the gate sequence. The pass that also reverses the
+// targets reads one buffer and writes another with permuted digit strides.
 //
-// Qubit butterflies omit the 1/sqrt(2) of H; the store multiplies by
-// 2^(-M/2) once.
-#include <cstdio>
-
+// Qubit steps run three at a time in registers (a thread holds the 8
+// amplitudes of a base); the next tile is copied in with cp.async while the
+// current one is transformed. Qubit butterflies omit the 1/sqrt(2) of H; the
+// store multiplies by 2^(-M/2) once.
 #include "kernels.hpp"
 
 namespace qgpu {
