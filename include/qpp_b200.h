@@ -483,6 +483,14 @@ qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double p_depol,
  * timed again. No reference counterpart. *chosen (if not NULL) receives the
  * width now in force. */
 qgpu_status qgpu_traj_tile_width(qgpu_ctx* ctx, uint32_t n, int set_T, int* chosen);
+/* Fusion width of batched (noiseless) registers of n qubits (1-22): the gates
+ * of a batched instance merge into dense blocks of at most this many qubits
+ * (2, 3 or 4; 8 x 8 and 16 x 16 blocks for 3 and 4). set_w = -1 queries
+ * (timing the widths on a two-layer random-matching program with the tuned
+ * tile width once on first use), 2..4 pins a width, -2 drops the choice so
+ * it is timed again. No reference counterpart. *chosen (if not NULL)
+ * receives the width now in force. */
+qgpu_status qgpu_traj_fusion_width(qgpu_ctx* ctx, uint32_t n, int set_w, int* chosen);
 
 /* ------------------------------------------------------ batched instances
  * n_inst independent instances, instance i running circuits[i] on

@@ -680,6 +680,15 @@ def batch_last_phases(ctx):
             "plain_ms": out[3], "check_ms": out[4], "teardown_ms": out[5]}
 
 
+def traj_fusion_width(ctx, n, w=None):
+    """Fusion width (2-4) of batched registers of n qubits: the tuned choice,
+    or pin w (w=-2 drops the choice so it is timed again)."""
+    out = ct.c_int()
+    check(lib().qgpu_traj_fusion_width(ctx.h, ct.c_uint32(n), ct.c_int(-1 if w is None else w),
+                                       ct.byref(out)))
+    return out.value
+
+
 def traj_tile_width(ctx, n, T=None):
     """Tile width of the trajectory kernel for n-qubit registers (15-22):
     T=None queries (tuned on first use), 0 pins the untiled form, 9..14

@@ -35,7 +35,7 @@ import time
 import numpy as np
 
 from . import (C64, C128, FUSED, KET, PLAIN, RHO, Circuit, Context, Engine, State,
-               batch_last_phases,
+               batch_last_phases, traj_fusion_width,
                run_batch, traj_tile_width)
 from .workloads import haar_unitary, ket_gate_sequence
 
@@ -355,6 +355,7 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
     res["graph_speedup_vs_plain_c64"] = res["c64_plain_loop"]["s"] / res["c64_graph"]["s"]
     res["accuracy_vs_plain_c128"] = _config4_accuracy(ctx, circs, states)
     res["tile_widths"] = {n: traj_tile_width(ctx, n) for n in range(15, 23)}
+    res["fusion_widths"] = {n: traj_fusion_width(ctx, n) for n in range(10, 23)}
     return res
 
 

@@ -182,7 +182,15 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             ok[i] = form == 1 && states[i]->prec == QGPU_C64 &&
                     (states[i]->kind == QGPU_KET ? qgpu::compile_traj(circuits[i], P)
                                                  : qgpu::compile_traj_rho(circuits[i], P));
-            if (ok[i]) qgpu::fold_1q_gates(P); // batch programs carry no noise
+        });
+        // batch programs carry no noise: gates fuse into dense blocks of the
+        // width tuned for each register size (timed serially on the GPU)
+        std::map<uint32_t, int> width_of;
+        for (uint32_t i = 0; i < n_inst; ++i)
+            if (ok[i] && !width_of.count(progs[i].n))
+                width_of.emplace(progs[i].n, qgpu::fusion_width(ctx, int(progs[i].n)));
+        pfor(n_inst, [&](size_t i) {
+            if (ok[i]) qgpu::fuse_blocks(progs[i], width_of.at(progs[i].n));
         });
         for (uint32_t i = 0; i < n_inst; ++i) {
             if (ok[i]) prog.emplace_back(i, std::move(progs[i]));
@@ -197,7 +205,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             auto all_gates = [](const qgpu::TProgram& P) {
                 for (const auto& I : P.ins)
                     if (I.op != qgpu::kTG1 && I.op != qgpu::kTCG1 && I.op != qgpu::kTG2 &&
-                        I.op != qgpu::kTG4)
+                        I.op != qgpu::kTG3 && I.op != qgpu::kTG4)
                         return false;
                 return true;
             };

@@ -58,7 +58,37 @@ __device__ double block_sum_d(double v, double* red) {
     return t;
 }
 
-// One gate instruction (G1, CG1, G2, G4) on a register of N amplitudes at
+// kTG3: 8 x 8 on bits (b0, b1, b2 = cmask & 255), row index 4 b0 + 2 b1 + b2;
+// each thread owns whole groups. The row loop stays rolled so that the 64
+// matrix entries are read per row (L1) rather than held in registers.
+__device__ __forceinline__ void tr_gate3(const TInstr& I, const float2* __restrict__ mats,
+                                      float2* psi, uint32_t N, int tid, int nt) {
+    const float2* m = mats + I.mat;
+    const int b2 = int(I.cmask & 255u);
+    int sb[3] = {I.b0, I.b1, b2};
+    if (sb[0] > sb[1]) { const int t = sb[0]; sb[0] = sb[1]; sb[1] = t; }
+    if (sb[1] > sb[2]) { const int t = sb[1]; sb[1] = sb[2]; sb[2] = t; }
+    if (sb[0] > sb[1]) { const int t = sb[0]; sb[0] = sb[1]; sb[1] = t; }
+    const uint32_t o4 = 1u << I.b0, o2 = 1u << I.b1, o1 = 1u << b2;
+    for (uint32_t g = tid; g < N / 8; g += nt) {
+        const uint32_t i = ins0(ins0(ins0(g, sb[0]), sb[1]), sb[2]);
+        float2 v[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            v[c] = psi[i + ((c & 4) ? o4 : 0u) + ((c & 2) ? o2 : 0u) + ((c & 1) ? o1 : 0u)];
+        // all eight inputs are in registers, so each row writes in place
+#pragma unroll 1
+        for (int row = 0; row < 8; ++row) {
+            const float2* mr = m + row;
+            float2 acc = c_mul(mr[0], v[0]);
+#pragma unroll
+            for (int c = 1; c < 8; ++c) acc = c_fma(mr[8 * c], v[c], acc);
+            psi[i + ((row & 4) ? o4 : 0u) + ((row & 2) ? o2 : 0u) + ((row & 1) ? o1 : 0u)] = acc;
+        }
+    }
+}
+
+// One gate instruction (G1, CG1, G2, G3, G4) on a register of N amplitudes at
 // psi (shared or global memory); every thread of the CTA calls it.
 __device__ __forceinline__ void tr_gate(const TInstr& I, const float2* __restrict__ mats,
                                         float2* psi, uint32_t N, int tid, int nt) {
@@ -111,6 +141,9 @@ __device__ __forceinline__ void tr_gate(const TInstr& I, const float2* __restric
             }
             break;
         }
+        case kTG3:
+            tr_gate3(I, mats, psi, N, tid, nt);
+            break;
         case kTG4: {
             // 16 x 16 on bits (b0, b1, b2, b3) = (b0, b1, cmask & 255,
             // cmask >> 8 & 255); row index 8 b0 + 4 b1 + 2 b2 + b3
@@ -350,6 +383,7 @@ __global__ void __launch_bounds__(256, 4)
                 case kTG1:
                 case kTCG1:
                 case kTG2:
+                case kTG3:
                 case kTG4:
                     tr_gate(I, W.mats, psi, N, tid, nt);
                     break;

@@ -116,7 +116,7 @@ bool compile_traj(const qgpu_circuit* c, TProgram& P) {
 namespace {
 
 bool tileable(const TInstr& I) {
-    return I.op == kTG1 || I.op == kTCG1 || I.op == kTG2 || I.op == kTG4;
+    return I.op == kTG1 || I.op == kTCG1 || I.op == kTG2 || I.op == kTG3 || I.op == kTG4;
 }
 
 // bits an instruction reads or writes (controls included)
@@ -125,6 +125,7 @@ uint32_t ins_bits(const TInstr& I) {
         case kTG1: return 1u << I.b0;
         case kTCG1: return (1u << I.b0) | I.cmask;
         case kTG2: return (1u << I.b0) | (1u << I.b1);
+        case kTG3: return (1u << I.b0) | (1u << I.b1) | (1u << (I.cmask & 255u));
         case kTG4:
             return (1u << I.b0) | (1u << I.b1) | (1u << (I.cmask & 255u)) |
                    (1u << ((I.cmask >> 8) & 255u));
@@ -270,7 +271,8 @@ void plan_tiles(TProgram& P, int T, size_t min_run) {
         for (size_t k = i; k < j; ++k) {
             TInstr I = P.ins[k];
             I.b0 = uint8_t(loc[I.b0]);
-            if (I.op == kTG2 || I.op == kTG4) I.b1 = uint8_t(loc[I.b1]);
+            if (I.op == kTG2 || I.op == kTG3 || I.op == kTG4) I.b1 = uint8_t(loc[I.b1]);
+            if (I.op == kTG3) I.cmask = uint32_t(loc[I.cmask & 255u]);
             if (I.op == kTCG1) {
                 I.cmask = remap(I.cmask);
                 I.cval = remap(I.cval);
@@ -295,18 +297,14 @@ void set_tile_width(qgpu_ctx* ctx, int n, int T) {
     else g_tile_chosen[{ctx->device, n}] = T;
 }
 
-int tile_width(qgpu_ctx* ctx, int n) {
-    if (n <= kTrajMaxQubits) return 0;
-    std::mutex& mu = g_tile_mu;
-    std::map<std::pair<int, int>, int>& chosen = g_tile_chosen;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = chosen.find({ctx->device, n});
-        if (it != chosen.end()) return it->second;
-    }
-    // calibration program: two layers of 1-qubit gates on every qubit and
-    // 2-qubit gates on (0,1), (2,3), ... (matrix values do not change the
-    // time; one layer under-rates the narrower tiles)
+namespace {
+
+// The calibration program of a register of n qubits: two layers of 1-qubit
+// gates on every qubit and 2-qubit gates on (0,1), (2,3), ... or, with
+// `matching`, on a fixed random matching (what fusion sees in layered
+// circuits). Matrix values do not change the time; one layer under-rates
+// the narrower tiles.
+TProgram calibration_program(int n, bool matching) {
     TProgram P;
     P.n = uint32_t(n);
     const float h = 0.70710678f;
@@ -314,9 +312,10 @@ int tile_width(qgpu_ctx* ctx, int n) {
     for (float v : g1) P.mats.push_back(v);
     for (int r = 0; r < 4; ++r)
         for (int c = 0; c < 4; ++c) {
-            P.mats.push_back(r == c ? 1.f : 0.f);
+            P.mats.push_back(r == c ? 0.5f : 0.5f * float((r + c) % 2));
             P.mats.push_back(0.f);
         }
+    uint32_t x = 12345u; // fixed matching sequence
     for (int layer = 0; layer < 2; ++layer) {
         for (int q = 0; q < n; ++q) {
             TInstr I{};
@@ -325,20 +324,32 @@ int tile_width(qgpu_ctx* ctx, int n) {
             I.flags = q == 0 ? kTNewStep : 0;
             P.ins.push_back(I);
         }
+        std::vector<int> perm(static_cast<size_t>(n));
+        for (int q = 0; q < n; ++q) perm[size_t(q)] = q;
+        for (int q = n - 1; q > 0 && matching; --q) {
+            x = x * 1664525u + 1013904223u;
+            std::swap(perm[size_t(q)], perm[size_t(x % uint32_t(q + 1))]);
+        }
         for (int q = 0; q + 1 < n; q += 2) {
             TInstr I{};
             I.op = kTG2;
-            I.b0 = uint8_t(q);
-            I.b1 = uint8_t(q + 1);
+            I.b0 = uint8_t(perm[size_t(q)]);
+            I.b1 = uint8_t(perm[size_t(q + 1)]);
             I.mat = 4;
             P.ins.push_back(I);
         }
     }
+    return P;
+}
+
+// Device time (ms) of one launch of K registers of n qubits running each
+// program of `forms` with its tile width; -1 for forms too large to stage.
+std::vector<float> time_forms(qgpu_ctx* ctx, int n, const std::vector<std::pair<TProgram, int>>& forms) {
     const uint64_t N = uint64_t(1) << n;
     const int K = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->num_sms) * 4,
                                                                (uint64_t(1) << 29) / (N * 8))));
     const size_t b_state = size_t(K) * N * sizeof(float2);
-    const size_t b_prog = 4096 * sizeof(TInstr), b_mat = 65536, b_work = K * sizeof(TWork);
+    const size_t b_prog = 4096 * sizeof(TInstr), b_mat = 262144, b_work = K * sizeof(TWork);
     unsigned char* buf = nullptr;
     QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf),
                              b_state + b_prog + b_mat + b_work + 64 * K));
@@ -363,20 +374,19 @@ int tile_width(qgpu_ctx* ctx, int n) {
             cudaEventDestroy(b);
         }
     } ev{e0, e1};
-    int best = 0;
-    float best_ms = 0;
-    for (int T : {0, 10, 11, 12, 13}) {
-        // from 17 qubits on the untiled form (one register pass per gate)
-        // is never competitive and the slowest to time
-        if (T >= n || (T == 0 && n >= 17)) continue;
-        TProgram Q = P;
-        plan_tiles(Q, T);
-        if (Q.ins.size() > 4096 || Q.mats.size() * sizeof(float) > b_mat) continue;
+    std::vector<float> out;
+    for (const auto& f : forms) {
+        const TProgram& Q = f.first;
+        const int T = f.second;
+        if (Q.ins.size() > 4096 || Q.mats.size() * sizeof(float) > b_mat) {
+            out.push_back(-1.f);
+            continue;
+        }
         QG_CUDA(cudaMemcpyAsync(dins, Q.ins.data(), Q.ins.size() * sizeof(TInstr),
                                 cudaMemcpyHostToDevice, ctx->stream));
         QG_CUDA(cudaMemcpyAsync(dmat, Q.mats.data(), Q.mats.size() * sizeof(float),
                                 cudaMemcpyHostToDevice, ctx->stream));
-        std::vector<TWork> work(K);
+        std::vector<TWork> work(static_cast<size_t>(K));
         for (int k = 0; k < K; ++k) {
             TWork w{};
             w.prog = dins;
@@ -386,9 +396,9 @@ int tile_width(qgpu_ctx* ctx, int n) {
             w.out = uint32_t(k);
             w.init = dstate + size_t(k) * N;
             w.fin = dstate + size_t(k) * N;
-            w.inplace = 1;
+            w.inplace = n > kTrajMaxQubits ? 1 : 0;
             w.diag = nullptr;
-            work[k] = w;
+            work[size_t(k)] = w;
         }
         QG_CUDA(cudaMemcpyAsync(dwork, work.data(), K * sizeof(TWork), cudaMemcpyHostToDevice,
                                 ctx->stream));
@@ -399,13 +409,201 @@ int tile_width(qgpu_ctx* ctx, int n) {
         QG_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (best_ms == 0 || ms < best_ms) {
-            best = T;
-            best_ms = ms;
-        }
+        out.push_back(ms);
     }
-    std::lock_guard<std::mutex> lock(mu);
-    chosen[{ctx->device, n}] = best;
+    return out;
+}
+
+std::map<std::pair<int, int>, int> g_fuse_chosen; // (device, n) -> fusion width
+
+} // namespace
+
+void fuse_blocks(TProgram& P, int w) {
+    using C = std::complex<double>;
+    struct Blk {
+        std::vector<int> bits; // bits[0]: most significant digit of the index
+        std::vector<C> U;      // column-major
+    };
+    auto ld = [&](uint32_t off, int count) {
+        std::vector<C> m(static_cast<size_t>(count));
+        for (int i = 0; i < count; ++i)
+            m[size_t(i)] = C(P.mats[2 * (size_t(off) + i)], P.mats[2 * (size_t(off) + i) + 1]);
+        return m;
+    };
+    // G on `gb` as an operator on `ub` (gb a subset, the other digits of the
+    // row and column equal)
+    auto embed = [](const std::vector<C>& G, const std::vector<int>& gb, const std::vector<int>& ub) {
+        const int K = int(ub.size()), k = int(gb.size());
+        const uint32_t D = 1u << K;
+        std::vector<int> at(static_cast<size_t>(k)); // position of gb[j] in ub
+        uint32_t gmask = 0;
+        for (int j = 0; j < k; ++j) {
+            at[size_t(j)] = int(std::find(ub.begin(), ub.end(), gb[size_t(j)]) - ub.begin());
+            gmask |= 1u << (K - 1 - at[size_t(j)]);
+        }
+        auto proj = [&](uint32_t x) {
+            uint32_t r = 0;
+            for (int j = 0; j < k; ++j) r = (r << 1) | ((x >> (K - 1 - at[size_t(j)])) & 1u);
+            return r;
+        };
+        std::vector<C> E(size_t(D) * D, C(0.0));
+        for (uint32_t c = 0; c < D; ++c)
+            for (uint32_t r = 0; r < D; ++r)
+                if ((r & ~gmask) == (c & ~gmask))
+                    E[r + size_t(c) * D] = G[proj(r) + (size_t(proj(c)) << k)];
+        return E;
+    };
+    auto matmul = [](const std::vector<C>& A, const std::vector<C>& B, uint32_t D) {
+        std::vector<C> R(size_t(D) * D, C(0.0));
+        for (uint32_t c = 0; c < D; ++c)
+            for (uint32_t k = 0; k < D; ++k) {
+                const C b = B[k + size_t(c) * D];
+                if (b == C(0.0)) continue;
+                for (uint32_t r = 0; r < D; ++r) R[r + size_t(c) * D] += A[r + size_t(k) * D] * b;
+            }
+        return R;
+    };
+    MatPool pool(P);
+    std::vector<TInstr> out;
+    out.reserve(P.ins.size());
+    std::vector<Blk> open; // acting on disjoint bits, so they commute
+    auto emit = [&](const Blk& B) {
+        TInstr I{};
+        const size_t k = B.bits.size();
+        I.op = k == 1 ? kTG1 : k == 2 ? kTG2 : k == 3 ? kTG3 : kTG4;
+        I.b0 = uint8_t(B.bits[0]);
+        if (k >= 2) I.b1 = uint8_t(B.bits[1]);
+        if (k == 3) I.cmask = uint32_t(B.bits[2]);
+        if (k == 4) I.cmask = uint32_t(B.bits[2]) | (uint32_t(B.bits[3]) << 8);
+        I.mat = pool.add(B.U);
+        out.push_back(I);
+    };
+    auto flush = [&](uint32_t mask) {
+        std::vector<Blk> keep;
+        for (Blk& B : open) {
+            bool hit = false;
+            for (int b : B.bits) hit = hit || ((mask >> b) & 1u);
+            if (hit) emit(B);
+            else keep.push_back(std::move(B));
+        }
+        open.swap(keep);
+    };
+    for (const TInstr& I : P.ins) {
+        std::vector<int> gb;
+        int dim = 0;
+        switch (I.op) {
+            case kTG1: gb = {I.b0}; dim = 2; break;
+            case kTG2: gb = {I.b0, I.b1}; dim = 4; break;
+            case kTG3: gb = {I.b0, I.b1, int(I.cmask & 255u)}; dim = 8; break;
+            case kTG4:
+                gb = {I.b0, I.b1, int(I.cmask & 255u), int((I.cmask >> 8) & 255u)};
+                dim = 16;
+                break;
+            default: break;
+        }
+        if (gb.empty()) { // not a dense gate: keep it, after the blocks it touches
+            flush(ins_bits(I) | (I.op == kTMeas ? (1u << I.b0) : 0u) |
+                  (I.op == kTTile ? 0xffffffffu : 0u));
+            out.push_back(I);
+            continue;
+        }
+        std::vector<C> G = ld(I.mat, dim * dim);
+        std::vector<int> ub = gb;
+        std::vector<size_t> touched;
+        for (size_t bi = 0; bi < open.size(); ++bi) {
+            bool hit = false;
+            for (int b : open[bi].bits) hit = hit || std::find(gb.begin(), gb.end(), b) != gb.end();
+            if (!hit) continue;
+            touched.push_back(bi);
+            for (int b : open[bi].bits)
+                if (std::find(ub.begin(), ub.end(), b) == ub.end()) ub.push_back(b);
+        }
+        if (int(ub.size()) > w) {
+            uint32_t m = 0;
+            for (int b : gb) m |= 1u << b;
+            flush(m); // emit the touched blocks, then start over with G
+            ub = gb;
+            touched.clear();
+            if (int(gb.size()) > w) { // wider than the fusion width: as is
+                out.push_back(I);
+                continue;
+            }
+        }
+        const uint32_t D = 1u << ub.size();
+        std::vector<C> M = embed(G, gb, ub);
+        for (size_t bi : touched) M = matmul(M, embed(open[bi].U, open[bi].bits, ub), D);
+        std::vector<Blk> keep;
+        for (size_t bi = 0; bi < open.size(); ++bi)
+            if (std::find(touched.begin(), touched.end(), bi) == touched.end())
+                keep.push_back(std::move(open[bi]));
+        open.swap(keep);
+        open.push_back(Blk{ub, std::move(M)});
+    }
+    flush(0xffffffffu);
+    P.ins.swap(out);
+}
+
+int tile_width(qgpu_ctx* ctx, int n) {
+    if (n <= kTrajMaxQubits) return 0;
+    {
+        std::lock_guard<std::mutex> lock(g_tile_mu);
+        auto it = g_tile_chosen.find({ctx->device, n});
+        if (it != g_tile_chosen.end()) return it->second;
+    }
+    const TProgram P = calibration_program(n, false);
+    std::vector<std::pair<TProgram, int>> forms;
+    for (int T : {0, 10, 11, 12, 13}) {
+        // from 17 qubits on the untiled form (one register pass per gate)
+        // is never competitive and the slowest to time
+        if (T >= n || (T == 0 && n >= 17)) continue;
+        TProgram Q = P;
+        plan_tiles(Q, T);
+        forms.emplace_back(std::move(Q), T);
+    }
+    const std::vector<float> ms = time_forms(ctx, n, forms);
+    int best = 0;
+    float best_ms = 0;
+    for (size_t i = 0; i < forms.size(); ++i)
+        if (ms[i] >= 0 && (best_ms == 0 || ms[i] < best_ms)) {
+            best = forms[i].second;
+            best_ms = ms[i];
+        }
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    g_tile_chosen[{ctx->device, n}] = best;
+    return best;
+}
+
+void set_fusion_width(qgpu_ctx* ctx, int n, int w) {
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    if (w < 0) g_fuse_chosen.erase({ctx->device, n});
+    else g_fuse_chosen[{ctx->device, n}] = w;
+}
+
+int fusion_width(qgpu_ctx* ctx, int n) {
+    {
+        std::lock_guard<std::mutex> lock(g_tile_mu);
+        auto it = g_fuse_chosen.find({ctx->device, n});
+        if (it != g_fuse_chosen.end()) return it->second;
+    }
+    const int T = tile_width(ctx, n);
+    const TProgram P = calibration_program(n, true);
+    std::vector<std::pair<TProgram, int>> forms;
+    for (int w = 2; w <= kFuseMaxWidth; ++w) {
+        TProgram Q = P;
+        fuse_blocks(Q, w);
+        if (T) plan_tiles(Q, T);
+        forms.emplace_back(std::move(Q), T);
+    }
+    const std::vector<float> ms = time_forms(ctx, n, forms);
+    int best = 2;
+    float best_ms = 0;
+    for (size_t i = 0; i < forms.size(); ++i)
+        if (ms[i] >= 0 && (best_ms == 0 || ms[i] < best_ms)) {
+            best = int(i) + 2;
+            best_ms = ms[i];
+        }
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    g_fuse_chosen[{ctx->device, n}] = best;
     return best;
 }
 
@@ -501,6 +699,20 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
         if (dump)
             for (size_t i = 0; i < dumpf.size(); ++i) dump[i] = double(dumpf[i]);
+    });
+}
+
+extern "C" qgpu_status qgpu_traj_fusion_width(qgpu_ctx* ctx, uint32_t n, int set_w, int* chosen) {
+    return guarded([&] {
+        need_handle(ctx);
+        const char* W = "qgpu_traj_fusion_width()";
+        if (n < 1 || n > uint32_t(qgpu::kTrajMaxGlobalQubits))
+            raise(QGPU_ERR_OUT_OF_RANGE, W, "n");
+        if (set_w > qgpu::kFuseMaxWidth || set_w == 0 || set_w == 1 || set_w < -2)
+            raise(QGPU_ERR_OUT_OF_RANGE, W, "set_w");
+        if (set_w >= 2) qgpu::set_fusion_width(ctx, int(n), set_w);
+        if (set_w == -2) qgpu::set_fusion_width(ctx, int(n), -1);
+        if (chosen) *chosen = qgpu::fusion_width(ctx, int(n));
     });
 }
 

@@ -11,12 +11,13 @@
 
 namespace qgpu {
 
+// kTG3: 8 x 8 on three bits (b0, b1, cmask & 255), row index 4 b0 + 2 b1 + b2
 // kTG4: 16 x 16 on four bits (b0, b1, cmask & 255, cmask >> 8 & 255)
 // kTTile: tile-pass header: the next `cmask` instructions act on the b0 = T
 // bits listed (one 32-bit word each, ascending, bits 0..4 first) at float2
 // offset `mat` of the matrix pool, with their bit positions renumbered
 // within that list
-enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4, kTG4 = 5, kTTile = 6 };
+enum : uint8_t { kTG1 = 1, kTG2 = 2, kTCG1 = 3, kTMeas = 4, kTG4 = 5, kTTile = 6, kTG3 = 7 };
 enum : uint8_t { kTNewStep = 1, kTDestructive = 2 };
 
 // One instruction; qubits are bit positions (LSB = 0) of the full register.
@@ -106,6 +107,20 @@ void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_
 // gates in between, which act on other qubits); products in FP64, rounded
 // to complex64 once. No reference counterpart.
 void fold_1q_gates(TProgram& P);
+// Noiseless programs only: consecutive dense gates (G1-G4) merge greedily into
+// dense blocks of at most w bits (open blocks act on disjoint bits, so they
+// commute; a gate joins the blocks it touches while their union stays within
+// w bits, otherwise those blocks are emitted first), emitted as G1-G4.
+// Products in FP64, rounded to complex64 once. Fusion width w = 2 holds 1- and
+// 2-qubit gates; wider blocks trade arithmetic for register passes.
+constexpr int kFuseMaxWidth = 4;
+void fuse_blocks(TProgram& P, int w);
+// The fusion width (2..kFuseMaxWidth) for batched registers of n qubits on
+// this device, chosen once per (device, n) by timing the calibration program
+// (two layers on random matchings) fused at each width with the tuned tile
+// width; call outside stream capture.
+int fusion_width(qgpu_ctx* ctx, int n);
+void set_fusion_width(qgpu_ctx* ctx, int n, int w);
 // min_run: the shortest run that becomes a pass (2 by default; 1 turns
 // every gate into a pass, as the layer-synchronous batches need).
 void plan_tiles(TProgram& P, int T, size_t min_run = 2);

@@ -58,6 +58,26 @@ static void gate(const TInstr& I, const float* mats, f2* psi, uint32_t N) {
                 psi[i + s] = cfma(m[3], v1, cmul(m[1], v0));
             }
             break;
+        case kTG3: {
+            // 8 x 8 on (b0, b1, cmask & 255), row index 4 b0 + 2 b1 + b2
+            int sb[3] = {I.b0, I.b1, int(I.cmask & 255u)};
+            std::sort(sb, sb + 3);
+            const uint32_t o4 = 1u << I.b0, o2 = 1u << I.b1, o1 = 1u << (I.cmask & 255u);
+            for (uint32_t p = 0; p < N / 8; ++p) {
+                const uint32_t i = ins0(ins0(ins0(p, sb[0]), sb[1]), sb[2]);
+                auto at = [&](int r) {
+                    return i + ((r & 4) ? o4 : 0u) + ((r & 2) ? o2 : 0u) + ((r & 1) ? o1 : 0u);
+                };
+                f2 v[8];
+                for (int c = 0; c < 8; ++c) v[c] = psi[at(c)];
+                for (int row = 0; row < 8; ++row) {
+                    f2 acc = cmul(m[row], v[0]);
+                    for (int c = 1; c < 8; ++c) acc = cfma(m[row + 8 * c], v[c], acc);
+                    psi[at(row)] = acc;
+                }
+            }
+            break;
+        }
         case kTG2: {
             int lo = std::min(I.b0, I.b1), hi = std::max(I.b0, I.b1);
             uint32_t s0 = 1u << I.b0, s1 = 1u << I.b1;
@@ -148,7 +168,8 @@ static void tile_pass(const std::vector<TInstr>& prog, const float* mats, size_t
             const TInstr& I = prog[i];
             // local bits inside the tile
             EXPECT(I.b0 < T);
-            if (I.op == kTG2 || I.op == kTG4) EXPECT(I.b1 < T);
+            if (I.op == kTG2 || I.op == kTG3 || I.op == kTG4) EXPECT(I.b1 < T);
+            if (I.op == kTG3) EXPECT((I.cmask & 255u) < uint32_t(T));
             if (I.op == kTCG1) EXPECT((I.cmask >> T) == 0);
             gate(I, mats, tile.data(), NT);
         }
@@ -300,6 +321,36 @@ int main() {
                 den = std::max(den, double(std::abs(a[i])));
             }
             EXPECT(num <= 1e-4 * den);
+        }
+        for (int w = 2; w <= kFuseMaxWidth; ++w) {
+            // dense blocks of at most w bits (wider gates pass as they are):
+            // same result up to complex64 rounding, also after tiling
+            TProgram F = U;
+            fuse_blocks(F, w);
+            size_t gates = 0, gates_u = 0;
+            for (const auto& I : F.ins) {
+                const int k = I.op == kTG1 ? 1 : I.op == kTG2 ? 2 : I.op == kTG3 ? 3 : I.op == kTG4 ? 4 : 0;
+                if (k) ++gates;
+                EXPECT(k <= w || I.op == kTG4);
+            }
+            for (const auto& I : U.ins) gates_u += I.op != kTMeas;
+            EXPECT(gates <= gates_u);
+            const uint32_t N = 1u << n;
+            std::vector<f2> a(N), c(N), t(N);
+            for (uint32_t i = 0; i < N; ++i) a[i] = c[i] = t[i] = f2(g(rng), g(rng));
+            run(U, a);
+            run(F, c);
+            TProgram FT = F;
+            plan_tiles(FT, 12, 1);
+            run(FT, t);
+            double num = 0, numt = 0, den = 0;
+            for (uint32_t i = 0; i < N; ++i) {
+                num = std::max(num, double(std::abs(a[i] - c[i])));
+                numt = std::max(numt, double(std::abs(c[i] - t[i])));
+                den = std::max(den, double(std::abs(a[i])));
+            }
+            EXPECT(num <= 1e-4 * den);
+            EXPECT(numt == 0.0); // tiling reorders nothing
         }
         const uint32_t N = 1u << n;
         std::vector<f2> x0(N);

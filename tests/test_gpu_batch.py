@@ -84,3 +84,33 @@ def test_batch_rejects_a_state_given_twice(ctx):
     with pytest.raises(qb.Duplicates):
         qb.run_batch(ctx, [c, c], [s, s], qb.FUSED)
     s.free()
+
+
+@pytest.mark.parametrize("w", [2, 3, 4])
+def test_every_fusion_width_matches_plain_loop(ctx, w):
+    """Pinned fusion widths 2-4 (8 x 8 and 16 x 16 blocks) on kets of 10-16
+    qubits and density matrices of 4-9: the graph form agrees with the plain
+    per-instance loop within 2e-5 relative."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(77 + w)
+    circuits, inputs = [], []
+    for i in range(16):
+        rho = i % 4 == 3
+        n = int(rng.integers(4, 10)) if rho else int(rng.integers(10, 17))
+        c, _ = layered(qb, rng, n, 3, rho)
+        circuits.append(c)
+        inputs.append(random_rho(rng, 2 ** n, 8) if rho else gaussian_ket(rng, 2 ** n))
+    sizes = sorted({int(np.log2(x.shape[0])) * (2 if x.ndim == 2 else 1) for x in inputs})
+    try:
+        for n in sizes:
+            assert qb.traj_fusion_width(ctx, n, w) == w
+        a = [qb.State.from_numpy(ctx, x, [2] * int(np.log2(len(x))), qb.C64) for x in inputs]
+        b = [qb.State.from_numpy(ctx, x, [2] * int(np.log2(len(x))), qb.C64) for x in inputs]
+        qb.run_batch(ctx, circuits, a, qb.FUSED)
+        qb.run_batch(ctx, circuits, b, qb.PLAIN)
+        for i in range(len(circuits)):
+            ga, gb = a[i].numpy(), b[i].numpy()
+            assert np.max(np.abs(ga - gb)) / np.max(np.abs(gb)) < 2e-5, (w, i)
+    finally:
+        for n in sizes:
+            qb.traj_fusion_width(ctx, n, -2)
