@@ -155,6 +155,55 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Output rows [P * DA / S, (P + 1) * DA / S) of one group, the matrix
+// entries taken as compile-time offsets into the parameter bank.
+template <typename R, int DA, int S, int P>
+__device__ __forceinline__ void reg_rows(Cplx<R>* psi, const RegParams<R, DA>& p, uint64_t base,
+                                         const Cplx<R> (&v)[DA]) {
+    using C = Cplx<R>;
+#pragma unroll
+    for (int k = 0; k < DA / S; ++k) {
+        constexpr int m0 = P * (DA / S);
+        C acc = cmul(p.A[m0 + k], v[0]);
+#pragma unroll
+        for (int c = 1; c < DA; ++c) acc = cfma(p.A[m0 + k + c * DA], v[c], acc);
+        psi[base + p.off[m0 + k]] = acc;
+    }
+}
+
+// k_reg with each group shared by 2 warps: lane l of warps 2j and 2j + 1
+// both load the group's DA inputs, and each forms half of the output rows,
+// so a thread does half the arithmetic and holds half the partial results.
+// A block barrier separates the loads of an iteration from its in-place
+// stores.
+template <typename R, int DA>
+__global__ void __launch_bounds__(256)
+    k_reg_split(Cplx<R>* __restrict__ psi, const __grid_constant__ RegParams<R, DA> p) {
+    using C = Cplx<R>;
+    const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
+    const int part = warp & 1; // uniform within a warp
+    const uint64_t per_block = blockDim.x / 2;
+    const uint64_t nth = uint64_t(gridDim.x) * per_block;
+    const uint64_t g_first = uint64_t(blockIdx.x) * per_block + uint64_t(warp >> 1) * 32 + lane;
+    // every thread of the block runs the same number of iterations
+    const uint64_t iters = (p.outer.count + nth - 1) / nth;
+    for (uint64_t it = 0; it < iters; ++it) {
+        const uint64_t g = g_first + it * nth;
+        const bool valid = g < p.outer.count;
+        const uint64_t base = valid ? seg_offset(p.outer, g) : 0;
+        C v[DA];
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < DA; ++c) v[c] = psi[base + p.off[c]];
+        }
+        __syncthreads();
+        if (valid) {
+            if (part == 0) reg_rows<R, DA, 2, 0>(psi, p, base, v);
+            else reg_rows<R, DA, 2, 1>(psi, p, base, v);
+        }
+    }
+}
+
 // Shared-memory variant for any DA: a block owns G groups at a time
 // (G * DA <= blockDim.x when DA <= 256), stages them, then each thread forms
 // output rows. A (column-major, state precision) and off live in global
@@ -272,6 +321,20 @@ static void reg(qgpu_ctx* ctx, void* data, const SegPlan& outer,
     after_launch(ctx, "k_reg");
 }
 
+template <typename R, int DA>
+static void reg_split(qgpu_ctx* ctx, void* data, const SegPlan& outer,
+                      const std::vector<uint64_t>& off, const cd* A) {
+    RegParams<R, DA> p;
+    p.outer = outer;
+    for (int i = 0; i < DA; ++i) p.off[i] = off[i];
+    for (int i = 0; i < DA * DA; ++i) p.A[i] = cv<R>(A[i]);
+    int blocks = grid_blocks(ctx, 4);
+    uint64_t need = (outer.count + 127) / 128;
+    if (need < uint64_t(blocks)) blocks = int(std::max<uint64_t>(need, 1));
+    k_reg_split<R, DA><<<blocks, 256, 0, ctx->stream>>>(static_cast<Cplx<R>*>(data), p);
+    after_launch(ctx, "k_reg_split");
+}
+
 template <typename R>
 static void smem(qgpu_ctx* ctx, void* data, const SegPlan& outer,
                  const std::vector<uint64_t>& off, const cd* A, uint64_t DA) {
@@ -318,7 +381,11 @@ static void generic(qgpu_ctx* ctx, void* data, const SegPlan& outer,
         case 4: return reg<R, 4>(ctx, data, outer, off, A);
         case 8: return reg<R, 8>(ctx, data, outer, off, A);
         case 9: return reg<R, 9>(ctx, data, outer, off, A);
-        case 16: return reg<R, 16>(ctx, data, outer, off, A);
+        case 16:
+            // complex128: two warps per group (a whole 16 x 16 per thread
+            // needs over 250 registers)
+            if (sizeof(R) == 8) return reg_split<R, 16>(ctx, data, outer, off, A);
+            return reg<R, 16>(ctx, data, outer, off, A);
         default: return smem<R>(ctx, data, outer, off, A, DA);
     }
 }
