@@ -58,24 +58,6 @@ __device__ inline uint64_t order_sum(const QftPlan& p, uint32_t idx, bool write_
     return acc;
 }
 
-// Asynchronous global -> shared copies of one amplitude (16 B for complex128
-// through L2 only, 8 B for complex64) and their group fences.
-template <typename C>
-__device__ __forceinline__ void cp_async_elem(C* dst, const C* src) {
-    const uint32_t a = uint32_t(__cvta_generic_to_shared(dst));
-    if constexpr (sizeof(C) == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(src) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // G consecutive qubit steps starting at step jf (forward: jf, jf + 1, ...;
 // inverse: jf, jf - 1, ...) on every base of the tile, in registers. Step j
 // sits on tile bit nr + M - 1 - j: the round's bits are [lo, lo + G) and step

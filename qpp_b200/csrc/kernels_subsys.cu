@@ -136,60 +136,108 @@ void launch_gather(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
 // When every digit's dimension is a power of two, a gather is a permutation
 // of index bits: out[o] = in[foff + sum_j bit_j(o) * in_stride[j]]. A plain
 // gather writes densely but reads with the stride of whatever input digit
-// lands on the output's lowest bits. The tiled form moves 2^tb elements per
+// lands on the output's lowest bits. The tiled form moves 2^10 elements per
 // tile through shared memory: the tile's bits are the output's five lowest
 // bits and the five bits with the smallest input strides (then more low
 // output bits), so 32 consecutive elements are read and 32 consecutive
-// elements are written per warp access.
+// elements are written per warp access. Every offset is a sum over index
+// bits, so each comes from two 32-entry tables (the tile's read and write
+// orders) or two 128-entry tables plus a short loop (the tile number); a
+// thread's low-table entries are fixed. The next tile is copied in with
+// cp.async while the current one is written out, and tile positions are
+// XOR-swizzled (the low five bits take bits 5..9 too) so that both the
+// scattered stores into shared memory and the runs read from it spread over
+// the banks.
+
+__device__ __forceinline__ uint32_t perm_swz(uint32_t p) { return p ^ ((p >> 5) & 31u); }
 
 template <typename R>
 __global__ void __launch_bounds__(256)
     k_permute_tiled(const Cplx<R>* __restrict__ in, Cplx<R>* __restrict__ out,
                     const __grid_constant__ PermPlan P) {
-    __shared__ Cplx<R> tile[1 << kPermTileBits];
-    __shared__ uint64_t in_off[1 << kPermTileBits];  // by read-order index
-    __shared__ uint64_t out_off[1 << kPermTileBits]; // by write-order index
-    __shared__ uint16_t pos_of[1 << kPermTileBits];  // read-order -> write-order
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const uint32_t NT = 1u << P.tb;
-    for (uint32_t l = tid; l < NT; l += nt) {
+    using C = Cplx<R>;
+    constexpr uint32_t NT = 1u << kPermTileBits; // 4 elements per thread of 256
+    __shared__ __align__(16) C tile[2][NT];
+    __shared__ uint64_t in_lo[32], in_hi[32];   // read order: input offsets
+    __shared__ uint32_t pos_lo[32], pos_hi[32]; // read order: write-order positions
+    __shared__ uint64_t out_lo[32], out_hi[32]; // write order: output offsets
+    __shared__ uint64_t tb_in[2][128], tb_out[2][128]; // tile number bits [0,7), [7,14)
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5;
+    const int r0 = P.nrest < 7 ? P.nrest : 7;
+    const int r1 = P.nrest - r0 < 7 ? P.nrest - r0 : 7;
+    if (tid < 64) {
+        const int h = tid >> 5, i = tid & 31; // h: bits 0-4 or 5-9 of the tile index
         uint64_t io = 0, oo = 0;
-        uint32_t lo = 0;
-        for (int j = 0; j < P.tb; ++j)
-            if ((l >> j) & 1u) {
-                io += P.in_stride[P.tin[j]];
-                lo |= 1u << P.tin_pos[j];
-                oo |= uint64_t(1) << P.tbits[j];
+        uint32_t po = 0;
+        for (int j = 0; j < 5; ++j)
+            if ((i >> j) & 1) {
+                io += P.in_stride[P.tin[5 * h + j]];
+                po |= 1u << P.tin_pos[5 * h + j];
+                oo |= uint64_t(1) << P.tbits[5 * h + j];
             }
-        in_off[l] = io;
-        out_off[l] = oo;
-        pos_of[l] = uint16_t(lo);
+        (h ? in_hi : in_lo)[i] = io;
+        (h ? pos_hi : pos_lo)[i] = po;
+        (h ? out_hi : out_lo)[i] = oo;
+    }
+    for (int i = tid; i < 256; i += nt) {
+        const int h = i >> 7, x = i & 127, lo = h ? r0 : 0, cnt = h ? r1 : r0;
+        uint64_t bi = 0, bo = 0;
+        for (int j = 0; j < cnt; ++j)
+            if ((x >> j) & 1) {
+                bi += P.in_stride[P.rest[lo + j]];
+                bo |= uint64_t(1) << P.rest[lo + j];
+            }
+        tb_in[h][x] = bi;
+        tb_out[h][x] = bo;
     }
     __syncthreads();
     const uint64_t ntiles = uint64_t(1) << P.nrest;
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint64_t bo = 0, bi = P.foff;
-        for (int j = 0; j < P.nrest; ++j)
+    const uint64_t m0 = (uint64_t(1) << r0) - 1, m1 = (uint64_t(1) << r1) - 1;
+    auto base = [&](uint64_t t, uint64_t& bi, uint64_t& bo) {
+        bi = P.foff + tb_in[0][t & m0] + tb_in[1][(t >> r0) & m1];
+        bo = tb_out[0][t & m0] | tb_out[1][(t >> r0) & m1];
+        for (int j = r0 + r1; j < P.nrest; ++j)
             if ((t >> j) & 1u) {
-                bo |= uint64_t(1) << P.rest[j];
                 bi += P.in_stride[P.rest[j]];
+                bo |= uint64_t(1) << P.rest[j];
             }
-        for (uint32_t l0 = 0; l0 < NT; l0 += 4u * nt) {
-            Cplx<R> v[4];
+    };
+    // this thread moves read-order elements lane + 32 (w + 8u), u < 4, and
+    // write-order elements of the same form
+    const uint64_t my_in = in_lo[lane], my_out = out_lo[lane];
+    const uint32_t my_pos = pos_lo[lane];
+    auto issue = [&](uint64_t bi, C* buf) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint32_t l = l0 + u * nt + tid;
-                if (l < NT) v[u] = in[bi + in_off[l]];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint32_t l = l0 + u * nt + tid;
-                if (l < NT) tile[pos_of[l]] = v[u];
-            }
+        for (int u = 0; u < 4; ++u) {
+            const int h = w + 8 * u;
+            cp_async_elem(buf + perm_swz(my_pos | pos_hi[h]), in + bi + my_in + in_hi[h]);
+        }
+        cp_async_commit();
+    };
+    uint64_t t = blockIdx.x;
+    if (t >= ntiles) return; // uniform across the CTA
+    uint64_t bi, bo;
+    base(t, bi, bo);
+    issue(bi, tile[0]);
+    for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
+        const C* cur = tile[it & 1];
+        const uint64_t tn = t + gridDim.x;
+        uint64_t bin = 0, bon = 0;
+        if (tn < ntiles) {
+            base(tn, bin, bon);
+            issue(bin, tile[(it + 1) & 1]);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
-        for (uint32_t l = tid; l < NT; l += nt) out[bo + out_off[l]] = tile[l];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int h = w + 8 * u;
+            out[bo + my_out + out_hi[h]] = cur[perm_swz((uint32_t(h) << 5) | uint32_t(lane))];
+        }
         __syncthreads();
+        bo = bon;
     }
 }
 

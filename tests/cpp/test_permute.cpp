@@ -49,6 +49,62 @@ static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& 
     }
     // the low five output bits are in the tile (coalesced writes)
     for (int j = 0; j < 5; ++j) EXPECT(P.tbits[j] == j);
+    // the kernel's split tables: every offset is a sum (or an OR) over index
+    // bits, so the low and high halves of a tile index combine exactly
+    {
+        uint64_t in_lo[32], in_hi[32], out_lo[32], out_hi[32];
+        uint32_t pos_lo[32], pos_hi[32];
+        for (int h = 0; h < 2; ++h)
+            for (int i = 0; i < 32; ++i) {
+                uint64_t io = 0, oo = 0;
+                uint32_t po = 0;
+                for (int j = 0; j < 5; ++j)
+                    if ((i >> j) & 1) {
+                        io += P.in_stride[P.tin[5 * h + j]];
+                        po |= 1u << P.tin_pos[5 * h + j];
+                        oo |= uint64_t(1) << P.tbits[5 * h + j];
+                    }
+                (h ? in_hi : in_lo)[i] = io;
+                (h ? pos_hi : pos_lo)[i] = po;
+                (h ? out_hi : out_lo)[i] = oo;
+            }
+        for (uint32_t l = 0; l < NT; ++l) {
+            EXPECT(in_lo[l & 31] + in_hi[l >> 5] == in_off[l]);
+            EXPECT((pos_lo[l & 31] | pos_hi[l >> 5]) == pos_of[l]);
+            EXPECT((out_lo[l & 31] | out_hi[l >> 5]) == out_off[l]);
+        }
+        // the tile-position swizzle is a bijection
+        std::vector<uint8_t> hit(NT, 0);
+        for (uint32_t p = 0; p < NT; ++p) hit[p ^ ((p >> 5) & 31u)]++;
+        for (uint8_t x : hit) EXPECT(x == 1);
+        // tile-number bases: two 7-bit tables plus the remaining bits
+        const int r0 = std::min(P.nrest, 7), r1 = std::min(P.nrest - r0, 7);
+        for (uint64_t t = 0; t < (uint64_t(1) << P.nrest); t += 1 + (t % 5)) {
+            uint64_t bi = 0, bo = 0, ci = 0, co = 0;
+            for (int j = 0; j < P.nrest; ++j)
+                if ((t >> j) & 1u) {
+                    bo |= uint64_t(1) << P.rest[j];
+                    bi += P.in_stride[P.rest[j]];
+                    if (j < r0 + r1) {
+                        co |= uint64_t(1) << P.rest[j];
+                        ci += P.in_stride[P.rest[j]];
+                    }
+                }
+            uint64_t ti = 0, to = 0;
+            for (int h = 0; h < 2; ++h) {
+                const uint64_t x = h ? (t >> r0) & ((uint64_t(1) << r1) - 1) : t & ((uint64_t(1) << r0) - 1);
+                const int lo = h ? r0 : 0, cnt = h ? r1 : r0;
+                for (int j = 0; j < cnt; ++j)
+                    if ((x >> j) & 1) {
+                        ti += P.in_stride[P.rest[lo + j]];
+                        to |= uint64_t(1) << P.rest[lo + j];
+                    }
+            }
+            EXPECT(ti == ci && to == co);
+            (void)bi;
+            (void)bo;
+        }
+    }
     std::vector<uint8_t> written(count, 0);
     for (uint64_t t = 0; t < (uint64_t(1) << P.nrest); ++t) {
         uint64_t bo = 0, bi = P.foff;
