@@ -389,6 +389,14 @@ typedef enum qgpu_form {
     QGPU_FORM_PLAIN = 0, /* one pass per qpp call, in the state precision */
     QGPU_FORM_FUSED = 1  /* fused blocks: c64 -> 6-qubit tcgen05 3xTF32 */
 } qgpu_form;
+/* Kets: the unitary steps (measurements and classical control need an
+ * engine). QGPU_FORM_FUSED on a complex64 qubit density matrix of <= 15
+ * qubits whose circuit holds only gates and 1- or 2-qubit channels:
+ * superoperators on the 2n virtual qubits (column digits, row digits) merged
+ * into blocks of <= 4 virtual qubits, one pass over the matrix per block
+ * (a layer's gates and pair channel on one qubit pair become one 16 x 16
+ * block); other density matrices return QGPU_ERR_NOT_SUPPORTED in that form.
+ * No reference counterpart for the fused forms. */
 qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form);
 /* One gate of k <= 6 qubits on a complex64 qubit ket of >= 13 qubits, as a
  * 64 x 64 block on the tensor cores (split-TF32, FP32 accumulation). */

@@ -32,9 +32,9 @@
 
 namespace qgpu {
 
-bool compile_traj_rho(const qgpu_circuit* c, TProgram& P) {
+bool compile_traj_rho(const qgpu_circuit* c, TProgram& P, int max_nv) {
     const int nq = int(c->nq), nv = 2 * nq;
-    if (c->d != 2 || nv > kTrajMaxGlobalQubits) return false;
+    if (c->d != 2 || nv > std::min(max_nv, 31)) return false;
     P = TProgram{};
     P.n = uint32_t(nv);
     P.ncreg = c->nc;

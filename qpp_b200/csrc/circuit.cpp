@@ -7,6 +7,7 @@
 
 #include "kernels.hpp"
 #include "ops.hpp"
+#include "traj.hpp"
 
 qgpu_circuit::~qgpu_circuit() {
     if (dB) cudaFree(dB);
@@ -276,6 +277,49 @@ static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
     c->plan_ctx = s->ctx;
 }
 
+// Fused form of a complex64 qubit density matrix (no reference counterpart).
+// The circuit compiles into superoperators on the 2n virtual qubits [column
+// digits, row digits] of the column-major matrix (compile_traj_rho: a 1-qubit
+// gate or channel is 4 x 4 on (column t, row t), a 2-qubit gate U on the row
+// digits and conj(U) on the column digits, a 2-qubit channel 16 x 16 on all
+// four). Consecutive superoperators merge into blocks of at most 4 virtual
+// qubits (fuse_blocks: FP64 products, rounded to complex64 once), so the
+// 1-qubit gates, 2-qubit gate and pair channel that a layer puts on one qubit
+// pair become a single 16 x 16 block, and every block is one in-place pass
+// over the matrix. Plain form: one pass per gate and per channel.
+// The program is built once per circuit (and again after steps are added).
+static void run_rho_fused(qgpu_state* s, qgpu_circuit* c) {
+    if (c->rho_steps != c->steps.size()) {
+        auto P = std::make_shared<TProgram>();
+        if (compile_traj_rho(c, *P, 30)) fuse_blocks(*P, 4);
+        else P.reset();
+        c->rho_prog = P;
+        c->rho_steps = c->steps.size();
+    }
+    if (s->prec != QGPU_C64 || !c->rho_prog)
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
+              "fused form of a density matrix needs complex64, qubits, at most 15 of them, and "
+              "only gates and 1- or 2-qubit channels");
+    const TProgram& P = *c->rho_prog;
+    const VSpace vs = vspace_rho(s->dims);
+    const int nv = int(P.n);
+    std::vector<cd> A;
+    for (const TInstr& I : P.ins) {
+        std::vector<int> vt;
+        vt.push_back(nv - 1 - I.b0);
+        if (I.op == kTG2 || I.op == kTG3 || I.op == kTG4) vt.push_back(nv - 1 - I.b1);
+        if (I.op == kTG3 || I.op == kTG4) vt.push_back(nv - 1 - int(I.cmask & 255u));
+        if (I.op == kTG4) vt.push_back(nv - 1 - int((I.cmask >> 8) & 255u));
+        if (I.op != kTG1 && vt.size() == 1)
+            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "superoperator program");
+        const uint64_t DA = uint64_t(1) << vt.size();
+        A.resize(DA * DA);
+        for (uint64_t j = 0; j < DA * DA; ++j)
+            A[j] = cd(P.mats[2 * (I.mat + j)], P.mats[2 * (I.mat + j) + 1]);
+        vapply(s, vs, vt, {}, A.data(), DA);
+    }
+}
+
 void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_t count) {
     for (const Step& st : c->steps)
         if (st.kind == StepKind::CondIf)
@@ -286,10 +330,14 @@ void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_
             apply_step(s, c->steps[i]);
         return;
     }
-    if (s->kind != QGPU_KET || c->d != 2)
-        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
     if (first != 0 || count < c->steps.size())
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form runs whole circuits");
+    if (s->kind == QGPU_RHO) {
+        run_rho_fused(s, c);
+        return;
+    }
+    if (c->d != 2)
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
     uint32_t k = s->prec == QGPU_C64 ? 6 : 3;
     prepare_plan(s, c, k);
     VSpace vs = vspace_ket(s->dims);

@@ -24,6 +24,7 @@
 namespace qgpu {
 
 using cd = std::complex<double>;
+struct TProgram;
 
 enum class StepKind {
     Gate,      // apply(U, target)           GType SINGLE/TWO/THREE/JOINT
@@ -80,6 +81,10 @@ struct qgpu_circuit {
     qgpu_ctx* plan_ctx = nullptr;
     float* dB = nullptr;
     std::vector<int64_t> block_slot; // plan index -> slot in dB, or -1
+    // fused density-matrix program (superoperator blocks), built for the
+    // first rho_steps steps (steps are only ever appended)
+    uint64_t rho_steps = ~uint64_t(0);
+    std::shared_ptr<qgpu::TProgram> rho_prog; // null: the form does not apply
     ~qgpu_circuit();
 };
 

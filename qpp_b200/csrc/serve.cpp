@@ -16,11 +16,15 @@
 //           of its HBM footprint against the budget) into the next launch;
 //   lane 1  kets of 15-20 qubits: the same kernel with each CTA on its own
 //           slot of global scratch (HBM), batched the same way;
-//   lane 2  everything else (larger density matrices, whose single run
-//           would occupy one CTA for seconds; kets above 20 qubits, whose
+//   lane 2  everything else, one request at a time: density matrices above
+//           7 qubits whose circuits are gates and channels only run in the
+//           fused superoperator form (qgpu_run_gates, QGPU_FORM_FUSED: a
+//           layer's gates and channel on one qubit pair are one 16 x 16 pass
+//           over the matrix; one CTA per matrix would take seconds); the rest
+//           (density matrices with measurements, kets above 20 qubits, whose
 //           one-at-a-time engine run keeps the state in L2 and beats an
-//           HBM-bound slot per shot; wider gates, classical control): the
-//           resident engine, one request at a time.
+//           HBM-bound slot per shot, wider gates, classical control) run on
+//           the resident engine.
 //   plain mode: every request on lane 2 in complex128, one at a time (the
 //           comparison form: one kernel launch per gate).
 //
@@ -56,6 +60,7 @@ struct Request {
     uint64_t shots = 1;
     uint64_t seed = 0;
     const TProgram* prog = nullptr; // compiled trajectory program, or null
+    bool fused_rho = false;         // a density matrix of gates and channels only
     Clock::time_point t_submit, t_done;
     bool done = false;
     qgpu_status status = QGPU_OK;
@@ -84,6 +89,7 @@ struct qgpu_server {
     uint64_t batches = 0, launched_traj = 0, engine_runs = 0;
     double busy_s = 0;
     std::unordered_map<const qgpu_circuit*, std::pair<bool, qgpu::TProgram>> progs, rho_progs;
+    std::unordered_map<const qgpu_circuit*, bool> rho_fused; // fused form applies
 };
 
 namespace qgpu {
@@ -92,10 +98,55 @@ namespace {
 void sample_diag(const std::vector<double>& diag, uint64_t shots, uint64_t seed,
                  uint64_t* out);
 
+// The shots of a density-matrix request: samples of the final diagonal
+// (one strided gather on the device, then the draws on the host).
+void sample_rho(qgpu_ctx* ctx, const qgpu_state* fin, Request* r) {
+    qgpu_state* dg = new_state(ctx, QGPU_KET, fin->prec, fin->dims, false);
+    struct DelD {
+        qgpu_state* s;
+        ~DelD() { free_state(s); }
+    } deld{dg};
+    SegPlan m{};
+    m.count = fin->D;
+    m.nseg = 1;
+    m.pow2 = 0;
+    m.size[0] = fin->D;
+    m.stride[0] = fin->D + 1;
+    launch_gather(ctx, fin->prec, fin->data, dg->data, m);
+    std::vector<double> h(2 * fin->D);
+    if (qgpu_state_download_c128(dg, h.data()) != QGPU_OK)
+        raise(QGPU_ERR_CUDA, "qgpu_server", "diagonal");
+    std::vector<double> d(fin->D);
+    for (uint64_t i = 0; i < fin->D; ++i) d[i] = h[2 * i];
+    sample_diag(d, r->shots, r->seed, r->samples.data());
+}
+
+// A density matrix of gates and channels only, in the fused superoperator
+// form in complex64 from |0...0><0...0| (no measurement, so its dits stay 0).
+void run_rho_fused(qgpu_ctx* ctx, Request* r) {
+    const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
+    r->dits.assign(r->shots * nc, 0);
+    r->samples.assign(r->shots, 0);
+    qgpu_state* st = new_state(ctx, QGPU_RHO, QGPU_C64,
+                               std::vector<uint64_t>(r->c->nq, r->c->d), true);
+    struct DelS {
+        qgpu_state* s;
+        ~DelS() { free_state(s); }
+    } dels{st};
+    static const float one[2] = {1.0f, 0.0f};
+    QG_CUDA(cudaMemcpyAsync(st->data, one, sizeof(one), cudaMemcpyHostToDevice, ctx->stream));
+    run_gates(st, r->c, 1, 0, r->c->steps.size());
+    sample_rho(ctx, st, r);
+}
+
 // Engine path: trajectories one shot at a time on the resident engine; a
 // density matrix evolves once (its noise is in the circuit's channels) and
 // the shots sample the final diagonal.
 void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec) {
+    if (r->fused_rho && prec == QGPU_C64) {
+        run_rho_fused(ctx, r);
+        return;
+    }
     const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
     r->dits.assign(r->shots * nc, 0);
     r->samples.assign(r->shots, 0);
@@ -133,25 +184,7 @@ void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec) {
             ~DelS() { qgpu_state_destroy(s); }
         } dels{fin};
         if (r->kind != QGPU_KET) {
-            // the diagonal once (a strided gather), then the shots on the host
-            qgpu_state* dg = new_state(ctx, QGPU_KET, fin->prec, fin->dims, false);
-            struct DelD {
-                qgpu_state* s;
-                ~DelD() { free_state(s); }
-            } deld{dg};
-            SegPlan m{};
-            m.count = fin->D;
-            m.nseg = 1;
-            m.pow2 = 0;
-            m.size[0] = fin->D;
-            m.stride[0] = fin->D + 1;
-            launch_gather(ctx, fin->prec, fin->data, dg->data, m);
-            std::vector<double> h(2 * fin->D);
-            if (qgpu_state_download_c128(dg, h.data()) != QGPU_OK)
-                raise(QGPU_ERR_CUDA, "qgpu_server", "diagonal");
-            std::vector<double> d(fin->D);
-            for (uint64_t i = 0; i < fin->D; ++i) d[i] = h[2 * i];
-            sample_diag(d, r->shots, r->seed, r->samples.data());
+            sample_rho(ctx, fin, r);
             for (uint64_t k = 0; k < r->shots; ++k)
                 for (uint32_t i = 0; i < nc; ++i) r->dits[k * nc + i] = uint32_t(dv[i]);
             continue;
@@ -442,7 +475,16 @@ qgpu_status qgpu_server_submit(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind, 
                     const uint32_t n = r->prog->n;
                     if (n <= uint32_t(qgpu::kTrajMaxQubits)) lane = 0;
                     else if (kind == QGPU_KET && n <= uint32_t(qgpu::kServeMaxSlotQubits)) lane = 1;
-                    else r->prog = nullptr; // one CTA per density matrix is too slow: engine
+                    else r->prog = nullptr; // one CTA per register is too slow
+                }
+                if (kind != QGPU_KET && !r->prog) {
+                    // fused superoperator passes on lane 2 when it compiles
+                    auto it = S->rho_fused.find(c);
+                    if (it == S->rho_fused.end()) {
+                        qgpu::TProgram P;
+                        it = S->rho_fused.emplace(c, qgpu::compile_traj_rho(c, P, 30)).first;
+                    }
+                    r->fused_rho = it->second;
                 }
             }
             S->lanes[lane].q.push_back(r);

@@ -164,7 +164,8 @@ bool compile_traj(const qgpu_circuit* c, TProgram& P);
 // A density-matrix run of `c` as a ket over 2n virtual qubits [column
 // digits, row digits]: 1-qubit gates and 1-qubit channels become 4 x 4
 // superoperators on (column t, row t); 2-qubit gates become U on the row
-// digits and conj(U) on the column digits. False for anything else.
-bool compile_traj_rho(const qgpu_circuit* c, TProgram& P);
+// digits and conj(U) on the column digits. False for anything else, and
+// above max_nv virtual qubits (at most 31: instruction bit masks are 32-bit).
+bool compile_traj_rho(const qgpu_circuit* c, TProgram& P, int max_nv = kTrajMaxGlobalQubits);
 
 } // namespace qgpu

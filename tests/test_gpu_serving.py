@@ -96,3 +96,33 @@ def test_plain_mode_serves_requests():
         assert lat > 0 and np.all(s < 2 ** r.n)
     assert srv.stats()["engine_runs"] == len(pool)
     srv.close()
+
+
+@pytest.mark.parametrize("n", [9, 12])
+def test_large_density_matrix_batched_matches_plain_mode(n):
+    """Density matrices above 7 qubits of gates and channels only run on the
+    engine lane in the fused superoperator form in complex64; their shots
+    (samples of the final diagonal, same seed) match the plain mode's
+    complex128 engine run in all but a boundary draw or two."""
+    from qpp_b200 import serving as sv
+    from qpp_b200.workloads import haar_unitary
+    rng = np.random.default_rng(900 + n)
+    c = sv.Circuit(n, 2, 1)
+    for layer in range(3):
+        for q in range(n):
+            c.gate(haar_unitary(rng, 2), [q])
+        perm = rng.permutation(n)
+        for i in range(n // 2):
+            a, b = int(perm[2 * i]), int(perm[2 * i + 1])
+            c.gate(haar_unitary(rng, 4), [a, b])
+            sv.c_channel(c, sv.pair_channel(), [a, b])
+    shots = 400
+    got = []
+    for mode in (sv.BATCHED, sv.PLAIN):
+        srv = sv.Server(0, mode=mode)
+        rid = srv.submit(c, sv.RHO, 0.0, shots, seed=42)
+        lat, s, d = srv.wait(rid, shots, 1)
+        srv.close()
+        assert np.all(s < 2 ** n) and np.all(d == 0)
+        got.append(s)
+    assert np.sum(got[0] == got[1]) >= shots - 2
