@@ -11,9 +11,11 @@
 // are all gates: cache-blocked tile passes at the tuned width, run
 // layer-synchronously on one more branch -- graph node k applies pass k of
 // every such register, all tiles in parallel, in place in the instances' own
-// states. Larger registers with measurements keep one CTA per instance. The
-// plain form loops over the instances with one kernel launch per gate
-// (qgpu_run_gates, QGPU_FORM_PLAIN).
+// states. Larger registers with measurements keep one CTA per instance.
+// Density matrices of 10-15 qubits run in their fused superoperator form
+// (qgpu_run_gates, QGPU_FORM_FUSED), their passes captured on up to eight
+// more branches. The plain form loops over the instances with one kernel
+// launch per gate (qgpu_run_gates, QGPU_FORM_PLAIN).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -31,6 +33,12 @@
 #include "traj.hpp"
 
 namespace qgpu {
+
+// Register bits (kets: qubits; density matrices: twice the qubits) from which
+// batched instances run in their fused form on graph branches, and the
+// number of those branches.
+constexpr int kBranchMinBits = 20;
+constexpr size_t kBranchStreams = 8;
 
 bool compile_traj_rho(const qgpu_circuit* c, TProgram& P, int max_nv) {
     const int nq = int(c->nq), nv = 2 * nq;
@@ -183,6 +191,60 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     (states[i]->kind == QGPU_KET ? qgpu::compile_traj(circuits[i], P)
                                                  : qgpu::compile_traj_rho(circuits[i], P));
         });
+        auto all_gates = [](const qgpu::TProgram& P) {
+            for (const auto& I : P.ins)
+                if (I.op != qgpu::kTG1 && I.op != qgpu::kTCG1 && I.op != qgpu::kTG2 &&
+                    I.op != qgpu::kTG3 && I.op != qgpu::kTG4)
+                    return false;
+            return true;
+        };
+        // Density matrices of at least kBranchMinBits virtual qubits (10-15
+        // qubits) run in their own fused form, one pass per superoperator
+        // block of <= 4 virtual qubits (a layer's gates and channels on one
+        // qubit pair in one pass), captured on parallel graph branches: a
+        // register that size fills the GPU by itself, and there the layer
+        // kernel's 4 x 4 superoperators ran at about a quarter of HBM
+        // bandwidth (175 density matrices of 10-11 qubits, depth 20: 443 ms
+        // layered, 147 ms on branches). Kets stay layered: on branches, their
+        // 6-qubit tensor-core form was no faster (545 vs 564 ms for 484 kets
+        // of 20-22 qubits) and costs tens of milliseconds of host planning per
+        // circuit; 4-qubit blocks ran at 363 ms but their 48,000 graph nodes
+        // took 170 ms more to capture and instantiate than that saved.
+        std::vector<uint32_t> branch;
+        std::vector<char> on_branch(n_inst, 0);
+        if (form == 1) {
+            std::vector<uint32_t> cand;
+            std::map<qgpu_circuit*, uint32_t> first_of; // one build per circuit
+            for (uint32_t i = 0; i < n_inst; ++i) {
+                const qgpu_state* s = states[i];
+                if (s->kind != QGPU_RHO || s->prec != QGPU_C64 || s->ctx != ctx ||
+                    circuits[i]->d != 2 || 2 * circuits[i]->nq < uint32_t(qgpu::kBranchMinBits))
+                    continue;
+                cand.push_back(i);
+                first_of.emplace(circuits[i], i);
+            }
+            std::vector<uint32_t> reps;
+            for (auto& kv : first_of) reps.push_back(kv.second);
+            std::vector<char> good(n_inst, 0);
+            pfor(reps.size(), [&](size_t k) {
+                try {
+                    qgpu::fused_prepare(states[reps[k]], circuits[reps[k]]);
+                    good[reps[k]] = 1;
+                } catch (const qgpu::Exc&) {
+                    // not expressible in the fused form: stays as compiled
+                }
+            });
+            for (uint32_t i : cand) {
+                if (!good[first_of.at(circuits[i])]) continue;
+                ok[i] = 0;
+                on_branch[i] = 1;
+                branch.push_back(i);
+            }
+            // largest registers first, so the longest chains start first
+            std::stable_sort(branch.begin(), branch.end(), [&](uint32_t a, uint32_t b) {
+                return states[a]->elems > states[b]->elems;
+            });
+        }
         // batch programs carry no noise: gates fuse into dense blocks of the
         // width tuned for each register size (timed serially on the GPU)
         std::map<uint32_t, int> width_of;
@@ -194,21 +256,14 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
         });
         for (uint32_t i = 0; i < n_inst; ++i) {
             if (ok[i]) prog.emplace_back(i, std::move(progs[i]));
-            else plain.push_back(i);
+            else if (!on_branch[i]) plain.push_back(i);
         }
-        if (!prog.empty()) {
+        if (!prog.empty() || !branch.empty()) {
             // Registers above shared-memory size whose programs are all gates
             // run layer-synchronously: every gate belongs to a tile pass of
             // the tuned width, and launch k runs pass k of every such
             // register, all tiles in parallel. Programs with measurements keep
             // one CTA per register (tile passes inside k_traj).
-            auto all_gates = [](const qgpu::TProgram& P) {
-                for (const auto& I : P.ins)
-                    if (I.op != qgpu::kTG1 && I.op != qgpu::kTCG1 && I.op != qgpu::kTG2 &&
-                        I.op != qgpu::kTG3 && I.op != qgpu::kTG4)
-                        return false;
-                return true;
-            };
             std::map<uint32_t, int> tile_of; // tuned serially (it times on the GPU)
             for (auto& pr : prog) {
                 const uint32_t n = pr.second.n;
@@ -352,14 +407,17 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             if (!pinst.empty())
                 QG_CUDA(cudaMemcpyAsync(dpass, pinst.data(), pinst.size() * sizeof(qgpu::PassInst),
                                         cudaMemcpyHostToDevice, ctx->stream));
-            int* dflag = launches.empty() ? nullptr : qgpu::ctx_error_flag(ctx);
+            int* dflag =
+                launches.empty() && branch.empty() ? nullptr : qgpu::ctx_error_flag(ctx);
+            uint64_t branch_kernels = 0;
             // one graph: a k_traj launch per register size on its own branch,
             // and the chain of layer launches on one more branch (all touch
             // disjoint states)
             qgpu::traj_prepare();
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
-            const size_t nbr = ranges.size() + (launches.empty() ? 0 : 1);
+            const size_t nbs = std::min<size_t>(branch.size(), qgpu::kBranchStreams);
+            const size_t nbr = ranges.size() + (launches.empty() ? 0 : 1) + nbs;
             std::vector<cudaStream_t> side(nbr, nullptr);
             std::vector<cudaEvent_t> ev(nbr + 1, nullptr);
             struct Rel {
@@ -386,6 +444,35 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     QG_CUDA(cudaEventRecord(ev[g + 1], side[g]));
                     QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
                     ++g;
+                }
+                if (nbs) {
+                    // each instance on the branch with the least work so far
+                    // (amplitudes x steps); the launchers issue on ctx->stream
+                    for (size_t j = 0; j < nbs; ++j)
+                        QG_CUDA(cudaStreamWaitEvent(side[g + j], ev[0], 0));
+                    std::vector<double> load(nbs, 0.0);
+                    const uint64_t l0 = ctx->launches.load();
+                    {
+                        struct Restore {
+                            qgpu_ctx* c;
+                            cudaStream_t s;
+                            ~Restore() { c->stream = s; }
+                        } restore{ctx, ctx->stream};
+                        for (uint32_t i : branch) {
+                            const size_t j = size_t(std::min_element(load.begin(), load.end()) -
+                                                    load.begin());
+                            load[j] += double(states[i]->elems) *
+                                       double(circuits[i]->steps.size());
+                            ctx->stream = side[g + j];
+                            qgpu::fused_launch(states[i], circuits[i]);
+                        }
+                    }
+                    branch_kernels = ctx->launches.load() - l0;
+                    for (size_t j = 0; j < nbs; ++j) {
+                        QG_CUDA(cudaEventRecord(ev[g + 1 + j], side[g + j]));
+                        QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1 + j], 0));
+                    }
+                    g += nbs;
                 }
                 for (const auto& rg : ranges) {
                     QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
@@ -430,9 +517,9 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             cudaGraphExecDestroy(exec);
             cudaGraphDestroy(graph);
             if (dflag && qgpu::fused_error(ctx))
-                raise(QGPU_ERR_TIMEOUT, W, "a bounded wait of the layer kernel gave up");
+                raise(QGPU_ERR_TIMEOUT, W, "a bounded wait of a batch kernel gave up");
             ctx->batch_ms[5] = ms_since(t_tear);
-            if (graph_kernels) *graph_kernels = ranges.size() + launches.size();
+            if (graph_kernels) *graph_kernels = ranges.size() + launches.size() + branch_kernels;
         }
         auto t_plain = clk::now();
         for (uint32_t i : plain) qgpu::run_gates(states[i], circuits[i], 0, 0, circuits[i]->steps.size());

@@ -288,7 +288,7 @@ static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
 // pair become a single 16 x 16 block, and every block is one in-place pass
 // over the matrix. Plain form: one pass per gate and per channel.
 // The program is built once per circuit (and again after steps are added).
-static void run_rho_fused(qgpu_state* s, qgpu_circuit* c) {
+static void rho_prepare(qgpu_state* s, qgpu_circuit* c) {
     if (c->rho_steps != c->steps.size()) {
         auto P = std::make_shared<TProgram>();
         if (compile_traj_rho(c, *P, 30)) fuse_blocks(*P, 4);
@@ -300,18 +300,20 @@ static void run_rho_fused(qgpu_state* s, qgpu_circuit* c) {
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
               "fused form of a density matrix needs complex64, qubits, at most 15 of them, and "
               "only gates and 1- or 2-qubit channels");
-    const TProgram& P = *c->rho_prog;
-    const VSpace vs = vspace_rho(s->dims);
+}
+
+void launch_program(qgpu_state* s, const TProgram& P) {
+    const VSpace vs = vspace_of(s);
     const int nv = int(P.n);
     std::vector<cd> A;
     for (const TInstr& I : P.ins) {
+        if (I.op != kTG1 && I.op != kTG2 && I.op != kTG3 && I.op != kTG4)
+            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "dense block program");
         std::vector<int> vt;
         vt.push_back(nv - 1 - I.b0);
-        if (I.op == kTG2 || I.op == kTG3 || I.op == kTG4) vt.push_back(nv - 1 - I.b1);
+        if (I.op != kTG1) vt.push_back(nv - 1 - I.b1);
         if (I.op == kTG3 || I.op == kTG4) vt.push_back(nv - 1 - int(I.cmask & 255u));
         if (I.op == kTG4) vt.push_back(nv - 1 - int((I.cmask >> 8) & 255u));
-        if (I.op != kTG1 && vt.size() == 1)
-            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "superoperator program");
         const uint64_t DA = uint64_t(1) << vt.size();
         A.resize(DA * DA);
         for (uint64_t j = 0; j < DA * DA; ++j)
@@ -320,26 +322,18 @@ static void run_rho_fused(qgpu_state* s, qgpu_circuit* c) {
     }
 }
 
-void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_t count) {
-    for (const Step& st : c->steps)
-        if (st.kind == StepKind::CondIf)
-            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
-                  "classical conditionals need an engine (qgpu_engine_execute)");
-    if (form == 0) {
-        for (uint64_t i = first; i < first + count && i < c->steps.size(); ++i)
-            apply_step(s, c->steps[i]);
-        return;
-    }
-    if (first != 0 || count < c->steps.size())
-        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form runs whole circuits");
-    if (s->kind == QGPU_RHO) {
-        run_rho_fused(s, c);
-        return;
-    }
+// Kets: qubits only; blocks of up to 6 qubits (complex64: 3-6 qubit blocks on
+// the tensor cores from 13 qubits on), 3 in complex128.
+void fused_prepare(qgpu_state* s, qgpu_circuit* c) {
+    if (s->kind == QGPU_RHO) return rho_prepare(s, c);
     if (c->d != 2)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
-    uint32_t k = s->prec == QGPU_C64 ? 6 : 3;
-    prepare_plan(s, c, k);
+    prepare_plan(s, c, s->prec == QGPU_C64 ? 6 : 3);
+    if (!c->block_slot.empty()) ctx_error_flag(s->ctx); // allocated outside any capture
+}
+
+void fused_launch(qgpu_state* s, qgpu_circuit* c) {
+    if (s->kind == QGPU_RHO) return launch_program(s, *c->rho_prog);
     VSpace vs = vspace_ket(s->dims);
     int nb = int(c->nq);
     for (size_t i = 0; i < c->plan.size(); ++i) {
@@ -357,7 +351,23 @@ void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_
         }
         vapply(s, vs, b.qubits, {}, b.U.data(), uint64_t(1) << b.qubits.size());
     }
-    if (!c->block_slot.empty() && fused_error(s->ctx))
+}
+
+void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_t count) {
+    for (const Step& st : c->steps)
+        if (st.kind == StepKind::CondIf)
+            raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
+                  "classical conditionals need an engine (qgpu_engine_execute)");
+    if (form == 0) {
+        for (uint64_t i = first; i < first + count && i < c->steps.size(); ++i)
+            apply_step(s, c->steps[i]);
+        return;
+    }
+    if (first != 0 || count < c->steps.size())
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form runs whole circuits");
+    fused_prepare(s, c);
+    fused_launch(s, c);
+    if (s->kind == QGPU_KET && !c->block_slot.empty() && fused_error(s->ctx))
         raise(QGPU_ERR_TIMEOUT, "qgpu_run_gates()", "tensor-core pass timed out");
 }
 

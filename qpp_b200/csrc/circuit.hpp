@@ -103,6 +103,18 @@ std::vector<Block> fuse(const std::vector<Step>& steps, uint32_t nq,
 // form 0 = plain (one pass per qpp call), form 1 = fused blocks.
 void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first,
                uint64_t count);
+// The fused form of a whole circuit in two parts, so that the launches can be
+// captured into a CUDA graph: fused_prepare does the host planning and the
+// one-time uploads (synchronous; raises QGPU_ERR_NOT_SUPPORTED where
+// run_gates' fused form would), fused_launch only enqueues kernels on
+// s->ctx->stream; the caller checks fused_error(ctx) once they have run.
+void fused_prepare(qgpu_state* s, qgpu_circuit* c);
+void fused_launch(qgpu_state* s, qgpu_circuit* c);
+// One pass per instruction of a program of dense blocks (G1-G4 only) on a
+// complex64 qubit state: bit b of the program is qubit n - 1 - b of a ket,
+// or virtual qubit 2n - 1 - b (column digits, then row digits) of a density
+// matrix. Launches only.
+void launch_program(qgpu_state* s, const TProgram& P);
 void apply_step(qgpu_state* s, const Step& st);
 
 } // namespace qgpu

@@ -341,6 +341,13 @@ static void smem(qgpu_ctx* ctx, void* data, const SegPlan& outer,
     if (DA > 4096)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_apply()",
               "gate dimension above 4096");
+    // the staging copy below reads a host vector that a graph would read
+    // only at its launch, after the vector is gone
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_apply()",
+              "gate dimension above 16 inside a stream capture");
     // staging: offsets then the matrix, in the context scratch
     size_t off_bytes = DA * sizeof(uint64_t);
     size_t a_off = (off_bytes + 255) / 256 * 256;

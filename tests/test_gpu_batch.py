@@ -114,3 +114,29 @@ def test_every_fusion_width_matches_plain_loop(ctx, w):
     finally:
         for n in sizes:
             qb.traj_fusion_width(ctx, n, -2)
+
+
+def test_large_registers_on_graph_branches_match_plain_loop(ctx):
+    """Density matrices of 10 and 12 qubits (20 and 24 virtual qubits) run in
+    their fused superoperator form on graph branches, beside kets of 11-21
+    qubits and smaller density matrices on the layered and shared-memory
+    paths, and agree with the plain per-instance loop within 2e-5 relative."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(2020)
+    spec = [("k", 20), ("k", 21), ("k", 16), ("k", 11), ("r", 10), ("r", 12), ("r", 8), ("r", 5)]
+    circuits, inputs = [], []
+    for kind, n in spec:
+        c, _ = layered(qb, rng, n, 2, kind == "r", pair=kind == "r")
+        circuits.append(c)
+        inputs.append(random_rho(rng, 2 ** n, 4) if kind == "r" else gaussian_ket(rng, 2 ** n))
+    a = [qb.State.from_numpy(ctx, x, [2] * int(np.log2(len(x))), qb.C64) for x in inputs]
+    b = [qb.State.from_numpy(ctx, x, [2] * int(np.log2(len(x))), qb.C64) for x in inputs]
+    kernels = qb.run_batch(ctx, circuits, a, qb.FUSED)
+    assert qb.batch_last_phases(ctx)["plain_ms"] < 50  # nothing fell back to the loop
+    qb.run_batch(ctx, circuits, b, qb.PLAIN)
+    assert kernels > 20  # the branch passes are graph kernels too
+    for i in range(len(circuits)):
+        ga, gb = a[i].numpy(), b[i].numpy()
+        assert np.max(np.abs(ga - gb)) / np.max(np.abs(gb)) < 2e-5, spec[i]
+    for s in a + b:
+        s.free()
