@@ -12,10 +12,12 @@
 // layer-synchronously on one more branch -- graph node k applies pass k of
 // every such register, all tiles in parallel, in place in the instances' own
 // states. Larger registers with measurements keep one CTA per instance.
-// Density matrices of 10-15 qubits run in their fused superoperator form
-// (qgpu_run_gates, QGPU_FORM_FUSED), their passes captured on up to eight
-// more branches. The plain form loops over the instances with one kernel
-// launch per gate (qgpu_run_gates, QGPU_FORM_PLAIN).
+// Registers of at least 2^18 amplitudes whose programs are all dense gates
+// (kets of 18-22 qubits, density matrices of 9-15 qubits) run block-layered
+// on one more branch instead: every program fused into blocks of <= 4
+// (virtual) qubits, launch j applies block j of every such register. The
+// plain form loops over the instances with one kernel launch per gate
+// (qgpu_run_gates, QGPU_FORM_PLAIN).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -35,10 +37,8 @@
 namespace qgpu {
 
 // Register bits (kets: qubits; density matrices: twice the qubits) from which
-// batched instances run in their fused form on graph branches, and the
-// number of those branches.
-constexpr int kBranchMinBits = 20;
-constexpr size_t kBranchStreams = 8;
+// batched instances run block-layered.
+constexpr int kBlockMinBits = 18;
 
 bool compile_traj_rho(const qgpu_circuit* c, TProgram& P, int max_nv) {
     const int nq = int(c->nq), nv = 2 * nq;
@@ -198,27 +198,26 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     return false;
             return true;
         };
-        // Density matrices of at least kBranchMinBits virtual qubits (10-15
-        // qubits) run in their own fused form, one pass per superoperator
-        // block of <= 4 virtual qubits (a layer's gates and channels on one
-        // qubit pair in one pass), captured on parallel graph branches: a
-        // register that size fills the GPU by itself, and there the layer
-        // kernel's 4 x 4 superoperators ran at about a quarter of HBM
-        // bandwidth (175 density matrices of 10-11 qubits, depth 20: 443 ms
-        // layered, 147 ms on branches). Kets stay layered: on branches, their
-        // 6-qubit tensor-core form was no faster (545 vs 564 ms for 484 kets
-        // of 20-22 qubits) and costs tens of milliseconds of host planning per
-        // circuit; 4-qubit blocks ran at 363 ms but their 48,000 graph nodes
-        // took 170 ms more to capture and instantiate than that saved.
-        std::vector<uint32_t> branch;
-        std::vector<char> on_branch(n_inst, 0);
+        // Block-layered registers (no reference counterpart): density matrices
+        // of at least kBlockMinBits virtual qubits (up to 15 qubits) and kets
+        // of at least kBlockMinBits qubits whose programs are dense gates. Each
+        // program is fused into blocks of <= 4 qubits (virtual qubits for a
+        // density matrix: a layer's gates and channels on one qubit pair
+        // become one block), and launch j of one chain applies block j of
+        // every such register, one HBM pass per block with one thread per
+        // group (k_block_batch). Above 2^18 amplitudes this beats the layered
+        // tile passes, whose per-gate barriers held them to about a quarter of
+        // HBM bandwidth there.
+        std::vector<uint32_t> blocked;
+        std::vector<char> on_block(n_inst, 0);
+        std::vector<qgpu::TProgram> bprog(n_inst); // kets' block programs
         if (form == 1) {
             std::vector<uint32_t> cand;
             std::map<qgpu_circuit*, uint32_t> first_of; // one build per circuit
             for (uint32_t i = 0; i < n_inst; ++i) {
                 const qgpu_state* s = states[i];
                 if (s->kind != QGPU_RHO || s->prec != QGPU_C64 || s->ctx != ctx ||
-                    circuits[i]->d != 2 || 2 * circuits[i]->nq < uint32_t(qgpu::kBranchMinBits))
+                    circuits[i]->d != 2 || 2 * circuits[i]->nq < uint32_t(qgpu::kBlockMinBits))
                     continue;
                 cand.push_back(i);
                 first_of.emplace(circuits[i], i);
@@ -237,13 +236,27 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             for (uint32_t i : cand) {
                 if (!good[first_of.at(circuits[i])]) continue;
                 ok[i] = 0;
-                on_branch[i] = 1;
-                branch.push_back(i);
+                on_block[i] = 1;
+                blocked.push_back(i);
             }
-            // largest registers first, so the longest chains start first
-            std::stable_sort(branch.begin(), branch.end(), [&](uint32_t a, uint32_t b) {
-                return states[a]->elems > states[b]->elems;
+            std::vector<uint32_t> kets;
+            for (uint32_t i = 0; i < n_inst; ++i) {
+                if (!ok[i] || states[i]->kind != QGPU_KET || states[i]->ctx != ctx ||
+                    progs[i].n < uint32_t(qgpu::kBlockMinBits) || !all_gates(progs[i]))
+                    continue;
+                bool dense = true;
+                for (const auto& I : progs[i].ins) dense = dense && I.op != qgpu::kTCG1;
+                if (dense) kets.push_back(i);
+            }
+            pfor(kets.size(), [&](size_t k) {
+                bprog[kets[k]] = std::move(progs[kets[k]]);
+                qgpu::fuse_blocks(bprog[kets[k]], 4);
             });
+            for (uint32_t i : kets) {
+                ok[i] = 0;
+                on_block[i] = 1;
+                blocked.push_back(i);
+            }
         }
         // batch programs carry no noise: gates fuse into dense blocks of the
         // width tuned for each register size (timed serially on the GPU)
@@ -256,9 +269,9 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
         });
         for (uint32_t i = 0; i < n_inst; ++i) {
             if (ok[i]) prog.emplace_back(i, std::move(progs[i]));
-            else if (!on_branch[i]) plain.push_back(i);
+            else if (!on_block[i]) plain.push_back(i);
         }
-        if (!prog.empty() || !branch.empty()) {
+        if (!prog.empty() || !blocked.empty()) {
             // Registers above shared-memory size whose programs are all gates
             // run layer-synchronously: every gate belongs to a tile pass of
             // the tuned width, and launch k runs pass k of every such
@@ -319,6 +332,67 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     }
                 kmax = std::max(kmax, passes[k].size());
             }
+            // block-layered registers: their programs' matrices (each program
+            // once, on a 16-byte boundary), then launch j's blocks
+            std::vector<float> bmats;
+            std::map<const qgpu::TProgram*, size_t> bbase; // float2 offset
+            std::vector<qgpu::BlockInst> binst;
+            std::vector<size_t> bmoff; // float2 offset of each block's matrix
+            std::vector<std::pair<size_t, std::pair<int, uint32_t>>> blaunch; // offset, (count, items)
+            {
+                std::vector<const qgpu::TProgram*> bp, uniq;
+                size_t jmax = 0, nfloat = 0;
+                for (uint32_t i : blocked) {
+                    const qgpu::TProgram* P =
+                        states[i]->kind == QGPU_KET ? &bprog[i] : circuits[i]->rho_prog.get();
+                    bp.push_back(P);
+                    jmax = std::max(jmax, P->ins.size());
+                    if (bbase.count(P)) continue;
+                    bbase[P] = nfloat / 2;
+                    uniq.push_back(P);
+                    nfloat += (P->mats.size() + 3) / 4 * 4; // next one 16-byte aligned
+                }
+                // one allocation, filled by host threads (about 200 MB for
+                // config 4's registers)
+                bmats.resize(nfloat);
+                pfor(uniq.size(), [&](size_t u) {
+                    const qgpu::TProgram* P = uniq[u];
+                    std::copy(P->mats.begin(), P->mats.end(), bmats.begin() + 2 * bbase.at(P));
+                });
+                for (size_t j = 0; j < jmax; ++j) {
+                    const size_t off = binst.size();
+                    uint32_t items = 0;
+                    for (size_t k = 0; k < blocked.size(); ++k) {
+                        const qgpu::TProgram& P = *bp[k];
+                        if (j >= P.ins.size()) continue;
+                        const qgpu::TInstr& I = P.ins[j];
+                        qgpu::BlockInst B{};
+                        B.k = I.op == qgpu::kTG1 ? 1 : I.op == qgpu::kTG2 ? 2
+                            : I.op == qgpu::kTG3 ? 3 : I.op == qgpu::kTG4 ? 4 : 0;
+                        if (!B.k) raise(QGPU_ERR_NOT_SUPPORTED, W, "block program");
+                        const uint8_t bits[4] = {I.b0, I.b1, uint8_t(I.cmask & 255u),
+                                                 uint8_t((I.cmask >> 8) & 255u)};
+                        uint32_t seen_bits = 0;
+                        for (int t = 0; t < B.k; ++t) {
+                            if (bits[t] >= P.n || (seen_bits >> bits[t] & 1u))
+                                raise(QGPU_ERR_NOT_SUPPORTED, W, "block bits");
+                            seen_bits |= 1u << bits[t];
+                            B.b[t] = bits[t];
+                        }
+                        const size_t moff = bbase.at(&P) + I.mat;
+                        if (moff % 2) raise(QGPU_ERR_NOT_SUPPORTED, W, "block matrix alignment");
+                        B.psi = static_cast<float2*>(states[blocked[k]]->data);
+                        if (reinterpret_cast<uintptr_t>(B.psi) % 16)
+                            raise(QGPU_ERR_INVALID_ARGUMENT, W, "state not 16-byte aligned");
+                        B.n = uint8_t(P.n);
+                        B.first_item = items;
+                        items += uint32_t(((uint64_t(1) << (P.n - B.k)) + 511) / 512);
+                        binst.push_back(B);
+                        bmoff.push_back(moff);
+                    }
+                    blaunch.push_back({off, {int(binst.size() - off), items}});
+                }
+            }
             auto al = [](size_t x) { return (x + 255) / 256 * 256; };
             size_t npass_total = 0;
             for (auto& v : passes) npass_total += v.size();
@@ -326,22 +400,31 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             size_t b_mat = std::max<size_t>(mats.size() * sizeof(float), 16);
             size_t b_work = std::max<size_t>(prog.size() * sizeof(qgpu::TWork), 16);
             size_t b_pass = std::max<size_t>(npass_total * sizeof(qgpu::PassInst), 16);
-            size_t b_out = prog.size() * (sizeof(uint64_t) + sizeof(uint32_t) * 8);
-            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_out);
+            // every region is taken on its own 256-byte boundary below
+            size_t b_samp = std::max<size_t>(prog.size() * sizeof(uint64_t), 16);
+            size_t b_dits = std::max<size_t>(prog.size() * sizeof(uint32_t) * 8, 16);
+            size_t b_bmat = std::max<size_t>(bmats.size() * sizeof(float), 16);
+            size_t b_binst = std::max<size_t>(binst.size() * sizeof(qgpu::BlockInst), 16);
+            size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_samp) +
+                           al(b_dits) + al(b_bmat) + al(b_binst);
             unsigned char* buf = nullptr;
             QG_CUDA(qgpu::ctx_malloc(ctx, reinterpret_cast<void**>(&buf), total));
             unsigned char* p = buf;
             auto take = [&](size_t b) {
                 unsigned char* q = p;
                 p += al(b);
+                if (size_t(p - buf) > total) raise(QGPU_ERR_CUDA, W, "batch buffer layout");
                 return q;
             };
             auto* dins = reinterpret_cast<qgpu::TInstr*>(take(b_ins));
             auto* dmat = reinterpret_cast<float2*>(take(b_mat));
             auto* dwork = reinterpret_cast<qgpu::TWork*>(take(b_work));
             auto* dpass = reinterpret_cast<qgpu::PassInst*>(take(b_pass));
-            auto* dsamp = reinterpret_cast<uint64_t*>(take(prog.size() * sizeof(uint64_t)));
-            auto* ddits = reinterpret_cast<uint32_t*>(take(prog.size() * sizeof(uint32_t) * 8));
+            auto* dsamp = reinterpret_cast<uint64_t*>(take(b_samp));
+            auto* ddits = reinterpret_cast<uint32_t*>(take(b_dits));
+            auto* dbmat = reinterpret_cast<float2*>(take(b_bmat));
+            auto* dbinst = reinterpret_cast<qgpu::BlockInst*>(take(b_binst));
+            for (size_t k = 0; k < binst.size(); ++k) binst[k].m = dbmat + bmoff[k];
             std::vector<qgpu::TWork> work;
             std::vector<std::pair<uint32_t, std::pair<size_t, size_t>>> ranges; // n -> [lo, hi)
             for (auto& kv : by_n) {
@@ -407,17 +490,20 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             if (!pinst.empty())
                 QG_CUDA(cudaMemcpyAsync(dpass, pinst.data(), pinst.size() * sizeof(qgpu::PassInst),
                                         cudaMemcpyHostToDevice, ctx->stream));
-            int* dflag =
-                launches.empty() && branch.empty() ? nullptr : qgpu::ctx_error_flag(ctx);
-            uint64_t branch_kernels = 0;
+            if (!binst.empty()) {
+                QG_CUDA(cudaMemcpyAsync(dbmat, bmats.data(), bmats.size() * sizeof(float),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+                QG_CUDA(cudaMemcpyAsync(dbinst, binst.data(), binst.size() * sizeof(qgpu::BlockInst),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+            }
+            int* dflag = launches.empty() ? nullptr : qgpu::ctx_error_flag(ctx);
             // one graph: a k_traj launch per register size on its own branch,
             // and the chain of layer launches on one more branch (all touch
             // disjoint states)
             qgpu::traj_prepare();
             cudaGraph_t graph = nullptr;
             cudaGraphExec_t exec = nullptr;
-            const size_t nbs = std::min<size_t>(branch.size(), qgpu::kBranchStreams);
-            const size_t nbr = ranges.size() + (launches.empty() ? 0 : 1) + nbs;
+            const size_t nbr = ranges.size() + (launches.empty() ? 0 : 1) + (blaunch.empty() ? 0 : 1);
             std::vector<cudaStream_t> side(nbr, nullptr);
             std::vector<cudaEvent_t> ev(nbr + 1, nullptr);
             struct Rel {
@@ -445,34 +531,14 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                     QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
                     ++g;
                 }
-                if (nbs) {
-                    // each instance on the branch with the least work so far
-                    // (amplitudes x steps); the launchers issue on ctx->stream
-                    for (size_t j = 0; j < nbs; ++j)
-                        QG_CUDA(cudaStreamWaitEvent(side[g + j], ev[0], 0));
-                    std::vector<double> load(nbs, 0.0);
-                    const uint64_t l0 = ctx->launches.load();
-                    {
-                        struct Restore {
-                            qgpu_ctx* c;
-                            cudaStream_t s;
-                            ~Restore() { c->stream = s; }
-                        } restore{ctx, ctx->stream};
-                        for (uint32_t i : branch) {
-                            const size_t j = size_t(std::min_element(load.begin(), load.end()) -
-                                                    load.begin());
-                            load[j] += double(states[i]->elems) *
-                                       double(circuits[i]->steps.size());
-                            ctx->stream = side[g + j];
-                            qgpu::fused_launch(states[i], circuits[i]);
-                        }
-                    }
-                    branch_kernels = ctx->launches.load() - l0;
-                    for (size_t j = 0; j < nbs; ++j) {
-                        QG_CUDA(cudaEventRecord(ev[g + 1 + j], side[g + j]));
-                        QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1 + j], 0));
-                    }
-                    g += nbs;
+                if (!blaunch.empty()) {
+                    QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
+                    for (auto& L : blaunch)
+                        qgpu::launch_block_batch(ctx, dbinst + L.first, L.second.first,
+                                                 L.second.second, side[g]);
+                    QG_CUDA(cudaEventRecord(ev[g + 1], side[g]));
+                    QG_CUDA(cudaStreamWaitEvent(ctx->stream, ev[g + 1], 0));
+                    ++g;
                 }
                 for (const auto& rg : ranges) {
                     QG_CUDA(cudaStreamWaitEvent(side[g], ev[0], 0));
@@ -519,7 +585,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             if (dflag && qgpu::fused_error(ctx))
                 raise(QGPU_ERR_TIMEOUT, W, "a bounded wait of a batch kernel gave up");
             ctx->batch_ms[5] = ms_since(t_tear);
-            if (graph_kernels) *graph_kernels = ranges.size() + launches.size() + branch_kernels;
+            if (graph_kernels) *graph_kernels = ranges.size() + launches.size() + blaunch.size();
         }
         auto t_plain = clk::now();
         for (uint32_t i : plain) qgpu::run_gates(states[i], circuits[i], 0, 0, circuits[i]->steps.size());

@@ -720,6 +720,121 @@ void launch_pass_batch(qgpu_ctx* ctx, const PassInst* dinsts, int ninst, uint32_
     after_launch(ctx, "k_pass_batch");
 }
 
+// Block-layered launches (no reference counterpart): each thread takes two
+// groups of 2^K amplitudes of one block (g0 and g0 + 256) at once (both loaded before any
+// arithmetic, so twice the loads are in flight), keeps all inputs in
+// registers before the in-place writes, and computes rows in pairs, so that
+// each matrix load is one float4 (entries (row, c) and (row + 1, c) are
+// adjacent in column-major order) feeding both groups. No barriers: a group
+// belongs to one thread, and a launch holds at most one block per register.
+template <int K>
+__device__ __forceinline__ void block_groups(const BlockInst& B, uint32_t g0, bool two) {
+    constexpr int D = 1 << K;
+    int sb[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) sb[j] = B.b[j];
+#pragma unroll
+    for (int x = 0; x < K - 1; ++x)
+#pragma unroll
+        for (int y = 0; y < K - 1 - x; ++y)
+            if (sb[y] > sb[y + 1]) {
+                const int t = sb[y];
+                sb[y] = sb[y + 1];
+                sb[y + 1] = t;
+            }
+    uint32_t i0 = g0, i1 = g0 + 256;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        i0 = ins0(i0, sb[j]);
+        i1 = ins0(i1, sb[j]);
+    }
+    uint32_t o[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) o[j] = 1u << B.b[j];
+    auto off = [&](int r) {
+        uint32_t x = 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) x += ((r >> (K - 1 - j)) & 1) ? o[j] : 0u;
+        return x;
+    };
+    float2* psi = B.psi;
+    if (!two) i1 = i0; // the second group repeats the first; only one is written
+    float2 v[D], w[D];
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        v[c] = psi[i0 + off(c)];
+        w[c] = psi[i1 + off(c)];
+    }
+    const float4* m4 = reinterpret_cast<const float4*>(B.m);
+#pragma unroll(K == 4 ? 1 : D / 2)
+    for (int row = 0; row < D; row += 2) {
+        float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            const float4 e = m4[(row + D * c) >> 1];
+            const float2 e0 = make_float2(e.x, e.y), e1 = make_float2(e.z, e.w);
+            a0 = c_fma(e0, v[c], a0);
+            a1 = c_fma(e1, v[c], a1);
+            b0 = c_fma(e0, w[c], b0);
+            b1 = c_fma(e1, w[c], b1);
+        }
+        psi[i0 + off(row)] = a0;
+        psi[i0 + off(row + 1)] = a1;
+        if (two) {
+            psi[i1 + off(row)] = b0;
+            psi[i1 + off(row + 1)] = b1;
+        }
+    }
+}
+
+// Items of 512 groups (thread t takes groups t and t + 256 of the item); the
+// blocks' first items sit in shared memory (up to kBlockSmemInsts of them),
+// so that finding an item's block is a short search there rather than a
+// chain of dependent global loads.
+constexpr int kBlockSmemInsts = 4096;
+
+__global__ void __launch_bounds__(256, 2)
+    k_block_batch(const BlockInst* __restrict__ insts, int ninst, uint32_t nitems) {
+    __shared__ uint32_t first[kBlockSmemInsts];
+    const bool in_smem = ninst <= kBlockSmemInsts;
+    if (in_smem)
+        for (int j = threadIdx.x; j < ninst; j += blockDim.x) first[j] = insts[j].first_item;
+    __syncthreads();
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        int lo = 0, hi = ninst - 1; // last block with first_item <= it
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if ((in_smem ? first[mid] : insts[mid].first_item) <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        const BlockInst B = insts[lo];
+        const uint32_t ngroups = 1u << (B.n - B.k);
+        const uint32_t g = (it - B.first_item) * 512u + threadIdx.x;
+        if (g >= ngroups) continue;
+        const bool two = g + 256 < ngroups;
+        switch (B.k) {
+            case 1: block_groups<1>(B, g, two); break;
+            case 2: block_groups<2>(B, g, two); break;
+            case 3: block_groups<3>(B, g, two); break;
+            default: block_groups<4>(B, g, two); break;
+        }
+    }
+}
+
+void launch_block_batch(qgpu_ctx* ctx, const BlockInst* dinsts, int ninst, uint32_t nitems,
+                        cudaStream_t stream) {
+    if (ninst <= 0 || nitems == 0) return;
+    static int per_sm = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_block_batch, 256, 0));
+        per_sm = std::max(1, per_sm);
+    });
+    const uint32_t grid = std::min<uint32_t>(nitems, uint32_t(ctx->num_sms) * uint32_t(per_sm));
+    k_block_batch<<<grid, 256, 0, stream ? stream : ctx->stream>>>(dinsts, ninst, nitems);
+    after_launch(ctx, "k_block_batch");
+}
+
 void traj_prepare() {
     static std::once_flag once;
     std::call_once(once, [] {

@@ -23,6 +23,9 @@ uint32_t MatPool::add(const std::vector<cd>& U) {
     }
     auto it = seen.find(key);
     if (it != seen.end()) return it->second;
+    // every matrix starts on a 16-byte boundary (two complex64 entries), so
+    // that a kernel may read adjacent rows as one float4
+    while (P.mats.size() % 4) P.mats.push_back(0.f);
     const uint32_t off = uint32_t(P.mats.size() / 2);
     P.mats.insert(P.mats.end(), k, k + 2 * U.size());
     seen.emplace(std::move(key), off);

@@ -78,7 +78,8 @@ struct TProgram {
 
 // Appends complex64 copies of gate matrices to a program's pool, each
 // distinct matrix once (a layered circuit drawn from a gate bank stores the
-// bank, not one copy per gate); returns the float2 offset.
+// bank, not one copy per gate); returns the float2 offset, always even (the
+// matrix starts on a 16-byte boundary of the pool).
 struct MatPool {
     explicit MatPool(TProgram& p) : P(p) {}
     uint32_t add(const std::vector<std::complex<double>>& U);
@@ -148,6 +149,24 @@ struct PassInst {
 // error word).
 void launch_pass_batch(qgpu_ctx* ctx, const PassInst* dinsts, int ninst, uint32_t nitems,
                        int tile_bits, int* err, cudaStream_t stream);
+// One dense block of one register in a block-layered launch (no reference
+// counterpart): every group of 2^k amplitudes of the 2^n-amplitude register
+// at psi that differ only in bits b[0..k-1] (b[0] the most significant digit
+// of the block's index, 1 <= k <= 4) is replaced by m times it (column-major
+// 2^k x 2^k complex64, 16-byte aligned). Items [first_item, first_item +
+// ceil(2^(n-k) / 512)) of the launch are this block's, 512 groups each.
+struct BlockInst {
+    float2* psi;
+    const float2* m;
+    uint32_t first_item;
+    uint8_t n, k;
+    uint8_t b[4];
+    uint8_t pad[6];
+};
+// One launch over `ninst` blocks of distinct registers (sorted by
+// first_item, nitems items in total); one thread per group, in place.
+void launch_block_batch(qgpu_ctx* ctx, const BlockInst* dinsts, int ninst, uint32_t nitems,
+                        cudaStream_t stream);
 // The context's device error word (allocated on first use: call outside
 // stream capture), and whether a kernel set it (reading clears it).
 int* ctx_error_flag(qgpu_ctx* ctx);

@@ -116,11 +116,13 @@ def test_every_fusion_width_matches_plain_loop(ctx, w):
             qb.traj_fusion_width(ctx, n, -2)
 
 
-def test_large_registers_on_graph_branches_match_plain_loop(ctx):
-    """Density matrices of 10 and 12 qubits (20 and 24 virtual qubits) run in
-    their fused superoperator form on graph branches, beside kets of 11-21
-    qubits and smaller density matrices on the layered and shared-memory
-    paths, and agree with the plain per-instance loop within 2e-5 relative."""
+def test_block_layered_registers_match_plain_loop(ctx):
+    """Kets of 20-21 qubits and density matrices of 10 and 12 qubits (20 and
+    24 virtual qubits) run block-layered (programs fused into blocks of <= 4
+    (virtual) qubits, launch j applying block j of every such register),
+    beside a 16-qubit ket on the layered tile passes and small instances in
+    shared memory, and agree with the plain per-instance loop within 2e-5
+    relative."""
     import qpp_b200 as qb
     rng = np.random.default_rng(2020)
     spec = [("k", 20), ("k", 21), ("k", 16), ("k", 11), ("r", 10), ("r", 12), ("r", 8), ("r", 5)]
