@@ -354,8 +354,13 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
             s.free()
     res["graph_speedup_vs_plain_c64"] = res["c64_plain_loop"]["s"] / res["c64_graph"]["s"]
     res["accuracy_vs_plain_c128"] = _config4_accuracy(ctx, circs, states)
-    res["tile_widths"] = {n: traj_tile_width(ctx, n) for n in range(15, 23)}
-    res["fusion_widths"] = {n: traj_fusion_width(ctx, n) for n in range(10, 23)}
+    # the tuned widths of the register sizes that ran on the tuned paths:
+    # shared memory (10-14 bits) and layered tile passes (15-17); from 18
+    # bits (kets of 18-22 qubits, density matrices of 9-11) the batch runs
+    # block-layered at width 4, and the tuner is not consulted
+    res["tile_widths"] = {n: traj_tile_width(ctx, n) for n in range(15, 18)}
+    res["fusion_widths"] = {n: traj_fusion_width(ctx, n) for n in range(10, 18)}
+    res["block_layered"] = {"register_bits": "18-22", "block_qubits": 4}
     return res
 
 
