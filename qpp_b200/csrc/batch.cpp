@@ -334,7 +334,8 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             }
             // block-layered registers: their programs' matrices (each program
             // once, on a 16-byte boundary), then launch j's blocks
-            std::vector<float> bmats;
+            std::unique_ptr<float[]> bmats; // not zero-filled: every float is copied in
+            size_t nbfloat = 0;
             std::map<const qgpu::TProgram*, size_t> bbase; // float2 offset
             std::vector<qgpu::BlockInst> binst;
             std::vector<size_t> bmoff; // float2 offset of each block's matrix
@@ -354,10 +355,13 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 }
                 // one allocation, filled by host threads (about 200 MB for
                 // config 4's registers)
-                bmats.resize(nfloat);
+                nbfloat = nfloat;
+                bmats.reset(new float[std::max<size_t>(nfloat, 1)]);
                 pfor(uniq.size(), [&](size_t u) {
                     const qgpu::TProgram* P = uniq[u];
-                    std::copy(P->mats.begin(), P->mats.end(), bmats.begin() + 2 * bbase.at(P));
+                    float* dst = bmats.get() + 2 * bbase.at(P);
+                    std::copy(P->mats.begin(), P->mats.end(), dst);
+                    std::fill(dst + P->mats.size(), dst + (P->mats.size() + 3) / 4 * 4, 0.f);
                 });
                 for (size_t j = 0; j < jmax; ++j) {
                     const size_t off = binst.size();
@@ -403,7 +407,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             // every region is taken on its own 256-byte boundary below
             size_t b_samp = std::max<size_t>(prog.size() * sizeof(uint64_t), 16);
             size_t b_dits = std::max<size_t>(prog.size() * sizeof(uint32_t) * 8, 16);
-            size_t b_bmat = std::max<size_t>(bmats.size() * sizeof(float), 16);
+            size_t b_bmat = std::max<size_t>(nbfloat * sizeof(float), 16);
             size_t b_binst = std::max<size_t>(binst.size() * sizeof(qgpu::BlockInst), 16);
             size_t total = al(b_ins) + al(b_mat) + al(b_work) + al(b_pass) + al(b_samp) +
                            al(b_dits) + al(b_bmat) + al(b_binst);
@@ -491,7 +495,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
                 QG_CUDA(cudaMemcpyAsync(dpass, pinst.data(), pinst.size() * sizeof(qgpu::PassInst),
                                         cudaMemcpyHostToDevice, ctx->stream));
             if (!binst.empty()) {
-                QG_CUDA(cudaMemcpyAsync(dbmat, bmats.data(), bmats.size() * sizeof(float),
+                QG_CUDA(cudaMemcpyAsync(dbmat, bmats.get(), nbfloat * sizeof(float),
                                         cudaMemcpyHostToDevice, ctx->stream));
                 QG_CUDA(cudaMemcpyAsync(dbinst, binst.data(), binst.size() * sizeof(qgpu::BlockInst),
                                         cudaMemcpyHostToDevice, ctx->stream));

@@ -423,48 +423,18 @@ std::map<std::pair<int, int>, int> g_fuse_chosen; // (device, n) -> fusion width
 
 void fuse_blocks(TProgram& P, int w) {
     using C = std::complex<double>;
+    // plain complex products (std::complex's operator* also handles infinities
+    // and NaNs through a library call)
+    auto mul = [](C a, C b) {
+        return C(a.real() * b.real() - a.imag() * b.imag(), a.real() * b.imag() + a.imag() * b.real());
+    };
+    w = std::max(1, std::min(w, kFuseMaxWidth));
+    // a block of nb <= 4 bits: bits[0] is the most significant digit of its
+    // index; U column-major (2^nb x 2^nb)
     struct Blk {
-        std::vector<int> bits; // bits[0]: most significant digit of the index
-        std::vector<C> U;      // column-major
-    };
-    auto ld = [&](uint32_t off, int count) {
-        std::vector<C> m(static_cast<size_t>(count));
-        for (int i = 0; i < count; ++i)
-            m[size_t(i)] = C(P.mats[2 * (size_t(off) + i)], P.mats[2 * (size_t(off) + i) + 1]);
-        return m;
-    };
-    // G on `gb` as an operator on `ub` (gb a subset, the other digits of the
-    // row and column equal)
-    auto embed = [](const std::vector<C>& G, const std::vector<int>& gb, const std::vector<int>& ub) {
-        const int K = int(ub.size()), k = int(gb.size());
-        const uint32_t D = 1u << K;
-        std::vector<int> at(static_cast<size_t>(k)); // position of gb[j] in ub
-        uint32_t gmask = 0;
-        for (int j = 0; j < k; ++j) {
-            at[size_t(j)] = int(std::find(ub.begin(), ub.end(), gb[size_t(j)]) - ub.begin());
-            gmask |= 1u << (K - 1 - at[size_t(j)]);
-        }
-        auto proj = [&](uint32_t x) {
-            uint32_t r = 0;
-            for (int j = 0; j < k; ++j) r = (r << 1) | ((x >> (K - 1 - at[size_t(j)])) & 1u);
-            return r;
-        };
-        std::vector<C> E(size_t(D) * D, C(0.0));
-        for (uint32_t c = 0; c < D; ++c)
-            for (uint32_t r = 0; r < D; ++r)
-                if ((r & ~gmask) == (c & ~gmask))
-                    E[r + size_t(c) * D] = G[proj(r) + (size_t(proj(c)) << k)];
-        return E;
-    };
-    auto matmul = [](const std::vector<C>& A, const std::vector<C>& B, uint32_t D) {
-        std::vector<C> R(size_t(D) * D, C(0.0));
-        for (uint32_t c = 0; c < D; ++c)
-            for (uint32_t k = 0; k < D; ++k) {
-                const C b = B[k + size_t(c) * D];
-                if (b == C(0.0)) continue;
-                for (uint32_t r = 0; r < D; ++r) R[r + size_t(c) * D] += A[r + size_t(k) * D] * b;
-            }
-        return R;
+        int nb;
+        int bits[4];
+        C U[256];
     };
     MatPool pool(P);
     std::vector<TInstr> out;
@@ -472,75 +442,137 @@ void fuse_blocks(TProgram& P, int w) {
     std::vector<Blk> open; // acting on disjoint bits, so they commute
     auto emit = [&](const Blk& B) {
         TInstr I{};
-        const size_t k = B.bits.size();
-        I.op = k == 1 ? kTG1 : k == 2 ? kTG2 : k == 3 ? kTG3 : kTG4;
+        I.op = B.nb == 1 ? kTG1 : B.nb == 2 ? kTG2 : B.nb == 3 ? kTG3 : kTG4;
         I.b0 = uint8_t(B.bits[0]);
-        if (k >= 2) I.b1 = uint8_t(B.bits[1]);
-        if (k == 3) I.cmask = uint32_t(B.bits[2]);
-        if (k == 4) I.cmask = uint32_t(B.bits[2]) | (uint32_t(B.bits[3]) << 8);
-        I.mat = pool.add(B.U);
+        if (B.nb >= 2) I.b1 = uint8_t(B.bits[1]);
+        if (B.nb == 3) I.cmask = uint32_t(B.bits[2]);
+        if (B.nb == 4) I.cmask = uint32_t(B.bits[2]) | (uint32_t(B.bits[3]) << 8);
+        const size_t D = size_t(1) << B.nb;
+        I.mat = pool.add(std::vector<C>(B.U, B.U + D * D));
         out.push_back(I);
     };
-    auto flush = [&](uint32_t mask) {
-        std::vector<Blk> keep;
-        for (Blk& B : open) {
-            bool hit = false;
-            for (int b : B.bits) hit = hit || ((mask >> b) & 1u);
-            if (hit) emit(B);
-            else keep.push_back(std::move(B));
-        }
-        open.swap(keep);
+    auto bits_of = [](const Blk& B) {
+        uint32_t m = 0;
+        for (int t = 0; t < B.nb; ++t) m |= 1u << B.bits[t];
+        return m;
     };
+    // emit (in order) the open blocks that touch `mask`, keep the rest
+    auto flush = [&](uint32_t mask) {
+        size_t keep = 0;
+        for (size_t i = 0; i < open.size(); ++i) {
+            if (bits_of(open[i]) & mask) emit(open[i]);
+            else {
+                if (keep != i) open[keep] = open[i];
+                ++keep;
+            }
+        }
+        open.resize(keep);
+    };
+    Blk nb{};
     for (const TInstr& I : P.ins) {
-        std::vector<int> gb;
-        int dim = 0;
+        int gb[4], k = 0;
         switch (I.op) {
-            case kTG1: gb = {I.b0}; dim = 2; break;
-            case kTG2: gb = {I.b0, I.b1}; dim = 4; break;
-            case kTG3: gb = {I.b0, I.b1, int(I.cmask & 255u)}; dim = 8; break;
+            case kTG1: gb[0] = I.b0; k = 1; break;
+            case kTG2: gb[0] = I.b0; gb[1] = I.b1; k = 2; break;
+            case kTG3: gb[0] = I.b0; gb[1] = I.b1; gb[2] = int(I.cmask & 255u); k = 3; break;
             case kTG4:
-                gb = {I.b0, I.b1, int(I.cmask & 255u), int((I.cmask >> 8) & 255u)};
-                dim = 16;
+                gb[0] = I.b0;
+                gb[1] = I.b1;
+                gb[2] = int(I.cmask & 255u);
+                gb[3] = int((I.cmask >> 8) & 255u);
+                k = 4;
                 break;
             default: break;
         }
-        if (gb.empty()) { // not a dense gate: keep it, after the blocks it touches
+        if (!k) { // not a dense gate: keep it, after the blocks it touches
             flush(ins_bits(I) | (I.op == kTMeas ? (1u << I.b0) : 0u) |
                   (I.op == kTTile ? 0xffffffffu : 0u));
             out.push_back(I);
             continue;
         }
-        std::vector<C> G = ld(I.mat, dim * dim);
-        std::vector<int> ub = gb;
-        std::vector<size_t> touched;
+        uint32_t gmask = 0;
+        for (int t = 0; t < k; ++t) gmask |= 1u << gb[t];
+        // union of the gate's bits and the open blocks it touches: the gate's
+        // bits first, then each touched block's, in the blocks' order
+        int ub[32], nu = 0;
+        for (int t = 0; t < k; ++t) ub[nu++] = gb[t];
+        size_t touched[32];
+        int nt = 0;
         for (size_t bi = 0; bi < open.size(); ++bi) {
-            bool hit = false;
-            for (int b : open[bi].bits) hit = hit || std::find(gb.begin(), gb.end(), b) != gb.end();
-            if (!hit) continue;
-            touched.push_back(bi);
-            for (int b : open[bi].bits)
-                if (std::find(ub.begin(), ub.end(), b) == ub.end()) ub.push_back(b);
+            if (!(bits_of(open[bi]) & gmask)) continue;
+            touched[nt++] = bi;
+            for (int t = 0; t < open[bi].nb; ++t)
+                if (!((gmask >> open[bi].bits[t]) & 1u) &&
+                    std::find(ub, ub + nu, open[bi].bits[t]) == ub + nu)
+                    ub[nu++] = open[bi].bits[t];
         }
-        if (int(ub.size()) > w) {
-            uint32_t m = 0;
-            for (int b : gb) m |= 1u << b;
-            flush(m); // emit the touched blocks, then start over with G
-            ub = gb;
-            touched.clear();
-            if (int(gb.size()) > w) { // wider than the fusion width: as is
+        if (nu > w) {
+            flush(gmask); // emit the touched blocks, then start over with G
+            nu = k;
+            nt = 0;
+            if (k > w) { // wider than the fusion width: as is
                 out.push_back(I);
                 continue;
             }
         }
-        const uint32_t D = 1u << ub.size();
-        std::vector<C> M = embed(G, gb, ub);
-        for (size_t bi : touched) M = matmul(M, embed(open[bi].U, open[bi].bits, ub), D);
-        std::vector<Blk> keep;
-        for (size_t bi = 0; bi < open.size(); ++bi)
-            if (std::find(touched.begin(), touched.end(), bi) == touched.end())
-                keep.push_back(std::move(open[bi]));
-        open.swap(keep);
-        open.push_back(Blk{ub, std::move(M)});
+        // position of register bit b in the new block's index
+        int pos[32];
+        for (int t = 0; t < nu; ++t) pos[ub[t]] = nu - 1 - t;
+        const uint32_t D = 1u << nu;
+        // M = the touched blocks' Kronecker product on ub (identity on the
+        // gate's bits that no block held)
+        uint32_t idm = 0;
+        for (int t = 0; t < k; ++t) idm |= 1u << pos[gb[t]];
+        uint32_t proj[32][16];
+        for (int j = 0; j < nt; ++j) {
+            const Blk& B = open[touched[j]];
+            for (int t = 0; t < B.nb; ++t) idm &= ~(1u << pos[B.bits[t]]);
+            for (uint32_t r = 0; r < D; ++r) {
+                uint32_t x = 0;
+                for (int t = 0; t < B.nb; ++t) x |= ((r >> pos[B.bits[t]]) & 1u) << (B.nb - 1 - t);
+                proj[j][r] = x;
+            }
+        }
+        C* M = nb.U;
+        for (uint32_t c = 0; c < D; ++c)
+            for (uint32_t r = 0; r < D; ++r) {
+                C v = ((r ^ c) & idm) ? C(0.0) : C(1.0);
+                for (int j = 0; j < nt && v != C(0.0); ++j) {
+                    const Blk& B = open[touched[j]];
+                    v = mul(v, B.U[proj[j][r] + (size_t(proj[j][c]) << B.nb)]);
+                }
+                M[r + size_t(c) * D] = v;
+            }
+        // M <- G M: G acts on the row digits at the gate's positions
+        const uint32_t g = 1u << k;
+        C G[256];
+        for (uint32_t e = 0; e < g * g; ++e)
+            G[e] = C(P.mats[2 * (size_t(I.mat) + e)], P.mats[2 * (size_t(I.mat) + e) + 1]);
+        uint32_t spread[16];
+        for (uint32_t j = 0; j < g; ++j) {
+            uint32_t x = 0;
+            for (int t = 0; t < k; ++t) x |= ((j >> (k - 1 - t)) & 1u) << pos[gb[t]];
+            spread[j] = x;
+        }
+        uint32_t gpos = 0;
+        for (int t = 0; t < k; ++t) gpos |= 1u << pos[gb[t]];
+        C x[16];
+        for (uint32_t c = 0; c < D; ++c)
+            for (uint32_t r0 = 0; r0 < D; ++r0) {
+                if (r0 & gpos) continue;
+                C* col = M + size_t(c) * D;
+                for (uint32_t j = 0; j < g; ++j) x[j] = col[r0 | spread[j]];
+                for (uint32_t i = 0; i < g; ++i) {
+                    C acc = 0.0;
+                    for (uint32_t j = 0; j < g; ++j) acc += mul(G[i + j * g], x[j]);
+                    col[r0 | spread[i]] = acc;
+                }
+            }
+        nb.nb = nu;
+        for (int t = 0; t < nu; ++t) nb.bits[t] = ub[t];
+        // drop the touched blocks (ascending indices), add the new one
+        for (int j = nt - 1; j >= 0; --j) open.erase(open.begin() + std::ptrdiff_t(touched[j]));
+        open.push_back(nb);
     }
     flush(0xffffffffu);
     P.ins.swap(out);
