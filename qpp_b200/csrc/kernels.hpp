@@ -33,6 +33,12 @@ void launch_apply_generic(qgpu_ctx* ctx, qgpu_prec prec, void* data,
                           const std::vector<uint64_t>& off, const cd* A,
                           uint64_t DA);
 
+// Generic 16 x 16 that factors as A (x) B (both 4 x 4, column-major): the
+// group's element (i, j) at base(g) + off[4 i + j] becomes
+// sum A[i, i'] B[j, j'] x(i', j').
+void launch_apply_kron4(qgpu_ctx* ctx, qgpu_prec prec, void* data, const SegPlan& outer,
+                        const std::vector<uint64_t>& off, const cd* A, const cd* B);
+
 // --- subsystem kernels (kernels_subsys.cu) --------------------------------
 // out[o] = in[map(o)], o over map.count.
 // Tiled bit permutation (see kernels_subsys.cu): when every output digit's

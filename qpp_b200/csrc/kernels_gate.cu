@@ -155,6 +155,130 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// A 16 x 16 operator that is a Kronecker product A (x) B of two 4 x 4 ones
+// (a product channel's superoperator on two qubits): the group's element
+// (i, j) sits at base + off[4 i + j]; A acts on i, B on j, both from the
+// parameter bank. 128 complex MACs per group instead of 256.
+template <typename R>
+struct KronParams {
+    SegPlan outer;
+    uint64_t off[16];
+    Cplx<R> A[16], B[16]; // column-major
+};
+
+// Complex128: a group split over two adjacent lanes (h = lane & 1). Lane h
+// loads columns j = 2h, 2h + 1 (eight elements) and applies A along i; the
+// pair then trades through shuffles so that lane h holds rows i = 2h, 2h + 1,
+// applies B along j and stores them. Eight elements per lane instead of
+// sixteen keep the kernel at two or more CTAs per SM without spills.
+template <typename R>
+__device__ __forceinline__ Cplx<R> shfl_pair(Cplx<R> v) {
+    Cplx<R> r;
+    r.x = __shfl_xor_sync(0xffffffffu, v.x, 1);
+    r.y = __shfl_xor_sync(0xffffffffu, v.y, 1);
+    return r;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, 2)
+    k_reg_kron_pair(Cplx<R>* __restrict__ psi, const __grid_constant__ KronParams<R> p) {
+    using C = Cplx<R>;
+    const uint32_t h = threadIdx.x & 1u;
+    const uint64_t pairs = uint64_t(gridDim.x) * (blockDim.x / 2);
+    const uint64_t g_first = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 1;
+    // every lane runs the same number of iterations (the shuffles need the
+    // whole warp)
+    const uint64_t iters = (p.outer.count + pairs - 1) / pairs;
+    for (uint64_t it = 0; it < iters; ++it) {
+        const uint64_t g = g_first + it * pairs;
+        const bool valid = g < p.outer.count;
+        const uint64_t base = valid ? seg_offset(p.outer, g) : 0;
+        C v[4][2]; // v[i][jj]: element (i, 2h + jj)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj) {
+                const uint64_t o = h ? p.off[4 * i + 2 + jj] : p.off[4 * i + jj];
+                if (valid) v[i][jj] = psi[base + o];
+                else v[i][jj].x = v[i][jj].y = R(0);
+            }
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+            C w[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C acc = cmul(p.A[r], v[0][jj]);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) acc = cfma(p.A[r + 4 * c], v[c][jj], acc);
+                w[r] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[r][jj] = w[r];
+        }
+        // mine[ii][j]: element (2h + ii, j)
+        C mine[2][4];
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj) {
+                const C keep = h ? v[2 + ii][jj] : v[ii][jj]; // (2h + ii, 2h + jj)
+                const C send = h ? v[ii][jj] : v[2 + ii][jj]; // (2(1 - h) + ii, 2h + jj)
+                const C recv = shfl_pair<R>(send);            // (2h + ii, 2(1 - h) + jj)
+                mine[ii][jj] = h ? recv : keep;
+                mine[ii][2 + jj] = h ? keep : recv;
+            }
+        if (!valid) continue;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C acc = cmul(p.B[r], mine[ii][0]);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) acc = cfma(p.B[r + 4 * c], mine[ii][c], acc);
+                const uint64_t o = h ? p.off[4 * (2 + ii) + r] : p.off[4 * ii + r];
+                psi[base + o] = acc;
+            }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, 3)
+    k_reg_kron(Cplx<R>* __restrict__ psi, const __grid_constant__ KronParams<R> p) {
+    using C = Cplx<R>;
+    const uint64_t nth = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < p.outer.count;
+         g += nth) {
+        const uint64_t base = seg_offset(p.outer, g);
+        C v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = psi[base + p.off[e]];
+        // A along i for each j
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            C w[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C acc = cmul(p.A[r], v[j]);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) acc = cfma(p.A[r + 4 * c], v[4 * c + j], acc);
+                w[r] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[4 * r + j] = w[r];
+        }
+        // B along j for each i, stored
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C acc = cmul(p.B[r], v[4 * i]);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) acc = cfma(p.B[r + 4 * c], v[4 * i + c], acc);
+                psi[base + p.off[4 * i + r]] = acc;
+            }
+    }
+}
+
 // Output rows [P * DA / S, (P + 1) * DA / S) of one group, the matrix
 // entries taken as compile-time offsets into the parameter bank.
 template <typename R, int DA, int S, int P>
@@ -403,6 +527,46 @@ void launch_apply_generic(qgpu_ctx* ctx, qgpu_prec prec, void* data,
                           uint64_t DA) {
     if (prec == QGPU_C128) generic<double>(ctx, data, outer, off, A, DA);
     else generic<float>(ctx, data, outer, off, A, DA);
+}
+
+template <typename R>
+static void kron4(qgpu_ctx* ctx, void* data, const SegPlan& outer, const std::vector<uint64_t>& off,
+                  const cd* A, const cd* B) {
+    if (outer.count == 0) return;
+    KronParams<R> p;
+    p.outer = outer;
+    for (int i = 0; i < 16; ++i) {
+        p.off[i] = off[size_t(i)];
+        p.A[i] = cv<R>(A[i]);
+        p.B[i] = cv<R>(B[i]);
+    }
+    // one full wave: the resident CTAs per SM times the SMs
+    static int per_sm = [] {
+        int b = 0;
+        if constexpr (sizeof(R) == 8)
+            QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_reg_kron_pair<R>, 256, 0));
+        else
+            QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_reg_kron<R>, 256, 0));
+        return std::max(1, b);
+    }();
+    int blocks = grid_blocks(ctx, per_sm);
+    if constexpr (sizeof(R) == 8) {
+        uint64_t need = (outer.count + 127) / 128;
+        if (need < uint64_t(blocks)) blocks = int(std::max<uint64_t>(need, 1));
+        k_reg_kron_pair<R><<<blocks, 256, 0, ctx->stream>>>(static_cast<Cplx<R>*>(data), p);
+        after_launch(ctx, "k_reg_kron_pair");
+    } else {
+        uint64_t need = (outer.count + 255) / 256;
+        if (need < uint64_t(blocks)) blocks = int(std::max<uint64_t>(need, 1));
+        k_reg_kron<R><<<blocks, 256, 0, ctx->stream>>>(static_cast<Cplx<R>*>(data), p);
+        after_launch(ctx, "k_reg_kron");
+    }
+}
+
+void launch_apply_kron4(qgpu_ctx* ctx, qgpu_prec prec, void* data, const SegPlan& outer,
+                        const std::vector<uint64_t>& off, const cd* A, const cd* B) {
+    if (prec == QGPU_C128) kron4<double>(ctx, data, outer, off, A, B);
+    else kron4<float>(ctx, data, outer, off, A, B);
 }
 
 } // namespace qgpu
