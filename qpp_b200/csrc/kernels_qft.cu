@@ -122,7 +122,7 @@ __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
 // s = -1), and the offset / tile-index tables of the read and write orders
 // split into a low and a high half.
 template <typename R, bool QB>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 3)
+__global__ void __launch_bounds__(256, 2)
     k_qft_pass(const Cplx<R>* in, Cplx<R>* out, const __grid_constant__ QftPlan p,
                const Cplx<R>* __restrict__ Wg, const Cplx<R>* __restrict__ F) {
     using C = Cplx<R>;
@@ -337,7 +337,7 @@ static void qft_launch(qgpu_ctx* ctx, const void* in, void* out, const QftPlan& 
                        const void* W, const void* F) {
     using C = Cplx<R>;
     const size_t sm = qft_smem_bytes(p, sizeof(C));
-    uint64_t blocks = uint64_t(grid_blocks(ctx, sizeof(R) == 8 ? 2 : 3));
+    uint64_t blocks = uint64_t(grid_blocks(ctx, 2));
     if (p.ntiles < blocks) blocks = p.ntiles;
     if (p.d == 2) {
         if (sm > 48 * 1024)
