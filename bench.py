@@ -23,8 +23,18 @@ cpu_baseline = the CPU restatement of qpp's qubit kernels (oracle/, OpenMP on
           all host cores, qpp's copy-per-call semantics) on a bounded sample
           of the same gates on the same 2^30 ket.
 
+fused   = the precision form on the same depth-40 circuit from the same seeded
+          input (complex64, <= 6-qubit blocks on the tensor cores), with its
+          infidelity against the plain complex128 result.
+parity_30q = three gates of the circuit applied on the GPU to the seeded 2^30
+          ket, against the CPU restatement's result on the same input.
+configs = (one GPU, rank 0) the other workloads of the metric: the 20-qubit
+          ket gate sequence, the 12-qubit density-matrix subsystem ops, the
+          batched uneven instances and the serving loop against the plain
+          form on the same requests, each with its CPU sample or oracle check.
+
 --impl reference times that CPU restatement alone (qpp itself needs Eigen,
-absent here) on the same metric, one gate per step.
+absent here) on the same metric, one gate per step, in the circuit's 1q:2q mix.
 """
 from __future__ import annotations
 
@@ -58,16 +68,20 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-fused", action="store_true", help="skip the fused complex64 leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads (configs 1, 2, 4 and serving)")
+    ap.add_argument("--only-configs", default="",
+                    help="comma list of config1,config2,config4,serving to run (default all)")
     return ap.parse_args()
 
 
-def fused_leg(args, qb, torch, ctx, stream, psi, layers, n, rank, plain_ms, dist):
-    """The fused form on the same depth-40 circuit from the same input: gates
-    merged into <= 6-qubit blocks, each block one pass of a complex64 state on
-    the tensor cores (tcgen05 kind::tf32, split-TF32 products, FP32
-    accumulation). Reports its time, the speed-up over the plain complex128
-    circuit time, and the infidelity against the plain complex128 result
-    (when the timed plain run covered exactly the circuit)."""
+def fused_leg(args, qb, torch, ctx, stream, plain_result, layers, n, rank, plain_ms, dist):
+    """The fused form on the same depth-40 circuit from the same seeded input:
+    gates merged into <= 6-qubit blocks, each block one pass of a complex64
+    state on the tensor cores (tcgen05, split products, FP32 accumulation).
+    Reports its time, the speed-up over the plain complex128 circuit time, and
+    the infidelity against `plain_result` (the plain complex128 run of the
+    whole circuit from the same input), or None when that run was skipped."""
     circ = qb.Circuit(n)
     for lay in layers:
         for U, t in lay:
@@ -83,30 +97,36 @@ def fused_leg(args, qb, torch, ctx, stream, psi, layers, n, rank, plain_ms, dist
     if dist:
         dist.barrier()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches()
     a.record(stream)
     circ.run(f64, qb.FUSED)
     b.record(stream)
     torch.cuda.synchronize()
+    launches = ctx.launches() - l0
     f_ms = a.elapsed_time(b)
     if dist:
         t = torch.tensor([f_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         f_ms = float(t.item())
     plain_circuit_ms = plain_ms / args.steps * DEPTH
+    peak, peak_kind = peaks()
+    pass_gbps = passes * 2 * 8 * 2 ** n / (f_ms / 1e3) / 1e9
     out = {"form": "complex64 state, gates fused into <= 6-qubit blocks, 64x64 complex blocks on "
-                   "tcgen05 (kind::tf32, 3xTF32 split products, FP32 accumulation)",
-           "gates": sum(len(lay) for lay in layers), "passes": passes, "ms": f_ms,
-           "plain_c128_circuit_ms": plain_circuit_ms,
+                   "tcgen05 (split products, FP32 accumulation)",
+           "gates": sum(len(lay) for lay in layers), "passes": passes, "launches": launches,
+           "ms": f_ms, "plain_c128_circuit_ms": plain_circuit_ms,
            "speedup_vs_plain_c128": plain_circuit_ms / f_ms,
-           "pass_bytes": 2 * 8 * 2 ** n,
-           "pass_GBps": passes * 2 * 8 * 2 ** n / (f_ms / 1e3) / 1e9,
+           "pass_bytes": 2 * 8 * 2 ** n, "pass_GBps": pass_gbps,
+           "pass_frac_of_hbm": pass_gbps / peak, "peak_kind": peak_kind,
            "gate_GBps_c128_equivalent": sum(len(lay) for lay in layers) * wl_gate_bytes(n)
-           / (f_ms / 1e3) / 1e9}
-    if args.steps == DEPTH:
+           / (f_ms / 1e3) / 1e9,
+           "infidelity_vs_plain_c128": None}
+    if plain_result is not None:
         tmp = qb.State(ctx, qb.KET, [2] * n, qb.C128).convert_from(f64)
-        ov = psi.inner(tmp)
-        fid = abs(ov) ** 2 / (psi.norm2() * tmp.norm2())
-        out["infidelity_vs_plain_c128"] = 1.0 - fid
+        ov = plain_result.inner(tmp)
+        fid = abs(ov) ** 2 / (plain_result.norm2() * tmp.norm2())
+        out["infidelity_vs_plain_c128"] = max(0.0, 1.0 - fid)
+        out["infidelity_target"] = 1e-6
         tmp.free()
     f64.free()
     return out
@@ -188,21 +208,34 @@ def reduce_over_ranks(dist, ms_local, bytes_local, device=None):
 
 
 def cpu_sample_gates(layers, count):
-    """The first `count` gates of the circuit in layer order, taking 1q and
-    2q gates in the circuit's 2:1 ratio."""
-    ones = [g for g in layers[0] if len(g[1]) == 1]
-    twos = [g for g in layers[0] if len(g[1]) == 2]
+    """`count` gates of the circuit in layer order, taking 1q and 2q gates in
+    the circuit's 2:1 ratio (1q, 1q, 2q, 1q, 1q, 2q, ...)."""
+    ones = [g for lay in layers for g in lay if len(g[1]) == 1]
+    twos = [g for lay in layers for g in lay if len(g[1]) == 2]
     out = []
     while len(out) < count:
         k = len(out)
-        out.append(twos[k // 3] if k % 3 == 2 else ones[k - k // 3])
+        out.append(twos[(k // 3) % len(twos)] if k % 3 == 2 else ones[(k - k // 3) % len(ones)])
     return out
 
 
-def cpu_baseline(n, layers, n_gates):
+def host_ram_gib():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 2 ** 20
+    except Exception:
+        pass
+    return None
+
+
+def cpu_baseline(n, layers, n_gates, gpu_result=None):
     """Time the oracle's restatement of qpp's qubit kernels (apply.hpp:57-265:
     full copy of the state, then the OpenMP pair/quad sweep into a fresh
-    result) on `n_gates` gates of the circuit on a 2^n ket."""
+    result) on `n_gates` gates of the circuit on the seeded 2^n ket. With
+    `gpu_result` (the GPU's result of the same gates from the same seed, as a
+    complex128 host array), also returns the max-norm relative difference."""
     from oracle import oracle as orc
     import ctypes as ct
     L = orc.lib()
@@ -210,6 +243,7 @@ def cpu_baseline(n, layers, n_gates):
     psi = np.empty(D, dtype=np.complex128)
     L.oracle_fill_gaussian(psi.ctypes.data_as(ct.POINTER(ct.c_double)), ct.c_uint64(D),
                            ct.c_uint64(SEED))
+    psi /= np.sqrt(np.vdot(psi, psi).real)  # qgpu_state_fill_gaussian normalises
     dims = [2] * n
     gates = cpu_sample_gates(layers, n_gates)
     t_total, b_total = 0.0, 0
@@ -221,14 +255,152 @@ def cpu_baseline(n, layers, n_gates):
         psi = out
         del out
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": b_total / t_total / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{len(gates)} gates of layer 0 (1q:2q = 2:1) on the 2^{n} complex128 "
-                      f"ket, qpp copy-per-call semantics, {t_total:.2f} s"}
+    rec = {"value": b_total / t_total / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{len(gates)} gates of the circuit (1q:2q = 2:1) on the 2^{n} complex128 "
+                     f"ket, qpp copy-per-call semantics, {t_total:.2f} s"}
+    parity = None
+    if gpu_result is not None:
+        chunk = 1 << 24
+        num = den = 0.0
+        for s in range(0, D, chunk):
+            a, b = gpu_result[s:s + chunk], psi[s:s + chunk]
+            num = max(num, float(np.max(np.abs(a - b))))
+            den = max(den, float(np.max(np.abs(b))))
+        parity = {"gates": [[len(t), t] for U, t in gates], "max_rel_err": num / den,
+                  "tol": 1e-12, "ok": num / den < 1e-12,
+                  "check": f"GPU plain complex128 vs the CPU restatement, same seeded 2^{n} ket"}
+    return rec, parity
+
+
+def _config1(cb, orc, ct, ctx, torch, stream, peak, cores):
+    rec, seq, final = cb.config1(ctx, torch, stream, peak)
+    n = 20
+    D = 2 ** n
+    psi = np.empty(D, dtype=np.complex128)
+    orc.lib().oracle_fill_gaussian(psi.ctypes.data_as(ct.POINTER(ct.c_double)),
+                                   ct.c_uint64(D), ct.c_uint64(1))
+    psi /= np.sqrt(np.vdot(psi, psi).real)
+    tc = time.perf_counter()
+    cpu_s = None
+    for i, (U, c, t) in enumerate(seq):
+        psi = orc.applyCTRL(psi, U, c, t, [2] * n, path=1) if c else \
+            orc.apply(psi, U, t, [2] * n, path=1)
+        if i == 199:
+            cpu_s = time.perf_counter() - tc
+    cb_bytes = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq[:200])
+    rec["cpu_baseline"] = {"value": 200 / cpu_s, "unit": "gates/s", "GBps": cb_bytes / cpu_s / 1e9,
+                           "cores": cores, "kind": "port",
+                           "sample": "first 200 gates of the sequence, qpp's qubit kernels "
+                                     "restated (copy per call)"}
+    err = float(np.max(np.abs(final - psi)) / np.max(np.abs(psi)))
+    rec["parity"] = {"max_rel_err": err, "tol": 1e-12, "ok": err < 1e-12,
+                     "check": "all 1100 gates, circuit form vs the oracle, same seeded ket"}
+    return rec
+
+
+def _config2(cb, orc, ctx, torch, stream, peak, cores):
+    rec, chk = cb.config2(ctx, torch, stream, peak)
+    dims, x = chk["dims"], chk["rho"]
+    c = {}
+    tc = time.perf_counter()
+    pt = orc.ptrace(x, chk["ptrace_target"], dims)
+    c["ptrace_ms"] = (time.perf_counter() - tc) * 1e3
+    tc = time.perf_counter()
+    ptt = orc.ptranspose(x, chk["ptranspose_target"], dims)
+    c["ptranspose_ms"] = (time.perf_counter() - tc) * 1e3
+    tc = time.perf_counter()
+    sp = orc.syspermute(x, chk["perm"], dims)
+    c["syspermute_ms"] = (time.perf_counter() - tc) * 1e3
+    c.update({"cores": cores, "kind": "port",
+              "sample": "the last step's ptrace / ptranspose / syspermute on the 4096^2 "
+                        "matrix (the restated generic 16-operator channel takes minutes at "
+                        "this size and is left out)"})
+    rec["cpu_baseline"] = c
+    e_pt = float(np.max(np.abs(chk["ptrace"] - pt)) / np.max(np.abs(pt)))
+    par = {"ptrace_max_rel_err": e_pt, "ptrace_tol": 1e-12,
+           "ptranspose_bit_exact": bool(np.array_equal(chk["ptranspose"], ptt)),
+           "syspermute_bit_exact": bool(np.array_equal(chk["syspermute"], sp)),
+           "check": "the last step's outputs vs the oracle on the same input"}
+    par["ok"] = e_pt < 1e-12 and par["ptranspose_bit_exact"] and par["syspermute_bit_exact"]
+    rec["parity"] = par
+    return rec
+
+
+def _config4(cb, ctx, torch, stream):
+    rec = cb.config4(ctx, torch, stream)
+    rec["workload"] = ("2048 kets of 10-22 qubits and 512 density matrices of 6-11 qubits "
+                       "(rank 8, depolarising p=0.005 after every layer), each its own "
+                       "depth-20 layered circuit; complex64 graph vs per-instance launches")
+    return rec
+
+
+def _serving(sb, qb, ctx):
+    rec = sb.measure(device=ctx.device)
+    rec["accuracy"] = serving_accuracy(qb, ctx)
+    return rec
+
+
+def configs_leg(args, qb, torch, ctx, stream):
+    """The metric's other workloads on this GPU (rank 0, one GPU), each with
+    its CPU sample or oracle check (the oracle as the checker only)."""
+    from qpp_b200 import configs_bench as cb
+    from qpp_b200 import serve_bench as sb
+    from oracle import oracle as orc
+    import ctypes as ct
+    peak, peak_kind = peaks()
+    want = set(x for x in args.only_configs.split(",") if x) or \
+        {"config1", "config2", "config4", "serving"}
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    out = {"peak_GBps": peak, "peak_kind": peak_kind}
+    t_leg = time.perf_counter()
+    legs = {"config1": lambda: _config1(cb, orc, ct, ctx, torch, stream, peak, cores),
+            "config2": lambda: _config2(cb, orc, ctx, torch, stream, peak, cores),
+            "config4": lambda: _config4(cb, ctx, torch, stream),
+            "serving": lambda: _serving(sb, qb, ctx)}
+    for name in ("config1", "config2", "config4", "serving"):
+        if name not in want:
+            continue
+        t0 = time.perf_counter()
+        try:
+            rec = legs[name]()
+        except Exception as e:  # one failing leg must not lose the others
+            rec = {"error": f"{type(e).__name__}: {e}"}
+        rec["leg_s"] = time.perf_counter() - t0
+        print(f"[bench] {name}: {rec['leg_s']:.1f} s", file=sys.stderr, flush=True)
+        out[name] = rec
+    out["leg_s"] = time.perf_counter() - t_leg
+    return out
+
+
+def serving_accuracy(qb, ctx, requests=4, shots=2):
+    """Shots of the serving pool's shared-memory ket requests through the
+    trajectory kernel with their final states, noise events and outcomes
+    dumped, each replayed through the oracle in complex128 with the same
+    Paulis and forced outcomes (QNoisyEngine semantics): infidelity."""
+    from qpp_b200 import serving as sv
+    from tests.test_gpu_traj import replay, run_traj
+    pool = sv.request_pool(64, seed=2025)
+    small = [r for r in pool if r.kind == sv.KET and r.n <= 13][:requests]
+    infid = []
+    for k, r in enumerate(small):
+        _, dits, states, events = run_traj(qb, ctx, r.circuit, r.n, r.p, shots, seed=31 + k,
+                                           max_events=256)
+        for s in range(shots):
+            ref, _ = replay(r.steps, r.n, dits[s], events[s])
+            got = states[s]
+            f = abs(np.vdot(ref, got)) ** 2 / (np.vdot(ref, ref).real * np.vdot(got, got).real)
+            infid.append(max(0.0, 1.0 - f))
+    return {"shots": len(infid), "requests": len(small),
+            "qubits": sorted(int(r.n) for r in small), "max_infidelity": max(infid),
+            "median_infidelity": float(np.median(infid)), "target": 1e-6,
+            "check": "complex64 trajectories vs the oracle's complex128 replay of the same "
+                     "noise draws and outcomes"}
 
 
 def run_reference(args):
     """--impl reference: the CPU restatement (qpp needs Eigen, absent here)
-    on all host cores, one gate of the circuit per step."""
+    on all host cores, one gate of the circuit per step, the gates taken in
+    the circuit's 1q:2q = 2:1 mix."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -238,7 +410,7 @@ def run_reference(args):
     os.environ.setdefault("OMP_PROC_BIND", "close")
     n = args.qubits
     layers = wl.layered_circuit(n, DEPTH, SEED)
-    gates = [g for layer in layers for g in layer]
+    gates = cpu_sample_gates(layers, args.warmup + args.steps)
     L = orc.lib()
     D = 2 ** n
     psi = np.empty(D, dtype=np.complex128)
@@ -247,7 +419,7 @@ def run_reference(args):
     dims = [2] * n
     times = []
     for i in range(args.warmup + args.steps):
-        U, t = gates[i % len(gates)]
+        U, t = gates[i]
         t0 = time.perf_counter()
         psi = orc.apply(psi, U, t, dims, path=1)
         dt = time.perf_counter() - t0
@@ -262,10 +434,11 @@ def run_reference(args):
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": {"workload": f"{n}-qubit ket, layered depth-{DEPTH} circuit, plain complex128, "
-                               "one gate per step", "qubits": n, "depth": DEPTH},
+                               "one gate per step (1q:2q = 2:1)", "qubits": n, "depth": DEPTH},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"one gate of the layered circuit per step on the 2^{n} "
-                                   "complex128 ket (qpp restatement, Eigen unavailable)"},
+                         "sample": f"one gate of the layered circuit per step (1q, 1q, 2q, ...) "
+                                   f"on the 2^{n} complex128 ket (qpp restatement, Eigen "
+                                   "unavailable)"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -316,8 +489,6 @@ def main():
 
     for w in range(args.warmup):
         layer(w)
-    # timed steps start from the seeded input at layer 0, so steps == DEPTH
-    # runs exactly the depth-40 circuit (the fused form's reference)
     psi.fill_gaussian(SEED + rank)
     ctx.synchronize()
     if dist:
@@ -347,15 +518,15 @@ def main():
     ach2 = gbytes / (statistics.mean(d2) / 1e3) / 1e9
     norm_err = abs(psi.norm2() - 1.0)
 
-    fused = None
-    if not args.no_fused:
-        fused = fused_leg(args, qb, torch, ctx, stream, psi, layers, n, rank, ms, dist)
-
     e2e = None
+    host = None
     if not args.no_e2e:
-        # public ABI, host -> device -> depth-40 circuit -> host
+        # public ABI, host -> device -> depth-40 circuit -> host, from the
+        # seeded input, so that psi then holds the plain complex128 result of
+        # the whole circuit (the fused form's reference)
         host = torch.empty(2 * D, dtype=torch.float64, pin_memory=True)
         lib = qb.lib()
+        psi.fill_gaussian(SEED + rank)
         qb.check(lib.qgpu_state_download(psi.h, qb.vp(host.data_ptr())))
         e2e_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         if dist:
@@ -378,12 +549,36 @@ def main():
                "ms_per_step": e_ms,
                "step": f"one depth-{DEPTH} circuit ({e_gates} gates) from a pinned host ket: "
                        "qgpu_state_upload, qgpu_apply per gate, qgpu_state_download"}
-        del host
 
-    cpu = None
+    fused = None
+    if not args.no_fused:
+        fused = fused_leg(args, qb, torch, ctx, stream, None if args.no_e2e else psi, layers,
+                          n, rank, ms, dist)
+
+    cpu = parity = configs = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        # the GPU side of the 2^n parity check: three gates of the circuit
+        # (1q, 1q, 2q) on the seeded ket, result to the host
+        gpu_res = None
+        ram = host_ram_gib()
+        if ram is None or ram > 3.5 * 16 * D / 2 ** 30:
+            if host is None:
+                host = torch.empty(2 * D, dtype=torch.float64, pin_memory=True)
+            psi.fill_gaussian(SEED)
+            for U, t in cpu_sample_gates(layers, 3):
+                psi.apply(U, t)
+            qb.check(qb.lib().qgpu_state_download(psi.h, qb.vp(host.data_ptr())))
+            gpu_res = host.numpy().view(np.complex128)
         psi.free()
-        cpu = cpu_baseline(n, layers, n_gates=3)
+        cpu, parity = cpu_baseline(n, layers, 3, gpu_res)
+        if parity is None:
+            parity = {"skipped": f"host memory available {ram:.0f} GiB is below 3.5x the state"}
+        gpu_res = None
+    host = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        if psi.h:
+            psi.free()
+        configs = configs_leg(args, qb, torch, ctx, stream)
 
     if rank == 0:
         line = {
@@ -407,6 +602,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fused": fused,
+            "parity_30q": parity,
+            "configs": configs,
             "gpu_launches": launches,
             "clocks": clk,
             "check": {"norm_error_after_run": norm_err},

@@ -93,6 +93,15 @@ qgpu_status qgpu_ctx_mem_info(qgpu_ctx* ctx, uint64_t* free_bytes,
 uint64_t qgpu_ctx_launch_count(const qgpu_ctx* ctx);
 /* The cudaStream_t every op of this context is issued on, as void*. */
 void* qgpu_ctx_stream(qgpu_ctx* ctx);
+/* Bounded-wait controls of the fused tensor-core passes (no counterpart in
+ * Quantum++, which has no device waits). spin_limit: iterations of each wait
+ * for the tensor cores (0 restores the default, 2^26). stall_next != 0: the
+ * next fused pass on this context first waits on a barrier that nothing
+ * completes, so that wait runs out: the pass records the timeout, lets its
+ * own tensor-core work finish, frees its tensor memory and returns, and the
+ * call reports QGPU_ERR_TIMEOUT; the context stays usable. For tests of the
+ * timeout path; one-shot. */
+qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall_next);
 
 /* ---------------------------------------------------------------- states */
 /* Allocate a ket (D x 1) or density matrix (D x D) over `dims` in HBM,

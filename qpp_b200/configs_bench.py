@@ -19,10 +19,11 @@
            complex64, against the same circuit run gate by gate (one pass per
            qpp gate) on the GPU.
 
-Device times are CUDA events on the library's stream. The CPU figures time
-the oracle (the CPU restatement of qpp, all host cores) on a bounded sample
-of the same work; the oracle is test infrastructure and is imported only
-for these baseline samples.
+Device times are CUDA events on the library's stream. Everything here runs
+on the GPU through the library; the CPU baselines and the oracle checks of
+these configurations are bench.py's (the oracle is test infrastructure).
+Each function returns its JSON record and, where bench.py checks the result
+against the oracle, the inputs and outputs it needs.
 """
 from __future__ import annotations
 
@@ -45,9 +46,17 @@ def _events(torch, stream):
     return a, b
 
 
-def config1(ctx, torch, stream, cpu=True):
+def _frac(gbps, peak):
+    return None if not peak else gbps / peak
+
+
+def config1(ctx, torch, stream, peak=None):
+    """20-qubit Gaussian ket (seed 1), 1000 Haar gates + 100 applyCTRL, complex128.
+    Returns (record, sequence, final state of the circuit form as numpy)."""
     n = 20
     seq = ket_gate_sequence(n, seed=1)
+    D = 2 ** n
+    byts = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq)
     s = State(ctx, KET, [2] * n, C128).fill_gaussian(1)
     for U, c, t in seq[:50]:  # warm-up
         s.apply_ctrl(U, c, t) if c else s.apply(U, t)
@@ -58,40 +67,39 @@ def config1(ctx, torch, stream, cpu=True):
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
-    D = 2 ** n
-    byts = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq)
-    out = {"gates": len(seq), "ms": ms, "gates_per_s": len(seq) / (ms / 1e3),
-           "GBps": byts / (ms / 1e3) / 1e9, "form": "one Python call per gate",
-           "note": "16 MiB state stays in the 126 MB L2: bandwidth is L2, not HBM"}
+    out = {"workload": "20-qubit Gaussian ket (2^20 complex128, 16 MiB: L2-resident), 1000 Haar "
+                       "gates (70% 1-qubit, 30% 2-qubit) then 100 applyCTRL with 1-3 controls",
+           "gates": len(seq), "algorithmic_bytes": byts,
+           "per_call": {"ms": ms, "gates_per_s": len(seq) / (ms / 1e3),
+                        "GBps": byts / (ms / 1e3) / 1e9, "form": "one State.apply per gate"}}
     # the same gates as one circuit: one C call, the host loop in C++
     c = Circuit(n)
     for U, cs, t in seq:
         c.CTRL(U, cs, t) if cs else c.gate(U, t)
     c.run(s, PLAIN)  # warm-up
-    a, b = _events(torch, stream)
-    a.record(stream)
-    c.run(s, PLAIN)
-    b.record(stream)
-    torch.cuda.synchronize()
-    ms2 = a.elapsed_time(b)
-    out["circuit"] = {"ms": ms2, "gates_per_s": len(seq) / (ms2 / 1e3),
-                      "GBps": byts / (ms2 / 1e3) / 1e9, "form": "qgpu_run_gates, plain"}
-    if cpu:
-        from oracle import oracle as orc  # CPU baseline sample only
-        psi = s.numpy()
-        t0 = time.perf_counter()
-        for U, c, t in seq[:200]:
-            psi = orc.applyCTRL(psi, U, c, t, [2] * n, path=1) if c else \
-                orc.apply(psi, U, t, [2] * n, path=1)
-        cpu_s = time.perf_counter() - t0
-        cb = sum(2 * 16 * D // (2 ** len(c)) for U, c, t in seq[:200])
-        out["cpu"] = {"gates_per_s": 200 / cpu_s, "GBps": cb / cpu_s / 1e9,
-                      "cores": os.cpu_count(), "sample": "first 200 gates", "kind": "port"}
+    times = []
+    for _ in range(5):
+        s.fill_gaussian(1)
+        a, b = _events(torch, stream)
+        a.record(stream)
+        c.run(s, PLAIN)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ms2 = float(np.median(times))
+    gbps = byts / (ms2 / 1e3) / 1e9
+    out["circuit"] = {"ms": ms2, "gates_per_s": len(seq) / (ms2 / 1e3), "GBps": gbps,
+                      "form": "qgpu_run_gates, plain complex128", "runs": len(times)}
+    out["roofline"] = {"bound": "hbm", "achieved": gbps, "peak": peak, "unit": "GB/s",
+                       "frac": _frac(gbps, peak),
+                       "note": "algorithmic bytes over the measured HBM copy bandwidth; the "
+                               "16 MiB state stays in the 126 MB L2, so the fraction can exceed 1"}
+    final = s.numpy()
     s.free()
-    return out
+    return out, seq, final
 
 
-def qft(ctx, torch, stream, sizes=(20, 26, 30), cpu=True):
+def qft(ctx, torch, stream, sizes=(20, 26, 30)):
     """QCircuit::QFT / TFQ on every qubit, QEngine reset + execute per
     iteration (benchmarks/src/qft_bench.cpp, tfq_bench.cpp). The engine runs
     the QFT block as ceil(n / 8) shared-memory passes; the bytes per
@@ -137,15 +145,6 @@ def qft(ctx, torch, stream, sizes=(20, 26, 30), cpu=True):
                 del e
                 rows.append(row)
     out = {"rows": rows}
-    if cpu:
-        from oracle import oracle as orc  # CPU baseline sample only
-        n = 18
-        psi = np.zeros(2 ** n, dtype=np.complex128)
-        psi[0] = 1
-        t0 = time.perf_counter()
-        orc.QFT(psi)
-        out["cpu"] = {"n": n, "ms": (time.perf_counter() - t0) * 1e3, "cores": os.cpu_count(),
-                      "kind": "port", "sample": "qpp's QFT gate sequence on 18 qubits"}
     return out
 
 
@@ -156,7 +155,11 @@ def _inv(p):
     return q
 
 
-def config2(ctx, torch, stream, cpu=True, steps=200):
+def config2(ctx, torch, stream, peak=None, steps=200):
+    """12-qubit density matrix (rank 64), `steps` x {pair channel, ptrace(6),
+    ptranspose(6), syspermute}, complex128, plus the mixed-dimension variant.
+    Returns (record, check) where check holds the last step's input matrix, its
+    targets and the three subsystem results, for a comparison with the oracle."""
     from .serving import pair_channel
     rng = np.random.default_rng(2)
     n, D = 12, 4096
@@ -172,6 +175,7 @@ def config2(ctx, torch, stream, cpu=True, steps=200):
                      [int(x) for x in rng.choice(n, 6, replace=False)],
                      [int(x) for x in rng.permutation(n)]))
     t = {"channel": 0.0, "ptrace": 0.0, "ptranspose": 0.0, "syspermute": 0.0}
+    check = None
     for i, (pair, A, T, perm) in enumerate(plan):
         ev = [_events(torch, stream) for _ in range(4)]
         ev[0][0].record(stream)
@@ -190,39 +194,26 @@ def config2(ctx, torch, stream, cpu=True, steps=200):
         if i >= 2:  # first two steps are warm-up
             for k, key in enumerate(t):
                 t[key] += ev[k][0].elapsed_time(ev[k][1])
+        if i == len(plan) - 1:
+            check = {"dims": [2] * n, "rho": s.numpy(), "ptrace_target": A, "ptrace": r.numpy(),
+                     "ptranspose_target": T, "ptranspose": p.numpy(), "perm": perm,
+                     "syspermute": s2.numpy()}
         r.free()
         p.free()
         s.free()
         s = s2
     m = steps - 2
     full = 2 * 16 * D * D
-    out = {"steps": steps}
+    out = {"workload": "12-qubit density matrix (4096 x 4096 complex128, rank 64); per step a "
+                       "16-operator 2-qubit channel, ptrace over 6, ptranspose over 6, syspermute",
+           "steps": steps}
     for key, byts in (("channel", full), ("ptrace", 16 * 64 ** 3 + 16 * 64 * 64),
                       ("ptranspose", full), ("syspermute", full)):
         ms = t[key] / m
-        out[key] = {"ms": ms, "GBps": byts / (ms / 1e3) / 1e9, "bytes": byts}
-    trace_err = abs(s.trace() - 1)
-    out["trace_error_after"] = trace_err
-    if cpu:
-        from oracle import oracle as orc
-        x = s.numpy()
-        pair, A, T, perm = plan[0]
-        c = {}
-        t0 = time.perf_counter()
-        orc.ptrace(x, A, [2] * n)
-        c["ptrace_s"] = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        orc.ptranspose(x, T, [2] * n)
-        c["ptranspose_s"] = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        orc.syspermute(x, perm, [2] * n)
-        c["syspermute_s"] = time.perf_counter() - t0
-        c["sample"] = "one step of ptrace / ptranspose / syspermute on the 4096^2 matrix " \
-                      "(the 16-operator channel is left out: the restated generic loop " \
-                      "takes minutes at this size)"
-        c["kind"] = "port"
-        c["cores"] = os.cpu_count()
-        out["cpu"] = c
+        gbps = byts / (ms / 1e3) / 1e9
+        out[key] = {"ms": ms, "GBps": gbps, "bytes": byts, "frac": _frac(gbps, peak)}
+    out["ptrace"]["note"] = "64 x 64 output: latency-bound, not an HBM figure"
+    out["trace_error_after"] = abs(s.trace() - 1)
     s.free()
     # mixed dimensions
     dims = [3, 3, 2, 2, 3, 2, 2, 3]
@@ -252,7 +243,7 @@ def config2(ctx, torch, stream, cpu=True, steps=200):
     out["mixed_dims"] = {"dims": dims, "steps": 20, "ms_per_step": a.elapsed_time(b) / 20,
                          "trace_error_after": abs(sm.trace() - 1)}
     sm.free()
-    return out
+    return out, check
 
 
 def _layered(rng, n, depth, rho, bank1, bank2, chan):
@@ -295,7 +286,7 @@ def _config4_accuracy(ctx, circs, states):
             "compared": len(ket_inf) + len(rho_err)}
 
 
-def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20, cpu=True):
+def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20):
     from .serving import _depol
     rng = np.random.default_rng(4)
     bank1 = [haar_unitary(rng, 2) for _ in range(64)]
@@ -368,10 +359,11 @@ def main():
     import argparse
 
     import torch
-    ap = argparse.ArgumentParser(description="configs 1, 2 and 4 and the QFT benchmark on one GPU")
+    ap = argparse.ArgumentParser(description="configs 1, 2 and 4 and the QFT benchmark on one GPU "
+                                             "(GPU only; bench.py adds the CPU baselines)")
     ap.add_argument("--only", choices=["config1", "config2", "config4", "qft"], action="append",
                     help="run only these configs (repeatable)")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline samples")
+    ap.add_argument("--no-cpu", action="store_true", help="accepted for compatibility (no-op)")
     ap.add_argument("--steps", type=int, default=200, help="config 2 steps")
     ap.add_argument("--kets", type=int, default=2048, help="config 4 kets")
     ap.add_argument("--rho", type=int, default=512, help="config 4 density matrices")
@@ -380,16 +372,15 @@ def main():
                     help="QFT benchmark qubit counts (repeatable; default 20, 26, 30)")
     a = ap.parse_args()
     run = set(a.only or ["config1", "config2", "config4", "qft"])
-    cpu = not a.no_cpu
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream())
     out = {}
     if "config1" in run:
-        out["config1"] = config1(ctx, torch, stream, cpu)
+        out["config1"] = config1(ctx, torch, stream)[0]
     if "config2" in run:
-        out["config2"] = config2(ctx, torch, stream, cpu, steps=max(a.steps, 3))
+        out["config2"] = config2(ctx, torch, stream, steps=max(a.steps, 3))[0]
     if "qft" in run:
-        out["qft"] = qft(ctx, torch, stream, sizes=tuple(a.qft_n or (20, 26, 30)), cpu=cpu)
+        out["qft"] = qft(ctx, torch, stream, sizes=tuple(a.qft_n or (20, 26, 30)))
     if "config4" in run:
         out["config4"] = config4(ctx, torch, stream, n_kets=a.kets, n_rho=a.rho, depth=a.depth)
     print(json.dumps(out), flush=True)

@@ -15,6 +15,7 @@
 #include "internal.hpp"
 #include "kernels.hpp"
 #include "ops.hpp"
+#include "traj.hpp"
 
 using qgpu::cd;
 using qgpu::Exc;
@@ -475,6 +476,17 @@ uint64_t qgpu_ctx_launch_count(const qgpu_ctx* ctx) {
 }
 
 void* qgpu_ctx_stream(qgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall_next) {
+    return guard([&] {
+        check_handle(ctx);
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        ctx->wait_limit = spin_limit;
+        ctx->stall_next = stall_next != 0;
+        // allocated here, outside any stream capture, for the pass that reports
+        qgpu::ctx_error_flag(ctx);
+    });
+}
 
 // --------------------------------------------------------------- states
 qgpu_status qgpu_state_create(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,

@@ -8,6 +8,7 @@
 #include "circuit.hpp"
 #include "kernels.hpp"
 #include "ops.hpp"
+#include "traj.hpp"
 
 using qgpu::cd;
 using qgpu::guarded;
@@ -16,10 +17,7 @@ using qgpu::raise;
 using qgpu::vec_of;
 
 namespace qgpu {
-void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
-                      const float* dB);
 void fused6_matrix(const cd* U, float* B);
-int fused_error(qgpu_ctx* ctx);
 } // namespace qgpu
 
 namespace {
@@ -410,12 +408,15 @@ qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U, const uint64_t* target
         std::vector<cd> U6 = qgpu::embed(G, q, q6);
         std::vector<float> B(128 * 128);
         qgpu::fused6_matrix(U6.data(), B.data());
+        // |psi|^2 first: its block partials use the context scratch, which
+        // the block matrix takes over after them in stream order
+        const double* norm2 = qgpu::fused_norm_prepare(s->ctx, s->data, s->elems);
         float* dB = static_cast<float*>(qgpu::ctx_scratch(s->ctx, B.size() * sizeof(float)));
         QG_CUDA(cudaMemcpyAsync(dB, B.data(), B.size() * sizeof(float), cudaMemcpyHostToDevice,
                                 s->ctx->stream));
         int tb[6];
         for (int j = 0; j < 6; ++j) tb[j] = n - 1 - q6[size_t(j)];
-        qgpu::launch_fused6_tc(s->ctx, s->data, n, tb, dB);
+        qgpu::launch_fused6_tc(s->ctx, s->data, n, tb, dB, norm2);
         if (qgpu::fused_error(s->ctx))
             raise(QGPU_ERR_TIMEOUT, W, "tensor-core pass timed out");
     });

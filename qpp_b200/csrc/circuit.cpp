@@ -15,10 +15,7 @@ qgpu_circuit::~qgpu_circuit() {
 
 namespace qgpu {
 
-void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
-                      const float* dB);
 void fused6_matrix(const cd* U, float* B);
-int fused_error(qgpu_ctx* ctx);
 
 // E on block qubits bq (big-endian), with G acting on gq (subset of bq).
 std::vector<cd> embed(const std::vector<cd>& G, const std::vector<int>& gq,
@@ -336,6 +333,7 @@ void fused_launch(qgpu_state* s, qgpu_circuit* c) {
     if (s->kind == QGPU_RHO) return launch_program(s, *c->rho_prog);
     VSpace vs = vspace_ket(s->dims);
     int nb = int(c->nq);
+    const double* norm2 = nullptr; // |psi|^2 for the tensor-core passes' fp16 scale
     for (size_t i = 0; i < c->plan.size(); ++i) {
         const Block& b = c->plan[i];
         if (b.step >= 0) {
@@ -345,8 +343,9 @@ void fused_launch(qgpu_state* s, qgpu_circuit* c) {
         if (!c->block_slot.empty() && c->block_slot[i] >= 0) {
             int tb[6];
             for (int j = 0; j < 6; ++j) tb[j] = nb - 1 - b.qubits[size_t(j)];
+            if (!norm2) norm2 = fused_norm_prepare(s->ctx, s->data, s->elems);
             launch_fused6_tc(s->ctx, s->data, nb, tb,
-                             c->dB + size_t(c->block_slot[i]) * 128 * 128);
+                             c->dB + size_t(c->block_slot[i]) * 128 * 128, norm2);
             continue;
         }
         vapply(s, vs, b.qubits, {}, b.U.data(), uint64_t(1) << b.qubits.size());

@@ -25,8 +25,14 @@ struct qgpu_ctx {
     // Pinned host buffer for small device -> host results.
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
-    // Device word where kernels with bounded waits record a timeout.
+    // Device words: [0] where kernels with bounded waits record a timeout,
+    // [8] the squared norm read by the fused tensor-core passes.
     int* dev_flag = nullptr;
+    // Bounded-wait test hooks (qgpu_ctx_set_wait_test): the iteration limit
+    // of the fused kernel's waits (0 = the default), and a one-shot request
+    // that the next fused launch waits first on a barrier nothing completes.
+    uint32_t wait_limit = 0;
+    int stall_next = 0;
     // Stream-ordered pool of every device buffer the context allocates
     // (states, transform buffers, batch arenas): freed blocks stay reserved
     // up to a threshold, so repeated large allocations skip the driver's

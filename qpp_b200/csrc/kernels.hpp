@@ -129,6 +129,9 @@ void launch_qft_pass(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
 // sum |x|^2 over n elements, FP64 accumulation; result to *host_out.
 double reduce_norm2(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
                     uint64_t n);
+// The same sum left on the device at dev_out (stream order, no host wait).
+void reduce_norm2_device(qgpu_ctx* ctx, qgpu_prec prec, const void* data, uint64_t n,
+                         double* dev_out);
 // sum_i x[i * stride] (complex, FP64 accumulation): the trace for stride D+1.
 cd reduce_strided_sum(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
                       uint64_t n, uint64_t stride);

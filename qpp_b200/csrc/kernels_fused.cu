@@ -1,5 +1,5 @@
 // kernels_fused.cu -- fused 6-qubit gate blocks on the 5th-generation tensor
-// cores (tcgen05, kind::tf32) with split-TF32 (3xTF32) products and FP32
+// cores (tcgen05, kind::f16) with split-FP16 (3 x FP16) products and FP32
 // accumulation, for complex64 kets.
 //
 // No reference counterpart: Quantum++ applies one gate per pass
@@ -14,55 +14,80 @@
 //     D[g, n] = sum_k A[g, k] B[k, n],   n = 2 t + ro,
 //     B = [[Ur, Ui], [-Ui, Ur]] arranged so that D holds (re, im) pairs.
 // Tile: 128 consecutive groups (M = 128), K = 128, N = 128.
-//   A (state tile)  -> tensor memory, one TMEM lane per group, hi and lo
-//                      TF32 halves in columns [0,128) and [128,256);
-//   B (block matrix) -> shared memory, K-major, 128-byte swizzle, hi and lo;
-//   D (accumulator) -> tensor memory columns [256,384), FP32.
-// D = A_hi B_hi + A_hi B_lo + A_lo B_hi (the dropped A_lo B_lo term and the
-// TF32 rounding of the lo halves are ~2^-22 relative).
-// Each of the 16 warps owns one TMEM lane quarter (warp % 4) and one quarter
-// of the components (warp / 4): it loads 16 complex inputs per group, and
-// after the MMA reads back and stores the same 16 outputs, so a thread
-// writes exactly the addresses it read (in place, no staging).
+//
+// Split products. Every FP32 value x is written as hi + lo with hi = fp16(x)
+// and lo = fp16(x - hi), and D = A_hi B_hi + A_hi B_lo + A_lo B_hi with FP32
+// accumulation: 22 significant bits per operand, the same as the split-TF32
+// form, at twice the tensor-core rate of kind::tf32. FP16 has a narrow
+// exponent range, so the state is scaled by 2^eA with eA = 14 - ceil(log2
+// |psi|) (every |amplitude| * 2^eA < 2^14; typical amplitudes of a 30-qubit
+// state land near 2^-1, where both halves are normal numbers) and the block
+// matrix by 2^6; the epilogue multiplies by 2^-(eA + 6). All scales are
+// powers of two, so they are exact. |psi|^2 is an FP64 reduction on the
+// device before the first block of a run (no host round trip, so a run can
+// be captured in a CUDA graph).
+//
+// Layout per CTA (two CTAs per SM, 256 threads each):
+//   A (state tile)  -> tensor memory: one TMEM lane per group; column m of
+//                      [0, 64) holds amplitude m of the group as packed
+//                      (re, im) fp16 hi halves, columns [64, 128) the lo
+//                      halves;
+//   B (block matrix) -> shared memory, K-major, 128-byte swizzle, hi and lo
+//                      (2 x 32 KB);
+//   D (accumulator) -> tensor memory columns [128, 256), FP32.
+// 8 warps: warp w owns TMEM lane quarter w % 4 and half w / 4 of the 64
+// amplitudes of each group; a thread loads its 32 complex inputs (one
+// coalesced 256-byte row per warp and amplitude when the low state bits are
+// not targets), and after the MMA reads back and stores the same 32 outputs,
+// so every thread writes exactly the addresses it read (in place).
+// Pipeline per CTA: the loads of tile i+1 are in flight while MMA(i) runs;
+// the two co-resident CTAs of an SM interleave their load, MMA and epilogue
+// phases.
 //
 // Every wait is bounded: on timeout the kernel records an error code in
-// *err, skips the remaining tiles, frees its tensor memory and returns.
+// *err, waits (again bounded) for its own MMAs in flight, frees its tensor
+// memory and returns.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
+#include "traj.hpp"
 
 namespace qgpu {
 
 struct Fused6Params {
-    uint64_t ntiles;  // groups / 128
-    int tb_sorted[6]; // target bit positions, ascending
-    uint32_t off[64]; // element offset of block index m (big-endian over the block qubits)
-    const float* B;   // 128 x 128 fp32, B[n * 128 + k]
-    int* err;         // error flag (0 = ok)
+    uint64_t ntiles;       // groups / 128
+    int tb_sorted[6];      // target bit positions, ascending
+    uint32_t off[64];      // element offset of block index m (big-endian over the block qubits)
+    const float* B;        // 128 x 128 fp32, B[n * 128 + k]
+    const double* norm2;   // device word: |psi|^2 (sets the fp16 scale)
+    int* err;              // error flag (0 = ok)
+    uint32_t spin_limit;   // iterations of the MMA-completion wait
+    uint32_t stall_first;  // test hook: the first wait is on a barrier nothing completes
 };
 
 constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr int kF6Threads = 256;
+constexpr int kBScaleExp = 6;
+// 80 KB of dynamic shared memory (64 KB used): at most two CTAs per SM, so
+// the two 256-column tensor-memory allocations always fit.
+constexpr size_t kF6Smem = 80 * 1024;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-    uint32_t r;
-    asm volatile("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-
 // byte offset of B element (n, k) in a K-major, 128B-swizzled tile of
-// 128 rows (n) x 128 fp32 (k): four 32-element K atoms of 16 KB each.
-__device__ __forceinline__ uint32_t b_swz(int n, int k) {
-    int ka = k >> 5, kk = k & 31;
-    int chunk = (kk >> 2) ^ (n & 7);
-    return uint32_t(ka * 16384 + n * 128 + chunk * 16 + (kk & 3) * 4);
+// 128 rows (n) x 128 fp16 (k): two 64-element K atoms of 16 KB each.
+__device__ __forceinline__ uint32_t b_swz16(int n, int k) {
+    int ka = k >> 6, kk = k & 63;
+    int chunk = (kk >> 3) ^ (n & 7);
+    return uint32_t(ka * 16384 + n * 128 + chunk * 16 + (kk & 7) * 2);
 }
 
 __device__ __forceinline__ uint64_t b_desc(uint32_t saddr) {
@@ -75,29 +100,25 @@ __device__ __forceinline__ uint64_t b_desc(uint32_t saddr) {
     return d;
 }
 
-// kind::tf32, D fp32, A/B tf32, K-major, M = 128, N = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) |
-                            ((128u >> 4) << 24);
+// kind::f16, D fp32, A/B fp16, both K-major, M = 128, N = 128
+constexpr uint32_t kIdescF16 = (1u << 4) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b,
-                                            uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b,
+                                           uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %3, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %4, p;\n\t}\n" ::"r"(d_tmem),
-        "r"(a_tmem), "l"(b), "r"(accumulate), "r"(kIdesc));
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %4, p;\n\t}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b), "r"(accumulate), "r"(kIdescF16));
 }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16]) {
     asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, "
-        "%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, "
-        "%27, %28, %29, %30, %31, %32};\n" ::"r"(taddr),
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, "
+        "%10, %11, %12, %13, %14, %15, %16};\n" ::"r"(taddr),
         "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
         "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
-        "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]),
-        "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]),
-        "r"(v[29]), "r"(v[30]), "r"(v[31]));
+        "r"(v[15]));
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
@@ -114,8 +135,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "r"(taddr));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -128,10 +149,21 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
-__global__ void __launch_bounds__(512, 1)
+// (x0, x1) -> packed fp16 hi halves and packed fp16 residuals; x0 in the low
+// 16 bits (the even K element of the TMEM column).
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+    __half2 h = __floats2half2_rn(x0, x1);
+    float2 hf = __half22float2(h);
+    __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+    hi = *reinterpret_cast<uint32_t*>(&h);
+    lo = *reinterpret_cast<uint32_t*>(&l);
+}
+
+__global__ void __launch_bounds__(kF6Threads, 2)
     k_fused6_tc(float2* __restrict__ psi, const __grid_constant__ Fused6Params p) {
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t stall_bar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ int abort_sh;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -139,27 +171,41 @@ __global__ void __launch_bounds__(512, 1)
 
     unsigned char* Bh = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* Bl = Bh + 65536;
+    unsigned char* Bl = Bh + 32768;
 
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(
             smem_u32(&tmem_base_sh)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
         abort_sh = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&stall_bar)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    // block matrix -> shared memory, split into TF32 hi and lo
+    // scales from |psi|^2: |a| * 2^eA < 2^14 for every amplitude
+    int eA = 14;
+    {
+        const double n2 = p.norm2 ? *p.norm2 : 1.0;
+        if (n2 > 0.0 && n2 < 1e300) {
+            int e2;
+            frexp(n2, &e2); // n2 < 2^e2, so |psi| < 2^ceil(e2 / 2)
+            eA = 14 - ((e2 + 1) >> 1);
+        }
+        eA = max(-100, min(100, eA));
+    }
+    const float sa = __int_as_float((127 + eA) << 23);
+    const float inv = __int_as_float((127 - eA - kBScaleExp) << 23); // 2^-(eA + 6), normal
+    // block matrix -> shared memory, scaled by 2^6 and split into fp16 hi and lo
     for (int e = tid; e < 128 * 128; e += blockDim.x) {
         int n = e >> 7, k = e & 127;
-        float x = p.B[e];
-        uint32_t hi = to_tf32(x);
-        uint32_t lo = to_tf32(x - __uint_as_float(hi));
-        uint32_t a = b_swz(n, k);
-        *reinterpret_cast<uint32_t*>(Bh + a) = hi;
-        *reinterpret_cast<uint32_t*>(Bl + a) = lo;
+        float x = p.B[e] * float(1 << kBScaleExp);
+        __half hi = __float2half_rn(x);
+        __half lo = __float2half_rn(x - __half2float(hi));
+        uint32_t a = b_swz16(n, k);
+        *reinterpret_cast<__half*>(Bh + a) = hi;
+        *reinterpret_cast<__half*>(Bl + a) = lo;
     }
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -170,11 +216,8 @@ __global__ void __launch_bounds__(512, 1)
     const uint32_t mb = smem_u32(&mbar);
     const uint32_t bh_addr = smem_u32(Bh), bl_addr = smem_u32(Bl);
     uint32_t parity = 0;
+    bool stall = p.stall_first != 0;
 
-    // Software pipeline over this CTA's tiles (D double-buffered in TMEM
-    // columns [256,384) and [384,512)):
-    //   loads of tile i+1 are in flight while MMA(i) runs;
-    //   MMA(i+1) runs while tile i is read back from TMEM and stored.
     auto tile_base = [&](uint64_t tile) {
         uint64_t base = tile * 128 + uint64_t(quarter * 32 + lane);
 #pragma unroll
@@ -185,35 +228,37 @@ __global__ void __launch_bounds__(512, 1)
         }
         return base;
     };
-    auto load = [&](uint64_t base, float2 (&v)[16]) {
+    auto load = [&](uint64_t base, float2 (&v)[32]) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = psi[base + p.off[kpart * 16 + j]];
+        for (int j = 0; j < 32; ++j) v[j] = psi[base + p.off[kpart * 32 + j]];
     };
-    auto stage = [&](const float2 (&v)[16]) {
-        uint32_t hi[32], lo[32];
+    // A halves of this thread's 32 amplitudes -> TMEM columns kpart*32 + j
+    // (hi) and 64 + kpart*32 + j (lo)
+    auto stage = [&](const float2 (&v)[32]) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            hi[2 * j] = to_tf32(v[j].x);
-            lo[2 * j] = to_tf32(v[j].x - __uint_as_float(hi[2 * j]));
-            hi[2 * j + 1] = to_tf32(v[j].y);
-            lo[2 * j + 1] = to_tf32(v[j].y - __uint_as_float(hi[2 * j + 1]));
+        for (int c = 0; c < 2; ++c) {
+            uint32_t hi[16], lo[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                split2(v[c * 16 + j].x * sa, v[c * 16 + j].y * sa, hi[j], lo[j]);
+            const uint32_t col = uint32_t(kpart * 32 + c * 16);
+            tmem_st16(tbase + lane_off + col, hi);
+            tmem_st16(tbase + lane_off + 64u + col, lo);
         }
-        tmem_st32(tbase + lane_off + uint32_t(kpart * 32), hi);
-        tmem_st32(tbase + lane_off + 128u + uint32_t(kpart * 32), lo);
         asm volatile("tcgen05.wait::st.sync.aligned;");
         asm volatile("tcgen05.fence::before_thread_sync;");
     };
-    auto issue = [&](uint32_t dcol) { // after a __syncthreads
+    auto issue = [&]() { // after a __syncthreads
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t d = tbase + dcol;
+            const uint32_t d = tbase + 128u;
 #pragma unroll 1
-            for (int ks = 0; ks < 16; ++ks) {
+            for (int ks = 0; ks < 8; ++ks) {
                 uint32_t koff = uint32_t((ks >> 2) * 16384 + (ks & 3) * 32);
                 uint64_t dh = b_desc(bh_addr + koff), dl = b_desc(bl_addr + koff);
-                mma_tf32_ts(d, tbase + uint32_t(ks * 8), dh, ks > 0 ? 1u : 0u);
-                mma_tf32_ts(d, tbase + uint32_t(ks * 8), dl, 1u);
-                mma_tf32_ts(d, tbase + 128u + uint32_t(ks * 8), dh, 1u);
+                mma_f16_ts(d, tbase + uint32_t(ks * 8), dh, ks > 0 ? 1u : 0u);
+                mma_f16_ts(d, tbase + uint32_t(ks * 8), dl, 1u);
+                mma_f16_ts(d, tbase + 64u + uint32_t(ks * 8), dh, 1u);
             }
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -223,13 +268,12 @@ __global__ void __launch_bounds__(512, 1)
 
     uint64_t tile = blockIdx.x;
     if (tile < p.ntiles) {
-        float2 v[16];
+        float2 v[32];
         uint64_t base_cur = tile_base(tile);
         load(base_cur, v);
         stage(v);
         __syncthreads();
-        issue(256u);
-        uint32_t dsel = 0;
+        issue();
         for (;;) {
             const uint64_t next = tile + gridDim.x;
             const bool has_next = next < p.ntiles;
@@ -238,52 +282,60 @@ __global__ void __launch_bounds__(512, 1)
                 base_next = tile_base(next);
                 load(base_next, v);
             }
-            bool ok = mbar_wait(mb, parity);
+            bool ok = stall ? mbar_wait(smem_u32(&stall_bar), 0u, p.spin_limit)
+                            : mbar_wait(mb, parity, p.spin_limit);
             if (!ok && lane == 0) {
                 atomicExch(p.err, 1);
                 abort_sh = 1;
             }
             __syncthreads();
             if (abort_sh) {
-                // let MMAs still in flight drain (bounded) before freeing TMEM
-                if (tid == 0) mbar_wait(mb, parity);
+                // let the MMAs still in flight drain (bounded) before freeing TMEM
+                if (tid == 0) mbar_wait(mb, parity, kSpinLimit);
                 break;
             }
             parity ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;");
-            if (has_next) {
-                stage(v);
-                __syncthreads();
-                issue(256u + 128u * (dsel ^ 1u));
-            }
-            uint32_t dv[32];
-            tmem_ld32(tbase + lane_off + 256u + 128u * dsel + uint32_t(kpart * 32), dv);
-            asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-                psi[base_cur + p.off[kpart * 16 + j]] =
-                    make_float2(__uint_as_float(dv[2 * j]), __uint_as_float(dv[2 * j + 1]));
+            for (int c = 0; c < 2; ++c) {
+                uint32_t dv[32];
+                tmem_ld32(tbase + lane_off + 128u + uint32_t(kpart * 64 + c * 32), dv);
+                asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    psi[base_cur + p.off[kpart * 32 + c * 16 + j]] =
+                        make_float2(__uint_as_float(dv[2 * j]) * inv,
+                                    __uint_as_float(dv[2 * j + 1]) * inv);
+            }
             asm volatile("tcgen05.fence::before_thread_sync;");
             if (!has_next) break;
+            stage(v);
+            __syncthreads();
+            issue();
             tile = next;
             base_cur = base_next;
-            dsel ^= 1u;
         }
     }
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tbase));
     }
 }
 
 // ------------------------------------------------------------- launcher
+// Device words of the context: [0] the bounded-wait error flag, [8] the
+// squared norm read by the fused kernel.
 int* ctx_error_flag(qgpu_ctx* ctx) {
     if (!ctx->dev_flag) {
-        QG_CUDA(cudaMalloc(&ctx->dev_flag, sizeof(int)));
-        QG_CUDA(cudaMemset(ctx->dev_flag, 0, sizeof(int)));
+        QG_CUDA(cudaMalloc(&ctx->dev_flag, 64));
+        QG_CUDA(cudaMemset(ctx->dev_flag, 0, 64));
     }
     return ctx->dev_flag;
+}
+
+double* ctx_norm_slot(qgpu_ctx* ctx) {
+    return reinterpret_cast<double*>(reinterpret_cast<char*>(ctx_error_flag(ctx)) + 8);
 }
 
 // Builds B[n * 128 + k] from the 64 x 64 complex block U (column-major):
@@ -300,8 +352,16 @@ void fused6_matrix(const cd* U, float* B) {
         }
 }
 
+// |psi|^2 of the complex64 ket into the context's norm slot (stream order;
+// read by the fused passes that follow).
+const double* fused_norm_prepare(qgpu_ctx* ctx, const void* data, uint64_t n) {
+    double* slot = ctx_norm_slot(ctx);
+    reduce_norm2_device(ctx, QGPU_C64, data, n, slot);
+    return slot;
+}
+
 void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
-                      const float* dB) {
+                      const float* dB, const double* norm2) {
     if (nbits < 13)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu fused", "fused tensor-core blocks need n >= 13");
     Fused6Params p;
@@ -318,16 +378,25 @@ void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
         p.off[m] = o;
     }
     p.B = dB;
+    p.norm2 = norm2;
     p.err = ctx_error_flag(ctx);
-    size_t smem = 2 * 65536 + 1024;
-    static bool attr = false;
-    if (!attr) {
-        QG_CUDA(cudaFuncSetAttribute(k_fused6_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(smem)));
-        attr = true;
+    p.spin_limit = ctx->wait_limit ? ctx->wait_limit : kSpinLimit;
+    p.stall_first = ctx->stall_next ? 1u : 0u;
+    ctx->stall_next = 0;
+    // the shared-memory opt-in is a per-device attribute of the function
+    static std::mutex mu;
+    static bool attr_set[64] = {};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const int dev = ctx->device;
+        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+            QG_CUDA(cudaFuncSetAttribute(k_fused6_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(kF6Smem)));
+            if (dev >= 0 && dev < 64) attr_set[dev] = true;
+        }
     }
-    int grid = int(std::min<uint64_t>(p.ntiles, uint64_t(ctx->num_sms)));
-    k_fused6_tc<<<grid, 512, smem, ctx->stream>>>(static_cast<float2*>(data), p);
+    int grid = int(std::min<uint64_t>(p.ntiles, uint64_t(ctx->num_sms) * 2));
+    k_fused6_tc<<<grid, kF6Threads, kF6Smem, ctx->stream>>>(static_cast<float2*>(data), p);
     after_launch(ctx, "k_fused6_tc");
 }
 

@@ -357,6 +357,21 @@ double reduce_norm2(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
     return r;
 }
 
+void reduce_norm2_device(qgpu_ctx* ctx, qgpu_prec prec, const void* data, uint64_t n,
+                         double* dev_out) {
+    int nb = std::min(kRedBlocks, nblocks(ctx, n));
+    double* part = static_cast<double*>(ctx_scratch(ctx, nb * sizeof(double)));
+    if (prec == QGPU_C128)
+        k_norm2_partial<double><<<nb, kRedThreads, 0, ctx->stream>>>(
+            static_cast<const double2*>(data), n, part);
+    else
+        k_norm2_partial<float><<<nb, kRedThreads, 0, ctx->stream>>>(
+            static_cast<const float2*>(data), n, part);
+    after_launch(ctx, "k_norm2_partial");
+    k_sum_partials<<<1, kRedThreads, 0, ctx->stream>>>(part, nb, 1, dev_out);
+    after_launch(ctx, "k_sum_partials");
+}
+
 cd reduce_strided_sum(qgpu_ctx* ctx, qgpu_prec prec, const void* data,
                       uint64_t n, uint64_t stride) {
     int nb = std::min(kRedBlocks, nblocks(ctx, n));

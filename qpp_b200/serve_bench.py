@@ -65,6 +65,64 @@ def run(rates, duration, pool_size, plain_requests, seed=2025, device=0, max_per
     return out
 
 
+def sequential(server, pool, count, seed=1000):
+    """One request at a time: submit, wait, next. Latency = service time."""
+    t0 = time.perf_counter()
+    lat = []
+    for k, r in enumerate(pool[:count]):
+        rid = server.submit(r.circuit, r.kind, r.p, r.shots, seed + k)
+        lat.append(server.wait(rid)[0])
+    return np.array(lat), count, time.perf_counter() - t0
+
+
+def measure(rates=(100, 300, 1000), duration=2.0, pool_size=64, same=24, seed=2025, device=0,
+            max_per_rate=400):
+    """The serving record of the benchmark line: the batched server's open-loop Poisson
+    sweep (circuits/s, p50/p99 latency per offered rate) and its saturated throughput;
+    then the first `same` requests of every arrival stream (the pool's first templates,
+    seeds 1000 + k as in the sweep) through the plain form one request at a time and
+    through the batched server, all at once and one at a time."""
+    pool = sv.request_pool(pool_size, seed=seed)
+    same = min(same, pool_size)
+    out = {"workload": "Poisson QNoisyEngine requests: 90% kets of 12-28 qubits (P(n) ~ "
+                       "2^-(n-12)), depth 10-60 layered circuits, depolarising p=1e-3 per qubit "
+                       "per step by trajectories, shots log-uniform 1-1000, 20% with mid-circuit "
+                       "Z measurements; 10% density matrices of 8-13 qubits with 16-operator "
+                       f"2-qubit channels; seeded pool of {pool_size} templates",
+           "pool": {"requests": pool_size,
+                    "ket_fraction": float(np.mean([r.kind == sv.KET for r in pool])),
+                    "mean_shots": float(np.mean([r.shots for r in pool])),
+                    "max_qubits": int(max(r.n for r in pool))}}
+    srv = sv.Server(device, mode=sv.BATCHED)
+    closed_loop(srv, pool, len(pool), seed=1)  # warm-up: programs, pools, autotuner
+    sweep = []
+    for rate in rates:
+        lat, done, wall = sv.run_open_loop(srv, pool, rate, duration, max_requests=max_per_rate)
+        sweep.append({"rate_req_s": rate, **sv.summarize(lat, done, wall)})
+    lat, done, wall = closed_loop(srv, pool, len(pool))
+    out["batched"] = {"sweep": sweep, "saturated_all_templates": sv.summarize(lat, done, wall)}
+    lat, done, wall = closed_loop(srv, pool, same, seed=1000)
+    b_all = sv.summarize(lat, done, wall)
+    lat, done, wall = sequential(srv, pool, same)
+    b_seq = sv.summarize(lat, done, wall)
+    out["batched"]["stats"] = srv.stats()
+    srv.close()
+    plain = sv.Server(device, mode=sv.PLAIN)
+    sequential(plain, pool, 2)  # warm-up
+    lat, done, wall = sequential(plain, pool, same)
+    p_seq = sv.summarize(lat, done, wall)
+    plain.close()
+    out["same_requests"] = {
+        "requests": same,
+        "rho_requests": int(sum(r.kind != sv.KET for r in pool[:same])),
+        "plain_one_at_a_time": p_seq,
+        "batched_all_at_once": b_all,
+        "batched_one_at_a_time": b_seq,
+        "speedup_circuits_per_s": b_all["circuits_per_s"] / max(p_seq["circuits_per_s"], 1e-12),
+        "plain_form": "resident engine in complex128, one request at a time, one launch per gate"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--rates", default="100,300,1000,3000,10000,20000")

@@ -1,11 +1,15 @@
-"""Fused complex64 form: 6-qubit tcgen05 blocks with split-TF32 products.
+"""Fused complex64 form: 6-qubit tcgen05 blocks with split-FP16 products.
 
 Tolerances: a single block agrees with the complex128 oracle within 1e-5
-relative (max-norm) -- FP32 accumulation of 3xTF32 products; the identity
-block reproduces its input within 2^-21 relative (the lo half keeps 11 of
-up to 13 significant bits of x - hi); a fused layered
+relative (max-norm) -- FP32 accumulation of 3 x FP16 split products of
+power-of-two-scaled operands; the identity block reproduces its input within
+2^-20 relative (hi and lo keep 11 significant bits each); a fused layered
 circuit keeps fidelity >= 1 - 1e-6 against the plain complex128 form.
+A bounded wait that runs out reports QGPU_ERR_TIMEOUT and leaves the
+context usable.
 """
+import ctypes as ct
+
 import numpy as np
 import pytest
 
@@ -62,3 +66,41 @@ def test_fused_layered_circuit_fidelity(ctx):
         for U, t in layer:
             psi = orc.apply(psi, U, t, [2] * n, path=1)
     assert relerr(a, psi) < 1e-12
+
+
+@pytest.mark.parametrize("scale", [1.0, 2.0 ** -40, 2.0 ** 30])
+def test_block_scale_follows_the_norm(ctx, scale):
+    """The fp16 scale comes from |psi|: unnormalised kets keep the accuracy."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(11)
+    n = 15
+    psi = (gaussian_ket(rng, 2 ** n) * scale).astype(np.complex64).astype(np.complex128)
+    U = haar_unitary(rng, 64)
+    targets = [14, 1, 7, 3, 10, 0]
+    s = qb.State.from_numpy(ctx, psi, [2] * n, qb.C64)
+    qb.apply_tc(s, U, targets)
+    ref = orc.apply(psi, U, targets, [2] * n)
+    assert relerr(s.numpy(), ref) < 1e-5
+
+
+def test_wait_runs_out_then_context_recovers(ctx):
+    """The next fused pass first waits on a barrier that nothing completes:
+    the wait gives up after its iteration limit, the call reports Timeout,
+    and the same context then runs a pass that matches the oracle."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(12)
+    n = 14
+    targets = [0, 2, 4, 6, 8, 10]
+    psi = gaussian_ket(rng, 2 ** n).astype(np.complex64).astype(np.complex128)
+    U = haar_unitary(rng, 64)
+    L = qb.lib()
+    s = qb.State.from_numpy(ctx, psi, [2] * n, qb.C64)
+    qb.check(L.qgpu_ctx_set_wait_test(ctx.h, ct.c_uint32(4096), ct.c_int(1)))
+    try:
+        with pytest.raises(qb.Timeout):
+            qb.apply_tc(s, U, targets)
+    finally:
+        qb.check(L.qgpu_ctx_set_wait_test(ctx.h, ct.c_uint32(0), ct.c_int(0)))
+    s2 = qb.State.from_numpy(ctx, psi, [2] * n, qb.C64)
+    qb.apply_tc(s2, U, targets)
+    assert relerr(s2.numpy(), orc.apply(psi, U, targets, [2] * n)) < 1e-5
