@@ -102,6 +102,13 @@ void* qgpu_ctx_stream(qgpu_ctx* ctx);
  * call reports QGPU_ERR_TIMEOUT; the context stays usable. For tests of the
  * timeout path; one-shot. */
 qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall_next);
+/* Largest tile, in state bits (5..14), of the tile passes that run the plain
+ * form of qgpu_run_gates on qubit kets (runs of 1- and 2-qubit gates, each run
+ * one read and one write of the state); 0 restores the default, which is
+ * also the cap: 13 for complex128 and 14 for complex64 (128 KB of shared
+ * memory per tile). No counterpart
+ * in Quantum++, which applies one gate per pass. */
+qgpu_status qgpu_ctx_set_tile_bits(qgpu_ctx* ctx, int bits);
 
 /* ---------------------------------------------------------------- states */
 /* Allocate a ket (D x 1) or density matrix (D x D) over `dims` in HBM,

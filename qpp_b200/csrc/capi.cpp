@@ -488,6 +488,15 @@ qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall
     });
 }
 
+qgpu_status qgpu_ctx_set_tile_bits(qgpu_ctx* ctx, int bits) {
+    return guard([&] {
+        check_handle(ctx);
+        if (bits != 0 && (bits < 5 || bits > 14))
+            raise(QGPU_ERR_OUT_OF_RANGE, "qgpu_ctx_set_tile_bits()", "bits");
+        ctx->tile_bits = bits;
+    });
+}
+
 // --------------------------------------------------------------- states
 qgpu_status qgpu_state_create(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
                               const uint64_t* dims, uint32_t n, qgpu_state** out) {

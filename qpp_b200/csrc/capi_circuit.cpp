@@ -411,12 +411,14 @@ qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U, const uint64_t* target
         // |psi|^2 first: its block partials use the context scratch, which
         // the block matrix takes over after them in stream order
         const double* norm2 = qgpu::fused_norm_prepare(s->ctx, s->data, s->elems);
-        float* dB = static_cast<float*>(qgpu::ctx_scratch(s->ctx, B.size() * sizeof(float)));
+        auto* scr = static_cast<unsigned char*>(qgpu::ctx_scratch(s->ctx, 2 * 65536));
+        float* dB = reinterpret_cast<float*>(scr);
         QG_CUDA(cudaMemcpyAsync(dB, B.data(), B.size() * sizeof(float), cudaMemcpyHostToDevice,
                                 s->ctx->stream));
+        qgpu::fused6_images(s->ctx, dB, scr + 65536, 1);
         int tb[6];
         for (int j = 0; j < 6; ++j) tb[j] = n - 1 - q6[size_t(j)];
-        qgpu::launch_fused6_tc(s->ctx, s->data, n, tb, dB, norm2);
+        qgpu::launch_fused6_tc(s->ctx, s->data, n, tb, scr + 65536, norm2);
         if (qgpu::fused_error(s->ctx))
             raise(QGPU_ERR_TIMEOUT, W, "tensor-core pass timed out");
     });

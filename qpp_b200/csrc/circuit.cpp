@@ -7,6 +7,7 @@
 
 #include "kernels.hpp"
 #include "ops.hpp"
+#include "tile_gates.hpp"
 #include "traj.hpp"
 
 qgpu_circuit::~qgpu_circuit() {
@@ -268,9 +269,16 @@ static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
         c->plan[i].U = U6;
         fused6_matrix(U6.data(), host.data() + size_t(c->block_slot[i]) * 128 * 128);
     }
-    QG_CUDA(cudaMalloc(&c->dB, host.size() * sizeof(float)));
-    QG_CUDA(cudaMemcpy(c->dB, host.data(), host.size() * sizeof(float),
-                       cudaMemcpyHostToDevice));
+    float* tmp = nullptr;
+    QG_CUDA(cudaMalloc(&tmp, host.size() * sizeof(float)));
+    struct FreeTmp {
+        float* p;
+        ~FreeTmp() { cudaFree(p); }
+    } free_tmp{tmp};
+    QG_CUDA(cudaMemcpy(tmp, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
+    QG_CUDA(cudaMalloc(&c->dB, size_t(nslot) * 65536));
+    fused6_images(s->ctx, tmp, c->dB, int(nslot));
+    QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
     c->plan_ctx = s->ctx;
 }
 
@@ -345,7 +353,7 @@ void fused_launch(qgpu_state* s, qgpu_circuit* c) {
             for (int j = 0; j < 6; ++j) tb[j] = nb - 1 - b.qubits[size_t(j)];
             if (!norm2) norm2 = fused_norm_prepare(s->ctx, s->data, s->elems);
             launch_fused6_tc(s->ctx, s->data, nb, tb,
-                             c->dB + size_t(c->block_slot[i]) * 128 * 128, norm2);
+                             c->dB + size_t(c->block_slot[i]) * 65536, norm2);
             continue;
         }
         vapply(s, vs, b.qubits, {}, b.U.data(), uint64_t(1) << b.qubits.size());
@@ -358,8 +366,16 @@ void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_
             raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()",
                   "classical conditionals need an engine (qgpu_engine_execute)");
     if (form == 0) {
-        for (uint64_t i = first; i < first + count && i < c->steps.size(); ++i)
+        // qubit kets: runs of 1- and 2-qubit gates as tile passes
+        const bool tiles = s->kind == QGPU_KET && c->d == 2 && !s->dims.empty();
+        std::vector<GateDesc> run;
+        for (uint64_t i = first; i < first + count && i < c->steps.size(); ++i) {
+            if (tiles && gate_desc_of(c->steps[i], int(c->nq), run)) continue;
+            run_tiled_gates(s, run);
+            run.clear();
             apply_step(s, c->steps[i]);
+        }
+        run_tiled_gates(s, run);
         return;
     }
     if (first != 0 || count < c->steps.size())

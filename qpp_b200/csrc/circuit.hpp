@@ -77,10 +77,11 @@ struct qgpu_circuit {
     // fused plan cache
     uint32_t plan_k = 0;
     std::vector<qgpu::Block> plan;
-    // device copies of the tensor-core block matrices (fp32, 128 x 128 each)
+    // device images of the tensor-core block matrices (65536 bytes each:
+    // fp16 hi and lo halves in the kernel's shared-memory layout)
     qgpu_ctx* plan_ctx = nullptr;
-    float* dB = nullptr;
-    std::vector<int64_t> block_slot; // plan index -> slot in dB, or -1
+    unsigned char* dB = nullptr;
+    std::vector<int64_t> block_slot; // plan index -> image slot in dB, or -1
     // fused density-matrix program (superoperator blocks), built for the
     // first rho_steps steps (steps are only ever appended)
     uint64_t rho_steps = ~uint64_t(0);

@@ -33,6 +33,9 @@ struct qgpu_ctx {
     // that the next fused launch waits first on a barrier nothing completes.
     uint32_t wait_limit = 0;
     int stall_next = 0;
+    // Largest tile (state bits) of the plain form's tile passes; 0 = the
+    // default (qgpu_ctx_set_tile_bits).
+    int tile_bits = 0;
     // Stream-ordered pool of every device buffer the context allocates
     // (states, transform buffers, batch arenas): freed blocks stay reserved
     // up to a threshold, so repeated large allocations skip the driver's

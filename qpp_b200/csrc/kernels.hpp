@@ -39,6 +39,46 @@ void launch_apply_generic(qgpu_ctx* ctx, qgpu_prec prec, void* data,
 void launch_apply_kron4(qgpu_ctx* ctx, qgpu_prec prec, void* data, const SegPlan& outer,
                         const std::vector<uint64_t>& off, const cd* A, const cd* B);
 
+// --- tile passes (kernels_tile.cu) -----------------------------------------
+// One gate of a tile pass on a qubit ket: op 1 = 2 x 2 on tile bit t0, op 2 =
+// 4 x 4 on tile bits (t0, t1) with row index 2 * b(t0) + b(t1); the matrix is
+// row-major at mats + mat (state precision). It acts on the amplitudes i of
+// the tile with (i & lmask) == lval, in tiles whose base offset b has
+// (b & gmask) == gval (controls on bits outside the tile). k0 / k1: the
+// positions of t0 / t1 in its sweep's bit list.
+struct TileGate {
+    uint32_t op;
+    int32_t t0, t1;
+    uint32_t lmask, lval;
+    uint32_t mat;
+    uint64_t gmask, gval;
+    uint32_t k0, k1;
+};
+// A sweep: consecutive gates of a pass whose targets lie in nb <= 3 tile bits
+// b[0..nb): every thread takes groups of 2^nb amplitudes (group element bit k
+// <-> tile bit b[k]) from shared memory into registers, applies the sweep's
+// gates in order there and writes the group back. Group numbers spell the
+// other tile bits in ascending order.
+struct TileSweep {
+    uint32_t nb;
+    int32_t b[3];
+    uint32_t first, ngates;
+};
+// A pass: tiles of 2^T amplitudes, tile bits = state bits 0..L-1 and hi[0..T-L)
+// (ascending); sweeps[first_sweep, first_sweep + nsweeps) in order; their
+// gates' matrices are the mat_elems entries from mats + mat_first.
+struct TilePassParams {
+    uint64_t ntiles;
+    int T, L;
+    int hi[16];
+    uint32_t first, ngates;
+    uint32_t first_sweep, nsweeps;
+    uint32_t mat_first, mat_elems;
+};
+size_t tile_pass_smem(qgpu_prec prec, const TilePassParams& p);
+void launch_tile_pass(qgpu_ctx* ctx, qgpu_prec prec, void* data, const TilePassParams& p,
+                      const TileGate* gates, const TileSweep* sweeps, const void* mats);
+
 // --- subsystem kernels (kernels_subsys.cu) --------------------------------
 // out[o] = in[map(o)], o over map.count.
 // Tiled bit permutation (see kernels_subsys.cu): when every output digit's

@@ -64,19 +64,26 @@ struct Fused6Params {
     uint64_t ntiles;       // groups / 128
     int tb_sorted[6];      // target bit positions, ascending
     uint32_t off[64];      // element offset of block index m (big-endian over the block qubits)
-    const float* B;        // 128 x 128 fp32, B[n * 128 + k]
+    uint32_t loc_m[64];    // stage-local index of block index m
+    uint32_t run_off[64];  // element offset of contiguous run j from the tile base
+    uint32_t nruns;        // contiguous runs per tile (2^(13 - r))
+    uint32_t run_bytes;    // bytes per run (2^r * 8, at least 1 KB)
+    uint8_t g_pos[7];      // state bit of group bit i (the 7 lowest non-target bits)
+    uint8_t g_loc[7];      // stage-local bit of group bit i
+    const unsigned char* Bimg; // 64 KB shared-memory image of the block (fused6_images)
     const double* norm2;   // device word: |psi|^2 (sets the fp16 scale)
     int* err;              // error flag (0 = ok)
-    uint32_t spin_limit;   // iterations of the MMA-completion wait
+    uint32_t spin_limit;   // iterations of each wait
     uint32_t stall_first;  // test hook: the first wait is on a barrier nothing completes
 };
 
 constexpr uint32_t kSpinLimit = 1u << 26;
-constexpr int kF6Threads = 256;
+constexpr int kF6Threads = 384;      // 12 warps: producer, MMA, 2 idle, 4 converter, 4 epilogue
 constexpr int kBScaleExp = 6;
-// 80 KB of dynamic shared memory (64 KB used): at most two CTAs per SM, so
-// the two 256-column tensor-memory allocations always fit.
-constexpr size_t kF6Smem = 80 * 1024;
+constexpr uint32_t kStageBytes = 65536; // one tile: 128 groups x 64 amplitudes x 8 B
+// B (64 KB, hi + lo) and two stages, 1 KB alignment slack: one CTA per SM,
+// which then owns all 512 tensor-memory columns
+constexpr size_t kF6Smem = 1024 + 65536 + 2 * size_t(kStageBytes);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -135,20 +142,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "r"(taddr));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t limit) {
-    for (uint32_t it = 0; it < limit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(parity));
-        if (done) return true;
-    }
-    return false;
-}
-
 // (x0, x1) -> packed fp16 hi halves and packed fp16 residuals; x0 in the low
 // 16 bits (the even K element of the TMEM column).
 __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
@@ -159,67 +152,93 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_
     lo = *reinterpret_cast<uint32_t*>(&l);
 }
 
-__global__ void __launch_bounds__(kF6Threads, 2)
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity));
+    return done != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_commit(uint32_t mbar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+        : "memory");
+}
+
+// Shared state of one CTA's pipeline. Barriers (phase k completes with the
+// k-th event): full[s] stage s landed (bulk copies, tx bytes); empty[s] the
+// converter warps released stage s; afull[a] the converter wrote A buffer a;
+// aempty[a] the MMAs reading A buffer a finished; dfull[d] the MMAs writing D
+// buffer d finished; dempty[d] the epilogue warps read D buffer d.
+struct F6Shared {
+    uint64_t full[2], empty[2], afull[2], aempty[2], dfull[2], dempty[2], drain, stall, bmat;
+    uint32_t tmem_base;
+    int abort;
+};
+
+// Bounded wait on phase `parity` of `bar`: false when the limit ran out (the
+// CTA is then marked aborted and *err set) or another role aborted.
+__device__ __forceinline__ bool f6_wait(F6Shared& S, uint32_t bar, uint32_t parity,
+                                        uint32_t limit, int* err) {
+    for (uint32_t it = 0; it < limit; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255u) == 255u && *reinterpret_cast<volatile int*>(&S.abort)) return false;
+    }
+    *reinterpret_cast<volatile int*>(&S.abort) = 1;
+    atomicExch(err, 1);
+    return false;
+}
+
+__global__ void __launch_bounds__(kF6Threads, 1)
     k_fused6_tc(float2* __restrict__ psi, const __grid_constant__ Fused6Params p) {
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ __align__(8) uint64_t stall_bar;
-    __shared__ uint32_t tmem_base_sh;
-    __shared__ int abort_sh;
+    __shared__ __align__(8) F6Shared S;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int quarter = warp & 3, kpart = warp >> 2;
 
     unsigned char* Bh = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* Bl = Bh + 32768;
+    unsigned char* stage0 = Bh + 65536;
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(
-            smem_u32(&tmem_base_sh)));
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+            smem_u32(&S.tmem_base)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        abort_sh = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&stall_bar)));
+        S.abort = 0;
+        for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.full[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&S.empty[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&S.afull[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.aempty[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.dfull[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&S.dempty[i])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.drain)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.stall)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bmat)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    // scales from |psi|^2: |a| * 2^eA < 2^14 for every amplitude
-    int eA = 14;
-    {
-        const double n2 = p.norm2 ? *p.norm2 : 1.0;
-        if (n2 > 0.0 && n2 < 1e300) {
-            int e2;
-            frexp(n2, &e2); // n2 < 2^e2, so |psi| < 2^ceil(e2 / 2)
-            eA = 14 - ((e2 + 1) >> 1);
-        }
-        eA = max(-100, min(100, eA));
-    }
-    const float sa = __int_as_float((127 + eA) << 23);
-    const float inv = __int_as_float((127 - eA - kBScaleExp) << 23); // 2^-(eA + 6), normal
-    // block matrix -> shared memory, scaled by 2^6 and split into fp16 hi and lo
-    for (int e = tid; e < 128 * 128; e += blockDim.x) {
-        int n = e >> 7, k = e & 127;
-        float x = p.B[e] * float(1 << kBScaleExp);
-        __half hi = __float2half_rn(x);
-        __half lo = __float2half_rn(x - __half2float(hi));
-        uint32_t a = b_swz16(n, k);
-        *reinterpret_cast<__half*>(Bh + a) = hi;
-        *reinterpret_cast<__half*>(Bl + a) = lo;
-    }
-    asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    const uint32_t tbase = tmem_base_sh;
-    const uint32_t lane_off = uint32_t(quarter * 32) << 16;
-    const uint32_t mb = smem_u32(&mbar);
-    const uint32_t bh_addr = smem_u32(Bh), bl_addr = smem_u32(Bl);
-    uint32_t parity = 0;
-    bool stall = p.stall_first != 0;
+    const uint32_t tbase = S.tmem_base;
+    const uint64_t my_tiles =
+        p.ntiles > blockIdx.x ? (p.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const uint32_t limit = p.spin_limit;
 
+    // group index (tile * 128) with zero bits inserted at the target bits
     auto tile_base = [&](uint64_t tile) {
-        uint64_t base = tile * 128 + uint64_t(quarter * 32 + lane);
+        uint64_t base = tile * 128;
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
             int b = p.tb_sorted[i];
@@ -228,98 +247,163 @@ __global__ void __launch_bounds__(kF6Threads, 2)
         }
         return base;
     };
-    auto load = [&](uint64_t base, float2 (&v)[32]) {
-#pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] = psi[base + p.off[kpart * 32 + j]];
-    };
-    // A halves of this thread's 32 amplitudes -> TMEM columns kpart*32 + j
-    // (hi) and 64 + kpart*32 + j (lo)
-    auto stage = [&](const float2 (&v)[32]) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            uint32_t hi[16], lo[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-                split2(v[c * 16 + j].x * sa, v[c * 16 + j].y * sa, hi[j], lo[j]);
-            const uint32_t col = uint32_t(kpart * 32 + c * 16);
-            tmem_st16(tbase + lane_off + col, hi);
-            tmem_st16(tbase + lane_off + 64u + col, lo);
-        }
-        asm volatile("tcgen05.wait::st.sync.aligned;");
-        asm volatile("tcgen05.fence::before_thread_sync;");
-    };
-    auto issue = [&]() { // after a __syncthreads
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t d = tbase + 128u;
-#pragma unroll 1
-            for (int ks = 0; ks < 8; ++ks) {
-                uint32_t koff = uint32_t((ks >> 2) * 16384 + (ks & 3) * 32);
-                uint64_t dh = b_desc(bh_addr + koff), dl = b_desc(bl_addr + koff);
-                mma_f16_ts(d, tbase + uint32_t(ks * 8), dh, ks > 0 ? 1u : 0u);
-                mma_f16_ts(d, tbase + uint32_t(ks * 8), dl, 1u);
-                mma_f16_ts(d, tbase + 64u + uint32_t(ks * 8), dh, 1u);
-            }
-            asm volatile(
-                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    mb));
-        }
-    };
 
-    uint64_t tile = blockIdx.x;
-    if (tile < p.ntiles) {
-        float2 v[32];
-        uint64_t base_cur = tile_base(tile);
-        load(base_cur, v);
-        stage(v);
-        __syncthreads();
-        issue();
-        for (;;) {
-            const uint64_t next = tile + gridDim.x;
-            const bool has_next = next < p.ntiles;
-            uint64_t base_next = 0;
-            if (has_next) {
-                base_next = tile_base(next);
-                load(base_next, v);
+    if (warp == 0) {
+        // ---- producer: each tile is nruns contiguous runs, one bulk copy each
+        if (lane == 0) {
+            // the block matrix image (hi and lo halves, swizzled) in one copy
+            const uint32_t bb = smem_u32(&S.bmat);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bb),
+                         "r"(65536u)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                "[%0], [%1], %2, [%3];" ::"r"(smem_u32(Bh)),
+                "l"(p.Bimg), "r"(65536u), "r"(bb)
+                : "memory");
+            uint64_t issued = 0;
+            for (uint64_t i = 0; i < my_tiles; ++i) {
+                const uint32_t st = uint32_t(i & 1), u = uint32_t(i >> 1);
+                if (u >= 1 && !f6_wait(S, smem_u32(&S.empty[st]), (u - 1) & 1u, limit, p.err))
+                    break;
+                const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
+                const uint32_t fb = smem_u32(&S.full[st]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                             "r"(kStageBytes)
+                             : "memory");
+                const uint32_t dst = smem_u32(stage0) + st * kStageBytes;
+                for (uint32_t j = 0; j < p.nruns; ++j)
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                        "[%0], [%1], %2, [%3];" ::"r"(dst + j * p.run_bytes),
+                        "l"(psi + base + p.run_off[j]), "r"(p.run_bytes), "r"(fb)
+                        : "memory");
+                ++issued;
             }
-            bool ok = stall ? mbar_wait(smem_u32(&stall_bar), 0u, p.spin_limit)
-                            : mbar_wait(mb, parity, p.spin_limit);
-            if (!ok && lane == 0) {
-                atomicExch(p.err, 1);
-                abort_sh = 1;
+            // copies still in flight land before the CTA exits (bounded)
+            f6_wait(S, bb, 0u, kSpinLimit, p.err);
+            for (uint64_t i = issued > 2 ? issued - 2 : 0; i < issued; ++i)
+                f6_wait(S, smem_u32(&S.full[i & 1]), uint32_t(i >> 1) & 1u, kSpinLimit, p.err);
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer: D[d] = A_hi B_hi + A_hi B_lo + A_lo B_hi
+        if (lane == 0) {
+            const uint32_t bh = smem_u32(Bh), bl = smem_u32(Bl);
+            const bool have_b = f6_wait(S, smem_u32(&S.bmat), 0u, limit, p.err);
+            for (uint64_t i = 0; have_b && i < my_tiles; ++i) {
+                const uint32_t b = uint32_t(i & 1), u = uint32_t(i >> 1);
+                if (!f6_wait(S, smem_u32(&S.afull[b]), u & 1u, limit, p.err)) break;
+                if (u >= 1 && !f6_wait(S, smem_u32(&S.dempty[b]), (u - 1) & 1u, limit, p.err))
+                    break;
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t a = tbase + b * 128u, d = tbase + 256u + b * 128u;
+#pragma unroll 1
+                for (int ks = 0; ks < 8; ++ks) {
+                    uint32_t koff = uint32_t((ks >> 2) * 16384 + (ks & 3) * 32);
+                    uint64_t dh = b_desc(bh + koff), dl = b_desc(bl + koff);
+                    mma_f16_ts(d, a + uint32_t(ks * 8), dh, ks > 0 ? 1u : 0u);
+                    mma_f16_ts(d, a + uint32_t(ks * 8), dl, 1u);
+                    mma_f16_ts(d, a + 64u + uint32_t(ks * 8), dh, 1u);
+                }
+                mbar_commit(smem_u32(&S.aempty[b]));
+                mbar_commit(smem_u32(&S.dfull[b]));
             }
-            __syncthreads();
-            if (abort_sh) {
-                // let the MMAs still in flight drain (bounded) before freeing TMEM
-                if (tid == 0) mbar_wait(mb, parity, kSpinLimit);
+            // every MMA this thread issued has finished before TMEM is freed
+            mbar_commit(smem_u32(&S.drain));
+            f6_wait(S, smem_u32(&S.drain), 0u, kSpinLimit, p.err);
+        }
+    } else if (warp >= 4 && warp < 8) {
+        // ---- converters: stage -> fp16 hi/lo -> A buffer (one TMEM lane per group)
+        const int g = (warp & 3) * 32 + lane;
+        uint32_t loc_g = 0;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) loc_g |= uint32_t((g >> i) & 1) << p.g_loc[i];
+        // scale from |psi|^2: |a| * 2^eA < 2^14 for every amplitude
+        int eA = 14;
+        {
+            const double n2 = p.norm2 ? *p.norm2 : 1.0;
+            if (n2 > 0.0 && n2 < 1e300) {
+                int e2;
+                frexp(n2, &e2); // n2 < 2^e2, so |psi| < 2^ceil(e2 / 2)
+                eA = 14 - ((e2 + 1) >> 1);
+            }
+            eA = max(-100, min(100, eA));
+        }
+        const float sa = __int_as_float((127 + eA) << 23);
+        const uint32_t lane_off = uint32_t((warp & 3) * 32) << 16;
+        bool stall = p.stall_first != 0;
+        for (uint64_t i = 0; i < my_tiles; ++i) {
+            const uint32_t b = uint32_t(i & 1), u = uint32_t(i >> 1);
+            if (stall) {
+                f6_wait(S, smem_u32(&S.stall), 0u, limit, p.err); // never completes
                 break;
             }
-            parity ^= 1u;
+            if (!f6_wait(S, smem_u32(&S.full[b]), u & 1u, limit, p.err)) break;
+            if (u >= 1 && !f6_wait(S, smem_u32(&S.aempty[b]), (u - 1) & 1u, limit, p.err)) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
+            const float2* stg = reinterpret_cast<const float2*>(stage0 + b * kStageBytes);
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
+            for (int c = 0; c < 4; ++c) {
+                uint32_t hi[16], lo[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const float2 v = stg[loc_g + p.loc_m[c * 16 + j]];
+                    split2(v.x * sa, v.y * sa, hi[j], lo[j]);
+                }
+                const uint32_t col = b * 128u + uint32_t(c * 16);
+                tmem_st16(tbase + lane_off + col, hi);
+                tmem_st16(tbase + lane_off + 64u + col, lo);
+            }
+            // the stage's reads are done: the producer may refill it
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&S.empty[b]));
+            asm volatile("tcgen05.wait::st.sync.aligned;");
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&S.afull[b]));
+        }
+    } else if (warp >= 8) {
+        // ---- epilogue: D buffer -> scaled FP32 -> the group's addresses in HBM
+        const int g = (warp & 3) * 32 + lane;
+        uint64_t base_low = 0;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) base_low |= uint64_t((g >> i) & 1) << p.g_pos[i];
+        int eA = 14;
+        {
+            const double n2 = p.norm2 ? *p.norm2 : 1.0;
+            if (n2 > 0.0 && n2 < 1e300) {
+                int e2;
+                frexp(n2, &e2);
+                eA = 14 - ((e2 + 1) >> 1);
+            }
+            eA = max(-100, min(100, eA));
+        }
+        const float inv = __int_as_float((127 - eA - kBScaleExp) << 23); // 2^-(eA + 6)
+        const uint32_t lane_off = uint32_t((warp & 3) * 32) << 16;
+        for (uint64_t i = 0; i < my_tiles; ++i) {
+            const uint32_t b = uint32_t(i & 1), u = uint32_t(i >> 1);
+            if (!f6_wait(S, smem_u32(&S.dfull[b]), u & 1u, limit, p.err)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            float2* out = psi + tile_base(blockIdx.x + i * gridDim.x) + base_low;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
                 uint32_t dv[32];
-                tmem_ld32(tbase + lane_off + 128u + uint32_t(kpart * 64 + c * 32), dv);
+                tmem_ld32(tbase + lane_off + 256u + b * 128u + uint32_t(c * 32), dv);
                 asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
-                    psi[base_cur + p.off[kpart * 32 + c * 16 + j]] =
-                        make_float2(__uint_as_float(dv[2 * j]) * inv,
-                                    __uint_as_float(dv[2 * j + 1]) * inv);
+                    out[p.off[c * 16 + j]] = make_float2(__uint_as_float(dv[2 * j]) * inv,
+                                                         __uint_as_float(dv[2 * j + 1]) * inv);
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
-            if (!has_next) break;
-            stage(v);
-            __syncthreads();
-            issue();
-            tile = next;
-            base_cur = base_next;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&S.dempty[b]));
         }
     }
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tbase));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase));
     }
 }
 
@@ -352,6 +436,32 @@ void fused6_matrix(const cd* U, float* B) {
         }
 }
 
+// 64 KB shared-memory images of `nblocks` block matrices (fp32 128 x 128,
+// fused6_matrix): each scaled by 2^6, split into fp16 hi and lo halves and
+// laid out K-major with the 128-byte swizzle at the offsets the kernel's
+// descriptors address (hi in the first 32 KB, lo in the second), so a pass
+// loads its matrix with one bulk copy.
+__global__ void __launch_bounds__(256)
+    k_fused6_image(const float* __restrict__ B, unsigned char* __restrict__ img) {
+    const float* b = B + size_t(blockIdx.x) * 128 * 128;
+    unsigned char* o = img + size_t(blockIdx.x) * 65536;
+    for (int e = threadIdx.x; e < 128 * 128; e += blockDim.x) {
+        int n = e >> 7, k = e & 127;
+        float x = b[e] * float(1 << kBScaleExp);
+        __half hi = __float2half_rn(x);
+        __half lo = __float2half_rn(x - __half2float(hi));
+        uint32_t a = b_swz16(n, k);
+        *reinterpret_cast<__half*>(o + a) = hi;
+        *reinterpret_cast<__half*>(o + 32768 + a) = lo;
+    }
+}
+
+void fused6_images(qgpu_ctx* ctx, const float* dB, void* dimg, int nblocks) {
+    if (nblocks <= 0) return;
+    k_fused6_image<<<nblocks, 256, 0, ctx->stream>>>(dB, static_cast<unsigned char*>(dimg));
+    after_launch(ctx, "k_fused6_image");
+}
+
 // |psi|^2 of the complex64 ket into the context's norm slot (stream order;
 // read by the fused passes that follow).
 const double* fused_norm_prepare(qgpu_ctx* ctx, const void* data, uint64_t n) {
@@ -361,7 +471,7 @@ const double* fused_norm_prepare(qgpu_ctx* ctx, const void* data, uint64_t n) {
 }
 
 void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
-                      const float* dB, const double* norm2) {
+                      const void* img, const double* norm2) {
     if (nbits < 13)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu fused", "fused tensor-core blocks need n >= 13");
     Fused6Params p;
@@ -371,13 +481,46 @@ void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
     for (int i = 0; i < 6; ++i) s[i] = tbits[i];
     std::sort(s, s + 6);
     for (int i = 0; i < 6; ++i) p.tb_sorted[i] = s[i];
-    for (int m = 0; m < 64; ++m) {
-        uint32_t o = 0;
-        for (int j = 0; j < 6; ++j)
-            if ((m >> (5 - j)) & 1) o |= uint32_t(1) << tbits[j];
-        p.off[m] = o;
+    // tile bits: the six targets and the seven lowest other bits, ascending;
+    // stage-local bit i holds tile bit tpos[i]
+    bool is_t[64] = {};
+    for (int i = 0; i < 6; ++i) is_t[s[i]] = true;
+    int tpos[13], nt = 0, ng = 0;
+    for (int b = 0; b < nbits && nt < 13; ++b) {
+        if (is_t[b]) {
+            tpos[nt++] = b;
+        } else if (ng < 7) {
+            p.g_pos[ng] = uint8_t(b);
+            p.g_loc[ng++] = uint8_t(nt);
+            tpos[nt++] = b;
+        }
     }
-    p.B = dB;
+    int r = 0; // the low r tile bits are state bits 0..r-1: runs of 2^r amplitudes
+    while (r < 13 && tpos[r] == r) ++r;
+    p.nruns = 1u << (13 - r);
+    p.run_bytes = (1u << r) * 8u;
+    for (uint32_t j = 0; j < p.nruns; ++j) {
+        uint32_t o = 0;
+        for (int i = r; i < 13; ++i)
+            if ((j >> (i - r)) & 1u) o |= 1u << tpos[i];
+        p.run_off[j] = o;
+    }
+    auto local_of = [&](int bit) {
+        for (int i = 0; i < 13; ++i)
+            if (tpos[i] == bit) return i;
+        return 0;
+    };
+    for (int m = 0; m < 64; ++m) {
+        uint32_t o = 0, l = 0;
+        for (int j = 0; j < 6; ++j)
+            if ((m >> (5 - j)) & 1) {
+                o |= uint32_t(1) << tbits[j];
+                l |= uint32_t(1) << local_of(tbits[j]);
+            }
+        p.off[m] = o;
+        p.loc_m[m] = l;
+    }
+    p.Bimg = static_cast<const unsigned char*>(img);
     p.norm2 = norm2;
     p.err = ctx_error_flag(ctx);
     p.spin_limit = ctx->wait_limit ? ctx->wait_limit : kSpinLimit;
@@ -395,7 +538,7 @@ void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
             if (dev >= 0 && dev < 64) attr_set[dev] = true;
         }
     }
-    int grid = int(std::min<uint64_t>(p.ntiles, uint64_t(ctx->num_sms) * 2));
+    int grid = int(std::min<uint64_t>(p.ntiles, uint64_t(ctx->num_sms)));
     k_fused6_tc<<<grid, kF6Threads, kF6Smem, ctx->stream>>>(static_cast<float2*>(data), p);
     after_launch(ctx, "k_fused6_tc");
 }

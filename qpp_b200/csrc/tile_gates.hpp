@@ -1,0 +1,44 @@
+// tile_gates.hpp -- planning and execution of gate runs as tile passes
+// (tile_gates.cpp, kernels_tile.cu).
+#pragma once
+
+#include <complex>
+#include <utility>
+#include <vector>
+
+#include "internal.hpp"
+#include "kernels.hpp"
+
+namespace qgpu {
+
+struct Step;
+
+// One 1- or 2-qubit gate of a qubit ket: state bits b0 (and b1 for op 2; the
+// matrix's row index is 2 * b(b0) + b(b1)), controls as (state bit, value),
+// the matrix column-major.
+struct GateDesc {
+    int op = 1;
+    int b0 = 0, b1 = 0;
+    std::vector<std::pair<int, int>> ctrl;
+    cd A[16];
+};
+
+// Appends the gates of step `st` on an nbits-qubit ket and returns true, or
+// returns false (appending nothing) when the step is not a 1- or 2-qubit
+// unitary, fan or controlled gate.
+bool gate_desc_of(const Step& st, int nbits, std::vector<GateDesc>& out);
+// Splits `gates` (in order) into tile passes of at most Tmax tile bits: the
+// low min(nbits, 5) state bits and the targets above them; each pass into
+// sweeps of consecutive gates on at most three tile bits. `dev` gets one
+// entry per gate with tile-local bits, `sweeps` the sweeps, `mats` the
+// row-major matrices.
+void plan_gate_tiles(const std::vector<GateDesc>& gates, int nbits, int Tmax,
+                     std::vector<TilePassParams>& passes, std::vector<TileGate>& dev,
+                     std::vector<TileSweep>& sweeps, std::vector<cd>& mats);
+// Largest tile (bits) for this context and precision: 13 for complex128 and
+// 14 for complex64 (128 KB of shared memory), or qgpu_ctx_set_tile_bits's.
+int tile_bits_max(const qgpu_ctx* ctx, qgpu_prec prec);
+// Runs `gates` on the qubit ket s as planned tile passes (stream order).
+void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates);
+
+} // namespace qgpu

@@ -173,11 +173,14 @@ int* ctx_error_flag(qgpu_ctx* ctx);
 int fused_error(qgpu_ctx* ctx);
 // The fused tensor-core pass (kernels_fused.cu): one 64 x 64 complex block on
 // six bits `tbits` (block index big-endian over them) of a complex64 ket of
-// 2^nbits amplitudes, in place; dB is the block's 128 x 128 real form
-// (fused6_matrix) and norm2 a device word holding |psi|^2, written by
+// 2^nbits amplitudes, in place; img is the block's 64 KB shared-memory image
+// (fused6_images) and norm2 a device word holding |psi|^2, written by
 // fused_norm_prepare earlier on the same stream.
 void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
-                      const float* dB, const double* norm2);
+                      const void* img, const double* norm2);
+// Images of nblocks consecutive 128 x 128 fp32 block matrices (fused6_matrix
+// layout) at dB into dimg (65536 bytes each), on the context stream.
+void fused6_images(qgpu_ctx* ctx, const float* dB, void* dimg, int nblocks);
 const double* fused_norm_prepare(qgpu_ctx* ctx, const void* data, uint64_t n);
 // The tile width T (0: untiled) for registers of n qubits on this device,
 // chosen once per (device, n) by timing calibration programs for T in
