@@ -201,9 +201,12 @@ qgpu_status qgpu_qft(qgpu_state* s, uint64_t d, int swap, int inverse);
  * The table of traced offsets lives in a fixed array of 65536 entries
  * (512 KB) that the library keeps on every GPU that loads it until the
  * process exits; a traced dimension prod dims[target] above 65536 is
- * rejected with QGPU_ERR_NOT_SUPPORTED. The first call on a device looks up
- * the array's device address (once per device) and should therefore come
- * before any stream capture. Every call shares that one array: calls whose
+ * rejected with QGPU_ERR_NOT_SUPPORTED. The first call on a device, and the
+ * first one after each qgpu_ctx_create on that device (a cudaDeviceReset in
+ * between can move the array), looks up the array's device address, so that
+ * call should come before any stream capture. Invalid targets are reported
+ * with where = "qgpu_ptrace_noalloc()". Every call shares that one array:
+ * calls whose
  * work overlaps on the GPU (different streams, different contexts of the
  * same device) race on it, so serialise them. The work is queued on the
  * state's context stream; synchronise that stream before reading d_out

@@ -424,6 +424,8 @@ qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out) {
                   "built for sm_100a (B200) only");
         }
         c->num_sms = prop.multiProcessorCount;
+        // the allocation-free ptrace looks its table's address up again
+        qgpu::noalloc_forget(device);
         QG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         cudaMemPoolProps pp;
         std::memset(&pp, 0, sizeof(pp));

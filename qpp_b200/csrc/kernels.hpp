@@ -76,6 +76,9 @@ struct TilePassParams {
     uint32_t mat_first, mat_elems;
 };
 size_t tile_pass_smem(qgpu_prec prec, const TilePassParams& p);
+// Drops the cached device address of qgpu_ptrace_noalloc's offset table for
+// `device` (kernels_subsys.cu); the next call looks it up again.
+void noalloc_forget(int device);
 void launch_tile_pass(qgpu_ctx* ctx, qgpu_prec prec, void* data, const TilePassParams& p,
                       const TileGate* gates, const TileSweep* sweeps, const void* mats);
 

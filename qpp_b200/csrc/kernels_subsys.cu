@@ -394,13 +394,23 @@ __global__ void __launch_bounds__(256)
 
 // Device address of g_noalloc_toff, looked up once per device with that
 // device current (the host-side symbol is only a stand-in, never a device
-// address).
+// address), and looked up again after qgpu_ctx_create on the device
+// (noalloc_forget), since a cudaDeviceReset in between reloads the module
+// and can move the array.
+static std::mutex g_noalloc_mu;
+static uint64_t* g_noalloc_addr[64] = {nullptr};
+
+void noalloc_forget(int device) {
+    if (device < 0 || device >= 64) return;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    g_noalloc_addr[device] = nullptr;
+}
+
 static uint64_t* noalloc_table(int device) {
-    static std::mutex mu;
-    static uint64_t* addr[64] = {nullptr};
+    uint64_t** addr = g_noalloc_addr;
     if (device < 0 || device >= 64)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_ptrace_noalloc()", "device index above 63");
-    std::lock_guard<std::mutex> lock(mu);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!addr[device]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_toff);
@@ -479,11 +489,11 @@ extern "C" qgpu_status qgpu_ptrace_noalloc(const qgpu_state* s, const uint64_t* 
         const int n = int(s->dims.size());
         if (n > 64) raise(QGPU_ERR_NOT_SUPPORTED, W, "more than 64 subsystems");
         if (k > uint32_t(n) || (k > 0 && !target))
-            raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, "qpp::ptrace()", "dims/target");
+            raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
         bool traced[64] = {false};
         for (uint32_t j = 0; j < k; ++j) {
             if (target[j] >= uint64_t(n) || traced[target[j]])
-                raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, "qpp::ptrace()", "dims/target");
+                raise(QGPU_ERR_SUBSYS_MISMATCH_DIMS, W, "dims/target");
             traced[target[j]] = true;
         }
         uint64_t stride[64];

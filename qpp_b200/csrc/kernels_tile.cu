@@ -51,36 +51,49 @@ __device__ __forceinline__ uint32_t tswz(uint32_t e) {
     return e ^ (h & ((1u << CB) - 1));
 }
 
+// The per-element control test selects between the new and the old values
+// instead of branching around the arithmetic, so the pairs' multiply-add
+// chains stay in one basic block and interleave; gates without tile-bit
+// controls (CTRL = false) skip the test.
+template <bool CTRL, typename C>
+__device__ __forceinline__ C pick(bool ok, const C& nv, const C& ov) {
+    if constexpr (!CTRL) return nv;
+    C r;
+    r.x = ok ? nv.x : ov.x;
+    r.y = ok ? nv.y : ov.y;
+    return r;
+}
+
 // 2 x 2 (row-major m) on group bit K of the registers v[0, 2^NB), for the
 // elements whose tile index (b + off[j]) passes the tile-bit controls.
-template <typename C, int NB, int K>
+template <typename C, int NB, int K, bool CTRL>
 __device__ __forceinline__ void group_1q(C (&v)[1 << NB], const C* m, uint32_t b,
                                          const uint32_t (&off)[1 << NB], uint32_t lmask,
                                          uint32_t lval) {
     const C a00 = m[0], a01 = m[1], a10 = m[2], a11 = m[3];
 #pragma unroll
     for (int j = 0; j < (1 << NB); ++j) {
-        if (j & (1 << K)) continue;
-        if (((b + off[j]) & lmask) != lval) continue;
+        if (j & (1 << K)) continue; // compile-time
+        const bool ok = ((b + off[j]) & lmask) == lval;
         const int j1 = j | (1 << K);
         C r0 = cmul(a00, v[j]);
         r0 = cfma(a01, v[j1], r0);
         C r1 = cmul(a10, v[j]);
         r1 = cfma(a11, v[j1], r1);
-        v[j] = r0;
-        v[j1] = r1;
+        v[j] = pick<CTRL>(ok, r0, v[j]);
+        v[j1] = pick<CTRL>(ok, r1, v[j1]);
     }
 }
 
 // 4 x 4 (row-major m, row index 2 * b(K0) + b(K1)) on group bits K0, K1.
-template <typename C, int NB, int K0, int K1>
+template <typename C, int NB, int K0, int K1, bool CTRL>
 __device__ __forceinline__ void group_2q(C (&v)[1 << NB], const C* m, uint32_t b,
                                          const uint32_t (&off)[1 << NB], uint32_t lmask,
                                          uint32_t lval) {
 #pragma unroll
     for (int j = 0; j < (1 << NB); ++j) {
-        if (j & ((1 << K0) | (1 << K1))) continue;
-        if (((b + off[j]) & lmask) != lval) continue;
+        if (j & ((1 << K0) | (1 << K1))) continue; // compile-time
+        const bool ok = ((b + off[j]) & lmask) == lval;
         const int j1 = j | (1 << K1), j2 = j | (1 << K0), j3 = j | (1 << K0) | (1 << K1);
         const C x0 = v[j], x1 = v[j1], x2 = v[j2], x3 = v[j3];
         C r[4];
@@ -92,23 +105,24 @@ __device__ __forceinline__ void group_2q(C (&v)[1 << NB], const C* m, uint32_t b
             acc = cfma(m[4 * row + 3], x3, acc);
             r[row] = acc;
         }
-        v[j] = r[0];
-        v[j1] = r[1];
-        v[j2] = r[2];
-        v[j3] = r[3];
+        v[j] = pick<CTRL>(ok, r[0], x0);
+        v[j1] = pick<CTRL>(ok, r[1], x1);
+        v[j2] = pick<CTRL>(ok, r[2], x2);
+        v[j3] = pick<CTRL>(ok, r[3], x3);
     }
 }
 
-template <typename C, int NB>
-__device__ __forceinline__ void group_gate(C (&v)[1 << NB], const TileGate& g, const C* m,
-                                           uint32_t b, const uint32_t (&off)[1 << NB]) {
-#define QG_1Q(K)                                                         \
-    case K:                                                              \
-        if constexpr (NB > K) group_1q<C, NB, K>(v, m, b, off, g.lmask, g.lval); \
+template <typename C, int NB, bool CTRL>
+__device__ __forceinline__ void group_gate_c(C (&v)[1 << NB], const TileGate& g, const C* m,
+                                             uint32_t b, const uint32_t (&off)[1 << NB]) {
+#define QG_1Q(K)                                                                     \
+    case K:                                                                          \
+        if constexpr (NB > K) group_1q<C, NB, K, CTRL>(v, m, b, off, g.lmask, g.lval); \
         break;
-#define QG_2Q(K0, K1)                                                                     \
-    case K0 * 4 + K1:                                                                     \
-        if constexpr (NB > K0 && NB > K1) group_2q<C, NB, K0, K1>(v, m, b, off, g.lmask, g.lval); \
+#define QG_2Q(K0, K1)                                                                           \
+    case K0 * 4 + K1:                                                                           \
+        if constexpr (NB > K0 && NB > K1)                                                       \
+            group_2q<C, NB, K0, K1, CTRL>(v, m, b, off, g.lmask, g.lval);                       \
         break;
     if (g.op == 1) {
         switch (g.k0) { QG_1Q(0) QG_1Q(1) QG_1Q(2) }
@@ -119,6 +133,13 @@ __device__ __forceinline__ void group_gate(C (&v)[1 << NB], const TileGate& g, c
     }
 #undef QG_1Q
 #undef QG_2Q
+}
+
+template <typename C, int NB>
+__device__ __forceinline__ void group_gate(C (&v)[1 << NB], const TileGate& g, const C* m,
+                                           uint32_t b, const uint32_t (&off)[1 << NB]) {
+    if (g.lmask) group_gate_c<C, NB, true>(v, g, m, b, off);
+    else group_gate_c<C, NB, false>(v, g, m, b, off);
 }
 
 // One sweep over the tile: groups of 2^NB amplitudes through registers. The

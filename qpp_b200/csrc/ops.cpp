@@ -2,6 +2,9 @@
 #include "ops.hpp"
 
 #include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 
@@ -341,32 +344,70 @@ static bool kron_factor_16(const std::vector<cd>& S, cd* A, cd* B) {
     return true;
 }
 
+// Superoperators of recently applied Kraus sets, keyed by their bytes: a
+// channel applied at every step of a circuit is built (and factored) once,
+// as qpp keeps one copy of each distinct gate matrix (cmat_hash_tbl_,
+// qcircuit.hpp:102-136).
+namespace {
+struct ChannelEntry {
+    std::vector<cd> Ks; // the key, compared in full
+    uint64_t DA = 0;
+    std::vector<cd> S;
+    bool factored = false;
+    cd A[16], B[16];
+};
+std::mutex g_chan_mu;
+std::vector<std::shared_ptr<ChannelEntry>> g_chan; // most recent last
+constexpr size_t kChanCache = 32;
+
+std::shared_ptr<ChannelEntry> channel_of(const cd* Ks, uint32_t nK, uint64_t DA) {
+    const size_t len = size_t(nK) * DA * DA;
+    {
+        std::lock_guard<std::mutex> lock(g_chan_mu);
+        for (size_t i = g_chan.size(); i-- > 0;) {
+            const auto& e = g_chan[i];
+            if (e->DA == DA && e->Ks.size() == len &&
+                std::memcmp(e->Ks.data(), Ks, len * sizeof(cd)) == 0)
+                return e;
+        }
+    }
+    auto e = std::make_shared<ChannelEntry>();
+    e->Ks.assign(Ks, Ks + len);
+    e->DA = DA;
+    const uint64_t DS = DA * DA;
+    e->S.assign(DS * DS, 0.0);
+    for (uint32_t i = 0; i < nK; ++i) {
+        std::vector<cd> K(Ks + size_t(i) * DA * DA, Ks + size_t(i + 1) * DA * DA);
+        std::vector<cd> t = kron_mat(conj_mat(K), DA, K, DA);
+        for (size_t j = 0; j < t.size(); ++j) e->S[j] += t[j];
+    }
+    if (DA == 4) e->factored = kron_factor_16(e->S, e->A, e->B);
+    std::lock_guard<std::mutex> lock(g_chan_mu);
+    if (g_chan.size() >= kChanCache) g_chan.erase(g_chan.begin());
+    g_chan.push_back(e);
+    return e;
+}
+} // namespace
+
 void op_apply_kraus(qgpu_state* s, const cd* Ks, uint32_t nK, uint64_t DA,
                     const std::vector<uint64_t>& target) {
     uint64_t DS = DA * DA;
     if (DS > 4096)
         raise(QGPU_ERR_NOT_SUPPORTED, "qpp::apply()",
               "Kraus superoperator above 4096 x 4096");
-    std::vector<cd> S(DS * DS, 0.0);
-    for (uint32_t i = 0; i < nK; ++i) {
-        std::vector<cd> K(Ks + size_t(i) * DA * DA, Ks + size_t(i + 1) * DA * DA);
-        std::vector<cd> t = kron_mat(conj_mat(K), DA, K, DA);
-        for (size_t j = 0; j < t.size(); ++j) S[j] += t[j];
-    }
+    const std::shared_ptr<ChannelEntry> ch = channel_of(Ks, nK, DA);
+    const std::vector<cd>& S = ch->S;
     VSpace vs = vspace_of(s);
     int n = int(s->dims.size());
     // a product channel on two qubits of a density matrix: one pass with the
     // two 4 x 4 factors (half the arithmetic of the 16 x 16)
     if (s->kind == QGPU_RHO && DA == 4 && target.size() == 2 && s->dims[target[0]] == 2 &&
-        s->dims[target[1]] == 2) {
-        cd A[16], B[16];
-        if (kron_factor_16(S, A, B)) {
-            const int a = int(target[0]), b = int(target[1]);
-            const std::vector<int> kt = {a, n + a, b, n + b};
-            launch_apply_kron4(s->ctx, s->prec, s->data, plan_free(vs, kt, 0),
-                               target_offsets(vs, kt), A, B);
-            return;
-        }
+        s->dims[target[1]] == 2 && ch->factored) {
+        const int a = int(target[0]), b = int(target[1]);
+        const std::vector<int> kt = {a, n + a, b, n + b};
+        launch_apply_kron4(s->ctx, s->prec, s->data, plan_free(vs, kt, 0),
+                           target_offsets(vs, kt), ch->A, ch->B);
+        return;
     }
     std::vector<int> vt = as_int(target), rows = as_int(target, n);
     vt.insert(vt.end(), rows.begin(), rows.end());
