@@ -227,7 +227,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
             std::vector<char> good(n_inst, 0);
             pfor(reps.size(), [&](size_t k) {
                 try {
-                    qgpu::fused_prepare(states[reps[k]], circuits[reps[k]]);
+                    qgpu::rho_program_prepare(states[reps[k]], circuits[reps[k]]);
                     good[reps[k]] = 1;
                 } catch (const qgpu::Exc&) {
                     // not expressible in the fused form: stays as compiled

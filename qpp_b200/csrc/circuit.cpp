@@ -12,6 +12,7 @@
 
 qgpu_circuit::~qgpu_circuit() {
     if (dB) cudaFree(dB);
+    if (rho_dB) cudaFree(rho_dB);
 }
 
 namespace qgpu {
@@ -240,6 +241,42 @@ void apply_step(qgpu_state* s, const Step& st) {
     }
 }
 
+// Tensor-core images of the plan's blocks of 3-6 qubits (each executed as a
+// 6-qubit block, padded with identity on the lowest free qubits), uploaded
+// once: slot[i] >= 0 is block i's image in *dB (65536 bytes each).
+constexpr uint32_t kRhoTcMinQubits = 11;
+
+static void upload_tc_blocks(qgpu_ctx* ctx, std::vector<Block>& plan, uint32_t nq,
+                             unsigned char** dB, std::vector<int64_t>& slot) {
+    slot.assign(plan.size(), -1);
+    int64_t nslot = 0;
+    for (size_t i = 0; i < plan.size(); ++i)
+        if (plan[i].step < 0 && plan[i].qubits.size() >= 3) slot[i] = nslot++;
+    if (nslot == 0) return;
+    std::vector<float> host(size_t(nslot) * 128 * 128);
+    for (size_t i = 0; i < plan.size(); ++i) {
+        if (slot[i] < 0) continue;
+        const Block& b = plan[i];
+        std::vector<int> q6 = b.qubits;
+        for (int x = 0; int(q6.size()) < 6 && x < int(nq); ++x)
+            if (std::find(q6.begin(), q6.end(), x) == q6.end()) q6.push_back(x);
+        std::vector<cd> U6 = embed(b.U, b.qubits, q6);
+        plan[i].qubits = q6; // executed as a 6-qubit block
+        plan[i].U = U6;
+        fused6_matrix(U6.data(), host.data() + size_t(slot[i]) * 128 * 128);
+    }
+    float* tmp = nullptr;
+    QG_CUDA(cudaMalloc(&tmp, host.size() * sizeof(float)));
+    struct FreeTmp {
+        float* p;
+        ~FreeTmp() { cudaFree(p); }
+    } free_tmp{tmp};
+    QG_CUDA(cudaMemcpy(tmp, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
+    QG_CUDA(cudaMalloc(dB, size_t(nslot) * 65536));
+    fused6_images(ctx, tmp, *dB, int(nslot));
+    QG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
     if (c->plan_k != k) {
         c->plan = fuse(c->steps, c->nq, k);
@@ -251,35 +288,107 @@ static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
         c->block_slot.clear();
     }
     bool tc = s->prec == QGPU_C64 && c->nq >= 13 && k == 6;
-    if (!tc || c->dB) return;
-    c->block_slot.assign(c->plan.size(), -1);
-    int64_t nslot = 0;
-    for (size_t i = 0; i < c->plan.size(); ++i)
-        if (c->plan[i].step < 0 && c->plan[i].qubits.size() >= 3) c->block_slot[i] = nslot++;
-    if (nslot == 0) return;
-    std::vector<float> host(size_t(nslot) * 128 * 128);
-    for (size_t i = 0; i < c->plan.size(); ++i) {
-        if (c->block_slot[i] < 0) continue;
-        const Block& b = c->plan[i];
-        std::vector<int> q6 = b.qubits;
-        for (int x = 0; int(q6.size()) < 6 && x < int(c->nq); ++x)
-            if (std::find(q6.begin(), q6.end(), x) == q6.end()) q6.push_back(x);
-        std::vector<cd> U6 = embed(b.U, b.qubits, q6);
-        c->plan[i].qubits = q6; // executed as a 6-qubit block
-        c->plan[i].U = U6;
-        fused6_matrix(U6.data(), host.data() + size_t(c->block_slot[i]) * 128 * 128);
-    }
-    float* tmp = nullptr;
-    QG_CUDA(cudaMalloc(&tmp, host.size() * sizeof(float)));
-    struct FreeTmp {
-        float* p;
-        ~FreeTmp() { cudaFree(p); }
-    } free_tmp{tmp};
-    QG_CUDA(cudaMemcpy(tmp, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
-    QG_CUDA(cudaMalloc(&c->dB, size_t(nslot) * 65536));
-    fused6_images(s->ctx, tmp, c->dB, int(nslot));
-    QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    if (!tc || c->dB || !c->block_slot.empty()) return;
+    upload_tc_blocks(s->ctx, c->plan, c->nq, &c->dB, c->block_slot);
     c->plan_ctx = s->ctx;
+}
+
+// Runs a fused plan on a complex64 (virtual) qubit ket of nb bits: blocks with
+// an image on the tensor cores, the rest as dense passes, unfused steps as
+// they are. Launches only.
+static void launch_blocks(qgpu_state* s, const VSpace& vs, int nb, const std::vector<Block>& plan,
+                          const unsigned char* dB, const std::vector<int64_t>& slot,
+                          const std::vector<Step>& steps) {
+    const double* norm2 = nullptr; // |psi|^2 for the tensor-core passes' fp16 scale
+    for (size_t i = 0; i < plan.size(); ++i) {
+        const Block& b = plan[i];
+        if (b.step >= 0) {
+            apply_step(s, steps[size_t(b.step)]);
+            continue;
+        }
+        if (!slot.empty() && slot[i] >= 0) {
+            int tb[6];
+            for (int j = 0; j < 6; ++j) tb[j] = nb - 1 - b.qubits[size_t(j)];
+            if (!norm2) norm2 = fused_norm_prepare(s->ctx, s->data, s->elems);
+            launch_fused6_tc(s->ctx, s->data, nb, tb, dB + size_t(slot[i]) * 65536, norm2);
+            continue;
+        }
+        vapply(s, vs, b.qubits, {}, b.U.data(), uint64_t(1) << b.qubits.size());
+    }
+}
+
+// A density-matrix circuit as dense gates on the 2n virtual qubits [column
+// digits, row digits] of the column-major matrix (FP64): a 1-qubit gate U is
+// conj(U) (x) U on (column t, row t); a 2-qubit gate is conj(U) on the two
+// column digits and U on the two row digits; a 1- or 2-qubit channel is its
+// superoperator sum_i conj(K_i) (x) K_i on (column digits, row digits). False
+// when the circuit holds anything else.
+static bool rho_virtual_steps(const qgpu_circuit* c, std::vector<Step>& out) {
+    const uint64_t n = c->nq;
+    auto gate = [&](std::vector<uint64_t> t, std::vector<cd> U) {
+        Step v;
+        v.kind = StepKind::Gate;
+        v.target = std::move(t);
+        v.DU = uint64_t(1) << v.target.size();
+        v.U = std::move(U);
+        out.push_back(std::move(v));
+    };
+    for (const Step& st : c->steps) {
+        if (st.kind == StepKind::Nop) continue;
+        if (st.kind == StepKind::Gate && st.target.size() == 1 && st.DU == 2) {
+            gate({st.target[0], n + st.target[0]}, kron_mat(conj_mat(st.U), 2, st.U, 2));
+        } else if (st.kind == StepKind::Gate && st.target.size() == 2 && st.DU == 4) {
+            gate({st.target[0], st.target[1]}, conj_mat(st.U));
+            gate({n + st.target[0], n + st.target[1]}, st.U);
+        } else if (st.kind == StepKind::Channel && (st.target.size() == 1 || st.target.size() == 2) &&
+                   st.DU == (uint64_t(1) << st.target.size())) {
+            const uint64_t DA = st.DU, DS = DA * DA;
+            std::vector<cd> S(DS * DS, 0.0);
+            for (uint32_t i = 0; i < st.nK; ++i) {
+                std::vector<cd> K(st.U.begin() + ptrdiff_t(i * DA * DA),
+                                  st.U.begin() + ptrdiff_t((i + 1) * DA * DA));
+                std::vector<cd> t = kron_mat(conj_mat(K), DA, K, DA);
+                for (size_t j = 0; j < t.size(); ++j) S[j] += t[j];
+            }
+            std::vector<uint64_t> vt = st.target;
+            for (uint64_t q : st.target) vt.push_back(n + q);
+            gate(vt, S);
+        } else {
+            return false;
+        }
+    }
+    return true;
+}
+
+// The tensor-core form of a complex64 density matrix of n >= 11 qubits (no
+// reference counterpart): the virtual gates merged
+// into blocks of <= 6 virtual qubits (fuse), each block one split-FP16
+// tcgen05 pass over the matrix. Built once per circuit (and again after steps
+// are added). False when the circuit does not qualify.
+static bool rho_tc_prepare(qgpu_state* s, qgpu_circuit* c) {
+    // from 11 qubits on; below, the launch-bound passes of the 4-virtual-qubit
+    // form are as fast (depth-30 serving circuits, one B200: 8 qubits 0.65 vs
+    // 0.77 ms, 10 qubits 1.01 vs 1.06 ms, 12 qubits 9.4 vs 6.9 ms)
+    if (s->prec != QGPU_C64 || c->d != 2 || c->nq < kRhoTcMinQubits || 2 * c->nq > 62)
+        return false;
+    if (c->rho_tc_steps != c->steps.size()) {
+        if (c->rho_dB) {
+            cudaFree(c->rho_dB);
+            c->rho_dB = nullptr;
+        }
+        c->rho_slot.clear();
+        c->rho_plan.clear();
+        std::vector<Step> vsteps;
+        c->rho_tc_ok = rho_virtual_steps(c, vsteps);
+        if (c->rho_tc_ok) {
+            c->rho_plan = fuse(vsteps, 2 * c->nq, 6);
+            for (const Block& b : c->rho_plan)
+                if (b.step >= 0) c->rho_tc_ok = false; // every virtual step is a gate
+        }
+        if (c->rho_tc_ok) upload_tc_blocks(s->ctx, c->rho_plan, 2 * c->nq, &c->rho_dB, c->rho_slot);
+        c->rho_tc_steps = c->steps.size();
+    }
+    return c->rho_tc_ok;
 }
 
 // Fused form of a complex64 qubit density matrix (no reference counterpart).
@@ -293,7 +402,7 @@ static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
 // pair become a single 16 x 16 block, and every block is one in-place pass
 // over the matrix. Plain form: one pass per gate and per channel.
 // The program is built once per circuit (and again after steps are added).
-static void rho_prepare(qgpu_state* s, qgpu_circuit* c) {
+void rho_program_prepare(qgpu_state* s, qgpu_circuit* c) {
     if (c->rho_steps != c->steps.size()) {
         auto P = std::make_shared<TProgram>();
         if (compile_traj_rho(c, *P, 30)) fuse_blocks(*P, 4);
@@ -330,7 +439,13 @@ void launch_program(qgpu_state* s, const TProgram& P) {
 // Kets: qubits only; blocks of up to 6 qubits (complex64: 3-6 qubit blocks on
 // the tensor cores from 13 qubits on), 3 in complex128.
 void fused_prepare(qgpu_state* s, qgpu_circuit* c) {
-    if (s->kind == QGPU_RHO) return rho_prepare(s, c);
+    if (s->kind == QGPU_RHO) {
+        if (rho_tc_prepare(s, c)) {
+            ctx_error_flag(s->ctx); // allocated outside any capture
+            return;
+        }
+        return rho_program_prepare(s, c);
+    }
     if (c->d != 2)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
     prepare_plan(s, c, s->prec == QGPU_C64 ? 6 : 3);
@@ -338,26 +453,15 @@ void fused_prepare(qgpu_state* s, qgpu_circuit* c) {
 }
 
 void fused_launch(qgpu_state* s, qgpu_circuit* c) {
-    if (s->kind == QGPU_RHO) return launch_program(s, *c->rho_prog);
-    VSpace vs = vspace_ket(s->dims);
-    int nb = int(c->nq);
-    const double* norm2 = nullptr; // |psi|^2 for the tensor-core passes' fp16 scale
-    for (size_t i = 0; i < c->plan.size(); ++i) {
-        const Block& b = c->plan[i];
-        if (b.step >= 0) {
-            apply_step(s, c->steps[size_t(b.step)]);
-            continue;
+    if (s->kind == QGPU_RHO) {
+        if (c->rho_tc_ok && c->rho_tc_steps == c->steps.size()) {
+            launch_blocks(s, vspace_of(s), int(2 * c->nq), c->rho_plan, c->rho_dB, c->rho_slot,
+                          c->steps);
+            return;
         }
-        if (!c->block_slot.empty() && c->block_slot[i] >= 0) {
-            int tb[6];
-            for (int j = 0; j < 6; ++j) tb[j] = nb - 1 - b.qubits[size_t(j)];
-            if (!norm2) norm2 = fused_norm_prepare(s->ctx, s->data, s->elems);
-            launch_fused6_tc(s->ctx, s->data, nb, tb,
-                             c->dB + size_t(c->block_slot[i]) * 65536, norm2);
-            continue;
-        }
-        vapply(s, vs, b.qubits, {}, b.U.data(), uint64_t(1) << b.qubits.size());
+        return launch_program(s, *c->rho_prog);
     }
+    launch_blocks(s, vspace_ket(s->dims), int(c->nq), c->plan, c->dB, c->block_slot, c->steps);
 }
 
 void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_t count) {
@@ -382,7 +486,9 @@ void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first, uint64_
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form runs whole circuits");
     fused_prepare(s, c);
     fused_launch(s, c);
-    if (s->kind == QGPU_KET && !c->block_slot.empty() && fused_error(s->ctx))
+    const bool tc = s->kind == QGPU_KET ? !c->block_slot.empty()
+                                        : c->rho_tc_ok && !c->rho_slot.empty();
+    if (tc && fused_error(s->ctx))
         raise(QGPU_ERR_TIMEOUT, "qgpu_run_gates()", "tensor-core pass timed out");
 }
 

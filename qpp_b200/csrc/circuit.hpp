@@ -86,6 +86,14 @@ struct qgpu_circuit {
     // first rho_steps steps (steps are only ever appended)
     uint64_t rho_steps = ~uint64_t(0);
     std::shared_ptr<qgpu::TProgram> rho_prog; // null: the form does not apply
+    // fused density-matrix form on the tensor cores (complex64, 2n >= 13
+    // virtual qubits): superoperator blocks of <= 6 virtual qubits, built for
+    // the first rho_tc_steps steps
+    uint64_t rho_tc_steps = ~uint64_t(0);
+    bool rho_tc_ok = false;
+    std::vector<qgpu::Block> rho_plan;
+    unsigned char* rho_dB = nullptr;
+    std::vector<int64_t> rho_slot;
     ~qgpu_circuit();
 };
 
@@ -110,6 +118,10 @@ void run_gates(qgpu_state* s, qgpu_circuit* c, int form, uint64_t first,
 // run_gates' fused form would), fused_launch only enqueues kernels on
 // s->ctx->stream; the caller checks fused_error(ctx) once they have run.
 void fused_prepare(qgpu_state* s, qgpu_circuit* c);
+// The superoperator program of a complex64 density-matrix circuit (blocks of
+// <= 4 virtual qubits, c->rho_prog), as the batched block-layered launches
+// use it; raises QGPU_ERR_NOT_SUPPORTED when the circuit does not compile.
+void rho_program_prepare(qgpu_state* s, qgpu_circuit* c);
 void fused_launch(qgpu_state* s, qgpu_circuit* c);
 // One pass per instruction of a program of dense blocks (G1-G4 only) on a
 // complex64 qubit state: bit b of the program is qubit n - 1 - b of a ket,

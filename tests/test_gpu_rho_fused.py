@@ -1,7 +1,9 @@
 """Fused superoperator form of a complex64 density matrix (Circuit.run with
 FUSED on a RHO state; no reference counterpart): gates and 1- or 2-qubit
 channels become superoperators on the 2n virtual qubits, merged into blocks
-of at most 4 virtual qubits, one pass per block. Against the FP64 oracle
+of at most 4 virtual qubits, one pass per block; from 11 qubits into blocks
+of at most 6 virtual qubits, each a split-FP16 tcgen05 pass (checked at 12
+qubits against the plain complex128 form, itself checked against the oracle). Against the FP64 oracle
 (qpp's apply and Kraus apply restated) within 2e-5 relative in the max-norm
 (complex64 arithmetic); against the plain complex128 form on the GPU at 12
 qubits; fewer passes than the plain form; unsupported cases raise
