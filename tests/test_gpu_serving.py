@@ -4,8 +4,10 @@ A request's trajectories draw from Philox streams keyed by its own seed and
 shot index, and its state never shares memory with another request, so its
 samples and measurement dits must be identical whether it runs alone or in
 a mix that arrives while other work is on the GPU (tolerance: exact). The
-same holds on the engine path (density matrices). The plain mode serves the
-same requests one at a time.
+same holds on the engine path (density matrices), and for requests with many
+shots arriving among others (the batching lanes slice requests by shots and
+keep two launches in flight). The plain mode serves the same requests one at
+a time.
 """
 import time
 
@@ -20,8 +22,8 @@ def _pool():
     return sv.request_pool(24, seed=31, max_ket_qubits=16, max_rho_qubits=9)
 
 
-def _ket_request(n):
-    """A 16-qubit ket request (the per-CTA global-slot lane)."""
+def _ket_request(n, shots=30):
+    """A ket request of n qubits (16: the per-CTA global-slot lane)."""
     from qpp_b200 import serving as sv
     from qpp_b200.workloads import haar_unitary
     rng = np.random.default_rng(n)
@@ -34,7 +36,7 @@ def _ket_request(n):
             c.gate(haar_unitary(rng, 4), [int(perm[2 * i]), int(perm[2 * i + 1])])
         if layer == 2:
             c.measure([3], 0, destructive=False)
-    return sv.Request(c, sv.KET, n, 1e-3, 30, 2)
+    return sv.Request(c, sv.KET, n, 1e-3, shots, 2)
 
 
 def _rho_request():
@@ -56,7 +58,8 @@ def test_result_same_alone_and_in_mix():
     from qpp_b200 import serving as sv
     pool = _pool()
     probe = [r for r in pool if r.kind == sv.KET and r.n <= 14][:1] + \
-        [_ket_request(16)] + [_rho_request()]
+        [_ket_request(16)] + [_rho_request()] + [_ket_request(12, shots=900)] + \
+        [_ket_request(16, shots=700)]
     srv = sv.Server(0, mode=sv.BATCHED)
     alone = []
     for k, r in enumerate(probe):
@@ -66,8 +69,8 @@ def test_result_same_alone_and_in_mix():
     ids = []
     for k, r in enumerate(pool):
         ids.append(("fill", srv.submit(r.circuit, r.kind, r.p, r.shots, seed=9000 + k), r))
-        if k in (3, 9, 15):
-            j = (3, 9, 15).index(k)
+        if k in (3, 9, 15, 18, 21):
+            j = (3, 9, 15, 18, 21).index(k)
             pr = probe[j]
             ids.append(("probe", srv.submit(pr.circuit, pr.kind, pr.p, pr.shots, seed=500 + j), j))
         time.sleep(0.001)
