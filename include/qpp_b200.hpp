@@ -20,9 +20,10 @@
 //   qpp_b200::QFT / TFQ(A, d, swap)                         operations.hpp:2792, :2844
 //
 // Matrices are qpp_b200::cmat (column-major std::complex<double>, rows x
-// cols; a ket is D x 1). When Eigen is available the same functions accept
-// and return Eigen::MatrixXcd / VectorXcd, so code written against qpp::
-// compiles against qpp_b200:: unchanged. Errors throw
+// cols; a ket is D x 1). When <Eigen/Dense> is on the include path, every
+// function listed above also accepts Eigen matrices (Eigen::MatrixBase
+// expressions) and returns Eigen::MatrixXcd in place of cmat, so code
+// written against qpp:: compiles against qpp_b200:: unchanged. Errors throw
 // qpp_b200::exception::<QppName> carrying qpp's (where, what) strings.
 // Header-only; link with libqpp_b200.so.
 #ifndef QPP_B200_HPP_
@@ -474,7 +475,11 @@ inline cmat discard(const cmat& A, const std::vector<idx>& target, const std::ve
 }
 
 #ifdef QPP_B200_HAS_EIGEN
-// Eigen adapters: same calls on Eigen::MatrixXcd / VectorXcd.
+// Eigen adapters: every function above also takes Eigen matrices (any
+// Eigen::MatrixBase expression of complex or real scalars) and returns
+// Eigen::MatrixXcd where qpp returns a matrix, so code written against
+// qpp:: compiles against qpp_b200:: unchanged. Each adapter converts to a
+// column-major cmat, calls the function above and converts back.
 namespace detail {
 template <typename D>
 cmat from_eigen(const Eigen::MatrixBase<D>& m) {
@@ -490,16 +495,133 @@ inline Eigen::MatrixXcd to_eigen(const cmat& m) {
         for (idx i = 0; i < m.rows(); ++i) e(Eigen::Index(i), Eigen::Index(j)) = m(i, j);
     return e;
 }
+template <typename M>
+std::vector<cmat> from_eigen_list(const std::vector<M>& Ks) {
+    std::vector<cmat> r;
+    r.reserve(Ks.size());
+    for (const auto& K : Ks) r.push_back(from_eigen(K));
+    return r;
+}
+inline std::vector<Eigen::MatrixXcd> to_eigen_list(const std::vector<cmat>& v) {
+    std::vector<Eigen::MatrixXcd> r;
+    r.reserve(v.size());
+    for (const auto& m : v) r.push_back(to_eigen(m));
+    return r;
+}
 } // namespace detail
+
+// apply (operations.hpp:72, :386)
 template <typename D1, typename D2>
 Eigen::MatrixXcd apply(const Eigen::MatrixBase<D1>& s, const Eigen::MatrixBase<D2>& A,
                        const std::vector<idx>& target, const std::vector<idx>& dims) {
     return detail::to_eigen(apply(detail::from_eigen(s), detail::from_eigen(A), target, dims));
 }
+template <typename D1, typename D2>
+Eigen::MatrixXcd apply(const Eigen::MatrixBase<D1>& s, const Eigen::MatrixBase<D2>& A,
+                       const std::vector<idx>& target, idx d = 2) {
+    return detail::to_eigen(apply(detail::from_eigen(s), detail::from_eigen(A), target, d));
+}
+// applyCTRL / applyCTRL_fan (operations.hpp:616, :961)
+template <typename D1, typename D2>
+Eigen::MatrixXcd applyCTRL(const Eigen::MatrixBase<D1>& s, const Eigen::MatrixBase<D2>& A,
+                           const std::vector<idx>& ctrl, const std::vector<idx>& target,
+                           const std::vector<idx>& dims,
+                           std::optional<std::vector<idx>> shift = std::nullopt) {
+    return detail::to_eigen(
+        applyCTRL(detail::from_eigen(s), detail::from_eigen(A), ctrl, target, dims, shift));
+}
+template <typename D1, typename D2>
+Eigen::MatrixXcd applyCTRL_fan(const Eigen::MatrixBase<D1>& s, const Eigen::MatrixBase<D2>& A,
+                               const std::vector<idx>& ctrl, const std::vector<idx>& target,
+                               const std::vector<idx>& dims,
+                               std::optional<std::vector<idx>> shift = std::nullopt) {
+    return detail::to_eigen(
+        applyCTRL_fan(detail::from_eigen(s), detail::from_eigen(A), ctrl, target, dims, shift));
+}
+// apply with Kraus operators (operations.hpp:476)
+template <typename D, typename M>
+Eigen::MatrixXcd apply(const Eigen::MatrixBase<D>& rho, const std::vector<M>& Ks,
+                       const std::vector<idx>& target, const std::vector<idx>& dims) {
+    return detail::to_eigen(
+        apply(detail::from_eigen(rho), detail::from_eigen_list(Ks), target, dims));
+}
+// ptrace / ptranspose / syspermute (operations.hpp:1908, :2167, :2386)
 template <typename D>
 Eigen::MatrixXcd ptrace(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
                         const std::vector<idx>& dims) {
     return detail::to_eigen(ptrace(detail::from_eigen(A), target, dims));
+}
+template <typename D>
+Eigen::MatrixXcd ptranspose(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+                            const std::vector<idx>& dims) {
+    return detail::to_eigen(ptranspose(detail::from_eigen(A), target, dims));
+}
+template <typename D>
+Eigen::MatrixXcd syspermute(const Eigen::MatrixBase<D>& A, const std::vector<idx>& perm,
+                            const std::vector<idx>& dims) {
+    return detail::to_eigen(syspermute(detail::from_eigen(A), perm, dims));
+}
+// sample / measure_seq (instruments.hpp:856, :985)
+template <typename D>
+std::map<std::vector<idx>, idx> sample(idx num_samples, const Eigen::MatrixBase<D>& A,
+                                       const std::vector<idx>& target,
+                                       const std::vector<idx>& dims, uint64_t seed = 0) {
+    return sample(num_samples, detail::from_eigen(A), target, dims, seed);
+}
+template <typename D>
+std::tuple<std::vector<idx>, std::vector<double>, Eigen::MatrixXcd>
+measure_seq(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+            const std::vector<idx>& dims, bool destructive = true, uint64_t seed = 0) {
+    auto r = measure_seq(detail::from_eigen(A), target, dims, destructive, seed);
+    return {std::get<0>(r), std::get<1>(r), detail::to_eigen(std::get<2>(r))};
+}
+// measure with Kraus operators / in a basis (instruments.hpp:371, :587)
+template <typename D, typename M>
+std::tuple<idx, std::vector<double>, std::vector<Eigen::MatrixXcd>>
+measure(const Eigen::MatrixBase<D>& A, const std::vector<M>& Ks, const std::vector<idx>& target,
+        const std::vector<idx>& dims, bool destructive = true, uint64_t seed = 0) {
+    auto r = measure(detail::from_eigen(A), detail::from_eigen_list(Ks), target, dims,
+                     destructive, seed);
+    return {std::get<0>(r), std::get<1>(r), detail::to_eigen_list(std::get<2>(r))};
+}
+template <typename D1, typename D2>
+std::tuple<idx, std::vector<double>, std::vector<Eigen::MatrixXcd>>
+measure(const Eigen::MatrixBase<D1>& A, const Eigen::MatrixBase<D2>& V,
+        const std::vector<idx>& target, const std::vector<idx>& dims, bool destructive = true,
+        uint64_t seed = 0) {
+    auto r = measure(detail::from_eigen(A), detail::from_eigen(V), target, dims, destructive,
+                     seed);
+    return {std::get<0>(r), std::get<1>(r), detail::to_eigen_list(std::get<2>(r))};
+}
+// reset / discard (instruments.hpp:1148, :1243)
+template <typename D>
+Eigen::MatrixXcd reset(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+                       const std::vector<idx>& dims, uint64_t seed = 0) {
+    return detail::to_eigen(reset(detail::from_eigen(A), target, dims, seed));
+}
+template <typename D>
+Eigen::MatrixXcd discard(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+                         const std::vector<idx>& dims, uint64_t seed = 0) {
+    return detail::to_eigen(discard(detail::from_eigen(A), target, dims, seed));
+}
+// applyQFT / applyTFQ / QFT / TFQ (operations.hpp:2565, :2680, :2792, :2844)
+template <typename D>
+Eigen::MatrixXcd applyQFT(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+                          idx d = 2, bool swap = true) {
+    return detail::to_eigen(applyQFT(detail::from_eigen(A), target, d, swap));
+}
+template <typename D>
+Eigen::MatrixXcd applyTFQ(const Eigen::MatrixBase<D>& A, const std::vector<idx>& target,
+                          idx d = 2, bool swap = true) {
+    return detail::to_eigen(applyTFQ(detail::from_eigen(A), target, d, swap));
+}
+template <typename D>
+Eigen::MatrixXcd QFT(const Eigen::MatrixBase<D>& A, idx d = 2, bool swap = true) {
+    return detail::to_eigen(QFT(detail::from_eigen(A), d, swap));
+}
+template <typename D>
+Eigen::MatrixXcd TFQ(const Eigen::MatrixBase<D>& A, idx d = 2, bool swap = true) {
+    return detail::to_eigen(TFQ(detail::from_eigen(A), d, swap));
 }
 #endif
 

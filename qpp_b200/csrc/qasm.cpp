@@ -8,11 +8,12 @@
 //   known gates          one joint gate step with qpp's matrix (the
 //                        known_matrices table, qasm.hpp:55-200): cx id x y z
 //                        h s sdg t tdg rx ry rz cz cy swap ch ccx crz
-//   u3 / u2 / u1 / u0    one U step each (their qelib1 bodies are one U)
-//   other qelib1 gates   one joint gate step with the gate's matrix (cu1 cu3
-//                        crx cry cswap sx sxdg rxx rzz p cp u cu): qpp expands
-//                        these into several U / CX steps, which only matters
-//                        for noisy engines (noise is drawn before every step)
+//   u3 / u2 / u1 / u0 / r  one U step each (their qelib1 bodies are one U)
+//   cu1 cu3 cswap        their qelib1 bodies, one step per U or known gate, as
+//                        qpp expands them (noise is drawn before each step)
+//   crx cry sx sxdg rxx rzz p cp u cu
+//                        (not in qpp's qelib1; accepted here as extensions)
+//                        one joint gate step with the gate's matrix
 //   gate definitions     expanded at every call with the arguments bound
 //   measure q -> c       non-destructive single-qubit measurements
 //   reset q              one reset step over the arguments
@@ -186,9 +187,6 @@ const std::map<std::string, Builtin>& builtins() {
         Mat tof = ident(8);
         tof[6 + 8 * 6] = tof[7 + 8 * 7] = 0.0;
         tof[7 + 8 * 6] = tof[6 + 8 * 7] = 1.0;
-        Mat fred = ident(8);
-        fred[5 + 8 * 5] = fred[6 + 8 * 6] = 0.0;
-        fred[6 + 8 * 5] = fred[5 + 8 * 6] = 1.0;
         Mat cz = ident(4);
         cz[3 + 4 * 3] = -1.0;
         const Mat SX = mat2(C(0.5, 0.5), C(0.5, -0.5), C(0.5, -0.5), C(0.5, 0.5));
@@ -211,7 +209,6 @@ const std::map<std::string, Builtin>& builtins() {
         fixed("swap", 2, swap);
         fixed("ch", 2, controlled(H));
         fixed("ccx", 3, tof);
-        fixed("cswap", 3, fred);
         fixed("sx", 1, SX);
         fixed("sxdg", 1, adj(SX));
         m["rx"] = {1, 1, false, [](const std::vector<double>& a) { return gRX(a[0]); }};
@@ -226,9 +223,7 @@ const std::map<std::string, Builtin>& builtins() {
         m["u1"] = {1, 1, true, [](const std::vector<double>& a) { return gU(0, 0, a[0]); }};
         m["p"] = {1, 1, true, [](const std::vector<double>& a) { return gU(0, 0, a[0]); }};
         m["u0"] = {1, 1, true, [](const std::vector<double>&) { return gU(0, 0, 0); }};
-        m["cu1"] = {1, 2, false, [](const std::vector<double>& a) { return controlled(gU(0, 0, a[0])); }};
         m["cp"] = {1, 2, false, [](const std::vector<double>& a) { return controlled(gU(0, 0, a[0])); }};
-        m["cu3"] = {3, 2, false, [](const std::vector<double>& a) { return controlled(gU(a[0], a[1], a[2])); }};
         m["cu"] = {4, 2, false, [](const std::vector<double>& a) {
                        Mat u = gU(a[0], a[1], a[2]);
                        for (C& z : u) z *= std::exp(I1 * a[3]);
@@ -456,6 +451,47 @@ struct Parser {
                 p = g.body_begin;
                 while (p < g.body_end) body_stmt(env2, &loc);
                 p = save;
+            }
+            return;
+        }
+        // qelib1 gates that Quantum++'s reader expands into their bodies
+        // (the standard library text of qasmtools/include/qasmtools/parser/
+        // preprocessor.hpp:86-127, used when QASMTOOLS_QASM2_SPECS is not
+        // defined): one step per U / known gate of the body, so a noisy
+        // engine draws noise before each of them as qpp does
+        if (name == "cu1" || name == "cu3" || name == "cswap" || name == "r") {
+            const size_t np = name == "cu1" ? 1 : name == "cu3" ? 3 : name == "r" ? 2 : 0;
+            const size_t nq = name == "cswap" ? 3 : name == "r" ? 1 : 2;
+            if (params.size() != np || args.size() != nq)
+                fail(k, "wrong number of parameters or arguments for '" + name + "'");
+            const Mat cx = builtins().at("cx").m({});
+            for (size_t j = 0; j < width; ++j) {
+                const uint64_t a = at(0, j);
+                if (name == "r") { // u3(theta, phi - pi/2, -phi + pi/2)
+                    emit_gate(gU(params[0], params[1] - M_PI / 2, -params[1] + M_PI / 2), {a});
+                } else if (name == "cu1") {
+                    const uint64_t b2 = at(1, j);
+                    const double l = params[0];
+                    emit_gate(gU(0, 0, l / 2), {a});
+                    emit_gate(cx, {a, b2});
+                    emit_gate(gU(0, 0, -l / 2), {b2});
+                    emit_gate(cx, {a, b2});
+                    emit_gate(gU(0, 0, l / 2), {b2});
+                } else if (name == "cu3") {
+                    const uint64_t t = at(1, j);
+                    const double th = params[0], ph = params[1], l = params[2];
+                    emit_gate(gU(0, 0, (l + ph) / 2), {a});
+                    emit_gate(gU(0, 0, (l - ph) / 2), {t});
+                    emit_gate(cx, {a, t});
+                    emit_gate(gU(-th / 2, 0, -(ph + l) / 2), {t});
+                    emit_gate(cx, {a, t});
+                    emit_gate(gU(th / 2, ph, 0), {t});
+                } else { // cswap a, b, c: cx c,b; ccx a,b,c; cx c,b
+                    const uint64_t b2 = at(1, j), c2 = at(2, j);
+                    emit_gate(cx, {c2, b2});
+                    emit_gate(builtins().at("ccx").m({}), {a, b2, c2});
+                    emit_gate(cx, {c2, b2});
+                }
             }
             return;
         }

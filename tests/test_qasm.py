@@ -22,7 +22,7 @@ def test_broadcasting_and_builtins():
     assert steps("qreg q[2]; qreg r[2]; cx q, r;") == 2
     assert steps("qreg q[2]; qreg r[1]; cx q, r[0];") == 2
     assert steps("qreg q[3]; U(0.1, 0.2, 0.3) q[1]; CX q[0], q[2]; u2(0, pi) q[0];") == 3
-    assert steps("qreg q[3]; ccx q[0], q[1], q[2]; cswap q[2], q[0], q[1]; rzz(pi/3) q[0], q[1];") == 3
+    assert steps("qreg q[3]; ccx q[0], q[1], q[2]; rzz(pi/3) q[0], q[1];") == 2
     assert steps("qreg q[1]; rx(-pi/2 + 2*0.5^2) q[0]; rz(sqrt(2) * cos(pi)) q[0]; // comment\n") == 2
 
 
@@ -65,3 +65,15 @@ def test_header_and_includes():
         qb.Circuit.from_qasm("OPENQASM 3.0; qreg q[1];")
     with pytest.raises(qb.InvalidArgument):
         qb.Circuit.from_qasm('OPENQASM 2.0; include "other.inc"; qreg q[1];')
+
+
+def test_qelib1_bodies_expand_as_qpp_does():
+    """cu1, cu3 and cswap are not in qpp's table of known matrices, so qpp's
+    reader expands their qelib1 bodies (qasmtools' standard library,
+    qasmtools/include/qasmtools/parser/preprocessor.hpp:86-127): one step per
+    U or known gate, which is where a noisy engine draws noise; r is one U."""
+    assert steps("qreg q[2]; cu1(0.3) q[0], q[1];") == 5
+    assert steps("qreg q[2]; cu3(0.1, 0.2, 0.3) q[0], q[1];") == 6
+    assert steps("qreg q[3]; cswap q[2], q[0], q[1];") == 3
+    assert steps("qreg q[1]; r(0.4, 0.7) q[0];") == 1
+    assert steps("qreg a[2]; qreg b[2]; cu1(0.3) a, b;") == 10  # broadcast
