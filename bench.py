@@ -31,7 +31,9 @@ parity_30q = three gates of the circuit applied on the GPU to the seeded 2^30
 configs = (one GPU, rank 0) the other workloads of the metric: the 20-qubit
           ket gate sequence, the 12-qubit density-matrix subsystem ops, the
           batched uneven instances and the serving loop against the plain
-          form on the same requests, each with its CPU sample or oracle check.
+          form on the same requests, each with its CPU sample or oracle check;
+          on several GPUs, the batched instances sharded across the ranks by
+          free HBM (the job's time is the slowest rank's).
 
 --impl reference times that CPU restatement alone (qpp itself needs Eigen,
 absent here) on the same metric, one gate per step, in the circuit's 1q:2q mix.
@@ -579,6 +581,13 @@ def main():
         if psi.h:
             psi.free()
         configs = configs_leg(args, qb, torch, ctx, stream)
+    elif world > 1 and not args.no_configs:
+        # several GPUs: the batched instances split across the ranks by free
+        # HBM (every rank takes part; rank 0 reports the slowest rank's time)
+        from qpp_b200 import configs_bench as cb
+        if psi.h:
+            psi.free()
+        configs = {"config4_sharded": cb.config4_shard(ctx, torch, stream, dist)}
 
     if rank == 0:
         line = {

@@ -367,6 +367,64 @@ def config4(ctx, torch, stream, n_kets=2048, n_rho=512, depth=20):
     return res
 
 
+def config4_shard(ctx, torch, stream, dist=None, n_kets=2048, n_rho=512, depth=20):
+    """Config 4 split across the ranks of a job by free HBM (sharding.assign on
+    the instances' state bytes): every rank builds the same seeded instances,
+    keeps its own share and runs it as one graph launch. Returns this rank's
+    instance count and device milliseconds, and the job's slowest rank."""
+    from .serving import _depol
+    from .sharding import instance_bytes, shard_for_rank
+    rng = np.random.default_rng(4)
+    bank1 = [haar_unitary(rng, 2) for _ in range(64)]
+    bank2 = [haar_unitary(rng, 4) for _ in range(64)]
+    chan = _depol(0.005)
+    ns = [int(x) for x in rng.integers(10, 23, size=n_kets)]
+    nr = [int(x) for x in rng.integers(6, 12, size=n_rho)]
+    circs = [_layered(rng, n, depth, False, bank1, bank2, chan) for n in ns] + \
+            [_layered(rng, n, depth, True, bank1, bank2, chan) for n in nr]
+    kinds = [KET] * n_kets + [RHO] * n_rho
+    sizes = ns + nr
+    nbytes = [instance_bytes(k == KET, n, 8) for k, n in zip(kinds, sizes)]
+    free, _ = ctx.mem_info()
+    mine = shard_for_rank(nbytes, free, dist)
+    st = []
+    for i in mine:
+        if kinds[i] == KET:
+            st.append(State(ctx, KET, [2] * sizes[i], C64).fill_gaussian(100 + i))
+        else:
+            w = State(ctx, KET, [2] * sizes[i] + [8], C64).fill_gaussian(100 + i)
+            st.append(w.ptrace([sizes[i]]))
+            w.free()
+    my_circs = [circs[i] for i in mine]
+    firsts = {}
+    for j, i in enumerate(mine):
+        firsts.setdefault((kinds[i], sizes[i]), j)
+    warm = sorted(firsts.values())
+    if warm:
+        run_batch(ctx, [my_circs[j] for j in warm], [st[j] for j in warm], FUSED)
+    ctx.synchronize()
+    if dist is not None and dist.is_initialized():
+        dist.barrier()
+    a, b = _events(torch, stream)
+    a.record(stream)
+    if mine:
+        run_batch(ctx, my_circs, st, FUSED)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    job_ms = ms
+    if dist is not None and dist.is_initialized():
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        job_ms = float(t.item())
+    for x in st:
+        x.free()
+    return {"instances": len(circs), "mine": len(mine),
+            "my_state_bytes": int(sum(nbytes[i] for i in mine)), "my_ms": ms, "job_ms": job_ms,
+            "instances_per_s": len(circs) / (job_ms / 1e3),
+            "placement": "instances by state bytes over the ranks' free HBM (sharding.assign)"}
+
+
 def main():
     import argparse
 
