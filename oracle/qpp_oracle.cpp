@@ -11,7 +11,7 @@
 // Parity is pinned by the known-answer tests of the reference's own suite
 // (unit_tests/tests/operations.cpp:16-397, classes/gates.cpp:170-207,
 // entropies.cpp:103-108, qasm/qasm.cpp:82-94), restated in
-// tests/test_oracle_kats.py, and by dense Kronecker-expansion cross-checks.
+// tests/test_kats.py, and by dense Kronecker-expansion cross-checks.
 //
 // Layout: complex<double> interleaved, column-major, big-endian mixed radix
 // (include/qpp/internal/util.hpp:58-116). Every function cites the reference

@@ -20,8 +20,13 @@ using namespace qpp_b200;
 static int fails = 0;
 #define EXPECT(c)                                                          \
     do {                                                                   \
-        if (!(c)) {                                                        \
-            std::printf("FAIL %s:%d %s\n", __FILE__, __LINE__, #c);        \
+        try {                                                              \
+            if (!(c)) {                                                    \
+                std::printf("FAIL %s:%d %s\n", __FILE__, __LINE__, #c);    \
+                ++fails;                                                   \
+            }                                                              \
+        } catch (const std::exception& e) {                                \
+            std::printf("FAIL %s:%d %s: %s\n", __FILE__, __LINE__, #c, e.what()); \
             ++fails;                                                       \
         }                                                                  \
     } while (0)
@@ -77,7 +82,7 @@ static bool same(const Eigen::MatrixXcd& e, const cmat& c) {
     return true;
 }
 
-int main() {
+static int run() {
     const std::vector<idx> dims = {2, 3, 2, 2};
     const idx D = 24;
     Eigen::MatrixXcd psi = rand_mat(D, 1), rho = rand_mat(D, D);
@@ -92,8 +97,8 @@ int main() {
     EXPECT(same(applyCTRL(psi, U2, {0}, {2}, dims), applyCTRL(cpsi, cU2, {0}, {2}, dims)));
     EXPECT(same(applyCTRL(rho, U2, {2}, {3}, dims, std::vector<idx>{1}),
                 applyCTRL(crho, cU2, {2}, {3}, dims, std::vector<idx>{1})));
-    EXPECT(same(applyCTRL_fan(psi, U2, {1}, {0, 3}, dims),
-                applyCTRL_fan(cpsi, cU2, {1}, {0, 3}, dims)));
+    EXPECT(same(applyCTRL_fan(psi, U2, {2}, {0, 3}, dims),
+                applyCTRL_fan(cpsi, cU2, {2}, {0, 3}, dims)));
     // Kraus operators: an amplitude-damping pair on qubit 3
     const double g = 0.3;
     Eigen::MatrixXcd K0(2, 2), K1(2, 2);
@@ -152,4 +157,13 @@ int main() {
     }
     std::printf("eigen adapters ok\n");
     return 0;
+}
+
+int main() {
+    try {
+        return run();
+    } catch (const std::exception& e) {
+        std::printf("unexpected exception: %s\n", e.what());
+        return 1;
+    }
 }
