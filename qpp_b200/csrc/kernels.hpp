@@ -92,15 +92,25 @@ struct PermPlan {
     uint64_t in_stride[64];  // input offset of output bit j
     uint64_t foff;
     int nb, tb, nrest;
-    uint8_t tbits[12];   // tile bits, ascending (write order)
-    uint8_t tin[12];     // the same bits by ascending input stride (read order)
-    uint8_t tin_pos[12]; // position of tin[j] within tbits
+    uint8_t tbits[16];   // tile bits, ascending (write order)
+    uint8_t tin[16];     // the same bits by ascending input stride (read order)
+    uint8_t tin_pos[16]; // position of tin[j] within tbits
     uint8_t rest[64];    // output bits outside the tile, ascending
+    // shared-memory swizzle of tile positions, linear over GF(2): position p
+    // is stored at the XOR of swz_bit[q] over p's set bits q. It is p with
+    // some high bits folded into the bank-selecting low bits, chosen per plan
+    // so that the warp's scattered stores (read order) and its row reads
+    // (write order) both touch every bank group equally.
+    uint16_t swz_bit[16];
 };
-constexpr int kPermTileBits = 10;
-// false when a dimension is not a power of two or there are <= 10 bits
+constexpr int kPermTileBits = 10; // the smallest tile
+// false when a dimension is not a power of two or there are <= tile_bits
+// bits. The tile holds the out_low lowest output bits and then the bits of
+// smallest input stride up to tile_bits (10-12); elem_bytes (8 or 16) sets
+// how many low position bits select a bank group.
 bool plan_permute(const std::vector<uint64_t>& out_dims, const std::vector<uint64_t>& src,
-                  uint64_t fixed_off, PermPlan& P);
+                  uint64_t fixed_off, PermPlan& P, int elem_bytes = 16,
+                  int tile_bits = kPermTileBits, int out_low = 5);
 // the tiled form of launch_gather(plan_gather(out_dims, src, fixed_off));
 // false (nothing launched) when plan_permute does not apply
 bool launch_permute_tiled(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
@@ -136,115 +137,143 @@ void launch_gather(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
 // When every digit's dimension is a power of two, a gather is a permutation
 // of index bits: out[o] = in[foff + sum_j bit_j(o) * in_stride[j]]. A plain
 // gather writes densely but reads with the stride of whatever input digit
-// lands on the output's lowest bits. The tiled form moves 2^10 elements per
-// tile through shared memory: the tile's bits are the output's five lowest
-// bits and the five bits with the smallest input strides (then more low
-// output bits), so 32 consecutive elements are read and 32 consecutive
-// elements are written per warp access. Every offset is a sum over index
-// bits, so each comes from two 32-entry tables (the tile's read and write
-// orders) or two 128-entry tables plus a short loop (the tile number); a
-// thread's low-table entries are fixed. The next tile is copied in with
-// cp.async while the current one is written out, and tile positions are
-// XOR-swizzled (the low five bits take bits 5..9 too) so that both the
-// scattered stores into shared memory and the runs read from it spread over
-// the banks.
+// lands on the output's lowest bits. The tiled form moves 2^TB elements per
+// tile through shared memory: the tile's bits are the output's lowest bits
+// and the bits with the smallest input strides, so every warp access reads
+// 32 consecutive input elements and writes 32 consecutive output elements.
+// Every offset is a sum over index bits, split three ways: the lane's five
+// bits and the warp's bits give per-thread constants, the remaining bits a
+// small table shared by the CTA, and tile bases come from two 128-entry
+// tables plus a short loop. The next tile is copied in with cp.async while
+// the current one is written out. Tile positions are swizzled by the plan's
+// linear map, which folds high position bits into the bank-selecting low
+// bits wherever the warp's scattered stores would otherwise pile onto a few
+// bank groups.
 
-__device__ __forceinline__ uint32_t perm_swz(uint32_t p) { return p ^ ((p >> 5) & 31u); }
+__device__ __forceinline__ uint32_t perm_swz(const PermPlan& P, uint32_t p, int tb) {
+    uint32_t r = 0;
+    for (int q = 0; q < tb; ++q)
+        if ((p >> q) & 1u) r ^= P.swz_bit[q];
+    return r;
+}
 
-template <typename R>
-__global__ void __launch_bounds__(256)
+template <typename R, typename OFF, int TB, int NTHR>
+struct PermShape {
+    static constexpr uint32_t NT = 1u << TB, NW = NTHR / 32, E = NT / NTHR;
+    static constexpr int WB = NW == 8 ? 3 : NW == 16 ? 4 : 5; // warp bits
+    static constexpr size_t kTile = size_t(2) * NT * sizeof(Cplx<R>);
+    static constexpr size_t kSmem = kTile + 512 * sizeof(OFF) + E * (2 * sizeof(OFF) + 8);
+};
+
+template <typename R, typename OFF, int TB, int NTHR>
+__global__ void __launch_bounds__(NTHR)
     k_permute_tiled(const Cplx<R>* __restrict__ in, Cplx<R>* __restrict__ out,
                     const __grid_constant__ PermPlan P) {
     using C = Cplx<R>;
-    constexpr uint32_t NT = 1u << kPermTileBits; // 4 elements per thread of 256
-    __shared__ __align__(16) C tile[2][NT];
-    __shared__ uint64_t in_lo[32], in_hi[32];   // read order: input offsets
-    __shared__ uint32_t pos_lo[32], pos_hi[32]; // read order: write-order positions
-    __shared__ uint64_t out_lo[32], out_hi[32]; // write order: output offsets
-    __shared__ uint64_t tb_in[2][128], tb_out[2][128]; // tile number bits [0,7), [7,14)
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5;
+    using S = PermShape<R, OFF, TB, NTHR>;
+    constexpr uint32_t NT = S::NT, E = S::E;
+    constexpr int LB = 5 + S::WB; // bits of the thread (lane, warp); the rest index u
+    extern __shared__ __align__(16) unsigned char perm_smem[];
+    C* tile = reinterpret_cast<C*>(perm_smem);                  // [2][NT]
+    OFF* tb_in = reinterpret_cast<OFF*>(perm_smem + S::kTile);  // [2][128] tile number bits
+    OFF* tb_out = tb_in + 256;                                  // [2][128]
+    OFF* u_in = tb_out + 256;                                   // [E]
+    OFF* u_out = u_in + E;                                      // [E]
+    uint32_t* u_spos = reinterpret_cast<uint32_t*>(u_out + E);  // [E]
+    uint32_t* u_rpos = u_spos + E;                              // [E]
+    const int tid = threadIdx.x;
     const int r0 = P.nrest < 7 ? P.nrest : 7;
     const int r1 = P.nrest - r0 < 7 ? P.nrest - r0 : 7;
-    if (tid < 64) {
-        const int h = tid >> 5, i = tid & 31; // h: bits 0-4 or 5-9 of the tile index
-        uint64_t io = 0, oo = 0;
-        uint32_t po = 0;
-        for (int j = 0; j < 5; ++j)
-            if ((i >> j) & 1) {
-                io += P.in_stride[P.tin[5 * h + j]];
-                po |= 1u << P.tin_pos[5 * h + j];
-                oo |= uint64_t(1) << P.tbits[5 * h + j];
-            }
-        (h ? in_hi : in_lo)[i] = io;
-        (h ? pos_hi : pos_lo)[i] = po;
-        (h ? out_hi : out_lo)[i] = oo;
-    }
-    for (int i = tid; i < 256; i += nt) {
+    for (int i = tid; i < 256; i += NTHR) {
         const int h = i >> 7, x = i & 127, lo = h ? r0 : 0, cnt = h ? r1 : r0;
-        uint64_t bi = 0, bo = 0;
+        OFF bi = 0, bo = 0;
         for (int j = 0; j < cnt; ++j)
             if ((x >> j) & 1) {
-                bi += P.in_stride[P.rest[lo + j]];
-                bo |= uint64_t(1) << P.rest[lo + j];
+                bi += OFF(P.in_stride[P.rest[lo + j]]);
+                bo |= OFF(1) << P.rest[lo + j];
             }
-        tb_in[h][x] = bi;
-        tb_out[h][x] = bo;
+        tb_in[i] = bi;
+        tb_out[i] = bo;
     }
+    // element l of a tile: bits [0, LB) are the thread (lane + 32 warp), bits
+    // [LB, TB) the index u < E of its elements; in read order, l's bits are
+    // the tile bits by ascending input stride (input offset, swizzled
+    // position of the write-order element it is), in write order the tile
+    // bits ascending (output offset, swizzled position)
+    auto parts = [&](uint32_t l, int j0, int j1, OFF& io, OFF& oo, uint32_t& sp, uint32_t& rp) {
+        io = 0;
+        oo = 0;
+        uint32_t po = 0;
+        for (int j = j0; j < j1; ++j)
+            if ((l >> j) & 1u) {
+                io += OFF(P.in_stride[P.tin[j]]);
+                po |= 1u << P.tin_pos[j];
+                oo |= OFF(1) << P.tbits[j];
+            }
+        sp = perm_swz(P, po, TB);
+        rp = perm_swz(P, l, TB);
+    };
+    if (tid < int(E)) {
+        OFF io, oo;
+        uint32_t sp, rp;
+        parts(uint32_t(tid) << LB, LB, TB, io, oo, sp, rp);
+        u_in[tid] = io;
+        u_out[tid] = oo;
+        u_spos[tid] = sp;
+        u_rpos[tid] = rp;
+    }
+    OFF t_in, t_out;
+    uint32_t t_spos, t_rpos;
+    parts(uint32_t(tid), 0, LB, t_in, t_out, t_spos, t_rpos);
     __syncthreads();
     const uint64_t ntiles = uint64_t(1) << P.nrest;
     const uint64_t m0 = (uint64_t(1) << r0) - 1, m1 = (uint64_t(1) << r1) - 1;
-    auto base = [&](uint64_t t, uint64_t& bi, uint64_t& bo) {
-        bi = P.foff + tb_in[0][t & m0] + tb_in[1][(t >> r0) & m1];
-        bo = tb_out[0][t & m0] | tb_out[1][(t >> r0) & m1];
+    auto base = [&](uint64_t t, OFF& bi, OFF& bo) {
+        bi = OFF(P.foff) + tb_in[t & m0] + tb_in[128 + ((t >> r0) & m1)];
+        bo = tb_out[t & m0] | tb_out[128 + ((t >> r0) & m1)];
         for (int j = r0 + r1; j < P.nrest; ++j)
             if ((t >> j) & 1u) {
-                bi += P.in_stride[P.rest[j]];
-                bo |= uint64_t(1) << P.rest[j];
+                bi += OFF(P.in_stride[P.rest[j]]);
+                bo |= OFF(1) << P.rest[j];
             }
     };
-    // this thread moves read-order elements lane + 32 (w + 8u), u < 4, and
-    // write-order elements of the same form
-    const uint64_t my_in = in_lo[lane], my_out = out_lo[lane];
-    const uint32_t my_pos = pos_lo[lane];
-    auto issue = [&](uint64_t bi, C* buf) {
+    auto issue = [&](OFF bi, C* buf) {
+        const C* src = in + bi + t_in;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int h = w + 8 * u;
-            cp_async_elem(buf + perm_swz(my_pos | pos_hi[h]), in + bi + my_in + in_hi[h]);
-        }
+        for (uint32_t u = 0; u < E; ++u) cp_async_elem(buf + (t_spos ^ u_spos[u]), src + u_in[u]);
         cp_async_commit();
     };
     uint64_t t = blockIdx.x;
     if (t >= ntiles) return; // uniform across the CTA
-    uint64_t bi, bo;
+    OFF bi, bo;
     base(t, bi, bo);
-    issue(bi, tile[0]);
+    issue(bi, tile);
     for (int it = 0; t < ntiles; t += gridDim.x, ++it) {
-        const C* cur = tile[it & 1];
+        const C* cur = tile + (it & 1) * NT;
         const uint64_t tn = t + gridDim.x;
-        uint64_t bin = 0, bon = 0;
+        OFF bin = 0, bon = 0;
         if (tn < ntiles) {
             base(tn, bin, bon);
-            issue(bin, tile[(it + 1) & 1]);
+            issue(bin, tile + ((it + 1) & 1) * NT);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
+        C* dst = out + bo + t_out;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int h = w + 8 * u;
-            out[bo + my_out + out_hi[h]] = cur[perm_swz((uint32_t(h) << 5) | uint32_t(lane))];
-        }
+        for (uint32_t u = 0; u < E; ++u) dst[u_out[u]] = cur[t_rpos ^ u_rpos[u]];
         __syncthreads();
         bo = bon;
     }
 }
 
 bool plan_permute(const std::vector<uint64_t>& out_dims, const std::vector<uint64_t>& src,
-                  uint64_t fixed_off, PermPlan& P) {
+                  uint64_t fixed_off, PermPlan& P, int elem_bytes, int tile_bits, int out_low) {
     std::memset(&P, 0, sizeof(P));
     P.foff = fixed_off;
+    if (tile_bits < kPermTileBits || tile_bits > 12 || out_low < 5 || out_low > tile_bits)
+        return false;
     // output bits from the least significant digit up
     for (size_t v = out_dims.size(); v-- > 0;) {
         uint64_t d = out_dims[v];
@@ -254,15 +283,15 @@ bool plan_permute(const std::vector<uint64_t>& out_dims, const std::vector<uint6
             P.in_stride[P.nb++] = s;
         }
     }
-    if (P.nb < kPermTileBits + 1) return false;
-    P.tb = kPermTileBits;
-    uint64_t mask = 31; // the five lowest output bits
+    if (P.nb < tile_bits + 1) return false;
+    P.tb = tile_bits;
+    uint64_t mask = (uint64_t(1) << out_low) - 1; // the lowest output bits
     std::vector<int> by_in(P.nb);
     for (int j = 0; j < P.nb; ++j) by_in[j] = j;
     std::stable_sort(by_in.begin(), by_in.end(),
                      [&](int a, int b) { return P.in_stride[a] < P.in_stride[b]; });
-    for (int k = 0; k < 5; ++k) mask |= uint64_t(1) << by_in[k];
-    for (int j = 5; j < P.nb && __builtin_popcountll(mask) < P.tb; ++j) mask |= uint64_t(1) << j;
+    for (int k = 0; k < P.nb && __builtin_popcountll(mask) < P.tb; ++k)
+        mask |= uint64_t(1) << by_in[k];
     int c = 0, r = 0;
     for (int j = 0; j < P.nb; ++j) {
         if (mask >> j & 1u) P.tbits[c++] = uint8_t(j);
@@ -277,22 +306,97 @@ bool plan_permute(const std::vector<uint64_t>& out_dims, const std::vector<uint6
                 if (P.tbits[q] == uint8_t(j)) P.tin_pos[c] = uint8_t(q);
             ++c;
         }
+    // Swizzle. A warp access of 128 bytes per wavefront covers 128 /
+    // elem_bytes consecutive positions, so the low lb position bits pick the
+    // bank group. The row reads vary positions 0-4 across the lanes, which
+    // already covers the low lb bits. The scattered stores vary the positions
+    // tin_pos[0..4]; each of the low lb bits that none of them is takes the
+    // place of one of those positions above lb (folded in by XOR), so the
+    // stores cover every bank group too. The map is unipotent, hence a
+    // bijection of the tile.
+    const int lb = elem_bytes >= 16 ? 3 : 4;
+    bool have[4] = {false, false, false, false};
+    for (int j = 0; j < 5; ++j)
+        if (P.tin_pos[j] < lb) have[P.tin_pos[j]] = true;
+    for (int q = 0; q < P.tb; ++q) P.swz_bit[q] = uint16_t(1u << q);
+    int next = 0;
+    for (int j = 0; j < 5; ++j) {
+        const int q = P.tin_pos[j];
+        if (q < lb) continue;
+        while (next < lb && have[next]) ++next;
+        if (next >= lb) break;
+        P.swz_bit[q] = uint16_t((1u << q) | (1u << next));
+        have[next] = true;
+    }
     return true;
 }
+
+namespace {
+template <typename R, typename OFF, int TB, int NTHR>
+void permute_launch(qgpu_ctx* ctx, const void* in, void* out, const PermPlan& P) {
+    using S = PermShape<R, OFF, TB, NTHR>;
+    auto* kern = k_permute_tiled<R, OFF, TB, NTHR>;
+    // the shared-memory opt-in is a per-device attribute of each function
+    static std::mutex mu;
+    static bool attr_set[64] = {};
+    static int per_sm[64] = {};
+    const int dev = ctx->device;
+    int resident = 1;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+            QG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(S::kSmem)));
+            int occ = 0;
+            QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NTHR, S::kSmem));
+            if (dev >= 0 && dev < 64) {
+                attr_set[dev] = true;
+                per_sm[dev] = std::max(occ, 1);
+            }
+            resident = std::max(occ, 1);
+        } else {
+            resident = per_sm[dev];
+        }
+    }
+    const uint64_t ntiles = uint64_t(1) << P.nrest;
+    const int b = int(std::min<uint64_t>(ntiles, uint64_t(ctx->num_sms) * resident));
+    kern<<<b, NTHR, S::kSmem, ctx->stream>>>(static_cast<const Cplx<R>*>(in),
+                                               static_cast<Cplx<R>*>(out), P);
+}
+
+template <typename R, typename OFF>
+void permute_dispatch(qgpu_ctx* ctx, const void* in, void* out, const PermPlan& P) {
+    switch (P.tb) {
+    case 10: permute_launch<R, OFF, 10, 256>(ctx, in, out, P); break;
+    case 11: permute_launch<R, OFF, 11, 512>(ctx, in, out, P); break;
+    default: permute_launch<R, OFF, 12, 512>(ctx, in, out, P); break;
+    }
+}
+} // namespace
+
+// The tile shape: TB tile bits, the OUT lowest output bits among them.
+constexpr int kPermTileTB = 10, kPermTileOut = 5;
 
 bool launch_permute_tiled(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
                           const std::vector<uint64_t>& out_dims,
                           const std::vector<uint64_t>& src, uint64_t fixed_off) {
     PermPlan P;
-    if (!plan_permute(out_dims, src, fixed_off, P)) return false;
-    const uint64_t ntiles = uint64_t(1) << P.nrest;
-    const int b = int(std::min<uint64_t>(ntiles, uint64_t(ctx->num_sms) * 6));
-    if (prec == QGPU_C128)
-        k_permute_tiled<double><<<b, 256, 0, ctx->stream>>>(
-            static_cast<const double2*>(in), static_cast<double2*>(out), P);
-    else
-        k_permute_tiled<float><<<b, 256, 0, ctx->stream>>>(
-            static_cast<const float2*>(in), static_cast<float2*>(out), P);
+    if (!plan_permute(out_dims, src, fixed_off, P, prec == QGPU_C128 ? 16 : 8, kPermTileTB,
+                      kPermTileOut))
+        return false;
+    // 32-bit offsets when every input and output offset fits (the output has
+    // 2^nb elements; the input offsets are bounded by the fixed offset plus
+    // every stride)
+    uint64_t in_max = P.foff;
+    for (int j = 0; j < P.nb; ++j) in_max += P.in_stride[j];
+    const bool narrow = P.nb <= 31 && in_max < (uint64_t(1) << 31);
+    if (prec == QGPU_C128) {
+        if (narrow) permute_dispatch<double, uint32_t>(ctx, in, out, P);
+        else permute_dispatch<double, uint64_t>(ctx, in, out, P);
+    } else {
+        if (narrow) permute_dispatch<float, uint32_t>(ctx, in, out, P);
+        else permute_dispatch<float, uint64_t>(ctx, in, out, P);
+    }
     after_launch(ctx, "k_permute_tiled");
     return true;
 }

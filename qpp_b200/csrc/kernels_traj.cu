@@ -865,6 +865,11 @@ static int traj_per_sm(size_t smem) {
     return b;
 }
 
+int traj_resident_slots(qgpu_ctx* ctx, int n) {
+    traj_prepare();
+    return ctx->num_sms * traj_per_sm((size_t(1) << n) * sizeof(float2));
+}
+
 void launch_traj(qgpu_ctx* ctx, const TWork* dwork, int nwork, int nmax, uint32_t* ddits,
                  int maxcreg, uint64_t* dsamples, float2* ddump, TEvent* devents,
                  int max_events, float2* gscratch, cudaStream_t stream, int tile_bits) {

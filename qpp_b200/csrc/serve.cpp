@@ -16,7 +16,8 @@
 //           of its HBM footprint against the budget) into the next launch;
 //   lane 1  kets of 15-20 qubits: the same kernel with each CTA on its own
 //           slot of global scratch (HBM), batched the same way;
-//   lane 2  everything else, one request at a time: density matrices above
+//   lane 2  everything else, one request at a time on each of two workers
+//           (own contexts, highest stream priority): density matrices above
 //           7 qubits whose circuits are gates and channels only run in the
 //           fused superoperator form (qgpu_run_gates, QGPU_FORM_FUSED: a
 //           layer's gates and channel on one qubit pair are one 16 x 16 pass
@@ -34,9 +35,10 @@
 // request with more shots spans several launches and finishes when its last
 // shot lands. Every shot draws from its own Philox counter (request seed,
 // shot index), so the results do not depend on how the shots were split.
-// Each of these lanes keeps two launches in flight: the host builds and
-// enqueues the next batch while the current one runs, and collects results
-// from pinned memory.
+// Each register size of these lanes has its own stream and keeps up to two
+// launches in flight: sizes run side by side and land independently, the
+// host builds and enqueues the next launch while the current one runs, and
+// results come back through pinned memory.
 //
 // Latency is measured from submit to the moment the lane has the result on
 // the host.
@@ -126,11 +128,24 @@ struct Pending {
     PinnedBuf* pin = nullptr;
 };
 
+// One register size of a batching lane: its own context (stream), so sizes
+// run concurrently and land independently, with at most two launches in
+// flight and their pinned result buffers.
+struct ClassRun {
+    qgpu_ctx* ctx = nullptr;
+    PinnedBuf pin[2];
+    int next_pin = 0;
+    std::deque<Pending> inflight;
+    ~ClassRun() {
+        if (ctx) qgpu_ctx_destroy(ctx);
+    }
+};
+
 struct Lane {
     qgpu_ctx* ctx = nullptr;
     std::deque<Request*> q;
     std::thread th;
-    PinnedBuf pin[2]; // results of the (at most) two batches in flight
+    std::map<uint32_t, std::unique_ptr<ClassRun>> cls; // batching lanes, by register size
 };
 
 } // namespace qgpu
@@ -141,6 +156,14 @@ struct qgpu_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     qgpu::Lane lanes[3];
+    // lane 2's second worker: its own context, so a long density matrix does
+    // not hold the small ones behind it
+    qgpu_ctx* engine2 = nullptr;
+    std::thread engine2_th;
+    // the lazily built per-circuit forms (fused programs, tensor-core block
+    // images) are prepared under this lock, so two workers never build the
+    // same circuit's at once
+    std::mutex prep_mu;
     std::unordered_map<uint64_t, qgpu::Request*> all;
     bool stop = false;
     uint64_t next_id = 1;
@@ -181,7 +204,7 @@ void sample_rho(qgpu_ctx* ctx, const qgpu_state* fin, Request* r) {
 
 // A density matrix of gates and channels only, in the fused superoperator
 // form in complex64 from |0...0><0...0| (no measurement, so its dits stay 0).
-void run_rho_fused(qgpu_ctx* ctx, Request* r) {
+void run_rho_fused(qgpu_ctx* ctx, Request* r, std::mutex& prep_mu) {
     const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
     r->dits.assign(r->shots * nc, 0);
     r->samples.assign(r->shots, 0);
@@ -193,6 +216,10 @@ void run_rho_fused(qgpu_ctx* ctx, Request* r) {
     } dels{st};
     static const float one[2] = {1.0f, 0.0f};
     QG_CUDA(cudaMemcpyAsync(st->data, one, sizeof(one), cudaMemcpyHostToDevice, ctx->stream));
+    {
+        std::lock_guard<std::mutex> lock(prep_mu);
+        fused_prepare(st, r->c); // once per circuit; a no-op afterwards
+    }
     run_gates(st, r->c, 1, 0, r->c->steps.size());
     sample_rho(ctx, st, r);
 }
@@ -200,9 +227,9 @@ void run_rho_fused(qgpu_ctx* ctx, Request* r) {
 // Engine path: trajectories one shot at a time on the resident engine; a
 // density matrix evolves once (its noise is in the circuit's channels) and
 // the shots sample the final diagonal.
-void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec) {
+void run_engine(qgpu_ctx* ctx, Request* r, qgpu_prec prec, std::mutex& prep_mu) {
     if (r->fused_rho && prec == QGPU_C64) {
-        run_rho_fused(ctx, r);
+        run_rho_fused(ctx, r, prep_mu);
         return;
     }
     const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
@@ -458,24 +485,44 @@ void complete_batch(qgpu_server* S, Pending& pd) {
     }
 }
 
-// Shots of one request in one launch, and shots per launch of a lane. Small
-// launches let new arrivals in sooner but leave waves half full; measured on
-// the serving mix (one B200, Poisson 1000 req/s), 256-shot slices in launches
-// of two CTA waves cut the median latency from 87 to 12 ms but the
-// throughput from 482 to 307 circuits/s, so launches stay large: a slice
-// holds up to 4096 shots (every request of the mix whole) and a launch up to
-// 64 CTAs per SM.
+// Shots of one request in one launch, and shots per launch of a register
+// size. A launch's results land when its last trajectory ends, so a launch
+// is sized in waves of the device's resident CTAs for that size: with a
+// fixed 64 shots per SM, a 14-qubit launch (one resident CTA per SM) ran 64
+// trajectories per CTA back to back and held its first requests' results
+// for hundreds of milliseconds. Each size runs on its own stream with two
+// launches in flight, so short launches keep the device full. A slice holds
+// up to 4096 shots (every request of the mix whole).
 constexpr uint64_t kChunkShots = 4096;
-uint64_t lane_shot_budget(const qgpu_ctx* ctx, int lane) {
-    return uint64_t(ctx->num_sms) * (lane == 0 ? 64 : 16);
+constexpr uint64_t kLaunchWaves = 4;
+uint64_t class_shot_budget(qgpu_ctx* ctx, int lane, uint32_t n) {
+    if (lane == 0) return uint64_t(traj_resident_slots(ctx, int(n))) * kLaunchWaves;
+    return uint64_t(ctx->num_sms) * 16; // global slots: two waves of 8 per SM
 }
 
-void lane_loop(qgpu_server* S, int li) {
+// Lane 2's streams run at the device's highest priority: its requests are
+// single long runs whose passes fill the GPU, and under load the batching
+// lanes' many trajectory blocks would otherwise take most SMs as they free
+// up, so the density matrices (the oldest work in the queue) finish last.
+void raise_priority(qgpu_ctx* ctx) {
+    int least = 0, greatest = 0;
+    QG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    cudaStream_t s = nullptr;
+    QG_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest));
+    QG_CUDA(cudaStreamDestroy(ctx->stream)); // nothing has been queued on it yet
+    ctx->stream = s;
+}
+
+// Batching lanes (0 and 1). Each register size has its own stream
+// (ClassRun), so a long launch of one size (a few shots of an 18-qubit ket
+// hold a few SMs for tens of milliseconds) delays neither the other sizes'
+// launches nor their results. The lane thread admits shots in arrival order
+// into the next launch of each size that has fewer than two launches in
+// flight, and retires launches as their events complete (polled every
+// 100 us while any is in flight).
+void batching_loop(qgpu_server* S, int li) {
     Lane& L = S->lanes[li];
     cudaSetDevice(L.ctx->device);
-    const bool batching = li < 2;
-    std::deque<Pending> inflight; // batching lanes: at most two
-    int next_pin = 0;
     auto fail_chunks = [&](const std::vector<Chunk>& chunks, const Exc& e) {
         for (const Chunk& ch : chunks) {
             if (ch.r->done) continue;
@@ -487,9 +534,9 @@ void lane_loop(qgpu_server* S, int li) {
             fail(S, ch.r, e.code, e.where + ": " + e.what);
         }
     };
-    auto retire = [&] {
-        Pending pd = std::move(inflight.front());
-        inflight.pop_front();
+    auto retire_front = [&](ClassRun& C) {
+        Pending pd = std::move(C.inflight.front());
+        C.inflight.pop_front();
         std::vector<Chunk> all;
         for (auto& cl : pd.classes) all.insert(all.end(), cl.cs.begin(), cl.cs.end());
         try {
@@ -498,83 +545,132 @@ void lane_loop(qgpu_server* S, int li) {
             fail_chunks(all, e);
         }
     };
-    for (;;) {
-        std::vector<Request*> got;
-        std::vector<Chunk> chunks;
-        {
-            std::unique_lock<std::mutex> lock(S->mu);
-            if (inflight.empty())
-                S->cv_work.wait(lock, [&] { return S->stop || !L.q.empty(); });
-            if (S->stop && L.q.empty() && inflight.empty()) return;
-            if (!batching) {
-                got.push_back(L.q.front());
-                L.q.pop_front();
-            } else {
-                // shots of the waiting requests in arrival order, at most
-                // kChunkShots of each, within the launch's shot budget and the
-                // HBM budget estimate (per-CTA slots for >= 15 qubits, outputs
-                // otherwise); fully issued requests leave the queue
-                const uint64_t shot_budget = lane_shot_budget(L.ctx, li);
-                uint64_t used = 0, shots = 0;
-                for (auto it = L.q.begin(); it != L.q.end() && shots < shot_budget;) {
-                    Request* r = *it;
-                    const bool rho = r->kind != QGPU_KET;
-                    uint64_t ns = rho ? r->shots
-                                      : std::min<uint64_t>({r->shots - r->issued, kChunkShots,
-                                                            shot_budget - shots});
-                    const uint64_t work = rho ? 1 : ns;
-                    const uint64_t need = work * 64 + (r->prog->n > uint32_t(kTrajMaxQubits)
-                                                           ? (uint64_t(8) << r->prog->n) * 8
-                                                           : 0);
-                    if (!chunks.empty() && used + need > S->budget) break;
-                    if (r->issued == 0) {
-                        const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
-                        r->dits.assign(r->shots * nc, 0);
-                        r->samples.assign(r->shots, 0);
-                    }
-                    chunks.push_back({r, r->issued, ns});
-                    r->issued += ns;
-                    used += need;
-                    shots += work;
-                    if (r->issued == r->shots) it = L.q.erase(it);
-                    else ++it;
-                }
+    auto class_of = [&](uint32_t n) -> ClassRun& {
+        auto& slot = L.cls[n];
+        if (!slot) {
+            slot.reset(new ClassRun);
+            qgpu_status st = qgpu_ctx_create(L.ctx->device, &slot->ctx);
+            if (st != QGPU_OK) {
+                slot.reset();
+                raise(st, "qgpu_server", "class context");
             }
         }
-        auto t0 = Clock::now();
-        if (batching) {
-            if (!chunks.empty()) {
-                // the pinned slot of the batch two launches back is free once
-                // that batch is retired
-                if (inflight.size() >= 2) retire();
-                try {
-                    inflight.push_back(launch_batch(S, L.ctx, chunks, &L.pin[next_pin]));
-                    next_pin ^= 1;
-                } catch (const Exc& e) {
-                    fail_chunks(chunks, e);
+        return *slot;
+    };
+    for (;;) {
+        // results first: every launch whose event has completed
+        size_t inflight = 0;
+        for (auto& kv : L.cls) {
+            ClassRun& C = *kv.second;
+            while (!C.inflight.empty() && cudaEventQuery(C.inflight.front().done) != cudaErrorNotReady)
+                retire_front(C);
+            inflight += C.inflight.size();
+        }
+        std::map<uint32_t, std::vector<Chunk>> by_n;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            if (inflight == 0)
+                S->cv_work.wait(lock, [&] { return S->stop || !L.q.empty(); });
+            if (S->stop && L.q.empty() && inflight == 0) return;
+            // shots of the waiting requests in arrival order, at most
+            // kChunkShots of each, within each size's launch budget and the
+            // HBM budget estimate (per-CTA slots for >= 15 qubits, outputs
+            // otherwise); sizes with two launches in flight wait; fully
+            // issued requests leave the queue
+            std::map<uint32_t, uint64_t> shots_of, budget_of;
+            uint64_t used = 0;
+            for (auto it = L.q.begin(); it != L.q.end();) {
+                Request* r = *it;
+                const uint32_t n = r->prog->n;
+                auto c = L.cls.find(n);
+                if (c != L.cls.end() && c->second && c->second->inflight.size() >= 2) {
+                    ++it;
+                    continue;
                 }
+                auto bud = budget_of.find(n);
+                if (bud == budget_of.end())
+                    bud = budget_of.emplace(n, class_shot_budget(L.ctx, li, n)).first;
+                const uint64_t shot_budget = bud->second;
+                uint64_t& shots = shots_of[n];
+                if (shots >= shot_budget) {
+                    ++it;
+                    continue;
+                }
+                const bool rho = r->kind != QGPU_KET;
+                uint64_t ns = rho ? r->shots
+                                  : std::min<uint64_t>({r->shots - r->issued, kChunkShots,
+                                                        shot_budget - shots});
+                const uint64_t work = rho ? 1 : ns;
+                const uint64_t need = work * 64 + (n > uint32_t(kTrajMaxQubits)
+                                                       ? (uint64_t(8) << n) * 8
+                                                       : 0);
+                if (!by_n.empty() && used + need > S->budget) break;
+                if (r->issued == 0) {
+                    const uint32_t nc = std::max<uint32_t>(r->c->nc, 1);
+                    r->dits.assign(r->shots * nc, 0);
+                    r->samples.assign(r->shots, 0);
+                }
+                by_n[n].push_back({r, r->issued, ns});
+                r->issued += ns;
+                used += need;
+                shots += work;
+                if (r->issued == r->shots) it = L.q.erase(it);
+                else ++it;
             }
-            // with nothing new to launch (or two in flight), wait for the oldest
-            if (!inflight.empty() && (chunks.empty() || inflight.size() >= 2)) retire();
-        } else {
-            for (Request* r : got) {
-                try {
-                    run_engine(L.ctx, r, S->mode == 1 ? QGPU_C128 : QGPU_C64);
-                    finish(S, r);
-                } catch (const Exc& e) {
-                    fail(S, r, e.code, e.where + ": " + e.what);
-                }
+            if (by_n.empty() && inflight > 0)
+                S->cv_work.wait_for(lock, std::chrono::microseconds(100),
+                                    [&] { return S->stop; });
+        }
+        if (by_n.empty()) continue;
+        auto t0 = Clock::now();
+        for (auto& kv : by_n) {
+            try {
+                ClassRun& C = class_of(kv.first);
+                C.inflight.push_back(launch_batch(S, C.ctx, kv.second, &C.pin[C.next_pin]));
+                C.next_pin ^= 1;
+            } catch (const Exc& e) {
+                fail_chunks(kv.second, e);
             }
         }
         std::lock_guard<std::mutex> lock(S->mu);
-        if (batching) {
-            if (!chunks.empty()) ++S->batches;
-        } else {
-            S->engine_runs += got.size();
-        }
+        S->batches += by_n.size();
         S->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
     }
 }
+
+// Lane 2: one request at a time per worker on the resident engine (or the
+// fused density-matrix form); two workers, each with its own context, take
+// requests from the lane's queue in arrival order.
+void engine_loop(qgpu_server* S, int li, qgpu_ctx* ctx) {
+    Lane& L = S->lanes[li];
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            S->cv_work.wait(lock, [&] { return S->stop || !L.q.empty(); });
+            if (S->stop && L.q.empty()) return;
+            r = L.q.front();
+            L.q.pop_front();
+        }
+        auto t0 = Clock::now();
+        try {
+            run_engine(ctx, r, S->mode == 1 ? QGPU_C128 : QGPU_C64, S->prep_mu);
+            finish(S, r);
+        } catch (const Exc& e) {
+            fail(S, r, e.code, e.where + ": " + e.what);
+        }
+        std::lock_guard<std::mutex> lock(S->mu);
+        S->engine_runs += 1;
+        S->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
+    }
+}
+
+void lane_loop(qgpu_server* S, int li) {
+    if (li < 2) batching_loop(S, li);
+    else engine_loop(S, li, S->lanes[li].ctx);
+}
+
 
 } // namespace
 } // namespace qgpu
@@ -593,16 +689,20 @@ qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode, qgpu_s
         auto* S = new qgpu_server;
         S->mode = mode;
         S->budget = hbm_budget;
-        for (auto& L : S->lanes) {
-            qgpu_status st = qgpu_ctx_create(device, &L.ctx);
+        qgpu_ctx** ctxs[4] = {&S->lanes[0].ctx, &S->lanes[1].ctx, &S->lanes[2].ctx, &S->engine2};
+        for (int i = 0; i < 4; ++i) {
+            qgpu_status st = qgpu_ctx_create(device, ctxs[i]);
+            if (st == QGPU_OK && i >= 2)
+                st = qgpu::guarded([&] { qgpu::raise_priority(*ctxs[i]); });
             if (st != QGPU_OK) {
-                for (auto& M : S->lanes)
-                    if (M.ctx) qgpu_ctx_destroy(M.ctx);
+                for (int j = 0; j < 4; ++j)
+                    if (*ctxs[j]) qgpu_ctx_destroy(*ctxs[j]);
                 delete S;
                 raise(st, "qgpu_server_create()", "context");
             }
         }
         for (int i = 0; i < 3; ++i) S->lanes[i].th = std::thread(qgpu::lane_loop, S, i);
+        S->engine2_th = std::thread(qgpu::engine_loop, S, 2, S->engine2);
         *out = S;
     });
 }
@@ -700,8 +800,13 @@ qgpu_status qgpu_server_destroy(qgpu_server* S) {
         S->cv_work.notify_all();
         for (auto& L : S->lanes)
             if (L.th.joinable()) L.th.join();
+        if (S->engine2_th.joinable()) S->engine2_th.join();
         for (auto& kv : S->all) delete kv.second;
-        for (auto& L : S->lanes) qgpu_ctx_destroy(L.ctx);
+        for (auto& L : S->lanes) {
+            L.cls.clear();
+            qgpu_ctx_destroy(L.ctx);
+        }
+        qgpu_ctx_destroy(S->engine2);
         delete S;
     });
 }

@@ -66,6 +66,9 @@ constexpr int kServeMaxSlotQubits = 20;
 // CTAs (= scratch slots) for a launch of nwork trajectories of n qubits:
 // at most 8 per SM and at most 4 GiB of slots.
 int traj_global_grid(qgpu_ctx* ctx, int nwork, int n);
+// Resident CTAs of a launch of shared-memory trajectories of n <=
+// kTrajMaxQubits qubits: one wave of the device.
+int traj_resident_slots(qgpu_ctx* ctx, int n);
 // Raises the kernel's shared-memory limit once (outside any stream capture).
 void traj_prepare();
 

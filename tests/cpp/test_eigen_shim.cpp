@@ -135,7 +135,16 @@ static int run() {
         for (size_t i = 0; i < std::get<2>(a).size(); ++i)
             EXPECT(same(std::get<2>(a)[i], std::get<2>(b)[i]));
     }
-    EXPECT(same(reset(psi, {1}, dims, 6), reset(cpsi, {1}, dims, 6)));
+    EXPECT(same(reset(psi, {2}, dims, 6), reset(cpsi, {2}, dims, 6)));
+    // qpp's reset takes the i-th target's dimension from dims[i]
+    // (instruments.hpp:1190-1192), so a qutrit target in first place throws
+    bool reset_thrown = false;
+    try {
+        reset(psi, {1}, dims, 6);
+    } catch (const exception::MatrixMismatchSubsys& e) {
+        reset_thrown = e.where() == "qpp::apply()";
+    }
+    EXPECT(reset_thrown);
     EXPECT(same(discard(rho, {0, 2}, dims, 6), discard(crho, {0, 2}, dims, 6)));
     Eigen::MatrixXcd k = rand_mat(16, 1);
     const cmat ck = detail::from_eigen(k);

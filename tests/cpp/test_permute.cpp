@@ -23,14 +23,20 @@ static int fails = 0;
         }                                                                    \
     } while (0)
 
-static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& src,
-                  uint64_t in_count) {
+static void check_shape(const std::vector<uint64_t>& od, const std::vector<uint64_t>& src,
+                        uint64_t in_count, int tb, int wl) {
     PermPlan P;
-    EXPECT(plan_permute(od, src, 0, P));
     uint64_t count = 1;
     for (uint64_t d : od) count *= d;
+    if (count < (uint64_t(2) << tb)) {
+        EXPECT(!plan_permute(od, src, 0, P, 16, tb, wl));
+        return;
+    }
+    EXPECT(plan_permute(od, src, 0, P, 16, tb, wl));
     EXPECT((uint64_t(1) << P.nb) == count);
-    EXPECT(P.tb == kPermTileBits && P.nrest == P.nb - P.tb);
+    EXPECT(P.tb == tb && P.nrest == P.nb - P.tb);
+    // the wl lowest output bits are in the tile
+    for (int j = 0; j < wl; ++j) EXPECT(P.tbits[j] == j);
     const uint32_t NT = 1u << P.tb;
     std::vector<uint64_t> in_off(NT), out_off(NT);
     std::vector<uint32_t> pos_of(NT);
@@ -47,18 +53,17 @@ static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& 
         out_off[l] = oo;
         pos_of[l] = lo;
     }
-    // the low five output bits are in the tile (coalesced writes)
-    for (int j = 0; j < 5; ++j) EXPECT(P.tbits[j] == j);
-    // the kernel's split tables: every offset is a sum (or an OR) over index
-    // bits, so the low and high halves of a tile index combine exactly
+    // the kernel's split: every offset is a sum (or an OR) over index bits,
+    // so the lane's five bits and the rest of a tile index combine exactly
     {
-        uint64_t in_lo[32], in_hi[32], out_lo[32], out_hi[32];
-        uint32_t pos_lo[32], pos_hi[32];
+        const uint32_t NH = NT >> 5;
+        std::vector<uint64_t> in_lo(32), in_hi(NH), out_lo(32), out_hi(NH);
+        std::vector<uint32_t> pos_lo(32), pos_hi(NH);
         for (int h = 0; h < 2; ++h)
-            for (int i = 0; i < 32; ++i) {
+            for (uint32_t i = 0; i < (h ? NH : 32u); ++i) {
                 uint64_t io = 0, oo = 0;
                 uint32_t po = 0;
-                for (int j = 0; j < 5; ++j)
+                for (int j = 0; j < (h ? P.tb - 5 : 5); ++j)
                     if ((i >> j) & 1) {
                         io += P.in_stride[P.tin[5 * h + j]];
                         po |= 1u << P.tin_pos[5 * h + j];
@@ -73,10 +78,33 @@ static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& 
             EXPECT((pos_lo[l & 31] | pos_hi[l >> 5]) == pos_of[l]);
             EXPECT((out_lo[l & 31] | out_hi[l >> 5]) == out_off[l]);
         }
-        // the tile-position swizzle is a bijection
-        std::vector<uint8_t> hit(NT, 0);
-        for (uint32_t p = 0; p < NT; ++p) hit[p ^ ((p >> 5) & 31u)]++;
-        for (uint8_t x : hit) EXPECT(x == 1);
+        // the tile-position swizzle is a bijection, and every warp access of
+        // the kernel touches each bank group equally: 4 wavefronts for 16-byte
+        // elements (8 bank groups), 2 for 8-byte ones (16), for the scattered
+        // stores in read order (lanes over pos_lo) and the row reads in write
+        // order (lanes over positions 0-4)
+        for (int eb : {16, 8}) {
+            PermPlan Q;
+            EXPECT(plan_permute(od, src, 0, Q, eb, tb, wl));
+            auto swz = [&](uint32_t p) {
+                uint32_t r = 0;
+                for (int q = 0; q < Q.tb; ++q)
+                    if ((p >> q) & 1u) r ^= Q.swz_bit[q];
+                return r;
+            };
+            std::vector<uint8_t> hit(NT, 0);
+            for (uint32_t p = 0; p < NT; ++p) hit[swz(p)]++;
+            for (uint8_t x : hit) EXPECT(x == 1);
+            const uint32_t groups = eb == 16 ? 8 : 16, best = 32 / groups;
+            for (uint32_t h = 0; h < NH; ++h) {
+                std::vector<uint32_t> st(groups, 0), rd(groups, 0);
+                for (int lane = 0; lane < 32; ++lane) {
+                    st[swz(pos_lo[lane] | pos_hi[h]) % groups]++;
+                    rd[swz((uint32_t(h) << 5) | uint32_t(lane)) % groups]++;
+                }
+                for (uint32_t g = 0; g < groups; ++g) EXPECT(st[g] == best && rd[g] == best);
+            }
+        }
         // tile-number bases: two 7-bit tables plus the remaining bits
         const int r0 = std::min(P.nrest, 7), r1 = std::min(P.nrest - r0, 7);
         for (uint64_t t = 0; t < (uint64_t(1) << P.nrest); t += 1 + (t % 5)) {
@@ -130,6 +158,14 @@ static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& 
         }
     }
     for (uint64_t o = 0; o < count; ++o) EXPECT(written[o] == 1);
+}
+
+// the tile shapes the kernel supports: 10 bits with the 5 lowest output
+// bits (the launcher's), and wider tiles that keep more of them
+static void check(const std::vector<uint64_t>& od, const std::vector<uint64_t>& src,
+                  uint64_t in_count) {
+    const int shapes[][2] = {{10, 5}, {10, 7}, {11, 6}, {12, 7}, {12, 5}};
+    for (const auto& sh : shapes) check_shape(od, src, in_count, sh[0], sh[1]);
 }
 
 int main() {
