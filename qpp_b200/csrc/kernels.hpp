@@ -156,6 +156,11 @@ struct QftPlan {
     uint32_t E, Rsize, CZ, Glo, Flo, wmul, nW;
     int ntd, nr, nz, nod, M, a, k, d, sigma, inverse, pow2, glo_shift, flo_shift;
     double scale; // qubit passes: 2^(-M/2)
+    // complex64 8- and 6-step passes (k_qft_pass8): the tile bits that a
+    // base index's bits select in round A (the tile bits outside that
+    // round's, by ascending read stride) and in round B (by ascending write
+    // stride); set by the launcher
+    uint8_t q8a[12], q8b[12];
 };
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes);
 // The passes of one transform (qft.cpp): fold[i] = pass i reads the state

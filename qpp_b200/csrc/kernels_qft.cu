@@ -29,6 +29,8 @@
 // amplitudes of a base); the next tile is copied in with cp.async while the
 // current one is transformed. Qubit butterflies omit the 1/sqrt(2) of H; the
 // store multiplies by 2^(-M/2) once.
+#include <algorithm>
+
 #include "kernels.hpp"
 
 namespace qgpu {
@@ -112,6 +114,89 @@ __device__ __forceinline__ void qubit_round(const QftPlan& p, Cplx<R>* tile,
         for (int m = 0; m < (1 << G); ++m) tile[eb | (uint32_t(m) << lo)] = v[m];
     }
 }
+
+// The same rounds with the pass shape known at compile time (M steps, NR run
+// bits, a tile of E = 2^(M + NR) amplitudes, roots W[e * 2^WS]): every bit
+// position, mask and trip count folds into the instructions. Used for the
+// shapes that full transforms of up to 30+ qubits consist of.
+template <typename R, int G, bool INV, int M, int NR, int WS, int JF, int NTHR>
+__device__ __forceinline__ void qubit_round_ct(Cplx<R>* tile, const Cplx<R>* T,
+                                               const Cplx<R>* B, const Cplx<R>* W,
+                                               uint32_t CZ) {
+    using C = Cplx<R>;
+    constexpr int JLOW = INV ? JF : JF + G - 1; // the step on the lowest bit
+    constexpr int LO = NR + M - 1 - JLOW;
+    constexpr uint32_t LOM = (1u << LO) - 1;
+    constexpr uint32_t NB = (1u << (M + NR)) >> G; // bases per tile
+    static_assert(NB % NTHR == 0, "bases per thread");
+    C cj[G];
+#pragma unroll
+    for (int u = 0; u < G; ++u) cj[u] = B[INV ? JF - u : JF + u];
+#pragma unroll
+    for (uint32_t q0 = 0; q0 < NB; q0 += NTHR) {
+        const uint32_t q = q0 + threadIdx.x;
+        const uint32_t eb = ((q & ~LOM) << G) | (q & LOM);
+        const C* cc = T + (eb & (CZ - 1));
+        const uint32_t grp = eb >> NR; // the group digits of the base
+        C v[1 << G];
+#pragma unroll
+        for (int m = 0; m < (1 << G); ++m) v[m] = tile[eb | (uint32_t(m) << LO)];
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+            const int j = INV ? JF - u : JF + u;
+            const int rel = INV ? u : G - 1 - u;
+            const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
+            const C cju = cmul(cj[u], cc[j * CZ]);
+            C ph[1 << (G - 1)];
+#pragma unroll
+            for (int lb = 0; lb < (1 << (G - 1)); ++lb) {
+                if (lb >= (1 << rel)) break;
+                const uint32_t L = (grp + (uint32_t(lb) << (LO - NR))) & Lmask;
+                ph[lb] = cmul(W[(L << j) << WS], cju);
+            }
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) {
+                if ((m >> rel) & 1) continue;
+                const int m1 = m | (1 << rel);
+                const C phm = ph[m & ((1 << rel) - 1)];
+                if (!INV) {
+                    const C x = v[m], y = v[m1];
+                    v[m] = cadd(x, y);
+                    v[m1] = cmul(csub(x, y), phm);
+                } else {
+                    const C x = v[m], y = cmul(v[m1], phm);
+                    v[m] = cadd(x, y);
+                    v[m1] = csub(x, y);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < (1 << G); ++m) tile[eb | (uint32_t(m) << LO)] = v[m];
+    }
+}
+
+// All rounds of a pass of shape (M, NR): three steps per round, the last
+// round takes the remainder; a barrier after each round.
+template <typename R, bool INV, int M, int NR, int WS, int S0, int NTHR>
+__device__ __forceinline__ void qubit_rounds_ct(Cplx<R>* tile, const Cplx<R>* T,
+                                                const Cplx<R>* B, const Cplx<R>* W,
+                                                uint32_t CZ) {
+    if constexpr (S0 < M) {
+        constexpr int G = M - S0 < 3 ? M - S0 : 3;
+        constexpr int JF = INV ? M - 1 - S0 : S0;
+        qubit_round_ct<R, G, INV, M, NR, WS, JF, NTHR>(tile, T, B, W, CZ);
+        __syncthreads();
+        qubit_rounds_ct<R, INV, M, NR, WS, S0 + 3, NTHR>(tile, T, B, W, CZ);
+    }
+}
+
+// the compile-time pass shapes: (M, NR) with E = 2^(M + NR) amplitudes per
+// tile (4096 in complex64, 2048 in complex128) and Mmax = 8
+template <typename R>
+struct QftShapes {
+    static constexpr int kE = sizeof(R) == 4 ? 12 : 11; // log2 of the tile
+    static constexpr int kNR8 = kE - 8, kNR6 = kE - 6;
+};
 
 } // namespace
 
@@ -210,6 +295,16 @@ __global__ void __launch_bounds__(256, 2)
     };
 
     const uint32_t Rs = p.Rsize, CZ = p.CZ;
+    // a compile-time pass shape (1: M = 8, 2: M = 6 with roots every 4th
+    // entry) when the plan is one, else 0: the runtime rounds
+    int shape = 0;
+    if constexpr (QB) {
+        using SH = QftShapes<R>;
+        if (nt == 256 && p.E == (1u << SH::kE)) {
+            if (p.M == 8 && p.nr == SH::kNR8 && p.wmul == 1) shape = 1;
+            else if (p.M == 6 && p.nr == SH::kNR6 && p.wmul == 4) shape = 2;
+        }
+    }
     uint64_t t = blockIdx.x;
     if (t >= p.ntiles) return;
     uint64_t rb, wb, z;
@@ -254,6 +349,16 @@ __global__ void __launch_bounds__(256, 2)
             // up to three consecutive steps per round in registers: step j
             // sits on tile bit nr + M - 1 - j, so the round's bits are
             // contiguous; each thread takes the 2^G amplitudes of a base
+            using SH = QftShapes<R>;
+            const C* Tc = cst;
+            const C* Bc = cst + M * CZ;
+            if (shape == 1) {
+                if (p.inverse) qubit_rounds_ct<R, true, 8, SH::kNR8, 0, 0, 256>(tile, Tc, Bc, W, CZ);
+                else qubit_rounds_ct<R, false, 8, SH::kNR8, 0, 0, 256>(tile, Tc, Bc, W, CZ);
+            } else if (shape == 2) {
+                if (p.inverse) qubit_rounds_ct<R, true, 6, SH::kNR6, 2, 0, 256>(tile, Tc, Bc, W, CZ);
+                else qubit_rounds_ct<R, false, 6, SH::kNR6, 2, 0, 256>(tile, Tc, Bc, W, CZ);
+            } else
             for (int s0 = 0; s0 < M; s0 += 3) {
                 const int G = M - s0 < 3 ? M - s0 : 3;
                 const int jf = p.inverse ? M - 1 - s0 : s0;
@@ -327,6 +432,247 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
+// Complex64 qubit passes of M = 8 or 6 steps over 2^12-amplitude tiles
+// (12 - M run bits): two rounds of G = M / 2 steps in registers. Each
+// thread copies the amplitudes of its round-A bases (cp.async, one tile
+// ahead) into the tile buffer at the positions it will read them from,
+// transforms them, writes them back to the same positions (no other thread
+// reads those in round A), and after one barrier reads its round-B bases,
+// transforms them and stores them straight to global memory. Round A holds
+// the steps on the tile bits [loA, loA + G), round B the rest (forward: steps
+// 0..G-1 then G..M-1; inverse: M-1..G then G-1..0). A thread's index bits
+// pick the other tile bits in ascending read stride for round A and in
+// ascending write stride for round B, so the copies and the stores run over
+// the smallest strides, also in the pass that reverses the targets (reading
+// one buffer, writing another). The buffer is swizzled (tile bits 4-7 folded
+// into 0-3) so that either order hits distinct banks. The phases are those
+// of qubit_round_ct.
+namespace {
+constexpr int kQ8E = 12, kQ8T = 256;
+
+__device__ __forceinline__ uint32_t q8_swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
+
+// G steps of a round on the 2^G amplitudes of base eb (round bits [lo, lo+G))
+template <bool INV, int G, int M>
+__device__ __forceinline__ void q8_round(float2* v, uint32_t eb, int lo, int jf,
+                                         const float2* T, const float2* B, const float2* W,
+                                         uint32_t CZ) {
+    constexpr int NR = kQ8E - M, WS = 8 - M; // roots: W[e * 2^WS], 2^8 of them
+    const float2* cc = T + (eb & (CZ - 1));
+    const uint32_t grp = eb >> NR;
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+        const int j = INV ? jf - u : jf + u;
+        const int rel = INV ? u : G - 1 - u;
+        const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
+        const float2 cju = cmul(B[j], cc[j * CZ]);
+        // one phase per value lb of the round bits below the step's bit,
+        // applied to the pairs with that value before the next is formed
+#pragma unroll
+        for (int lb = 0; lb < (1 << (G - 1)); ++lb) {
+            if (lb >= (1 << rel)) break;
+            const uint32_t L = (grp + (uint32_t(lb) << (lo - NR))) & Lmask;
+            const float2 phm = cmul(W[(L << j) << WS], cju);
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) {
+                if (((m >> rel) & 1) || (m & ((1 << rel) - 1)) != lb) continue;
+                const int m1 = m | (1 << rel);
+                if (!INV) {
+                    const float2 x = v[m], y = v[m1];
+                    v[m] = cadd(x, y);
+                    v[m1] = cmul(csub(x, y), phm);
+                } else {
+                    const float2 x = v[m], y = cmul(v[m1], phm);
+                    v[m] = cadd(x, y);
+                    v[m1] = csub(x, y);
+                }
+            }
+        }
+    }
+}
+} // namespace
+
+template <bool INV, typename OFF, int M>
+__global__ void __launch_bounds__(kQ8T, 2)
+    k_qft_pass8(const float2* in, float2* out, const __grid_constant__ QftPlan p,
+                const float2* __restrict__ Wg) {
+    constexpr int G = M / 2, NR = kQ8E - M;
+    constexpr int NQ = kQ8E - G;                 // tile bits outside a round
+    constexpr int BPT = (1 << NQ) / kQ8T;        // bases per thread per round
+    constexpr int QB = NQ - 8;                   // base index bits above the thread's
+    constexpr uint32_t E = 1u << kQ8E;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* bufs = reinterpret_cast<float2*>(smem_raw);      // [2][E]
+    float2* T = bufs + 2 * E;                                // M x CZ
+    const uint32_t CZ = p.CZ;
+    float2* Bs = T + M * CZ;                                 // [2][M] per-tile constants
+    float2* W = Bs + 2 * M;                                  // 2^8 roots
+    const int tid = threadIdx.x;
+    for (uint32_t i = tid; i < 256u; i += kQ8T) {
+        float2 w = Wg[i];
+        w.y *= float(p.sigma);
+        W[i] = w;
+    }
+    for (uint32_t i = tid; i < uint32_t(M) * CZ; i += kQ8T) {
+        const uint32_t c = i % CZ;
+        const int j = int(i / CZ);
+        uint64_t zz = 0;
+        for (int q = 0; q < p.nz; ++q) zz += uint64_t((c >> q) & 1u) * p.tzw[q];
+        double sn, cs;
+        sincospi(ldexp(double(zz), 1 - (p.k - p.a - j)), &sn, &cs);
+        T[i] = float2{float(cs), float(p.sigma * sn)};
+    }
+    auto tile_base = [&](uint64_t t, OFF& rb, OFF& wb, uint64_t& z) {
+        rb = wb = 0;
+        z = 0;
+        for (int q = 0; q < p.nod; ++q) {
+            const uint64_t dg = (t >> p.oshift[q]) & (p.odim[q] - 1);
+            rb += OFF(dg * p.ors[q]);
+            wb += OFF(dg * p.ows[q]);
+            z += dg * p.ozw[q];
+        }
+    };
+    auto set_b = [&](uint64_t z, float2* b) {
+        if (tid < M) {
+            double sn, cs;
+            sincospi(ldexp(double(z), 1 - (p.k - p.a - tid)), &sn, &cs);
+            b[tid] = float2{float(cs), float(p.sigma * sn)};
+        }
+    };
+    constexpr int loA = INV ? NR : NR + G, loB = INV ? NR + G : NR;
+    constexpr int jfA = INV ? M - 1 : 0, jfB = INV ? G - 1 : G;
+    // the thread's bases (index tid + 256 c, c < BPT) in each round
+    uint32_t ebA[BPT], ebB[BPT];
+    OFF oA[BPT], oB[BPT];
+#pragma unroll
+    for (int c = 0; c < BPT; ++c) {
+        const uint32_t q = uint32_t(tid) + (uint32_t(c) << 8);
+        uint32_t ea = 0, ew = 0;
+        for (int i = 0; i < NQ; ++i) {
+            ea |= ((q >> i) & 1u) << p.q8a[i];
+            ew |= ((q >> i) & 1u) << p.q8b[i];
+        }
+        OFF a = 0, w = 0;
+        for (int b = 0; b < kQ8E; ++b) {
+            if ((ea >> b) & 1u) a += OFF(p.trs[b]);
+            if ((ew >> b) & 1u) w += OFF(p.tws[b]);
+        }
+        ebA[c] = ea;
+        ebB[c] = ew;
+        oA[c] = a;
+        oB[c] = w;
+    }
+    (void)QB;
+    auto m_off = [&](const uint64_t* st, int lo, int m) {
+        OFF o = 0;
+#pragma unroll
+        for (int b = 0; b < G; ++b)
+            if ((m >> b) & 1) o += OFF(st[lo + b]);
+        return o;
+    };
+    // copies of a tile's round-A amplitudes into buffer `buf`
+    auto issue = [&](OFF rb, float2* buf) {
+#pragma unroll
+        for (int c = 0; c < BPT; ++c)
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m)
+                cp_async_elem(buf + q8_swz(ebA[c] | (uint32_t(m) << loA)),
+                              in + rb + oA[c] + m_off(p.trs, loA, m));
+        cp_async_commit();
+    };
+    __syncthreads();
+
+    uint64_t t = blockIdx.x;
+    if (t >= p.ntiles) return;
+    OFF rb, wb;
+    uint64_t z;
+    tile_base(t, rb, wb, z);
+    set_b(z, Bs);
+    issue(rb, bufs);
+    const float sc = float(p.scale);
+    for (int it = 0; t < p.ntiles; t += gridDim.x, ++it) {
+        const float2* B = Bs + (it & 1) * M;
+        float2* buf = bufs + (it & 1) * E;
+        cp_async_wait<0>();
+        // every thread is past the previous tile's round B: the other buffer
+        // and the other constant slot are free for the next tile
+        __syncthreads();
+        const uint64_t tn = t + gridDim.x;
+        OFF wbn = 0;
+        if (tn < p.ntiles) {
+            OFF rbn;
+            uint64_t zn;
+            tile_base(tn, rbn, wbn, zn);
+            set_b(zn, Bs + ((it + 1) & 1) * M);
+            issue(rbn, bufs + ((it + 1) & 1) * E);
+        }
+#pragma unroll
+        for (int c = 0; c < BPT; ++c) {
+            float2 v[1 << G];
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) v[m] = buf[q8_swz(ebA[c] | (uint32_t(m) << loA))];
+            q8_round<INV, G, M>(v, ebA[c], loA, jfA, T, B, W, CZ);
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) buf[q8_swz(ebA[c] | (uint32_t(m) << loA))] = v[m];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < BPT; ++c) {
+            float2 v[1 << G];
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) v[m] = buf[q8_swz(ebB[c] | (uint32_t(m) << loB))];
+            q8_round<INV, G, M>(v, ebB[c], loB, jfB, T, B, W, CZ);
+#pragma unroll
+            for (int m = 0; m < (1 << G); ++m) {
+                float2 x = v[m];
+                x.x *= sc;
+                x.y *= sc;
+                out[wb + oB[c] + m_off(p.tws, loB, m)] = x;
+            }
+        }
+        wb = wbn;
+    }
+}
+
+// whether k_qft_pass8 applies: complex64 qubits, 8 or 6 steps over tiles of
+// 2^12 amplitudes; in place, or (the pass that reverses the targets) into
+// another buffer
+static bool qft_pass8_applies(qgpu_prec prec, const void* in, const void* out,
+                              const QftPlan& p) {
+    if (prec != QGPU_C64 || p.d != 2 || (p.M != 8 && p.M != 6) || p.nr != kQ8E - p.M ||
+        p.E != (1u << kQ8E) || p.wmul != (1u << (8 - p.M)) || p.ntd != kQ8E || p.nW != 256u ||
+        !p.pow2)
+        return false;
+    bool same = true;
+    for (int q = 0; q < p.ntd; ++q) {
+        if (p.tdim[q] != 2) return false;
+        same = same && p.trs[q] == p.tws[q];
+    }
+    for (int q = 0; q < p.nod; ++q) same = same && p.ors[q] == p.ows[q];
+    return in != out || same;
+}
+
+// the thread-to-base maps of k_qft_pass8: the tile bits outside a round's
+// [lo, lo + G), by ascending stride
+static void qft_pass8_maps(QftPlan& p) {
+    const int G = p.M / 2, NR = kQ8E - p.M;
+    const int loA = p.inverse ? NR : NR + G, loB = p.inverse ? NR + G : NR;
+    auto fill = [&](int lo, const uint64_t* st, uint8_t* out) {
+        int bits[kQ8E], c = 0;
+        for (int b = 0; b < kQ8E; ++b)
+            if (b < lo || b >= lo + G) bits[c++] = b;
+        std::stable_sort(bits, bits + c, [&](int x, int y) { return st[x] < st[y]; });
+        for (int i = 0; i < c; ++i) out[i] = uint8_t(bits[i]);
+    };
+    fill(loA, p.trs, p.q8a);
+    fill(loB, p.tws, p.q8b);
+}
+
+static size_t qft_pass8_smem(const QftPlan& p) {
+    return (2 * (size_t(1) << kQ8E) + size_t(p.M) * p.CZ + 2 * size_t(p.M) + 256) *
+           sizeof(float2);
+}
+
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes) {
     return (2 * size_t(p.E) + size_t(p.M) * p.d * p.CZ + p.M + p.nW) * elem_bytes +
            (p.Glo + p.E / p.Glo + p.Flo + p.E / p.Flo) * (sizeof(uint64_t) + sizeof(uint32_t));
@@ -360,6 +706,29 @@ static void qft_launch(qgpu_ctx* ctx, const void* in, void* out, const QftPlan& 
 void launch_qft_pass(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
                      const QftPlan& p, const void* W, const void* F) {
     if (p.ntiles == 0) return;
+    if (qft_pass8_applies(prec, in, out, p)) {
+        QftPlan q = p;
+        qft_pass8_maps(q);
+        const size_t sm = qft_pass8_smem(q);
+        uint64_t blocks = uint64_t(grid_blocks(ctx, 2));
+        if (q.ntiles < blocks) blocks = q.ntiles;
+        // 32-bit offsets when the state has fewer than 2^31 amplitudes
+        const bool narrow = q.ntiles <= (uint64_t(1) << (31 - kQ8E));
+        using K = void (*)(const float2*, float2*, const QftPlan, const float2*);
+        K kern;
+        if (q.M == 8)
+            kern = narrow ? (q.inverse ? K(k_qft_pass8<true, uint32_t, 8>) : K(k_qft_pass8<false, uint32_t, 8>))
+                          : (q.inverse ? K(k_qft_pass8<true, uint64_t, 8>) : K(k_qft_pass8<false, uint64_t, 8>));
+        else
+            kern = narrow ? (q.inverse ? K(k_qft_pass8<true, uint32_t, 6>) : K(k_qft_pass8<false, uint32_t, 6>))
+                          : (q.inverse ? K(k_qft_pass8<true, uint64_t, 6>) : K(k_qft_pass8<false, uint64_t, 6>));
+        QG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        kern<<<unsigned(blocks), kQ8T, sm, ctx->stream>>>(static_cast<const float2*>(in),
+                                                          static_cast<float2*>(out), q,
+                                                          static_cast<const float2*>(W));
+        after_launch(ctx, "k_qft_pass8");
+        return;
+    }
     if (prec == QGPU_C128) qft_launch<double>(ctx, in, out, p, W, F);
     else qft_launch<float>(ctx, in, out, p, W, F);
 }

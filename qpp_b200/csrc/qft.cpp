@@ -180,7 +180,10 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
     for (int v : run)
         if (qidx[size_t(v)] >= b) CZ *= vs.dims[size_t(v)];
     // then the next lowest digits in read order while the tile fits: larger
-    // tiles spread the per-tile work over more amplitudes
+    // tiles spread the per-tile work over more amplitudes. The step-constant
+    // table stays within 256 entries, or 768 for complex64 qubits, whose
+    // 6-step passes then still fill 2^12-amplitude tiles (k_qft_pass8)
+    const uint64_t cz_cap = (d == 2 && Emax == 4096) ? 768 : 256;
     {
         std::vector<int> order(N);
         std::iota(order.begin(), order.end(), 0);
@@ -190,7 +193,7 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
             const uint64_t dim = vs.dims[size_t(v)];
             if (E * dim > Emax) break;
             const bool later = qidx[size_t(v)] >= b;
-            if (later && uint64_t(ps.M) * d * CZ * dim > 256) break;
+            if (later && uint64_t(ps.M) * d * CZ * dim > cz_cap) break;
             if (later) CZ *= dim;
             in_tile[size_t(v)] = 1;
             E *= dim;
@@ -351,15 +354,25 @@ bool plan_qft(bool rho, uint64_t D, uint64_t d, size_t elem_bytes,
     S.Mmax = Mmax;
     S.nW = 1;
     for (int e = 0; e < Mmax; ++e) S.nW *= d;
-    // group g covers targets [g * Mmax, min(k, (g + 1) * Mmax))
+    // groups of consecutive targets; in complex64 the partial one (k mod
+    // Mmax targets) comes first, so that the pass carrying the reversal (the
+    // last forward pass, the first inverse one) is a full one, which the
+    // register-round kernel takes: group g covers targets [start(g),
+    // start(g + 1))
     const size_t npass_half = (k + size_t(Mmax) - 1) / size_t(Mmax);
+    const size_t part = elem_bytes == 8 ? k % size_t(Mmax) : 0;
+    auto start = [&](size_t g) {
+        if (g == 0) return size_t(0);
+        return std::min(k, (part ? part : size_t(Mmax)) + (g - 1) * size_t(Mmax));
+    };
+    // (with part = 0 this is g * Mmax, capped at k)
     std::vector<PassSpec> passes;
     for (size_t h = 0; h < halves.size(); ++h) {
         for (size_t gi = 0; gi < npass_half; ++gi) {
             const size_t g = inverse ? npass_half - 1 - gi : gi;
             PassSpec ps;
-            ps.a = int(g * size_t(Mmax));
-            ps.M = int(std::min(k, (g + 1) * size_t(Mmax)) - g * size_t(Mmax));
+            ps.a = int(start(g));
+            ps.M = int(start(g + 1) - start(g));
             for (int j = 0; j < ps.M; ++j) ps.group.push_back(halves[h][size_t(ps.a + j)]);
             ps.sigma = hsig[h];
             ps.half = &halves[h];

@@ -75,7 +75,7 @@ def test_whole_qft_tfq(ctx):
 
 
 def test_resident_qft_c128_c64_and_pass_count(ctx):
-    """The resident op: 20 qubits in 3 passes (8 + 8 + 4 targets, the
+    """The resident op: 20 qubits in 3 passes (4 + 8 + 8 targets, the
     reversal riding on the last), matching numpy's DFT; complex64 too."""
     import qpp_b200 as qb
     rng = np.random.default_rng(11)
@@ -94,6 +94,45 @@ def test_resident_qft_c128_c64_and_pass_count(ctx):
     s64 = qb.State.from_numpy(ctx, psi, [2] * n, prec=qb.C64)
     s64.apply_qft(list(range(n)))
     assert relerr(s64.numpy(), ref) < TOL64
+
+
+@pytest.mark.parametrize("n", [14, 22])
+def test_pass_shapes_compiled_and_runtime(ctx, n):
+    """The passes of full transforms: 14 = 6 + 8 and 22 = 6 + 8 + 8 targets
+    (the 8-target pass that reverses the targets reads one buffer and writes
+    another), 6- and 8-target passes of 2^11 (complex128) and 2^12
+    (complex64) amplitudes; forward against numpy's DFT, inverse back to the
+    input, both precisions."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(100 + n)
+    psi = gaussian_ket(rng, 2 ** n)
+    ref = np.fft.ifft(psi) * np.sqrt(2 ** n)
+    for prec, tol in ((qb.C128, TOL128), (qb.C64, TOL64)):
+        s = qb.State.from_numpy(ctx, psi, [2] * n, prec=prec)
+        s.apply_qft(list(range(n)))
+        assert relerr(s.numpy(), ref) < tol, (prec, "qft")
+        s.apply_tfq(list(range(n)))
+        assert relerr(s.numpy(), psi) < tol, (prec, "tfq")
+        s.free()
+
+
+def test_complex64_density_matrix_passes(ctx):
+    """A complex64 density matrix of 8 qubits: U on the row digits and
+    conj(U) on the column digits, each an 8-step pass, against the oracle."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(808)
+    n = 8
+    rho = random_rho(rng, 2 ** n, 4)
+    for inverse in (False, True):
+        s = qb.State.from_numpy(ctx, rho, [2] * n, prec=qb.C64)
+        if inverse:
+            s.apply_tfq(list(range(n)))
+            ref = orc.applyTFQ(rho, list(range(n)), 2, True)
+        else:
+            s.apply_qft(list(range(n)))
+            ref = orc.applyQFT(rho, list(range(n)), 2, True)
+        assert relerr(s.numpy(), ref) < TOL64, inverse
+        s.free()
 
 
 def test_round_trip_26_qubits(ctx):
