@@ -56,8 +56,8 @@ static void run_pass(const QftPlan& p, size_t eb, const std::vector<cdd>& Wg,
     EXPECT(p.nW == Wg.size());
     for (int q = 0; q < p.nr; ++q) EXPECT((p.tzw[q] != 0) == (q < p.nz));
     max_smem = std::max(max_smem, qft_smem_bytes(p, eb));
-    // two CTAs per SM for complex128, three for complex64
-    EXPECT(qft_smem_bytes(p, eb) <= (eb == 16 ? 110 : 75) * 1024);
+    // two CTAs per SM (the kernel's launch bounds)
+    EXPECT(qft_smem_bytes(p, eb) <= 110 * 1024);
     const uint32_t Glo = p.Glo, Flo = p.Flo;
     std::vector<uint64_t> goff_lo(Glo), goff_hi(p.E / Glo), woff_lo(Flo), woff_hi(p.E / Flo);
     std::vector<uint32_t> ge_lo(Glo), ge_hi(p.E / Glo), we_lo(Flo), we_hi(p.E / Flo);
