@@ -432,57 +432,57 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
-// Complex64 qubit passes of M = 8 or 6 steps over 2^12-amplitude tiles
-// (12 - M run bits): two rounds of G = M / 2 steps in registers. Each
-// thread copies the amplitudes of its round-A bases (cp.async, one tile
-// ahead) into the tile buffer at the positions it will read them from,
-// transforms them, writes them back to the same positions (no other thread
-// reads those in round A), and after one barrier reads its round-B bases,
-// transforms them and stores them straight to global memory. Round A holds
-// the steps on the tile bits [loA, loA + G), round B the rest (forward: steps
-// 0..G-1 then G..M-1; inverse: M-1..G then G-1..0). A thread's index bits
-// pick the other tile bits in ascending read stride for round A and in
-// ascending write stride for round B, so the copies and the stores run over
-// the smallest strides, also in the pass that reverses the targets (reading
-// one buffer, writing another). The buffer is swizzled (tile bits 4-7 folded
-// into 0-3) so that either order hits distinct banks. The phases are those
-// of qubit_round_ct.
+// Qubit passes of M = 8 or 6 steps over tiles of 2^EB amplitudes (EB = 12
+// in complex64, 11 in complex128; EB - M run bits): two rounds of G = M / 2
+// steps in registers. Each thread copies the amplitudes of its round-A bases
+// (cp.async, one tile ahead) into the tile buffer at the positions it will
+// read them from, transforms them, writes them back to the same positions
+// (no other thread reads those in round A), and after one barrier reads its
+// round-B bases, transforms them and stores them straight to global memory.
+// Round A holds the steps on the tile bits [loA, loA + G), round B the rest
+// (forward: steps 0..G-1 then G..M-1; inverse: M-1..G then G-1..0). A
+// thread's index bits pick the other tile bits in ascending read stride for
+// round A and in ascending write stride for round B, so the copies and the
+// stores run over the smallest strides, also in the pass that reverses the
+// targets (reading one buffer, writing another). The buffer is swizzled (tile
+// bits 4-7 folded into 0-3) so that either order hits distinct banks. The
+// phases are those of qubit_round_ct.
 namespace {
-constexpr int kQ8E = 12, kQ8T = 256;
 
 __device__ __forceinline__ uint32_t q8_swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
 
 // G steps of a round on the 2^G amplitudes of base eb (round bits [lo, lo+G))
-template <bool INV, int G, int M>
-__device__ __forceinline__ void q8_round(float2* v, uint32_t eb, int lo, int jf,
-                                         const float2* T, const float2* B, const float2* W,
-                                         uint32_t CZ) {
-    constexpr int NR = kQ8E - M, WS = 8 - M; // roots: W[e * 2^WS], 2^8 of them
-    const float2* cc = T + (eb & (CZ - 1));
+template <typename R, bool INV, int G, int M, int EB>
+__device__ __forceinline__ void q8_round(Cplx<R>* v, uint32_t eb, int lo, int jf,
+                                         const Cplx<R>* T, const Cplx<R>* B,
+                                         const Cplx<R>* W, uint32_t CZ) {
+    using C = Cplx<R>;
+    constexpr int NR = EB - M, WS = 8 - M; // roots: W[e * 2^WS], 2^8 of them
+    const C* cc = T + (eb & (CZ - 1));
     const uint32_t grp = eb >> NR;
 #pragma unroll
     for (int u = 0; u < G; ++u) {
         const int j = INV ? jf - u : jf + u;
         const int rel = INV ? u : G - 1 - u;
         const uint32_t Lmask = (1u << (M - 1 - j)) - 1;
-        const float2 cju = cmul(B[j], cc[j * CZ]);
+        const C cju = cmul(B[j], cc[j * CZ]);
         // one phase per value lb of the round bits below the step's bit,
         // applied to the pairs with that value before the next is formed
 #pragma unroll
         for (int lb = 0; lb < (1 << (G - 1)); ++lb) {
             if (lb >= (1 << rel)) break;
             const uint32_t L = (grp + (uint32_t(lb) << (lo - NR))) & Lmask;
-            const float2 phm = cmul(W[(L << j) << WS], cju);
+            const C phm = cmul(W[(L << j) << WS], cju);
 #pragma unroll
             for (int m = 0; m < (1 << G); ++m) {
                 if (((m >> rel) & 1) || (m & ((1 << rel) - 1)) != lb) continue;
                 const int m1 = m | (1 << rel);
                 if (!INV) {
-                    const float2 x = v[m], y = v[m1];
+                    const C x = v[m], y = v[m1];
                     v[m] = cadd(x, y);
                     v[m1] = cmul(csub(x, y), phm);
                 } else {
-                    const float2 x = v[m], y = cmul(v[m1], phm);
+                    const C x = v[m], y = cmul(v[m1], phm);
                     v[m] = cadd(x, y);
                     v[m1] = csub(x, y);
                 }
@@ -490,37 +490,47 @@ __device__ __forceinline__ void q8_round(float2* v, uint32_t eb, int lo, int jf,
         }
     }
 }
+
+// the register-round pass shapes: tile bits and threads per CTA
+template <typename R>
+struct Q8Shape {
+    static constexpr int EB = sizeof(R) == 4 ? 12 : 11;
+    static constexpr int NTHR = sizeof(R) == 4 ? 256 : 128;
+    static constexpr int MINB = sizeof(R) == 4 ? 2 : 3; // resident CTAs per SM
+};
 } // namespace
 
-template <bool INV, typename OFF, int M>
-__global__ void __launch_bounds__(kQ8T, 2)
-    k_qft_pass8(const float2* in, float2* out, const __grid_constant__ QftPlan p,
-                const float2* __restrict__ Wg) {
-    constexpr int G = M / 2, NR = kQ8E - M;
-    constexpr int NQ = kQ8E - G;                 // tile bits outside a round
-    constexpr int BPT = (1 << NQ) / kQ8T;        // bases per thread per round
-    constexpr int QB = NQ - 8;                   // base index bits above the thread's
-    constexpr uint32_t E = 1u << kQ8E;
+template <typename R, bool INV, typename OFF, int M>
+__global__ void __launch_bounds__(Q8Shape<R>::NTHR, Q8Shape<R>::MINB)
+    k_qft_pass8(const Cplx<R>* in, Cplx<R>* out, const __grid_constant__ QftPlan p,
+                const Cplx<R>* __restrict__ Wg) {
+    using C = Cplx<R>;
+    constexpr int EB = Q8Shape<R>::EB, NTHR = Q8Shape<R>::NTHR;
+    constexpr int G = M / 2, NR = EB - M;
+    constexpr int NQ = EB - G;                   // tile bits outside a round
+    constexpr int BPT = (1 << NQ) / NTHR;        // bases per thread per round
+    static_assert(BPT >= 1, "bases per thread");
+    constexpr uint32_t E = 1u << EB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* bufs = reinterpret_cast<float2*>(smem_raw);      // [2][E]
-    float2* T = bufs + 2 * E;                                // M x CZ
+    C* bufs = reinterpret_cast<C*>(smem_raw);                // [2][E]
+    C* T = bufs + 2 * E;                                     // M x CZ
     const uint32_t CZ = p.CZ;
-    float2* Bs = T + M * CZ;                                 // [2][M] per-tile constants
-    float2* W = Bs + 2 * M;                                  // 2^8 roots
+    C* Bs = T + M * CZ;                                      // [2][M] per-tile constants
+    C* W = Bs + 2 * M;                                       // 2^8 roots
     const int tid = threadIdx.x;
-    for (uint32_t i = tid; i < 256u; i += kQ8T) {
-        float2 w = Wg[i];
-        w.y *= float(p.sigma);
+    for (uint32_t i = tid; i < 256u; i += NTHR) {
+        C w = Wg[i];
+        w.y *= R(p.sigma);
         W[i] = w;
     }
-    for (uint32_t i = tid; i < uint32_t(M) * CZ; i += kQ8T) {
+    for (uint32_t i = tid; i < uint32_t(M) * CZ; i += NTHR) {
         const uint32_t c = i % CZ;
         const int j = int(i / CZ);
         uint64_t zz = 0;
         for (int q = 0; q < p.nz; ++q) zz += uint64_t((c >> q) & 1u) * p.tzw[q];
         double sn, cs;
         sincospi(ldexp(double(zz), 1 - (p.k - p.a - j)), &sn, &cs);
-        T[i] = float2{float(cs), float(p.sigma * sn)};
+        T[i] = C{R(cs), R(p.sigma * sn)};
     }
     auto tile_base = [&](uint64_t t, OFF& rb, OFF& wb, uint64_t& z) {
         rb = wb = 0;
@@ -532,28 +542,28 @@ __global__ void __launch_bounds__(kQ8T, 2)
             z += dg * p.ozw[q];
         }
     };
-    auto set_b = [&](uint64_t z, float2* b) {
+    auto set_b = [&](uint64_t z, C* b) {
         if (tid < M) {
             double sn, cs;
             sincospi(ldexp(double(z), 1 - (p.k - p.a - tid)), &sn, &cs);
-            b[tid] = float2{float(cs), float(p.sigma * sn)};
+            b[tid] = C{R(cs), R(p.sigma * sn)};
         }
     };
     constexpr int loA = INV ? NR : NR + G, loB = INV ? NR + G : NR;
     constexpr int jfA = INV ? M - 1 : 0, jfB = INV ? G - 1 : G;
-    // the thread's bases (index tid + 256 c, c < BPT) in each round
+    // the thread's bases (index tid + NTHR c, c < BPT) in each round
     uint32_t ebA[BPT], ebB[BPT];
     OFF oA[BPT], oB[BPT];
 #pragma unroll
     for (int c = 0; c < BPT; ++c) {
-        const uint32_t q = uint32_t(tid) + (uint32_t(c) << 8);
+        const uint32_t q = uint32_t(tid) + uint32_t(c) * NTHR;
         uint32_t ea = 0, ew = 0;
         for (int i = 0; i < NQ; ++i) {
             ea |= ((q >> i) & 1u) << p.q8a[i];
             ew |= ((q >> i) & 1u) << p.q8b[i];
         }
         OFF a = 0, w = 0;
-        for (int b = 0; b < kQ8E; ++b) {
+        for (int b = 0; b < EB; ++b) {
             if ((ea >> b) & 1u) a += OFF(p.trs[b]);
             if ((ew >> b) & 1u) w += OFF(p.tws[b]);
         }
@@ -562,7 +572,6 @@ __global__ void __launch_bounds__(kQ8T, 2)
         oA[c] = a;
         oB[c] = w;
     }
-    (void)QB;
     auto m_off = [&](const uint64_t* st, int lo, int m) {
         OFF o = 0;
 #pragma unroll
@@ -571,7 +580,7 @@ __global__ void __launch_bounds__(kQ8T, 2)
         return o;
     };
     // copies of a tile's round-A amplitudes into buffer `buf`
-    auto issue = [&](OFF rb, float2* buf) {
+    auto issue = [&](OFF rb, C* buf) {
 #pragma unroll
         for (int c = 0; c < BPT; ++c)
 #pragma unroll
@@ -589,10 +598,10 @@ __global__ void __launch_bounds__(kQ8T, 2)
     tile_base(t, rb, wb, z);
     set_b(z, Bs);
     issue(rb, bufs);
-    const float sc = float(p.scale);
+    const R sc = R(p.scale);
     for (int it = 0; t < p.ntiles; t += gridDim.x, ++it) {
-        const float2* B = Bs + (it & 1) * M;
-        float2* buf = bufs + (it & 1) * E;
+        const C* B = Bs + (it & 1) * M;
+        C* buf = bufs + (it & 1) * E;
         cp_async_wait<0>();
         // every thread is past the previous tile's round B: the other buffer
         // and the other constant slot are free for the next tile
@@ -608,23 +617,23 @@ __global__ void __launch_bounds__(kQ8T, 2)
         }
 #pragma unroll
         for (int c = 0; c < BPT; ++c) {
-            float2 v[1 << G];
+            C v[1 << G];
 #pragma unroll
             for (int m = 0; m < (1 << G); ++m) v[m] = buf[q8_swz(ebA[c] | (uint32_t(m) << loA))];
-            q8_round<INV, G, M>(v, ebA[c], loA, jfA, T, B, W, CZ);
+            q8_round<R, INV, G, M, EB>(v, ebA[c], loA, jfA, T, B, W, CZ);
 #pragma unroll
             for (int m = 0; m < (1 << G); ++m) buf[q8_swz(ebA[c] | (uint32_t(m) << loA))] = v[m];
         }
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < BPT; ++c) {
-            float2 v[1 << G];
+            C v[1 << G];
 #pragma unroll
             for (int m = 0; m < (1 << G); ++m) v[m] = buf[q8_swz(ebB[c] | (uint32_t(m) << loB))];
-            q8_round<INV, G, M>(v, ebB[c], loB, jfB, T, B, W, CZ);
+            q8_round<R, INV, G, M, EB>(v, ebB[c], loB, jfB, T, B, W, CZ);
 #pragma unroll
             for (int m = 0; m < (1 << G); ++m) {
-                float2 x = v[m];
+                C x = v[m];
                 x.x *= sc;
                 x.y *= sc;
                 out[wb + oB[c] + m_off(p.tws, loB, m)] = x;
@@ -634,14 +643,14 @@ __global__ void __launch_bounds__(kQ8T, 2)
     }
 }
 
-// whether k_qft_pass8 applies: complex64 qubits, 8 or 6 steps over tiles of
-// 2^12 amplitudes; in place, or (the pass that reverses the targets) into
-// another buffer
+// whether k_qft_pass8 applies: qubits, 8 or 6 steps over tiles of 2^EB
+// amplitudes; in place, or (the pass that reverses the targets) into another
+// buffer
 static bool qft_pass8_applies(qgpu_prec prec, const void* in, const void* out,
                               const QftPlan& p) {
-    if (prec != QGPU_C64 || p.d != 2 || (p.M != 8 && p.M != 6) || p.nr != kQ8E - p.M ||
-        p.E != (1u << kQ8E) || p.wmul != (1u << (8 - p.M)) || p.ntd != kQ8E || p.nW != 256u ||
-        !p.pow2)
+    const int EB = prec == QGPU_C64 ? Q8Shape<float>::EB : Q8Shape<double>::EB;
+    if (p.d != 2 || (p.M != 8 && p.M != 6) || p.nr != EB - p.M || p.E != (1u << EB) ||
+        p.wmul != (1u << (8 - p.M)) || p.ntd != EB || p.nW != 256u || !p.pow2)
         return false;
     bool same = true;
     for (int q = 0; q < p.ntd; ++q) {
@@ -654,12 +663,12 @@ static bool qft_pass8_applies(qgpu_prec prec, const void* in, const void* out,
 
 // the thread-to-base maps of k_qft_pass8: the tile bits outside a round's
 // [lo, lo + G), by ascending stride
-static void qft_pass8_maps(QftPlan& p) {
-    const int G = p.M / 2, NR = kQ8E - p.M;
+static void qft_pass8_maps(QftPlan& p, int EB) {
+    const int G = p.M / 2, NR = EB - p.M;
     const int loA = p.inverse ? NR : NR + G, loB = p.inverse ? NR + G : NR;
     auto fill = [&](int lo, const uint64_t* st, uint8_t* out) {
-        int bits[kQ8E], c = 0;
-        for (int b = 0; b < kQ8E; ++b)
+        int bits[16], c = 0;
+        for (int b = 0; b < EB; ++b)
             if (b < lo || b >= lo + G) bits[c++] = b;
         std::stable_sort(bits, bits + c, [&](int x, int y) { return st[x] < st[y]; });
         for (int i = 0; i < c; ++i) out[i] = uint8_t(bits[i]);
@@ -668,9 +677,31 @@ static void qft_pass8_maps(QftPlan& p) {
     fill(loB, p.tws, p.q8b);
 }
 
-static size_t qft_pass8_smem(const QftPlan& p) {
-    return (2 * (size_t(1) << kQ8E) + size_t(p.M) * p.CZ + 2 * size_t(p.M) + 256) *
-           sizeof(float2);
+template <typename R>
+static void qft_pass8_launch(qgpu_ctx* ctx, const void* in, void* out, const QftPlan& p0,
+                             const void* W) {
+    using C = Cplx<R>;
+    using S = Q8Shape<R>;
+    QftPlan q = p0;
+    qft_pass8_maps(q, S::EB);
+    const size_t sm = (2 * (size_t(1) << S::EB) + size_t(q.M) * q.CZ + 2 * size_t(q.M) + 256) *
+                      sizeof(C);
+    uint64_t blocks = uint64_t(grid_blocks(ctx, S::MINB));
+    if (q.ntiles < blocks) blocks = q.ntiles;
+    // 32-bit offsets when the state has fewer than 2^31 amplitudes
+    const bool narrow = q.ntiles <= (uint64_t(1) << (31 - S::EB));
+    using K = void (*)(const C*, C*, const QftPlan, const C*);
+    K kern;
+    if (q.M == 8)
+        kern = narrow ? (q.inverse ? K(k_qft_pass8<R, true, uint32_t, 8>) : K(k_qft_pass8<R, false, uint32_t, 8>))
+                      : (q.inverse ? K(k_qft_pass8<R, true, uint64_t, 8>) : K(k_qft_pass8<R, false, uint64_t, 8>));
+    else
+        kern = narrow ? (q.inverse ? K(k_qft_pass8<R, true, uint32_t, 6>) : K(k_qft_pass8<R, false, uint32_t, 6>))
+                      : (q.inverse ? K(k_qft_pass8<R, true, uint64_t, 6>) : K(k_qft_pass8<R, false, uint64_t, 6>));
+    QG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    kern<<<unsigned(blocks), S::NTHR, sm, ctx->stream>>>(static_cast<const C*>(in),
+                                                         static_cast<C*>(out), q,
+                                                         static_cast<const C*>(W));
 }
 
 size_t qft_smem_bytes(const QftPlan& p, size_t elem_bytes) {
@@ -707,25 +738,8 @@ void launch_qft_pass(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
                      const QftPlan& p, const void* W, const void* F) {
     if (p.ntiles == 0) return;
     if (qft_pass8_applies(prec, in, out, p)) {
-        QftPlan q = p;
-        qft_pass8_maps(q);
-        const size_t sm = qft_pass8_smem(q);
-        uint64_t blocks = uint64_t(grid_blocks(ctx, 2));
-        if (q.ntiles < blocks) blocks = q.ntiles;
-        // 32-bit offsets when the state has fewer than 2^31 amplitudes
-        const bool narrow = q.ntiles <= (uint64_t(1) << (31 - kQ8E));
-        using K = void (*)(const float2*, float2*, const QftPlan, const float2*);
-        K kern;
-        if (q.M == 8)
-            kern = narrow ? (q.inverse ? K(k_qft_pass8<true, uint32_t, 8>) : K(k_qft_pass8<false, uint32_t, 8>))
-                          : (q.inverse ? K(k_qft_pass8<true, uint64_t, 8>) : K(k_qft_pass8<false, uint64_t, 8>));
-        else
-            kern = narrow ? (q.inverse ? K(k_qft_pass8<true, uint32_t, 6>) : K(k_qft_pass8<false, uint32_t, 6>))
-                          : (q.inverse ? K(k_qft_pass8<true, uint64_t, 6>) : K(k_qft_pass8<false, uint64_t, 6>));
-        QG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-        kern<<<unsigned(blocks), kQ8T, sm, ctx->stream>>>(static_cast<const float2*>(in),
-                                                          static_cast<float2*>(out), q,
-                                                          static_cast<const float2*>(W));
+        if (prec == QGPU_C64) qft_pass8_launch<float>(ctx, in, out, p, W);
+        else qft_pass8_launch<double>(ctx, in, out, p, W);
         after_launch(ctx, "k_qft_pass8");
         return;
     }

@@ -181,9 +181,9 @@ bool build_pass(const VSpace& vs, const PassSpec& ps, uint64_t d, size_t k,
         if (qidx[size_t(v)] >= b) CZ *= vs.dims[size_t(v)];
     // then the next lowest digits in read order while the tile fits: larger
     // tiles spread the per-tile work over more amplitudes. The step-constant
-    // table stays within 256 entries, or 768 for complex64 qubits, whose
-    // 6-step passes then still fill 2^12-amplitude tiles (k_qft_pass8)
-    const uint64_t cz_cap = (d == 2 && Emax == 4096) ? 768 : 256;
+    // table stays within 256 entries, or 768 for qubits, whose 6-step passes
+    // then still fill whole tiles (k_qft_pass8)
+    const uint64_t cz_cap = d == 2 ? 768 : 256;
     {
         std::vector<int> order(N);
         std::iota(order.begin(), order.end(), 0);
@@ -354,13 +354,13 @@ bool plan_qft(bool rho, uint64_t D, uint64_t d, size_t elem_bytes,
     S.Mmax = Mmax;
     S.nW = 1;
     for (int e = 0; e < Mmax; ++e) S.nW *= d;
-    // groups of consecutive targets; in complex64 the partial one (k mod
-    // Mmax targets) comes first, so that the pass carrying the reversal (the
-    // last forward pass, the first inverse one) is a full one, which the
+    // groups of consecutive targets; for qubits the partial one (k mod Mmax
+    // targets) comes first, so that the pass carrying the reversal (the last
+    // forward pass, the first inverse one) is a full one, which the
     // register-round kernel takes: group g covers targets [start(g),
     // start(g + 1))
     const size_t npass_half = (k + size_t(Mmax) - 1) / size_t(Mmax);
-    const size_t part = elem_bytes == 8 ? k % size_t(Mmax) : 0;
+    const size_t part = d == 2 ? k % size_t(Mmax) : 0;
     auto start = [&](size_t g) {
         if (g == 0) return size_t(0);
         return std::min(k, (part ? part : size_t(Mmax)) + (g - 1) * size_t(Mmax));
