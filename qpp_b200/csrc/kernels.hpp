@@ -182,6 +182,14 @@ std::vector<std::complex<double>> qft_roots(uint64_t nW);
 // F: the d x d Fourier matrix of the pass, column-major (qudits only).
 void launch_qft_pass(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
                      const QftPlan& p, const void* W, const void* F);
+// The register-round qubit passes (k_qft_pass8, which launch_qft_pass takes
+// when they apply): log2 of their tile (12 complex64, 11 complex128); whether
+// a plan is one of theirs (8 or 6 steps over a whole tile; in place, or
+// into another buffer); and the thread-to-base maps the launcher sets
+// (q8a, q8b) for a tile of 2^EB amplitudes.
+int qft_pass8_tile_bits(qgpu_prec prec);
+bool qft_pass8_applies(qgpu_prec prec, const void* in, const void* out, const QftPlan& p);
+void qft_pass8_maps(QftPlan& p, int EB);
 
 // --- reductions and elementwise (kernels_reduce.cu) ----------------------
 // sum |x|^2 over n elements, FP64 accumulation; result to *host_out.

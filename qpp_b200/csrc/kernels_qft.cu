@@ -445,11 +445,14 @@ __global__ void __launch_bounds__(256, 2)
 // round A and in ascending write stride for round B, so the copies and the
 // stores run over the smallest strides, also in the pass that reverses the
 // targets (reading one buffer, writing another). The buffer is swizzled (tile
-// bits 4-7 folded into 0-3) so that either order hits distinct banks. The
-// phases are those of qubit_round_ct.
+// bits 4-7 and 8-11 folded into 0-3) so that either order hits distinct banks,
+// also when the lanes run over the tile's highest bits (the group digits are
+// the lowest in memory). The phases are those of qubit_round_ct.
 namespace {
 
-__device__ __forceinline__ uint32_t q8_swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
+__device__ __forceinline__ uint32_t q8_swz(uint32_t e) {
+    return e ^ ((e >> 4) & 15u) ^ ((e >> 8) & 15u);
+}
 
 // G steps of a round on the 2^G amplitudes of base eb (round bits [lo, lo+G))
 template <typename R, bool INV, int G, int M, int EB>
@@ -643,27 +646,50 @@ __global__ void __launch_bounds__(Q8Shape<R>::NTHR, Q8Shape<R>::MINB)
     }
 }
 
+int qft_pass8_tile_bits(qgpu_prec prec) {
+    return prec == QGPU_C64 ? Q8Shape<float>::EB : Q8Shape<double>::EB;
+}
+
 // whether k_qft_pass8 applies: qubits, 8 or 6 steps over tiles of 2^EB
 // amplitudes; in place, or (the pass that reverses the targets) into another
 // buffer
-static bool qft_pass8_applies(qgpu_prec prec, const void* in, const void* out,
-                              const QftPlan& p) {
-    const int EB = prec == QGPU_C64 ? Q8Shape<float>::EB : Q8Shape<double>::EB;
+bool qft_pass8_applies(qgpu_prec prec, const void* in, const void* out, const QftPlan& p) {
+    const int EB = qft_pass8_tile_bits(prec);
     if (p.d != 2 || (p.M != 8 && p.M != 6) || p.nr != EB - p.M || p.E != (1u << EB) ||
         p.wmul != (1u << (8 - p.M)) || p.ntd != EB || p.nW != 256u || !p.pow2)
         return false;
     bool same = true;
     for (int q = 0; q < p.ntd; ++q) {
-        if (p.tdim[q] != 2) return false;
+        if (p.tdim[q] != 2 || p.tpitch[q] != (1u << q)) return false;
         same = same && p.trs[q] == p.tws[q];
     }
     for (int q = 0; q < p.nod; ++q) same = same && p.ors[q] == p.ows[q];
-    return in != out || same;
+    if (in == out && !same) return false;
+    // both rounds must reach 128-byte runs across a warp's lanes: when the
+    // lowest memory digits are a round's own bits (the pass whose targets
+    // are the lowest digits, without the reversal), each thread would hold
+    // a contiguous run itself and the lanes' accesses would scatter; such a
+    // pass stays with the shared-memory rounds, which write in memory order
+    QftPlan q = p;
+    qft_pass8_maps(q, EB);
+    const int NQ = EB - p.M / 2;
+    const uint32_t run = prec == QGPU_C64 ? 16 : 8;
+    for (int r = 0; r < 2; ++r) {
+        const uint8_t* map = r ? q.q8b : q.q8a;
+        const uint64_t* st = r ? q.tws : q.trs;
+        for (uint32_t l = 1; l < run; ++l) {
+            uint64_t o = 0;
+            for (int i = 0; i < NQ; ++i)
+                if ((l >> i) & 1u) o += st[map[i]];
+            if (o != l) return false;
+        }
+    }
+    return true;
 }
 
 // the thread-to-base maps of k_qft_pass8: the tile bits outside a round's
 // [lo, lo + G), by ascending stride
-static void qft_pass8_maps(QftPlan& p, int EB) {
+void qft_pass8_maps(QftPlan& p, int EB) {
     const int G = p.M / 2, NR = EB - p.M;
     const int loA = p.inverse ? NR : NR + G, loB = p.inverse ? NR + G : NR;
     auto fill = [&](int lo, const uint64_t* st, uint8_t* out) {

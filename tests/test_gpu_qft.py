@@ -116,6 +116,25 @@ def test_pass_shapes_compiled_and_runtime(ctx, n):
         s.free()
 
 
+def test_transforms_without_reversal(ctx):
+    """swap = false: the pass on the lowest digits keeps the shared-memory
+    rounds, the others run in register rounds. 14 qubits against the oracle
+    in both precisions, 22 qubits as a QFT-then-TFQ round trip."""
+    import qpp_b200 as qb
+    rng = np.random.default_rng(1414)
+    for n in (14, 22):
+        psi = gaussian_ket(rng, 2 ** n)
+        ref = orc.applyQFT(psi, list(range(n)), 2, False) if n == 14 else None
+        for prec, tol in ((qb.C128, TOL128), (qb.C64, TOL64)):
+            s = qb.State.from_numpy(ctx, psi, [2] * n, prec=prec)
+            s.apply_qft(list(range(n)), swap=False)
+            if ref is not None:
+                assert relerr(s.numpy(), ref) < tol, (n, prec)
+            s.apply_tfq(list(range(n)), swap=False)
+            assert relerr(s.numpy(), psi) < tol, (n, prec, "round trip")
+            s.free()
+
+
 def test_complex64_density_matrix_passes(ctx):
     """A complex64 density matrix of 8 qubits: U on the row digits and
     conj(U) on the column digits, each an 8-step pass, against the oracle."""
