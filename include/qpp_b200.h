@@ -544,14 +544,20 @@ qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst,
 qgpu_status qgpu_batch_last_phases(qgpu_ctx* ctx, double* phases_ms);
 
 /* ------------------------------------------------------------ serving loop
- * QNoisyEngine requests on one GPU. A worker thread drains the queue.
- * mode 0 (batched): requests that arrive while a launch runs are admitted in
- * arrival order while their estimated HBM footprint fits hbm_budget, and all
- * their trajectories share the next trajectory-kernel launch; requests the
- * kernel cannot run (density matrices, > 20 qubits, wider gates) run on the
- * resident engine on a second stream at the same time. mode 1 (plain): one
- * request at a time on the resident engine in complex128, one launch per
- * gate. A request's circuit must stay alive until its wait returns. */
+ * QNoisyEngine requests on one GPU, submitted from any thread.
+ * mode 0 (batched): kets of up to 20 qubits and density matrices of up to 7
+ * run as trajectories; waiting requests are admitted in arrival order, a
+ * slice of their shots at a time, into the next launch of their register
+ * size while their estimated HBM footprint fits hbm_budget. Each register
+ * size has its own stream with up to two launches in flight, so sizes run
+ * side by side and a request finishes when its last shot lands. Requests the
+ * trajectory kernel cannot run (larger density matrices, kets above 20
+ * qubits, wider gates) run one at a time on each of two engine workers with
+ * high-priority streams, density matrices of gates and channels in the fused
+ * superoperator form. mode 1 (plain): one request at a time on the resident
+ * engine in complex128, one launch per gate. Results do not depend on what
+ * else is in flight. A request's circuit must stay alive until its wait
+ * returns. */
 typedef struct qgpu_server qgpu_server;
 qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode,
                                qgpu_server** out);
