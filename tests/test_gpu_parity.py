@@ -268,3 +268,28 @@ def test_states_outlive_a_closed_context():
     del a
     assert b.numpy().shape == (256, 256)
     del b
+
+
+def test_plain_gates_with_64_bit_indices():
+    """A 31-qubit complex64 ket (16 GiB): a one-qubit gate's grid, one pair
+    per thread over the whole state, has a last loop step past 2^32, so the
+    kernel indexes in 64 bits; the same gate as U (x) I on a two-qubit group
+    (whose kernel stays in 32 bits) must give the same state."""
+    import qpp_b200 as qb
+    ctx = qb.Context(0)
+    n = 31
+    rng = np.random.default_rng(31)
+    s = qb.State(ctx, qb.KET, [2] * n, qb.C64)
+    s.fill_gaussian(3)
+    s.normalize()
+    t = s.clone()
+    for q, p in ((0, 5), (17, 30), (30, 0)):
+        U = haar_unitary(rng, 2)
+        s.apply(U, [q])
+        t.apply(np.kron(U, np.eye(2)), [q, p])
+    ov = s.inner(t)
+    assert abs(abs(ov) - 1.0) < 1e-5, ov
+    assert abs(s.norm2() - 1.0) < 1e-5
+    s.free()
+    t.free()
+    ctx.close()
