@@ -62,20 +62,28 @@ __device__ __forceinline__ void ptrace_term(const Cplx<R>* in, uint64_t a0,
     }
 }
 
+// The traced offsets: a device array, or (up to kPtraceTab of them) a table
+// passed by value with the launch, which spares the copy to the device.
+constexpr int kPtraceTab = 256;
+struct PtraceTab {
+    uint64_t t[kPtraceTab];
+    __device__ __forceinline__ uint64_t operator[](uint64_t a) const { return t[a]; }
+};
+
 // one thread per output element (many outputs)
-template <typename R, bool KET>
+template <typename R, bool KET, typename TABLE>
 __global__ void __launch_bounds__(256)
     k_ptrace_thread(const Cplx<R>* __restrict__ in, Cplx<R>* __restrict__ out,
                     const __grid_constant__ SegPlan ma,
                     const __grid_constant__ SegPlan mb,
-                    const uint64_t* __restrict__ toff, uint64_t DS) {
+                    const __grid_constant__ TABLE toff, uint64_t DS) {
     const uint64_t nth = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t o = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
          o < ma.count; o += nth) {
         uint64_t a0 = seg_offset(ma, o), b0 = KET ? seg_offset(mb, o) : 0;
         double sr = 0, si = 0;
         for (uint64_t a = 0; a < DS; ++a)
-            ptrace_term<R, KET>(in, a0, b0, __ldg(&toff[a]), sr, si);
+            ptrace_term<R, KET>(in, a0, b0, toff[a], sr, si);
         Cplx<R> r;
         r.x = R(sr);
         r.y = R(si);
@@ -84,12 +92,12 @@ __global__ void __launch_bounds__(256)
 }
 
 // one warp per output element (few outputs, long sums)
-template <typename R, bool KET>
+template <typename R, bool KET, typename TABLE>
 __global__ void __launch_bounds__(256)
     k_ptrace_warp(const Cplx<R>* __restrict__ in, Cplx<R>* __restrict__ out,
                   const __grid_constant__ SegPlan ma,
                   const __grid_constant__ SegPlan mb,
-                  const uint64_t* __restrict__ toff, uint64_t DS) {
+                  const __grid_constant__ TABLE toff, uint64_t DS) {
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
@@ -97,7 +105,7 @@ __global__ void __launch_bounds__(256)
         uint64_t a0 = seg_offset(ma, o), b0 = KET ? seg_offset(mb, o) : 0;
         double sr = 0, si = 0;
         for (uint64_t a = lane; a < DS; a += 32)
-            ptrace_term<R, KET>(in, a0, b0, __ldg(&toff[a]), sr, si);
+            ptrace_term<R, KET>(in, a0, b0, toff[a], sr, si);
 #pragma unroll
         for (int s = 16; s > 0; s >>= 1) {
             sr += __shfl_down_sync(0xffffffffu, sr, s);
@@ -408,32 +416,47 @@ void launch_gather_outer(qgpu_ctx* ctx, qgpu_prec prec, const void* in,
     after_launch(ctx, "k_gather_outer");
 }
 
-template <typename R>
-static void ptr(qgpu_ctx* ctx, const void* in, void* out, const SegPlan& ma,
-                const SegPlan& mb, const std::vector<uint64_t>& toff,
-                bool is_ket) {
-    uint64_t DS = toff.size();
-    uint64_t* dt = static_cast<uint64_t*>(ctx_scratch(ctx, DS * sizeof(uint64_t)));
-    QG_CUDA(cudaMemcpyAsync(dt, toff.data(), DS * sizeof(uint64_t),
-                            cudaMemcpyHostToDevice, ctx->stream));
-    const Cplx<R>* i = static_cast<const Cplx<R>*>(in);
-    Cplx<R>* o = static_cast<Cplx<R>*>(out);
+template <typename R, typename TABLE>
+static void ptr_launch(qgpu_ctx* ctx, const Cplx<R>* i, Cplx<R>* o, const SegPlan& ma,
+                       const SegPlan& mb, const TABLE& t, uint64_t DS, bool is_ket) {
     // few outputs with long sums: a warp per output
     bool warp = ma.count < uint64_t(ctx->num_sms) * 2048 && DS >= 32;
     if (warp) {
         int b = blocks_for(ctx, ma.count * 32, 8);
         if (is_ket)
-            k_ptrace_warp<R, true><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, dt, DS);
+            k_ptrace_warp<R, true, TABLE><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, t, DS);
         else
-            k_ptrace_warp<R, false><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, dt, DS);
+            k_ptrace_warp<R, false, TABLE><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, t, DS);
     } else {
         int b = blocks_for(ctx, ma.count, 8);
         if (is_ket)
-            k_ptrace_thread<R, true><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, dt, DS);
+            k_ptrace_thread<R, true, TABLE><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, t, DS);
         else
-            k_ptrace_thread<R, false><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, dt, DS);
+            k_ptrace_thread<R, false, TABLE><<<b, 256, 0, ctx->stream>>>(i, o, ma, mb, t, DS);
     }
     after_launch(ctx, "k_ptrace");
+}
+
+template <typename R>
+static void ptr(qgpu_ctx* ctx, const void* in, void* out, const SegPlan& ma,
+                const SegPlan& mb, const std::vector<uint64_t>& toff,
+                bool is_ket) {
+    uint64_t DS = toff.size();
+    const Cplx<R>* i = static_cast<const Cplx<R>*>(in);
+    Cplx<R>* o = static_cast<Cplx<R>*>(out);
+    if (DS <= uint64_t(kPtraceTab)) {
+        // small tables travel with the launch (no host-to-device copy)
+        PtraceTab tab;
+        std::memset(&tab, 0, sizeof(tab));
+        std::copy(toff.begin(), toff.end(), tab.t);
+        ptr_launch<R, PtraceTab>(ctx, i, o, ma, mb, tab, DS, is_ket);
+        return;
+    }
+    uint64_t* dt = static_cast<uint64_t*>(ctx_scratch(ctx, DS * sizeof(uint64_t)));
+    QG_CUDA(cudaMemcpyAsync(dt, toff.data(), DS * sizeof(uint64_t),
+                            cudaMemcpyHostToDevice, ctx->stream));
+    const uint64_t* cdt = dt;
+    ptr_launch<R, const uint64_t*>(ctx, i, o, ma, mb, cdt, DS, is_ket);
 }
 
 void launch_ptrace(qgpu_ctx* ctx, qgpu_prec prec, const void* in, void* out,
