@@ -275,7 +275,7 @@ def cpu_baseline(n, layers, n_gates, gpu_result=None):
 
 
 def _config1(cb, orc, ct, ctx, torch, stream, peak, cores):
-    rec, seq, final = cb.config1(ctx, torch, stream, peak)
+    rec, seq, finals = cb.config1(ctx, torch, stream, peak)
     n = 20
     D = 2 ** n
     psi = np.empty(D, dtype=np.complex128)
@@ -294,9 +294,12 @@ def _config1(cb, orc, ct, ctx, torch, stream, peak, cores):
                            "cores": cores, "kind": "port",
                            "sample": "first 200 gates of the sequence, qpp's qubit kernels "
                                      "restated (copy per call)"}
-    err = float(np.max(np.abs(final - psi)) / np.max(np.abs(psi)))
+    err = float(np.max(np.abs(finals["circuit"] - psi)) / np.max(np.abs(psi)))
     rec["parity"] = {"max_rel_err": err, "tol": 1e-12, "ok": err < 1e-12,
                      "check": "all 1100 gates, circuit form vs the oracle, same seeded ket"}
+    errf = float(np.max(np.abs(finals["fused"] - psi)) / np.max(np.abs(psi)))
+    rec["fused"]["parity"] = {"max_rel_err": errf, "tol": 1e-12, "ok": errf < 1e-12,
+                              "check": "all 1100 gates, fused form vs the oracle, same seeded ket"}
     return rec
 
 

@@ -406,10 +406,13 @@ qgpu_status qgpu_circuit_fuse(qgpu_circuit* c, uint32_t max_k,
 /* Execution forms of the unitary steps of a circuit on a resident state. */
 typedef enum qgpu_form {
     QGPU_FORM_PLAIN = 0, /* one pass per qpp call, in the state precision */
-    QGPU_FORM_FUSED = 1  /* fused blocks: c64 -> 6-qubit tcgen05 3xTF32 */
+    QGPU_FORM_FUSED = 1  /* fused blocks: c64 -> 6-qubit tcgen05 split-FP16 */
 } qgpu_form;
 /* Kets: the unitary steps (measurements and classical control need an
- * engine). QGPU_FORM_FUSED on a complex64 qubit density matrix of <= 15
+ * engine). QGPU_FORM_FUSED on a qubit ket merges gates into blocks: of <= 6
+ * qubits in complex64 (on the tensor cores from 13 qubits); in complex128,
+ * of <= 2 qubits run as tile passes up to 22 qubits and of <= 3 qubits as
+ * dense passes above. QGPU_FORM_FUSED on a complex64 qubit density matrix of <= 15
  * qubits whose circuit holds only gates and 1- or 2-qubit channels:
  * superoperators on the 2n virtual qubits (column digits, row digits) merged
  * into blocks of <= 4 virtual qubits, one pass over the matrix per block
@@ -418,7 +421,7 @@ typedef enum qgpu_form {
  * No reference counterpart for the fused forms. */
 qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form);
 /* One gate of k <= 6 qubits on a complex64 qubit ket of >= 13 qubits, as a
- * 64 x 64 block on the tensor cores (split-TF32, FP32 accumulation). */
+ * 64 x 64 block on the tensor cores (split-FP16, FP32 accumulation). */
 qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U,
                           const uint64_t* target, uint32_t k);
 

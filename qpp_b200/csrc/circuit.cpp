@@ -436,8 +436,48 @@ void launch_program(qgpu_state* s, const TProgram& P) {
     }
 }
 
+// Complex128 qubit kets of up to 22 qubits (64 MiB, half the L2) run the
+// fused form as tile passes over blocks of <= 2 qubits. Such a state is read
+// from the L2, so a pass's time follows its FP64 work per amplitude, and
+// blocks of <= 2 qubits keep that work lowest: a 1-qubit gate merged into a
+// neighbouring 2-qubit block costs nothing, where a 3-qubit block costs as
+// much as two 2-qubit gates. Larger complex128 kets are HBM-bound and take
+// blocks of <= 3 qubits as dense passes, fewer trips through HBM.
+constexpr size_t kFusedTileQubitsC128 = 22;
+
+static bool fused_tiles(const qgpu_state* s) {
+    return s->kind == QGPU_KET && s->prec == QGPU_C128 && !s->dims.empty() &&
+           s->dims.size() <= kFusedTileQubitsC128;
+}
+
+// The fused plan's blocks (<= 2 qubits) and its unfused steps in circuit
+// order, as tile passes (kernels_tile.cu); a step the passes do not take runs
+// as it is between them.
+static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
+    const int nq = int(c->nq);
+    std::vector<GateDesc> run;
+    for (const Block& b : c->plan) {
+        if (b.step >= 0) {
+            const Step& st = c->steps[size_t(b.step)];
+            if (gate_desc_of(st, nq, run)) continue;
+            run_tiled_gates(s, run);
+            run.clear();
+            apply_step(s, st);
+            continue;
+        }
+        GateDesc g;
+        g.op = int(b.qubits.size());
+        g.b0 = nq - 1 - b.qubits[0];
+        if (g.op == 2) g.b1 = nq - 1 - b.qubits[1];
+        std::copy(b.U.begin(), b.U.end(), g.A);
+        run.push_back(g);
+    }
+    run_tiled_gates(s, run);
+}
+
 // Kets: qubits only; blocks of up to 6 qubits (complex64: 3-6 qubit blocks on
-// the tensor cores from 13 qubits on), 3 in complex128.
+// the tensor cores from 13 qubits on); in complex128, 2 (as tile passes) up to
+// 22 qubits and 3 above.
 void fused_prepare(qgpu_state* s, qgpu_circuit* c) {
     if (s->kind == QGPU_RHO) {
         if (rho_tc_prepare(s, c)) {
@@ -448,7 +488,7 @@ void fused_prepare(qgpu_state* s, qgpu_circuit* c) {
     }
     if (c->d != 2)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
-    prepare_plan(s, c, s->prec == QGPU_C64 ? 6 : 3);
+    prepare_plan(s, c, s->prec == QGPU_C64 ? 6 : fused_tiles(s) ? 2 : 3);
     if (!c->block_slot.empty()) ctx_error_flag(s->ctx); // allocated outside any capture
 }
 
@@ -461,6 +501,7 @@ void fused_launch(qgpu_state* s, qgpu_circuit* c) {
         }
         return launch_program(s, *c->rho_prog);
     }
+    if (fused_tiles(s)) return launch_tiled_blocks(s, c);
     launch_blocks(s, vspace_ket(s->dims), int(c->nq), c->plan, c->dB, c->block_slot, c->steps);
 }
 

@@ -68,6 +68,52 @@ def test_fused_layered_circuit_fidelity(ctx):
     assert relerr(a, psi) < 1e-12
 
 
+@pytest.mark.parametrize("n,n_gates", [(9, 120), (20, 300), (23, 60)])
+def test_fused_complex128_circuit_matches_oracle(ctx, n, n_gates):
+    """The fused form in complex128: blocks of <= 2 qubits as tile passes up
+    to 22 qubits, blocks of <= 3 qubits as dense passes above. The circuit
+    mixes 1- and 2-qubit gates with controlled gates of 1-3 controls (some
+    with shifts) in between, a fan gate and a 3-qubit gate (steps the
+    planner leaves unfused); within 1e-12 of the oracle applying the steps one
+    by one."""
+    import qpp_b200 as qb
+    from qpp_b200.workloads import ket_gate_sequence
+    rng = np.random.default_rng(n)
+    seq = ket_gate_sequence(n, seed=n, n_gates=n_gates, n_ctrl=n_gates // 10)
+    plain, ctrl = seq[:n_gates], seq[n_gates:]
+    steps = []  # (kind, U, ctrl, target, shift)
+    for i, (U, c, t) in enumerate(plain):
+        steps.append(("gate", U, c, t, None))
+        if i % 10 == 5 and ctrl:
+            U2, c2, t2 = ctrl.pop()
+            shift = [int(x) for x in rng.integers(0, 2, size=len(c2))] if i % 20 == 5 else None
+            steps.append(("ctrl", U2, c2, t2, shift))
+        if i == n_gates // 2:
+            steps.append(("fan", haar_unitary(rng, 2), [], [0, n - 1, n // 2], None))
+            steps.append(("gate", haar_unitary(rng, 8), [], [1, n - 2, n // 3], None))
+    c = qb.Circuit(n)
+    for kind, U, cs, t, sh in steps:
+        if kind == "gate":
+            c.gate(U, t)
+        elif kind == "fan":
+            c.gate_fan(U, t)
+        else:
+            c.CTRL(U, cs, t, shift=sh)
+    s = qb.State(ctx, qb.KET, [2] * n, qb.C128).fill_gaussian(3)
+    psi = s.numpy()
+    c.run(s, qb.FUSED)
+    dims = [2] * n
+    for kind, U, cs, t, sh in steps:
+        if kind == "gate":
+            psi = orc.apply(psi, U, t, dims)
+        elif kind == "fan":
+            for q in t:
+                psi = orc.apply(psi, U, [q], dims)
+        else:
+            psi = orc.applyCTRL(psi, U, cs, t, dims, shift=sh)
+    assert relerr(s.numpy(), psi) < 1e-12
+
+
 @pytest.mark.parametrize("scale", [1.0, 2.0 ** -40, 2.0 ** 30])
 def test_block_scale_follows_the_norm(ctx, scale):
     """The fp16 scale comes from |psi|: unnormalised kets keep the accuracy."""
