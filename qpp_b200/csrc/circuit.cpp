@@ -10,9 +10,36 @@
 #include "tile_gates.hpp"
 #include "traj.hpp"
 
+namespace qgpu {
+
+// Makes `dev` the current device for a scope and then restores the caller's
+// (a circuit may run on states of several GPUs in one process, and its
+// device images live on the device they were built for).
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev) {
+        if (dev < 0 || cudaGetDevice(&prev) != cudaSuccess || prev == dev ||
+            cudaSetDevice(dev) != cudaSuccess)
+            prev = -1;
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Frees a circuit's device image on the device that holds it.
+static void free_image(unsigned char*& p, int dev) {
+    if (!p) return;
+    DeviceScope on(dev);
+    cudaFree(p);
+    p = nullptr;
+}
+
+} // namespace qgpu
+
 qgpu_circuit::~qgpu_circuit() {
-    if (dB) cudaFree(dB);
-    if (rho_dB) cudaFree(rho_dB);
+    qgpu::free_image(dB, dB_dev);
+    qgpu::free_image(rho_dB, rho_dB_dev);
 }
 
 namespace qgpu {
@@ -248,6 +275,7 @@ constexpr uint32_t kRhoTcMinQubits = 11;
 
 static void upload_tc_blocks(qgpu_ctx* ctx, std::vector<Block>& plan, uint32_t nq,
                              unsigned char** dB, std::vector<int64_t>& slot) {
+    DeviceScope on(ctx->device);
     slot.assign(plan.size(), -1);
     int64_t nslot = 0;
     for (size_t i = 0; i < plan.size(); ++i)
@@ -278,18 +306,18 @@ static void upload_tc_blocks(qgpu_ctx* ctx, std::vector<Block>& plan, uint32_t n
 }
 
 static void prepare_plan(qgpu_state* s, qgpu_circuit* c, uint32_t k) {
+    // block images held by another device are rebuilt on this one
+    if (c->dB && c->dB_dev != s->ctx->device) c->plan_k = 0;
     if (c->plan_k != k) {
         c->plan = fuse(c->steps, c->nq, k);
         c->plan_k = k;
-        if (c->dB) {
-            cudaFree(c->dB);
-            c->dB = nullptr;
-        }
+        free_image(c->dB, c->dB_dev);
         c->block_slot.clear();
     }
     bool tc = s->prec == QGPU_C64 && c->nq >= 13 && k == 6;
     if (!tc || c->dB || !c->block_slot.empty()) return;
     upload_tc_blocks(s->ctx, c->plan, c->nq, &c->dB, c->block_slot);
+    c->dB_dev = s->ctx->device;
     c->plan_ctx = s->ctx;
 }
 
@@ -371,11 +399,8 @@ static bool rho_tc_prepare(qgpu_state* s, qgpu_circuit* c) {
     // 0.77 ms, 10 qubits 1.01 vs 1.06 ms, 12 qubits 9.4 vs 6.9 ms)
     if (s->prec != QGPU_C64 || c->d != 2 || c->nq < kRhoTcMinQubits || 2 * c->nq > 62)
         return false;
-    if (c->rho_tc_steps != c->steps.size()) {
-        if (c->rho_dB) {
-            cudaFree(c->rho_dB);
-            c->rho_dB = nullptr;
-        }
+    if (c->rho_tc_steps != c->steps.size() || (c->rho_dB && c->rho_dB_dev != s->ctx->device)) {
+        free_image(c->rho_dB, c->rho_dB_dev);
         c->rho_slot.clear();
         c->rho_plan.clear();
         std::vector<Step> vsteps;
@@ -386,6 +411,7 @@ static bool rho_tc_prepare(qgpu_state* s, qgpu_circuit* c) {
                 if (b.step >= 0) c->rho_tc_ok = false; // every virtual step is a gate
         }
         if (c->rho_tc_ok) upload_tc_blocks(s->ctx, c->rho_plan, 2 * c->nq, &c->rho_dB, c->rho_slot);
+        c->rho_dB_dev = s->ctx->device;
         c->rho_tc_steps = c->steps.size();
     }
     return c->rho_tc_ok;

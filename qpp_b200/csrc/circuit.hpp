@@ -81,6 +81,7 @@ struct qgpu_circuit {
     // fp16 hi and lo halves in the kernel's shared-memory layout)
     qgpu_ctx* plan_ctx = nullptr;
     unsigned char* dB = nullptr;
+    int dB_dev = -1; // the device holding dB
     std::vector<int64_t> block_slot; // plan index -> image slot in dB, or -1
     // fused density-matrix program (superoperator blocks), built for the
     // first rho_steps steps (steps are only ever appended)
@@ -93,6 +94,7 @@ struct qgpu_circuit {
     bool rho_tc_ok = false;
     std::vector<qgpu::Block> rho_plan;
     unsigned char* rho_dB = nullptr;
+    int rho_dB_dev = -1; // the device holding rho_dB
     std::vector<int64_t> rho_slot;
     ~qgpu_circuit();
 };
