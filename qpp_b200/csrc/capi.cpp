@@ -8,6 +8,8 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -49,6 +51,19 @@ void after_launch(qgpu_ctx* ctx, const char* name) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) raise(QGPU_ERR_CUDA, name, cudaGetErrorString(e));
     ctx->launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void ensure_smem(const void* func, size_t bytes) {
+    if (bytes <= 48 * 1024) return; // the default limit
+    int dev = 0;
+    QG_CUDA(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> limit;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& have = limit[{func, dev}];
+    if (bytes <= have) return;
+    QG_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    have = bytes;
 }
 
 void* ctx_scratch(qgpu_ctx* ctx, size_t bytes) {

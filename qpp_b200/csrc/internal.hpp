@@ -95,6 +95,12 @@ void clear_error();
 // Checks the last launch on this thread and counts it on the context.
 void after_launch(qgpu_ctx* ctx, const char* name);
 
+// Raises kernel `func`'s dynamic shared-memory limit on the current device to
+// at least `bytes`. The limit is an attribute of each (function, device) and
+// is only ever raised, so a launch with a smaller need on another thread
+// stays valid.
+void ensure_smem(const void* func, size_t bytes);
+
 // Frees the context's stream, buffers and the context itself.
 void destroy_ctx(qgpu_ctx* ctx);
 

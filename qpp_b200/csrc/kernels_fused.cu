@@ -52,7 +52,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
@@ -526,18 +525,7 @@ void launch_fused6_tc(qgpu_ctx* ctx, void* data, int nbits, const int* tbits,
     p.spin_limit = ctx->wait_limit ? ctx->wait_limit : kSpinLimit;
     p.stall_first = ctx->stall_next ? 1u : 0u;
     ctx->stall_next = 0;
-    // the shared-memory opt-in is a per-device attribute of the function
-    static std::mutex mu;
-    static bool attr_set[64] = {};
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        const int dev = ctx->device;
-        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-            QG_CUDA(cudaFuncSetAttribute(k_fused6_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(kF6Smem)));
-            if (dev >= 0 && dev < 64) attr_set[dev] = true;
-        }
-    }
+    ensure_smem(reinterpret_cast<const void*>(k_fused6_tc), kF6Smem);
     int grid = int(std::min<uint64_t>(p.ntiles, uint64_t(ctx->num_sms)));
     k_fused6_tc<<<grid, kF6Threads, kF6Smem, ctx->stream>>>(static_cast<float2*>(data), p);
     after_launch(ctx, "k_fused6_tc");

@@ -491,10 +491,7 @@ static void smem(qgpu_ctx* ctx, void* data, const SegPlan& outer,
                             ctx->stream));
     int G = DA >= 256 ? 1 : int(256 / DA);
     size_t sm = size_t(G) * DA * sizeof(Cplx<R>);
-    if (sm > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_smem<R>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(sm)));
+    ensure_smem(reinterpret_cast<const void*>(k_smem<R>), sm);
     int blocks = grid_blocks(ctx, 4);
     uint64_t need = (outer.count + G - 1) / G;
     if (need < uint64_t(blocks)) blocks = int(std::max<uint64_t>(need, 1));

@@ -727,7 +727,7 @@ static void qft_pass8_launch(qgpu_ctx* ctx, const void* in, void* out, const Qft
     else
         kern = narrow ? (q.inverse ? K(k_qft_pass8<R, true, uint32_t, 6>) : K(k_qft_pass8<R, false, uint32_t, 6>))
                       : (q.inverse ? K(k_qft_pass8<R, true, uint64_t, 6>) : K(k_qft_pass8<R, false, uint64_t, 6>));
-    QG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    ensure_smem(reinterpret_cast<const void*>(kern), sm);
     kern<<<unsigned(blocks), S::NTHR, sm, ctx->stream>>>(static_cast<const C*>(in),
                                                          static_cast<C*>(out), q,
                                                          static_cast<const C*>(W));
@@ -746,16 +746,12 @@ static void qft_launch(qgpu_ctx* ctx, const void* in, void* out, const QftPlan& 
     uint64_t blocks = uint64_t(grid_blocks(ctx, 2));
     if (p.ntiles < blocks) blocks = p.ntiles;
     if (p.d == 2) {
-        if (sm > 48 * 1024)
-            QG_CUDA(cudaFuncSetAttribute(k_qft_pass<R, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        ensure_smem(reinterpret_cast<const void*>(k_qft_pass<R, true>), sm);
         k_qft_pass<R, true><<<unsigned(blocks), 256, sm, ctx->stream>>>(
             static_cast<const C*>(in), static_cast<C*>(out), p, static_cast<const C*>(W),
             static_cast<const C*>(F));
     } else {
-        if (sm > 48 * 1024)
-            QG_CUDA(cudaFuncSetAttribute(k_qft_pass<R, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        ensure_smem(reinterpret_cast<const void*>(k_qft_pass<R, false>), sm);
         k_qft_pass<R, false><<<unsigned(blocks), 256, sm, ctx->stream>>>(
             static_cast<const C*>(in), static_cast<C*>(out), p, static_cast<const C*>(W),
             static_cast<const C*>(F));

@@ -344,18 +344,7 @@ template <typename R, typename OFF, int TB, int NTHR>
 void permute_launch(qgpu_ctx* ctx, const void* in, void* out, const PermPlan& P) {
     using S = PermShape<R, OFF, TB, NTHR>;
     auto* kern = k_permute_tiled<R, OFF, TB, NTHR>;
-    // the shared-memory opt-in is a per-device attribute of each function
-    static std::mutex mu;
-    static bool attr_set[64] = {};
-    const int dev = ctx->device;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-            QG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(S::kSmem)));
-            if (dev >= 0 && dev < 64) attr_set[dev] = true;
-        }
-    }
+    ensure_smem(reinterpret_cast<const void*>(kern), S::kSmem);
     // one tile per CTA: on a 2^24-element state the tiles moved 5.4 TB/s on
     // average over random permutations this way against 4.9 TB/s with one
     // wave of resident CTAs looping (the next tile's prefetch then has

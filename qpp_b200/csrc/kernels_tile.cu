@@ -29,7 +29,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 
 #include "common.cuh"
 #include "kernels.hpp"
@@ -268,24 +267,9 @@ void launch_tile_pass(qgpu_ctx* ctx, qgpu_prec prec, void* data, const TilePassP
     const size_t smem = tile_pass_smem(prec, p);
     if (smem > kTileSmemMax)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "tile above the shared memory");
-    // the shared-memory opt-in is a per-device attribute of each function
-    static std::mutex mu;
-    static bool attr_set[2][64] = {};
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        const int dev = ctx->device, k = prec == QGPU_C128 ? 0 : 1;
-        if (dev < 0 || dev >= 64 || !attr_set[k][dev]) {
-            if (prec == QGPU_C128)
-                QG_CUDA(cudaFuncSetAttribute(k_tile_pass<double>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(kTileSmemMax)));
-            else
-                QG_CUDA(cudaFuncSetAttribute(k_tile_pass<float>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(kTileSmemMax)));
-            if (dev >= 0 && dev < 64) attr_set[k][dev] = true;
-        }
-    }
+    ensure_smem(prec == QGPU_C128 ? reinterpret_cast<const void*>(k_tile_pass<double>)
+                                  : reinterpret_cast<const void*>(k_tile_pass<float>),
+                kTileSmemMax);
     // residency per SM from shared memory (228 KB, 1 KB reserved per CTA)
     // and threads (2048)
     const int per_sm = std::max(1, std::min(2048 / kTileThreads, int(232448 / (smem + 1024))));

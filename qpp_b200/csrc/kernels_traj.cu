@@ -702,12 +702,8 @@ void launch_pass_batch(qgpu_ctx* ctx, const PassInst* dinsts, int ninst, uint32_
     if (ninst == 0 || nitems == 0) return;
     if (tile_bits < 9 || tile_bits > 13)
         raise(QGPU_ERR_INVALID_ARGUMENT, "launch_pass_batch()", "tile_bits");
-    static std::once_flag once;
-    std::call_once(once, [] {
-        QG_CUDA(cudaFuncSetAttribute(k_pass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int((size_t(2) << 13) * sizeof(float2) +
-                                         (size_t(2) << 8) * sizeof(uint32_t))));
-    });
+    ensure_smem(reinterpret_cast<const void*>(k_pass_batch),
+                (size_t(2) << 13) * sizeof(float2) + (size_t(2) << 8) * sizeof(uint32_t));
     // two tile buffers and two row tables
     const size_t smem = (size_t(2) << tile_bits) * sizeof(float2) +
                         (size_t(2) << (tile_bits - 5)) * sizeof(uint32_t);
@@ -836,13 +832,10 @@ void launch_block_batch(qgpu_ctx* ctx, const BlockInst* dinsts, int ninst, uint3
 }
 
 void traj_prepare() {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        // a 2^14-amplitude register, or a tile of up to 2^14 amplitudes with
-        // its offset table
-        QG_CUDA(cudaFuncSetAttribute(k_traj, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int((size_t(1) << kTrajMaxQubits) * sizeof(float2) + 4096)));
-    });
+    // a 2^14-amplitude register, or a tile of up to 2^14 amplitudes with its
+    // offset table
+    ensure_smem(reinterpret_cast<const void*>(k_traj),
+                (size_t(1) << kTrajMaxQubits) * sizeof(float2) + 4096);
 }
 
 int traj_global_grid(qgpu_ctx* ctx, int nwork, int n) {
