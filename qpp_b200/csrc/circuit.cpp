@@ -476,19 +476,17 @@ static bool fused_tiles(const qgpu_state* s) {
            s->dims.size() <= kFusedTileQubitsC128;
 }
 
-// The fused plan's blocks (<= 2 qubits) and its unfused steps in circuit
-// order, as tile passes (kernels_tile.cu); a step the passes do not take runs
-// as it is between them.
-static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
+void tiled_runs(const qgpu_circuit* c, std::vector<TiledRun>& out) {
+    out.clear();
     const int nq = int(c->nq);
-    std::vector<GateDesc> run;
+    out.emplace_back();
     for (const Block& b : c->plan) {
         if (b.step >= 0) {
             const Step& st = c->steps[size_t(b.step)];
-            if (gate_desc_of(st, nq, run)) continue;
-            run_tiled_gates(s, run);
-            run.clear();
-            apply_step(s, st);
+            if (gate_desc_of(st, nq, out.back().gates)) continue;
+            out.emplace_back();
+            out.back().step = b.step;
+            out.emplace_back();
             continue;
         }
         GateDesc g;
@@ -496,9 +494,20 @@ static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
         g.b0 = nq - 1 - b.qubits[0];
         if (g.op == 2) g.b1 = nq - 1 - b.qubits[1];
         std::copy(b.U.begin(), b.U.end(), g.A);
-        run.push_back(g);
+        out.back().gates.push_back(g);
     }
-    run_tiled_gates(s, run);
+}
+
+// The fused plan's blocks (<= 2 qubits) and its unfused steps in circuit
+// order, as tile passes (kernels_tile.cu); a step the passes do not take runs
+// as it is between them.
+static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
+    std::vector<TiledRun> runs;
+    tiled_runs(c, runs);
+    for (const TiledRun& r : runs) {
+        if (r.step >= 0) apply_step(s, c->steps[size_t(r.step)]);
+        else run_tiled_gates(s, r.gates);
+    }
 }
 
 // Kets: qubits only; blocks of up to 6 qubits (complex64: 3-6 qubit blocks on

@@ -41,4 +41,14 @@ int tile_bits_max(const qgpu_ctx* ctx, qgpu_prec prec);
 // Runs `gates` on the qubit ket s as planned tile passes (stream order).
 void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates);
 
+// A piece of a fused complex128 ket plan: a run of gate descriptors for the
+// tile passes (step < 0; possibly empty), or one step run as it is.
+struct TiledRun {
+    std::vector<GateDesc> gates;
+    int64_t step = -1;
+};
+// The circuit's fused plan (blocks of <= 2 qubits, c->plan) and its unfused
+// steps, in circuit order, as tile-pass runs and steps.
+void tiled_runs(const qgpu_circuit* c, std::vector<TiledRun>& out);
+
 } // namespace qgpu
