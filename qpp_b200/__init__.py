@@ -645,14 +645,21 @@ class Circuit:
         return n.value
 
     def fused_passes(self, max_k=6):
+        """Entries of the fused plan with blocks of <= max_k qubits: the
+        merged blocks and the steps left as they are (host planning only)."""
         n = ct.c_uint64()
         check(lib().qgpu_circuit_fuse(self.h, ct.c_uint32(max_k), ct.byref(n)))
         return n.value
 
     def run(self, state, form=PLAIN):
-        """Apply the unitary steps to a resident State (in place). FUSED on a
-        complex64 qubit density matrix runs gates and channels as merged
-        superoperator blocks of <= 4 virtual qubits."""
+        """Apply the unitary steps to a resident State (in place). PLAIN keeps
+        qpp's arithmetic per gate. FUSED merges gates into blocks: on a
+        complex64 qubit ket of <= 6 qubits each (the tensor cores from 13
+        qubits), on a complex128 qubit ket of <= 2 qubits run as tile passes
+        (up to 22 qubits) or <= 3 qubits as dense passes (above); on a
+        complex64 qubit density matrix, gates and channels as superoperator
+        blocks of <= 4 virtual qubits (6 on the tensor cores from 11
+        qubits)."""
         check(lib().qgpu_run_gates(state.h, self.h, ct.c_int(form)))
         return state
 
