@@ -133,7 +133,7 @@ using qgpu::raise;
 extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circuit* const* circuits,
                                       qgpu_state* const* states, int form,
                                       uint64_t* graph_kernels) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(ctx);
         const char* W = "qgpu_run_batch()";
         using clk = std::chrono::steady_clock;
@@ -599,7 +599,7 @@ extern "C" qgpu_status qgpu_run_batch(qgpu_ctx* ctx, uint32_t n_inst, qgpu_circu
 }
 
 extern "C" qgpu_status qgpu_batch_last_phases(qgpu_ctx* ctx, double* phases_ms) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(ctx);
         if (phases_ms) std::copy(ctx->batch_ms, ctx->batch_ms + 6, phases_ms);
     });

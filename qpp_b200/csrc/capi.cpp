@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "capi_common.hpp"
 #include "internal.hpp"
 #include "kernels.hpp"
 #include "ops.hpp"
@@ -312,24 +313,6 @@ void check_handle(const void* p) {
     if (!p) raise(QGPU_ERR_INVALID_HANDLE, "qgpu", "null handle");
 }
 
-template <typename F>
-qgpu_status guard(F&& f) {
-    try {
-        qgpu::clear_error();
-        f();
-        return QGPU_OK;
-    } catch (const Exc& e) {
-        qgpu::record_error(e.code, e.where, e.what);
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        qgpu::record_error(QGPU_ERR_OUT_OF_MEMORY, "qgpu", "host allocation failed");
-        return QGPU_ERR_OUT_OF_MEMORY;
-    } catch (const std::exception& e) {
-        qgpu::record_error(QGPU_ERR_INVALID_ARGUMENT, "qgpu", e.what());
-        return QGPU_ERR_INVALID_ARGUMENT;
-    }
-}
-
 const cd* C(const double* p) { return reinterpret_cast<const cd*>(p); }
 
 void upload_c128(qgpu_state* s, const double* host) {
@@ -422,7 +405,7 @@ const char* qgpu_status_name(qgpu_status s) {
 
 // ------------------------------------------------------------- context
 qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_ctx_create()", "out");
         int n = 0;
         QG_CUDA(cudaGetDeviceCount(&n));
@@ -456,7 +439,7 @@ qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out) {
 }
 
 qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         // states still alive keep the context (their memory lives on its
         // stream); the last qgpu_state_destroy tears it down
@@ -466,14 +449,14 @@ qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx) {
 }
 
 qgpu_status qgpu_ctx_synchronize(qgpu_ctx* ctx) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 
 qgpu_status qgpu_ctx_mem_info(qgpu_ctx* ctx, uint64_t* free_b, uint64_t* total_b) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         size_t f = 0, t = 0;
         QG_CUDA(cudaSetDevice(ctx->device));
@@ -495,7 +478,7 @@ uint64_t qgpu_ctx_launch_count(const qgpu_ctx* ctx) {
 void* qgpu_ctx_stream(qgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall_next) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::lock_guard<std::mutex> lock(ctx->mu);
         ctx->wait_limit = spin_limit;
@@ -506,7 +489,7 @@ qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall
 }
 
 qgpu_status qgpu_ctx_set_tile_bits(qgpu_ctx* ctx, int bits) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         if (bits != 0 && (bits < 5 || bits > 14))
             raise(QGPU_ERR_OUT_OF_RANGE, "qgpu_ctx_set_tile_bits()", "bits");
@@ -517,7 +500,7 @@ qgpu_status qgpu_ctx_set_tile_bits(qgpu_ctx* ctx, int bits) {
 // --------------------------------------------------------------- states
 qgpu_status qgpu_state_create(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
                               const uint64_t* dims, uint32_t n, qgpu_state** out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_state_create()", "out");
         std::vector<uint64_t> d = vec(dims, n);
@@ -531,13 +514,13 @@ qgpu_status qgpu_state_create(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
 }
 
 qgpu_status qgpu_state_destroy(qgpu_state* s) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         if (s) qgpu::free_state(s);
     });
 }
 
 qgpu_status qgpu_state_clone(const qgpu_state* s, qgpu_state** out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         qgpu_state* c = qgpu::new_state(s->ctx, s->kind, s->prec, s->dims, false);
         cudaError_t e = cudaMemcpyAsync(c->data, s->data, s->bytes(),
@@ -551,7 +534,7 @@ qgpu_status qgpu_state_clone(const qgpu_state* s, qgpu_state** out) {
 }
 
 qgpu_status qgpu_state_upload(qgpu_state* s, const void* host) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         QG_CUDA(cudaMemcpyAsync(s->data, host, s->bytes(), cudaMemcpyHostToDevice,
                                 s->ctx->stream));
@@ -560,7 +543,7 @@ qgpu_status qgpu_state_upload(qgpu_state* s, const void* host) {
 }
 
 qgpu_status qgpu_state_download(const qgpu_state* s, void* host) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         QG_CUDA(cudaMemcpyAsync(host, s->data, s->bytes(), cudaMemcpyDeviceToHost,
                                 s->ctx->stream));
@@ -569,7 +552,7 @@ qgpu_status qgpu_state_download(const qgpu_state* s, void* host) {
 }
 
 qgpu_status qgpu_state_upload_c128(qgpu_state* s, const double* host) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         upload_c128(s, host);
         QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
@@ -577,7 +560,7 @@ qgpu_status qgpu_state_upload_c128(qgpu_state* s, const double* host) {
 }
 
 qgpu_status qgpu_state_download_c128(const qgpu_state* s, double* host) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         download_c128(s, host);
     });
@@ -585,7 +568,7 @@ qgpu_status qgpu_state_download_c128(const qgpu_state* s, double* host) {
 
 qgpu_status qgpu_state_info(const qgpu_state* s, qgpu_kind* kind, qgpu_prec* prec,
                             uint32_t* n, uint64_t* dims, uint64_t* D) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         if (kind) *kind = s->kind;
         if (prec) *prec = s->prec;
@@ -598,7 +581,7 @@ qgpu_status qgpu_state_info(const qgpu_state* s, qgpu_kind* kind, qgpu_prec* pre
 void* qgpu_state_device_ptr(qgpu_state* s) { return s ? s->data : nullptr; }
 
 qgpu_status qgpu_state_fill_gaussian(qgpu_state* s, uint64_t seed) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         qgpu::launch_fill_gaussian(s->ctx, s->prec, s->data, s->elems, seed);
         if (!qgpu::op_normalize(s))
@@ -607,7 +590,7 @@ qgpu_status qgpu_state_fill_gaussian(qgpu_state* s, uint64_t seed) {
 }
 
 qgpu_status qgpu_state_convert(const qgpu_state* src, qgpu_state* dst) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(src);
         check_handle(dst);
         if (src->kind != dst->kind || src->dims != dst->dims)
@@ -620,7 +603,7 @@ qgpu_status qgpu_state_convert(const qgpu_state* src, qgpu_state* dst) {
 // ------------------------------------------------------ resident ops
 qgpu_status qgpu_apply(qgpu_state* s, const double* A, uint64_t DA,
                        const uint64_t* target, uint32_t k) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -634,7 +617,7 @@ qgpu_status qgpu_apply_ctrl(qgpu_state* s, const double* A, uint64_t DA,
                             const uint64_t* ctrl, uint32_t nc,
                             const uint64_t* target, uint32_t k,
                             const uint64_t* shift) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -648,7 +631,7 @@ qgpu_status qgpu_apply_ctrl_fan(qgpu_state* s, const double* A, uint64_t DA,
                                 const uint64_t* ctrl, uint32_t nc,
                                 const uint64_t* target, uint32_t k,
                                 const uint64_t* shift) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -660,7 +643,7 @@ qgpu_status qgpu_apply_ctrl_fan(qgpu_state* s, const double* A, uint64_t DA,
 
 qgpu_status qgpu_apply_kraus(qgpu_state* s, const double* Ks, uint32_t nK,
                              uint64_t DA, const uint64_t* target, uint32_t k) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -672,7 +655,7 @@ qgpu_status qgpu_apply_kraus(qgpu_state* s, const double* Ks, uint32_t nK,
 
 qgpu_status qgpu_ptrace(const qgpu_state* s, const uint64_t* target, uint32_t k,
                         qgpu_state** out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -684,7 +667,7 @@ qgpu_status qgpu_ptrace(const qgpu_state* s, const uint64_t* target, uint32_t k,
 
 qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
                             uint32_t k, qgpu_state** out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -696,7 +679,7 @@ qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
 
 qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
                             uint32_t n, qgpu_state** out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -707,14 +690,14 @@ qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
 }
 
 qgpu_status qgpu_norm2(const qgpu_state* s, double* out) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         *out = qgpu::op_norm2(s);
     });
 }
 
 qgpu_status qgpu_trace(const qgpu_state* s, double* re, double* im) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         cd t = qgpu::op_trace(s);
         if (re) *re = t.real();
@@ -723,7 +706,7 @@ qgpu_status qgpu_trace(const qgpu_state* s, double* re, double* im) {
 }
 
 qgpu_status qgpu_normalize(qgpu_state* s) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         if (!qgpu::op_normalize(s))
             raise(QGPU_ERR_DIVISION_BY_ZERO, "qpp::normalize()", "Division by zero!");
@@ -732,7 +715,7 @@ qgpu_status qgpu_normalize(qgpu_state* s) {
 
 qgpu_status qgpu_inner(const qgpu_state* a, const qgpu_state* b, double* re,
                        double* im) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(a);
         check_handle(b);
         if (a->kind != b->kind || a->dims != b->dims || a->prec != b->prec)
@@ -748,7 +731,7 @@ qgpu_status qgpu_host_apply(qgpu_ctx* ctx, const double* state, uint64_t rows,
                             uint64_t cols, const double* A, uint64_t ar,
                             uint64_t ac, const uint64_t* target, uint32_t k,
                             const uint64_t* dims, uint32_t n, double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         uint64_t DA = check_apply(rows, cols, ar, ac, t, d);
@@ -765,7 +748,7 @@ qgpu_status qgpu_host_apply_ctrl(qgpu_ctx* ctx, const double* state,
                                  uint32_t nc, const uint64_t* target, uint32_t k,
                                  const uint64_t* dims, uint32_t n,
                                  const uint64_t* shift, int fan, double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> cv = vec(ctrl, nc), t = vec(target, k), d = vec(dims, n);
         auto sh = check_ctrl(rows, cols, ar, ac, cv, t, d, shift, fan != 0);
@@ -782,7 +765,7 @@ qgpu_status qgpu_host_apply_kraus(qgpu_ctx* ctx, const double* state,
                                   const uint64_t* target, uint32_t k,
                                   const uint64_t* dims, uint32_t n,
                                   double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         uint64_t DA = check_kraus(rows, cols, nK, kr, kc, t, d);
@@ -796,7 +779,7 @@ qgpu_status qgpu_host_apply_kraus(qgpu_ctx* ctx, const double* state,
 qgpu_status qgpu_host_ptrace(qgpu_ctx* ctx, const double* state, uint64_t rows,
                              uint64_t cols, const uint64_t* target, uint32_t k,
                              const uint64_t* dims, uint32_t n, double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         check_subsys_op("qpp::ptrace()", rows, cols, t, d);
@@ -812,7 +795,7 @@ qgpu_status qgpu_host_ptranspose(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* target, uint32_t k,
                                  const uint64_t* dims, uint32_t n,
                                  double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         check_subsys_op("qpp::ptranspose()", rows, cols, t, d);
@@ -828,7 +811,7 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* perm, uint32_t np,
                                  const uint64_t* dims, uint32_t n,
                                  double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> p = vec(perm, np), d = vec(dims, n);
         check_perm(rows, cols, p, d);
@@ -842,7 +825,7 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
 // ------------------------------------------------------- Fourier transforms
 qgpu_status qgpu_apply_qft(qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t d,
                            int swap, int inverse) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -853,7 +836,7 @@ qgpu_status qgpu_apply_qft(qgpu_state* s, const uint64_t* target, uint32_t k, ui
 }
 
 qgpu_status qgpu_qft(qgpu_state* s, uint64_t d, int swap, int inverse) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
@@ -867,7 +850,7 @@ qgpu_status qgpu_qft(qgpu_state* s, uint64_t d, int swap, int inverse) {
 static qgpu_status host_qft(qgpu_ctx* ctx, const double* state, uint64_t rows,
                             uint64_t cols, const uint64_t* target, uint32_t k, bool whole,
                             uint64_t d, int swap, int inverse, double* result) {
-    return guard([&] {
+    return qgpu::guarded(__func__, [&] {
         check_handle(ctx);
         std::vector<uint64_t> t = vec(target, k);
         const char* W = whole ? (inverse ? "qpp::TFQ()" : "qpp::QFT()")

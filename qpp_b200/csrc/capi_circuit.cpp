@@ -61,7 +61,7 @@ extern "C" {
 
 qgpu_status qgpu_circuit_create(uint32_t nq, uint64_t d, uint32_t nc,
                                 qgpu_circuit** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_circuit_create()", "out");
         if (nq == 0) raise(QGPU_ERR_ZERO_SIZE, "qpp::QCircuit::QCircuit()", "nq");
         if (d < 2) raise(QGPU_ERR_DIMS_INVALID, "qpp::QCircuit::QCircuit()", "d");
@@ -74,12 +74,12 @@ qgpu_status qgpu_circuit_create(uint32_t nq, uint64_t d, uint32_t nc,
 }
 
 qgpu_status qgpu_circuit_destroy(qgpu_circuit* c) {
-    return guarded([&] { delete c; });
+    return guarded(__func__, [&] { delete c; });
 }
 
 qgpu_status qgpu_circuit_gate(qgpu_circuit* c, const double* U, uint64_t DU,
                               const uint64_t* target, uint32_t k) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = "qpp::QCircuit::gate()";
         auto t = vec_of(target, k);
@@ -98,7 +98,7 @@ qgpu_status qgpu_circuit_gate(qgpu_circuit* c, const double* U, uint64_t DU,
 
 qgpu_status qgpu_circuit_gate_fan(qgpu_circuit* c, const double* U, uint64_t DU,
                                   const uint64_t* target, uint32_t k) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = "qpp::QCircuit::gate_fan()";
         auto t = vec_of(target, k);
@@ -118,7 +118,7 @@ qgpu_status qgpu_circuit_ctrl(qgpu_circuit* c, const double* U, uint64_t DU,
                               const uint64_t* ctrl, uint32_t nc,
                               const uint64_t* target, uint32_t k,
                               const uint64_t* shift, int fan) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = fan ? "qpp::QCircuit::CTRL_fan()" : "qpp::QCircuit::CTRL()";
         auto cv = vec_of(ctrl, nc), t = vec_of(target, k);
@@ -151,7 +151,7 @@ qgpu_status qgpu_circuit_cctrl(qgpu_circuit* c, const double* U, uint64_t DU,
                                const uint64_t* ctrl_dits, uint32_t nc,
                                const uint64_t* target, uint32_t k,
                                const uint64_t* shift, int fan) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = fan ? "qpp::QCircuit::cCTRL_fan()" : "qpp::QCircuit::cCTRL()";
         auto cv = vec_of(ctrl_dits, nc), t = vec_of(target, k);
@@ -178,7 +178,7 @@ qgpu_status qgpu_circuit_cctrl(qgpu_circuit* c, const double* U, uint64_t DU,
 
 qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target, uint32_t k,
                                  uint64_t c_reg, int destructive) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = k > 1 ? "qpp::QCircuit::measure_many()" : "qpp::QCircuit::measure()";
         auto t = vec_of(target, k);
@@ -196,7 +196,7 @@ qgpu_status qgpu_circuit_measure(qgpu_circuit* c, const uint64_t* target, uint32
 
 // QCircuit::reset (qcircuit.hpp): RESET / RESET_MANY measurement steps.
 qgpu_status qgpu_circuit_reset(qgpu_circuit* c, const uint64_t* target, uint32_t k) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = k > 1 ? "qpp::QCircuit::reset_many()" : "qpp::QCircuit::reset()";
         auto t = vec_of(target, k);
@@ -213,7 +213,7 @@ qgpu_status qgpu_circuit_reset(qgpu_circuit* c, const uint64_t* target, uint32_t
 // the dits (dits[0] the least significant bit) spell `value`.
 qgpu_status qgpu_circuit_cond_if(qgpu_circuit* c, const uint64_t* dits, uint32_t n,
                                  uint64_t value) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = "qpp::QCircuit::cond_if()";
         for (const auto& st : c->steps)
@@ -239,7 +239,7 @@ qgpu_status qgpu_circuit_cond_if(qgpu_circuit* c, const uint64_t* dits, uint32_t
 // target == NULL takes every qudit not yet measured (QFT(bool swap)).
 qgpu_status qgpu_circuit_qft(qgpu_circuit* c, const uint64_t* target, uint32_t k, int swap,
                              int inverse) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = inverse ? "qpp::QCircuit::TFQ()" : "qpp::QCircuit::QFT()";
         auto meas = measured_of(c);
@@ -304,7 +304,7 @@ qgpu_status qgpu_circuit_qft(qgpu_circuit* c, const uint64_t* target, uint32_t k
 }
 
 qgpu_status qgpu_circuit_cond_end(qgpu_circuit* c) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         size_t open = c->steps.size();
         for (size_t i = c->steps.size(); i-- > 0;)
@@ -324,7 +324,7 @@ qgpu_status qgpu_circuit_cond_end(qgpu_circuit* c) {
 
 qgpu_status qgpu_circuit_channel(qgpu_circuit* c, const double* Ks, uint32_t nK, uint64_t DK,
                                  const uint64_t* target, uint32_t k) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         const char* W = "qgpu_circuit_channel()";
         auto t = vec_of(target, k);
@@ -344,7 +344,7 @@ qgpu_status qgpu_circuit_channel(qgpu_circuit* c, const double* Ks, uint32_t nK,
 }
 
 qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq, uint64_t* n_steps) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         if (nq) *nq = c->nq;
         if (n_steps) *n_steps = c->steps.size();
@@ -352,7 +352,7 @@ qgpu_status qgpu_circuit_info(const qgpu_circuit* c, uint32_t* nq, uint64_t* n_s
 }
 
 qgpu_status qgpu_circuit_shape(const qgpu_circuit* c, uint32_t* nq, uint64_t* d, uint32_t* nc) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         if (nq) *nq = c->nq;
         if (d) *d = c->d;
@@ -361,7 +361,7 @@ qgpu_status qgpu_circuit_shape(const qgpu_circuit* c, uint32_t* nq, uint64_t* d,
 }
 
 qgpu_status qgpu_circuit_fuse(qgpu_circuit* c, uint32_t max_k, uint64_t* n_passes) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(c);
         if (c->d != 2) raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_circuit_fuse()", "qubit circuits only");
         if (max_k < 1 || max_k > 12)
@@ -372,7 +372,7 @@ qgpu_status qgpu_circuit_fuse(qgpu_circuit* c, uint32_t max_k, uint64_t* n_passe
 }
 
 qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         need_handle(c);
         if (s->dims.size() != c->nq)
@@ -384,7 +384,7 @@ qgpu_status qgpu_run_gates(qgpu_state* s, qgpu_circuit* c, int form) {
 }
 
 qgpu_status qgpu_apply_tc(qgpu_state* s, const double* U, const uint64_t* target, uint32_t k) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         const char* W = "qgpu_apply_tc()";
         auto t = vec_of(target, k);

@@ -662,7 +662,7 @@ extern "C" {
 
 qgpu_status qgpu_engine_create(qgpu_ctx* ctx, qgpu_circuit* c, qgpu_kind kind,
                                qgpu_prec prec, qgpu_engine** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(ctx);
         need_handle(c);
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_engine_create()", "out");
@@ -677,11 +677,11 @@ qgpu_status qgpu_engine_create(qgpu_ctx* ctx, qgpu_circuit* c, qgpu_kind kind,
 }
 
 qgpu_status qgpu_engine_destroy(qgpu_engine* e) {
-    return guarded([&] { delete e; });
+    return guarded(__func__, [&] { delete e; });
 }
 
 qgpu_status qgpu_engine_set_seed(qgpu_engine* e, uint64_t seed) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         e->gen.seed(static_cast<std::mt19937::result_type>(seed));
     });
@@ -689,7 +689,7 @@ qgpu_status qgpu_engine_set_seed(qgpu_engine* e, uint64_t seed) {
 
 qgpu_status qgpu_engine_set_noise(qgpu_engine* e, const double* Ks, uint32_t nK, uint64_t d,
                                   const double* probs) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         if (nK == 0) {
             e->noisy = false;
@@ -716,7 +716,7 @@ qgpu_status qgpu_engine_set_noise(qgpu_engine* e, const double* Ks, uint32_t nK,
 }
 
 qgpu_status qgpu_engine_set_state(qgpu_engine* e, const qgpu_state* s) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         need_handle(s);
         // QEngineT::set_state (qengine.hpp:1191-1214): the state must match
@@ -743,7 +743,7 @@ qgpu_status qgpu_engine_set_state(qgpu_engine* e, const qgpu_state* s) {
 }
 
 qgpu_status qgpu_engine_reset(qgpu_engine* e, int reset_stats) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         // QEngineT::reset (qengine.hpp:1251-1260) / QNoisyEngineT::reset
         qgpu::free_state(e->st);
@@ -756,7 +756,7 @@ qgpu_status qgpu_engine_reset(qgpu_engine* e, int reset_stats) {
 
 qgpu_status qgpu_engine_set_replay(qgpu_engine* e, const uint64_t* outcomes, uint64_t n_out,
                                    const uint64_t* noise, uint64_t n_noise) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         e->replay = outcomes != nullptr || noise != nullptr;
         e->forced_outcomes.assign(outcomes, outcomes ? outcomes + n_out : outcomes);
@@ -766,7 +766,7 @@ qgpu_status qgpu_engine_set_replay(qgpu_engine* e, const uint64_t* outcomes, uin
 }
 
 qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         if (reps == 0)
             raise(QGPU_ERR_OUT_OF_RANGE,
@@ -813,7 +813,7 @@ qgpu_status qgpu_engine_execute(qgpu_engine* e, uint64_t reps) {
 }
 
 qgpu_status qgpu_engine_get_dits(const qgpu_engine* e, uint64_t* dits, double* probs) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         if (dits) std::copy(e->dits.begin(), e->dits.end(), dits);
         if (probs) std::copy(e->probs.begin(), e->probs.end(), probs);
@@ -821,7 +821,7 @@ qgpu_status qgpu_engine_get_dits(const qgpu_engine* e, uint64_t* dits, double* p
 }
 
 qgpu_status qgpu_engine_get_state(const qgpu_engine* e, qgpu_state** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         if (!e->st) raise(QGPU_ERR_INVALID_HANDLE, "qpp::QEngineT::get_state()", "not executed");
         qgpu_state* c = qgpu::new_state(e->ctx, e->st->kind, e->st->prec, e->st->dims, false);
@@ -834,7 +834,7 @@ qgpu_status qgpu_engine_get_state(const qgpu_engine* e, qgpu_state** out) {
 // number of distinct outcome vectors, then (counts, dits) when arrays given
 qgpu_status qgpu_engine_get_stats(const qgpu_engine* e, uint64_t* n_distinct,
                                   uint64_t* counts, uint64_t* outcomes) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         if (n_distinct) *n_distinct = e->stats.size();
         size_t i = 0, nc = e->circ->nc;
@@ -850,7 +850,7 @@ qgpu_status qgpu_engine_get_stats(const qgpu_engine* e, uint64_t* n_distinct,
 // (in execution order) and Kraus indices (step by step, qudit by qudit)
 qgpu_status qgpu_engine_get_record(const qgpu_engine* e, uint64_t* n_out, uint64_t* outcomes,
                                    uint64_t* n_noise, uint64_t* noise) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(e);
         if (n_out) *n_out = e->rec_outcomes.size();
         if (outcomes) std::copy(e->rec_outcomes.begin(), e->rec_outcomes.end(), outcomes);
@@ -878,7 +878,7 @@ bool targets_ok(const std::vector<uint64_t>& t, size_t n) {
 qgpu_status qgpu_sample(const qgpu_state* s, const uint64_t* target, uint32_t k,
                         uint64_t num_samples, uint64_t seed, const double* u,
                         uint64_t* results) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         const char* W = "qpp::sample()";
         std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
@@ -910,7 +910,7 @@ qgpu_status qgpu_sample(const qgpu_state* s, const uint64_t* target, uint32_t k,
 qgpu_status qgpu_measure_seq(const qgpu_state* s, const uint64_t* target, uint32_t k,
                              int destructive, uint64_t seed, const uint64_t* forced,
                              uint64_t* results, double* probs, qgpu_state** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         const char* W = "qpp::measure_seq()";
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "out");
@@ -1036,7 +1036,7 @@ qgpu_status qgpu_measure_kraus(const qgpu_state* s, const double* Ks, uint32_t n
                                const uint64_t* target, uint32_t k, int destructive,
                                uint64_t seed, uint64_t* result, double* probs,
                                qgpu_state** outs) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
         check_kraus_shape(s, tgt, nK, DK);
@@ -1056,7 +1056,7 @@ qgpu_status qgpu_measure_basis(const qgpu_state* s, const double* V, uint64_t ro
                                const uint64_t* target, uint32_t k, int destructive,
                                uint64_t seed, uint64_t* result, double* probs,
                                qgpu_state** outs) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         std::vector<uint64_t> tgt = qgpu::vec_of(target, k);
         if (!targets_ok(tgt, s->dims.size()))
@@ -1113,7 +1113,7 @@ qgpu_status qgpu_measure_basis(const qgpu_state* s, const double* V, uint64_t ro
 // the i-th target as qpp indexes it.
 qgpu_status qgpu_reset(const qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t seed,
                        qgpu_state** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         const char* W = "qpp::reset()";
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "out");
@@ -1150,7 +1150,7 @@ qgpu_status qgpu_reset(const qgpu_state* s, const uint64_t* target, uint32_t k, 
 // with destruction, keeping only the post-measurement state.
 qgpu_status qgpu_discard(const qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t seed,
                          qgpu_state** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(s);
         const char* W = "qpp::discard()";
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, W, "out");

@@ -691,7 +691,7 @@ extern "C" {
 
 // qpp::qasm::read_from_string (qasm.hpp:800-806)
 qgpu_status qgpu_qasm_read(const char* source, qgpu_circuit** out) {
-    return qgpu::guarded([&] {
+    return qgpu::guarded(__func__, [&] {
         if (!source || !out) qgpu::raise(QGPU_ERR_INVALID_ARGUMENT, kRead, "source/out");
         *out = build(source);
     });
@@ -699,7 +699,7 @@ qgpu_status qgpu_qasm_read(const char* source, qgpu_circuit** out) {
 
 // qpp::qasm::read_from_file (qasm.hpp:815-820)
 qgpu_status qgpu_qasm_read_file(const char* path, qgpu_circuit** out) {
-    return qgpu::guarded([&] {
+    return qgpu::guarded(__func__, [&] {
         if (!path || !out) qgpu::raise(QGPU_ERR_INVALID_ARGUMENT, kRead, "path/out");
         std::ifstream f(path);
         if (!f) qgpu::raise(QGPU_ERR_INVALID_ARGUMENT, kRead, std::string("cannot open ") + path);

@@ -682,7 +682,7 @@ using qgpu::raise;
 extern "C" {
 
 qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode, qgpu_server** out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_server_create()", "out");
         if (mode != 0 && mode != 1)
             raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_server_create()", "mode");
@@ -693,7 +693,7 @@ qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode, qgpu_s
         for (int i = 0; i < 4; ++i) {
             qgpu_status st = qgpu_ctx_create(device, ctxs[i]);
             if (st == QGPU_OK && i >= 2)
-                st = qgpu::guarded([&] { qgpu::raise_priority(*ctxs[i]); });
+                st = qgpu::guarded(__func__, [&] { qgpu::raise_priority(*ctxs[i]); });
             if (st != QGPU_OK) {
                 for (int j = 0; j < 4; ++j)
                     if (*ctxs[j]) qgpu_ctx_destroy(*ctxs[j]);
@@ -709,7 +709,7 @@ qgpu_status qgpu_server_create(int device, uint64_t hbm_budget, int mode, qgpu_s
 
 qgpu_status qgpu_server_submit(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind, double p,
                                uint64_t shots, uint64_t seed, uint64_t* id) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(S);
         need_handle(c);
         if (shots == 0) raise(QGPU_ERR_OUT_OF_RANGE, "qgpu_server_submit()", "shots");
@@ -755,7 +755,7 @@ qgpu_status qgpu_server_submit(qgpu_server* S, qgpu_circuit* c, qgpu_kind kind, 
 // request is released after a successful wait.
 qgpu_status qgpu_server_wait(qgpu_server* S, uint64_t id, double timeout_s, double* latency_s,
                              uint64_t* samples, uint32_t* dits) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(S);
         qgpu::Request* r = nullptr;
         {
@@ -780,7 +780,7 @@ qgpu_status qgpu_server_wait(qgpu_server* S, uint64_t id, double timeout_s, doub
 
 qgpu_status qgpu_server_stats(qgpu_server* S, uint64_t* batches, uint64_t* trajectories,
                               uint64_t* engine_runs, double* busy_s) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(S);
         std::lock_guard<std::mutex> lock(S->mu);
         if (batches) *batches = S->batches;
@@ -791,7 +791,7 @@ qgpu_status qgpu_server_stats(qgpu_server* S, uint64_t* batches, uint64_t* traje
 }
 
 qgpu_status qgpu_server_destroy(qgpu_server* S) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (!S) return;
         {
             std::lock_guard<std::mutex> lock(S->mu);

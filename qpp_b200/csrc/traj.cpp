@@ -652,7 +652,7 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
                                          uint64_t shots, uint64_t seed, uint64_t* samples,
                                          uint32_t* dits, double* dump, uint32_t* events,
                                          uint32_t max_events) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(ctx);
         need_handle(c);
         const char* W = "qgpu_trajectories()";
@@ -738,7 +738,7 @@ extern "C" qgpu_status qgpu_trajectories(qgpu_ctx* ctx, qgpu_circuit* c, double 
 }
 
 extern "C" qgpu_status qgpu_traj_fusion_width(qgpu_ctx* ctx, uint32_t n, int set_w, int* chosen) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(ctx);
         const char* W = "qgpu_traj_fusion_width()";
         if (n < 1 || n > uint32_t(qgpu::kTrajMaxGlobalQubits))
@@ -752,7 +752,7 @@ extern "C" qgpu_status qgpu_traj_fusion_width(qgpu_ctx* ctx, uint32_t n, int set
 }
 
 extern "C" qgpu_status qgpu_traj_tile_width(qgpu_ctx* ctx, uint32_t n, int set_T, int* chosen) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         need_handle(ctx);
         const char* W = "qgpu_traj_tile_width()";
         if (n == 0 || n > uint32_t(qgpu::kTrajMaxGlobalQubits)) raise(QGPU_ERR_OUT_OF_RANGE, W, "n");
