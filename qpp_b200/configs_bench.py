@@ -97,7 +97,7 @@ def config1(ctx, torch, stream, peak=None):
                                "16 MiB state stays in the 126 MB L2, so the fraction can exceed 1"}
     finals = {"circuit": s.numpy()}
     # the fused form: the gates merged into blocks of <= 2 qubits (a 1-qubit
-    # gate folded into a neighbouring block), run as tile passes
+    # gate folded into a neighbouring block), list-scheduled into tile passes
     c.run(s, FUSED)  # warm-up: builds the plan
     times = []
     for _ in range(5):
@@ -113,7 +113,7 @@ def config1(ctx, torch, stream, peak=None):
                     "plan_entries": c.fused_passes(2), "runs": len(times),
                     "form": "qgpu_run_gates, fused complex128: gates merged into blocks of "
                             "<= 2 qubits (controlled gates with more controls as they are), "
-                            "run as tile passes"}
+                            "list-scheduled into tile passes"}
     finals["fused"] = s.numpy()
     s.free()
     return out, seq, finals

@@ -499,14 +499,16 @@ void tiled_runs(const qgpu_circuit* c, std::vector<TiledRun>& out) {
 }
 
 // The fused plan's blocks (<= 2 qubits) and its unfused steps in circuit
-// order, as tile passes (kernels_tile.cu); a step the passes do not take runs
-// as it is between them.
+// order, as tile passes (kernels_tile.cu), each run list-scheduled into
+// fewer passes and sweeps; a step the passes do not take runs as it is
+// between them.
 static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
     std::vector<TiledRun> runs;
     tiled_runs(c, runs);
+    const int Tmax = tile_bits_max(s->ctx, s->prec);
     for (const TiledRun& r : runs) {
         if (r.step >= 0) apply_step(s, c->steps[size_t(r.step)]);
-        else run_tiled_gates(s, r.gates);
+        else run_tiled_gates(s, schedule_gates(r.gates, int(c->nq), Tmax));
     }
 }
 

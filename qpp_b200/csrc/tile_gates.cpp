@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <set>
 
 #include "circuit.hpp"
 #include "kernels.hpp"
@@ -109,6 +110,94 @@ bool gate_desc_of(const Step& st, int nbits, std::vector<GateDesc>& out) {
     }
 }
 
+// Tile of at most Tmax bits on an nbits-qubit ket: the L lowest state bits
+// (five: coalesced runs; fewer when the tile must still hold the two targets
+// of any 2-qubit gate above them) and up to nfree = T - L others.
+static void tile_split(int nbits, int Tmax, int& L, int& nfree) {
+    const int T = std::min(nbits, Tmax);
+    L = std::min(T, 5);
+    if (T < nbits && T - L < 2) L = std::max(0, T - 2);
+    nfree = T - L;
+}
+
+std::vector<GateDesc> schedule_gates(const std::vector<GateDesc>& gates, int nbits, int Tmax) {
+    int L = 0, nfree = 0;
+    tile_split(nbits, Tmax, L, nfree);
+    const size_t N = gates.size();
+    // gate j waits for the last earlier gate on each of its bits (targets
+    // and controls)
+    std::vector<uint32_t> npred(N, 0);
+    std::vector<std::vector<uint32_t>> succ(N);
+    std::vector<int64_t> last(size_t(std::max(nbits, 1)), -1);
+    for (size_t j = 0; j < N; ++j) {
+        const GateDesc& g = gates[j];
+        std::vector<int> bits{g.b0};
+        if (g.op == 2) bits.push_back(g.b1);
+        for (const auto& c : g.ctrl) bits.push_back(c.first);
+        std::vector<int64_t> pred;
+        for (int b : bits) {
+            if (last[size_t(b)] >= 0) pred.push_back(last[size_t(b)]);
+            last[size_t(b)] = int64_t(j);
+        }
+        std::sort(pred.begin(), pred.end());
+        pred.erase(std::unique(pred.begin(), pred.end()), pred.end());
+        for (int64_t p : pred) succ[size_t(p)].push_back(uint32_t(j));
+        npred[j] = uint32_t(pred.size());
+    }
+    std::set<uint32_t> ready; // in circuit order
+    for (size_t j = 0; j < N; ++j)
+        if (!npred[j]) ready.insert(uint32_t(j));
+    std::vector<GateDesc> out;
+    out.reserve(N);
+    while (!ready.empty()) {
+        // one pass: ready gates while their targets above the low L bits fit
+        // in nfree bits, those that extend the current sweep (<= 3 target
+        // bits) first
+        uint64_t hi = 0;
+        int sw[kSweepBits], nsw = 0;
+        size_t in_pass = 0;
+        while (in_pass < kTileMaxGates) {
+            int64_t pick = -1;
+            bool pick_in_sweep = false;
+            for (uint32_t j : ready) {
+                const GateDesc& g = gates[j];
+                uint64_t h2 = hi;
+                for (int b : {g.b0, g.op == 2 ? g.b1 : -1})
+                    if (b >= L) h2 |= uint64_t(1) << b;
+                if (__builtin_popcountll(h2) > nfree) continue;
+                int n2 = nsw;
+                for (int b : {g.b0, g.op == 2 ? g.b1 : -1}) {
+                    bool have = false;
+                    for (int x = 0; x < nsw; ++x) have |= sw[x] == b;
+                    if (b >= 0 && !have) ++n2;
+                }
+                if (n2 <= kSweepBits) {
+                    pick = j;
+                    pick_in_sweep = true;
+                    break;
+                }
+                if (pick < 0) pick = j;
+            }
+            if (pick < 0) break;
+            const GateDesc& g = gates[size_t(pick)];
+            if (!pick_in_sweep) nsw = 0;
+            for (int b : {g.b0, g.op == 2 ? g.b1 : -1}) {
+                if (b < 0) continue;
+                if (b >= L) hi |= uint64_t(1) << b;
+                bool have = false;
+                for (int x = 0; x < nsw; ++x) have |= sw[x] == b;
+                if (!have) sw[nsw++] = b;
+            }
+            out.push_back(g);
+            ++in_pass;
+            ready.erase(uint32_t(pick));
+            for (uint32_t s2 : succ[size_t(pick)])
+                if (--npred[s2] == 0) ready.insert(s2);
+        }
+    }
+    return out;
+}
+
 void plan_gate_tiles(const std::vector<GateDesc>& gates, int nbits, int Tmax,
                      std::vector<TilePassParams>& passes, std::vector<TileGate>& dev,
                      std::vector<TileSweep>& sweeps, std::vector<cd>& mats) {
@@ -116,12 +205,8 @@ void plan_gate_tiles(const std::vector<GateDesc>& gates, int nbits, int Tmax,
     dev.clear();
     sweeps.clear();
     mats.clear();
-    const int T = std::min(nbits, Tmax);
-    // low bits: five (coalesced runs), fewer when the tile must still hold the
-    // two targets of any 2-qubit gate above them
-    int L = std::min(T, 5);
-    if (T < nbits && T - L < 2) L = std::max(0, T - 2);
-    const int nfree = T - L;
+    int L = 0, nfree = 0;
+    tile_split(nbits, Tmax, L, nfree);
     size_t i = 0;
     while (i < gates.size()) {
         // greedy run: targets outside the low L bits within nfree bits

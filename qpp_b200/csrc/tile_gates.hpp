@@ -35,6 +35,12 @@ bool gate_desc_of(const Step& st, int nbits, std::vector<GateDesc>& out);
 void plan_gate_tiles(const std::vector<GateDesc>& gates, int nbits, int Tmax,
                      std::vector<TilePassParams>& passes, std::vector<TileGate>& dev,
                      std::vector<TileSweep>& sweeps, std::vector<cd>& mats);
+// The gates reordered for fewer tile passes and sweeps (list scheduling):
+// every gate still follows the earlier gates it shares a bit with (target or
+// control), so the product is the same up to rounding, but each pass takes
+// every ready gate whose targets fit the tile, those that extend the current
+// sweep first. For forms that do not promise the gate-by-gate arithmetic.
+std::vector<GateDesc> schedule_gates(const std::vector<GateDesc>& gates, int nbits, int Tmax);
 // Largest tile (bits) for this context and precision: 13 for complex128 and
 // 14 for complex64 (128 KB of shared memory), or qgpu_ctx_set_tile_bits's.
 int tile_bits_max(const qgpu_ctx* ctx, qgpu_prec prec);

@@ -5,9 +5,12 @@
 // runs' gate descriptors applied one by one on the host, with the runs' steps
 // in between, must equal the circuit's steps applied one by one within 1e-12
 // (relative, max-norm): the blocks' qubit order, their column-major matrices
-// and the cut into runs and steps are what the tile passes execute. The tile
-// passes' own addressing is checked against gate-by-gate application by
-// test_gate_tiles.cpp. Built and run by tests/test_fused_tiles.py.
+// and the cut into runs and steps are what the tile passes execute. Each run
+// list-scheduled (qgpu::schedule_gates, tiles of 5-13 bits) must give the
+// same product within 1e-12 and plan into no more passes than circuit order.
+// The tile passes' own addressing is checked against gate-by-gate
+// application by test_gate_tiles.cpp. Built and run by
+// tests/test_fused_tiles.py.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -126,6 +129,7 @@ static std::vector<uint64_t> distinct(std::mt19937_64& rng, int n, int k) {
 int main() {
     std::mt19937_64 rng(7);
     int cases = 0, with_steps = 0;
+    size_t passes_in_order = 0, passes_scheduled = 0, sweeps_in_order = 0, sweeps_scheduled = 0;
     for (int n = 1; n <= 12; ++n)
         for (int rep = 0; rep < 4; ++rep) {
             qgpu_circuit* c = nullptr;
@@ -170,17 +174,19 @@ int main() {
             std::vector<C> psi(size_t(1) << n);
             std::normal_distribution<double> nd;
             for (auto& x : psi) x = C(nd(rng), nd(rng));
-            std::vector<C> ref = psi, got = psi;
+            std::vector<C> ref = psi, got = psi, sch = psi;
             for (const Step& st : c->steps) apply_step_host(ref, n, st);
             c->plan = fuse(c->steps, c->nq, 2);
             c->plan_k = 2;
             std::vector<TiledRun> runs;
             tiled_runs(c, runs);
             size_t gates = 0;
+            const int Tmax = 5 + int(rng() % 9); // tiles of 5-13 bits
             for (const TiledRun& r : runs) {
                 if (r.step >= 0) {
                     EXPECT(r.gates.empty());
                     apply_step_host(got, n, c->steps[size_t(r.step)]);
+                    apply_step_host(sch, n, c->steps[size_t(r.step)]);
                     ++with_steps;
                     continue;
                 }
@@ -191,20 +197,41 @@ int main() {
                     apply_desc(got, g);
                     ++gates;
                 }
+                // the list-scheduled order: the same gates, no more passes
+                // than circuit order, the same product up to rounding
+                const std::vector<GateDesc> s2 = schedule_gates(r.gates, n, Tmax);
+                EXPECT(s2.size() == r.gates.size());
+                for (const GateDesc& g : s2) apply_desc(sch, g);
+                std::vector<TilePassParams> p0, p1;
+                std::vector<TileGate> d;
+                std::vector<TileSweep> sw0, sw1;
+                std::vector<cd> m;
+                plan_gate_tiles(r.gates, n, Tmax, p0, d, sw0, m);
+                plan_gate_tiles(s2, n, Tmax, p1, d, sw1, m);
+                EXPECT(p1.size() <= p0.size());
+                passes_in_order += p0.size();
+                passes_scheduled += p1.size();
+                sweeps_in_order += sw0.size();
+                sweeps_scheduled += sw1.size();
             }
             EXPECT(gates <= c->steps.size() * 3); // fan gates expand, blocks merge
-            double err = 0, scale = 0;
+            double err = 0, err_s = 0, scale = 0;
             for (size_t i = 0; i < ref.size(); ++i) {
                 err = std::max(err, std::abs(got[i] - ref[i]));
+                err_s = std::max(err_s, std::abs(sch[i] - ref[i]));
                 scale = std::max(scale, std::abs(ref[i]));
             }
             EXPECT(err <= 1e-12 * scale);
-            if (err > 1e-12 * scale)
-                std::printf("n=%d rep=%d: rel err %.3e\n", n, rep, err / scale);
+            EXPECT(err_s <= 1e-12 * scale);
+            if (err > 1e-12 * scale || err_s > 1e-12 * scale)
+                std::printf("n=%d rep=%d: rel err %.3e, scheduled %.3e\n", n, rep, err / scale,
+                            err_s / scale);
             qgpu_circuit_destroy(c);
             ++cases;
         }
     std::printf("%d circuits, %d steps run as they are\n", cases, with_steps);
+    std::printf("tile passes %zu in circuit order, %zu scheduled; sweeps %zu / %zu\n",
+                passes_in_order, passes_scheduled, sweeps_in_order, sweeps_scheduled);
     std::printf(fails ? "fused tiles FAILED (%d)\n" : "fused tiles ok\n", fails);
     return fails ? 1 : 0;
 }
