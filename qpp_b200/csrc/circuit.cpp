@@ -498,17 +498,38 @@ void tiled_runs(const qgpu_circuit* c, std::vector<TiledRun>& out) {
     }
 }
 
-// The fused plan's blocks (<= 2 qubits) and its unfused steps in circuit
-// order, as tile passes (kernels_tile.cu), each run list-scheduled into
-// fewer passes and sweeps; a step the passes do not take runs as it is
-// between them.
-static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
+// Plans the fused plan's blocks (<= 2 qubits, c->plan) and its unfused
+// steps as tile programs once per circuit (again after steps are added or
+// the tile size changes): each run list-scheduled into fewer passes and
+// sweeps, then cut into passes.
+static void prepare_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
+    const int Tmax = tile_bits_max(s->ctx, s->prec);
+    if (c->ftiles && c->ftiles->nsteps == c->steps.size() && c->ftiles->Tmax == Tmax) return;
+    auto F = std::make_shared<FusedTiles>();
+    F->nsteps = c->steps.size();
+    F->Tmax = Tmax;
     std::vector<TiledRun> runs;
     tiled_runs(c, runs);
-    const int Tmax = tile_bits_max(s->ctx, s->prec);
     for (const TiledRun& r : runs) {
-        if (r.step >= 0) apply_step(s, c->steps[size_t(r.step)]);
-        else run_tiled_gates(s, schedule_gates(r.gates, int(c->nq), Tmax));
+        if (r.step >= 0) {
+            F->runs.push_back({r.step, TileProgram{}});
+        } else if (!r.gates.empty()) {
+            TileProgram P;
+            plan_tile_program(schedule_gates(r.gates, int(c->nq), Tmax), int(c->nq), Tmax, P);
+            F->runs.push_back({-1, std::move(P)});
+        }
+    }
+    c->ftiles = std::move(F);
+}
+
+// The planned tile programs in order, a step the passes do not take run as
+// it is between them.
+static void launch_tiled_blocks(qgpu_state* s, qgpu_circuit* c) {
+    prepare_plan(s, c, 2); // both no-ops after fused_prepare
+    prepare_tiled_blocks(s, c);
+    for (const auto& r : c->ftiles->runs) {
+        if (r.first >= 0) apply_step(s, c->steps[size_t(r.first)]);
+        else run_tile_program(s, r.second);
     }
 }
 
@@ -526,6 +547,7 @@ void fused_prepare(qgpu_state* s, qgpu_circuit* c) {
     if (c->d != 2)
         raise(QGPU_ERR_NOT_SUPPORTED, "qgpu_run_gates()", "fused form needs a qubit ket");
     prepare_plan(s, c, s->prec == QGPU_C64 ? 6 : fused_tiles(s) ? 2 : 3);
+    if (fused_tiles(s)) prepare_tiled_blocks(s, c);
     if (!c->block_slot.empty()) ctx_error_flag(s->ctx); // allocated outside any capture
 }
 

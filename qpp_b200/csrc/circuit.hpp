@@ -25,6 +25,7 @@ namespace qgpu {
 
 using cd = std::complex<double>;
 struct TProgram;
+struct FusedTiles;
 
 enum class StepKind {
     Gate,      // apply(U, target)           GType SINGLE/TWO/THREE/JOINT
@@ -87,6 +88,9 @@ struct qgpu_circuit {
     // first rho_steps steps (steps are only ever appended)
     uint64_t rho_steps = ~uint64_t(0);
     std::shared_ptr<qgpu::TProgram> rho_prog; // null: the form does not apply
+    // fused complex128 ket form as tile passes (blocks of <= 2 qubits),
+    // planned for the first ftiles->nsteps steps
+    std::shared_ptr<qgpu::FusedTiles> ftiles;
     // fused density-matrix form on the tensor cores (complex64, 2n >= 13
     // virtual qubits): superoperator blocks of <= 6 virtual qubits, built for
     // the first rho_tc_steps steps

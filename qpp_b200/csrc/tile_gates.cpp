@@ -303,14 +303,22 @@ int tile_bits_max(const qgpu_ctx* ctx, qgpu_prec prec) {
     return cap;
 }
 
-void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates) {
-    if (gates.empty()) return;
-    const int nbits = int(s->dims.size());
-    std::vector<TilePassParams> passes;
-    std::vector<TileGate> dev;
-    std::vector<TileSweep> sweeps;
-    std::vector<cd> mats;
-    plan_gate_tiles(gates, nbits, tile_bits_max(s->ctx, s->prec), passes, dev, sweeps, mats);
+void plan_tile_program(const std::vector<GateDesc>& gates, int nbits, int Tmax, TileProgram& P) {
+    P.nbits = nbits;
+    P.Tmax = Tmax;
+    P.gates = gates;
+    plan_gate_tiles(gates, nbits, Tmax, P.passes, P.dev, P.sweeps, P.mats);
+}
+
+void run_tile_program(qgpu_state* s, const TileProgram& P) {
+    if (P.gates.empty()) return;
+    if (P.nbits != int(s->dims.size()))
+        raise(QGPU_ERR_DIMS_MISMATCH_CVECTOR, "qgpu_run_gates()", "tile program / state");
+    const int nbits = P.nbits;
+    const auto& passes = P.passes;
+    const auto& dev = P.dev;
+    const auto& sweeps = P.sweeps;
+    const auto& mats = P.mats;
     // a pass of one uncontrolled gate runs on the one-gate kernels
     bool any_tiled = false;
     for (const auto& p : passes)
@@ -341,7 +349,7 @@ void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates) {
     }
     size_t gi = 0;
     for (const auto& p : passes) {
-        const GateDesc& g0 = gates[gi];
+        const GateDesc& g0 = P.gates[gi];
         if (p.ngates == 1 && g0.ctrl.empty()) {
             if (g0.op == 1) launch_qubit_1q(s->ctx, s->prec, s->data, nbits, g0.b0, g0.A);
             else launch_qubit_2q(s->ctx, s->prec, s->data, nbits, g0.b0, g0.b1, g0.A);
@@ -352,6 +360,13 @@ void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates) {
         gi += p.ngates;
     }
     if (buf) QG_CUDA(cudaFreeAsync(buf, s->ctx->stream));
+}
+
+void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates) {
+    if (gates.empty()) return;
+    TileProgram P;
+    plan_tile_program(gates, int(s->dims.size()), tile_bits_max(s->ctx, s->prec), P);
+    run_tile_program(s, P);
 }
 
 } // namespace qgpu

@@ -44,8 +44,30 @@ std::vector<GateDesc> schedule_gates(const std::vector<GateDesc>& gates, int nbi
 // Largest tile (bits) for this context and precision: 13 for complex128 and
 // 14 for complex64 (128 KB of shared memory), or qgpu_ctx_set_tile_bits's.
 int tile_bits_max(const qgpu_ctx* ctx, qgpu_prec prec);
+// A run of gates planned as tile passes on an nbits-qubit ket (host side;
+// uploaded by run_tile_program each time it runs).
+struct TileProgram {
+    int nbits = 0, Tmax = 0;
+    std::vector<GateDesc> gates; // in pass order
+    std::vector<TilePassParams> passes;
+    std::vector<TileGate> dev;
+    std::vector<TileSweep> sweeps;
+    std::vector<cd> mats;
+};
+void plan_tile_program(const std::vector<GateDesc>& gates, int nbits, int Tmax, TileProgram& P);
+// Uploads P's tables and launches its passes on s (stream order).
+void run_tile_program(qgpu_state* s, const TileProgram& P);
 // Runs `gates` on the qubit ket s as planned tile passes (stream order).
 void run_tiled_gates(qgpu_state* s, const std::vector<GateDesc>& gates);
+
+// The fused complex128 tile form of a circuit, planned once: list-scheduled
+// tile programs and the unfused steps between them, for the circuit's first
+// nsteps steps and tiles of at most Tmax bits.
+struct FusedTiles {
+    uint64_t nsteps = 0;
+    int Tmax = 0;
+    std::vector<std::pair<int64_t, TileProgram>> runs; // first >= 0: that step as it is
+};
 
 // A piece of a fused complex128 ket plan: a run of gate descriptors for the
 // tile passes (step < 0; possibly empty), or one step run as it is.
