@@ -25,7 +25,10 @@
  * (where, what) strings, e.g. ("qpp::apply()", "dims/target").
  *
  * Threading: a context may be used from several threads; a state handle may
- * not be used by two threads at once. Errors are recorded per thread.
+ * not be used by two threads at once. A circuit keeps the plans of its fused
+ * forms (built by the first qgpu_run_gates in that form, again after steps
+ * are added): run it in a fused form from one thread at a time, or run it
+ * once before sharing it. Errors are recorded per thread.
  */
 #ifndef QPP_B200_H_
 #define QPP_B200_H_
