@@ -8,7 +8,8 @@
 // and the cut into runs and steps are what the tile passes execute. Each run
 // list-scheduled (qgpu::schedule_gates, tiles of 5-13 bits) must give the
 // same product within 1e-12 and plan into no more passes than circuit order.
-// The tile passes' own addressing is checked against gate-by-gate
+// On kets of 20-30 qubits the schedule keeps every bit's gates in circuit
+// order. The tile passes' own addressing is checked against gate-by-gate
 // application by test_gate_tiles.cpp. Built and run by
 // tests/test_fused_tiles.py.
 #include <algorithm>
@@ -126,8 +127,61 @@ static std::vector<uint64_t> distinct(std::mt19937_64& rng, int n, int k) {
     return all;
 }
 
+// Large runs (kets of 20-30 qubits, 2000 gates; too large to simulate here):
+// the schedule is a permutation of the gates in which the gates on each bit
+// (targets and controls) keep their circuit order, and it plans into no more
+// passes than circuit order.
+static void check_large_schedules(std::mt19937_64& rng) {
+    for (int n : {20, 24, 30})
+        for (int Tmax : {10, 13}) {
+            std::vector<GateDesc> g;
+            for (int i = 0; i < 2000; ++i) {
+                GateDesc d;
+                d.op = (rng() % 10 < 7) ? 1 : 2;
+                d.b0 = int(rng() % uint64_t(n));
+                if (d.op == 2)
+                    do d.b1 = int(rng() % uint64_t(n));
+                    while (d.b1 == d.b0);
+                if (rng() % 10 == 0) {
+                    int c;
+                    do c = int(rng() % uint64_t(n));
+                    while (c == d.b0 || (d.op == 2 && c == d.b1));
+                    d.ctrl.push_back({c, int(rng() % 2)});
+                }
+                d.A[0] = cd(double(i), 0.0); // the gate's identity
+                g.push_back(d);
+            }
+            const std::vector<GateDesc> s = schedule_gates(g, n, Tmax);
+            EXPECT(s.size() == g.size());
+            std::vector<int> seen(g.size(), 0);
+            std::vector<std::vector<int>> on_bit(static_cast<size_t>(n));
+            for (const GateDesc& d : s) {
+                const int id = int(d.A[0].real());
+                EXPECT(id >= 0 && id < int(g.size()));
+                if (id < 0 || id >= int(g.size())) return;
+                ++seen[size_t(id)];
+                std::vector<int> bits{d.b0};
+                if (d.op == 2) bits.push_back(d.b1);
+                for (const auto& c : d.ctrl) bits.push_back(c.first);
+                for (int b : bits) on_bit[size_t(b)].push_back(id);
+            }
+            for (int x : seen) EXPECT(x == 1);
+            for (const auto& v : on_bit) EXPECT(std::is_sorted(v.begin(), v.end()));
+            std::vector<TilePassParams> p0, p1;
+            std::vector<TileGate> dv;
+            std::vector<TileSweep> sw;
+            std::vector<cd> m;
+            plan_gate_tiles(g, n, Tmax, p0, dv, sw, m);
+            plan_gate_tiles(s, n, Tmax, p1, dv, sw, m);
+            EXPECT(p1.size() <= p0.size());
+            std::printf("n=%d tiles of %d bits: %zu passes in circuit order, %zu scheduled\n", n,
+                        Tmax, p0.size(), p1.size());
+        }
+}
+
 int main() {
     std::mt19937_64 rng(7);
+    check_large_schedules(rng);
     int cases = 0, with_steps = 0;
     size_t passes_in_order = 0, passes_scheduled = 0, sweeps_in_order = 0, sweeps_scheduled = 0;
     for (int n = 1; n <= 12; ++n)
