@@ -309,10 +309,6 @@ void shape_of(const qgpu_state* s, uint64_t& rows, uint64_t& cols) {
     cols = s->kind == QGPU_KET ? 1 : s->D;
 }
 
-void check_handle(const void* p) {
-    if (!p) raise(QGPU_ERR_INVALID_HANDLE, "qgpu", "null handle");
-}
-
 const cd* C(const double* p) { return reinterpret_cast<const cd*>(p); }
 
 void upload_c128(qgpu_state* s, const double* host) {
@@ -440,7 +436,7 @@ qgpu_status qgpu_ctx_create(int device, qgpu_ctx** out) {
 
 qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         // states still alive keep the context (their memory lives on its
         // stream); the last qgpu_state_destroy tears it down
         ctx->closing.store(true);
@@ -450,14 +446,14 @@ qgpu_status qgpu_ctx_destroy(qgpu_ctx* ctx) {
 
 qgpu_status qgpu_ctx_synchronize(qgpu_ctx* ctx) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         QG_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 
 qgpu_status qgpu_ctx_mem_info(qgpu_ctx* ctx, uint64_t* free_b, uint64_t* total_b) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         size_t f = 0, t = 0;
         QG_CUDA(cudaSetDevice(ctx->device));
         QG_CUDA(cudaMemGetInfo(&f, &t));
@@ -479,7 +475,7 @@ void* qgpu_ctx_stream(qgpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr
 
 qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall_next) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::lock_guard<std::mutex> lock(ctx->mu);
         ctx->wait_limit = spin_limit;
         ctx->stall_next = stall_next != 0;
@@ -490,7 +486,7 @@ qgpu_status qgpu_ctx_set_wait_test(qgpu_ctx* ctx, uint32_t spin_limit, int stall
 
 qgpu_status qgpu_ctx_set_tile_bits(qgpu_ctx* ctx, int bits) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         if (bits != 0 && (bits < 5 || bits > 14))
             raise(QGPU_ERR_OUT_OF_RANGE, "qgpu_ctx_set_tile_bits()", "bits");
         ctx->tile_bits = bits;
@@ -501,7 +497,7 @@ qgpu_status qgpu_ctx_set_tile_bits(qgpu_ctx* ctx, int bits) {
 qgpu_status qgpu_state_create(qgpu_ctx* ctx, qgpu_kind kind, qgpu_prec prec,
                               const uint64_t* dims, uint32_t n, qgpu_state** out) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         if (!out) raise(QGPU_ERR_INVALID_ARGUMENT, "qgpu_state_create()", "out");
         std::vector<uint64_t> d = vec(dims, n);
         if (!dims_ok(d)) raise(QGPU_ERR_DIMS_INVALID, "qgpu_state_create()", "dims");
@@ -521,7 +517,7 @@ qgpu_status qgpu_state_destroy(qgpu_state* s) {
 
 qgpu_status qgpu_state_clone(const qgpu_state* s, qgpu_state** out) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         qgpu_state* c = qgpu::new_state(s->ctx, s->kind, s->prec, s->dims, false);
         cudaError_t e = cudaMemcpyAsync(c->data, s->data, s->bytes(),
                                         cudaMemcpyDeviceToDevice, s->ctx->stream);
@@ -535,7 +531,7 @@ qgpu_status qgpu_state_clone(const qgpu_state* s, qgpu_state** out) {
 
 qgpu_status qgpu_state_upload(qgpu_state* s, const void* host) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         QG_CUDA(cudaMemcpyAsync(s->data, host, s->bytes(), cudaMemcpyHostToDevice,
                                 s->ctx->stream));
         QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
@@ -544,7 +540,7 @@ qgpu_status qgpu_state_upload(qgpu_state* s, const void* host) {
 
 qgpu_status qgpu_state_download(const qgpu_state* s, void* host) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         QG_CUDA(cudaMemcpyAsync(host, s->data, s->bytes(), cudaMemcpyDeviceToHost,
                                 s->ctx->stream));
         QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
@@ -553,7 +549,7 @@ qgpu_status qgpu_state_download(const qgpu_state* s, void* host) {
 
 qgpu_status qgpu_state_upload_c128(qgpu_state* s, const double* host) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         upload_c128(s, host);
         QG_CUDA(cudaStreamSynchronize(s->ctx->stream));
     });
@@ -561,7 +557,7 @@ qgpu_status qgpu_state_upload_c128(qgpu_state* s, const double* host) {
 
 qgpu_status qgpu_state_download_c128(const qgpu_state* s, double* host) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         download_c128(s, host);
     });
 }
@@ -569,7 +565,7 @@ qgpu_status qgpu_state_download_c128(const qgpu_state* s, double* host) {
 qgpu_status qgpu_state_info(const qgpu_state* s, qgpu_kind* kind, qgpu_prec* prec,
                             uint32_t* n, uint64_t* dims, uint64_t* D) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         if (kind) *kind = s->kind;
         if (prec) *prec = s->prec;
         if (n) *n = uint32_t(s->dims.size());
@@ -582,7 +578,7 @@ void* qgpu_state_device_ptr(qgpu_state* s) { return s ? s->data : nullptr; }
 
 qgpu_status qgpu_state_fill_gaussian(qgpu_state* s, uint64_t seed) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         qgpu::launch_fill_gaussian(s->ctx, s->prec, s->data, s->elems, seed);
         if (!qgpu::op_normalize(s))
             raise(QGPU_ERR_DIVISION_BY_ZERO, "qpp::normalize()", "Division by zero!");
@@ -591,8 +587,8 @@ qgpu_status qgpu_state_fill_gaussian(qgpu_state* s, uint64_t seed) {
 
 qgpu_status qgpu_state_convert(const qgpu_state* src, qgpu_state* dst) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(src);
-        check_handle(dst);
+        qgpu::need_handle(src);
+        qgpu::need_handle(dst);
         if (src->kind != dst->kind || src->dims != dst->dims)
             raise(QGPU_ERR_DIMS_NOT_EQUAL, "qgpu_state_convert()", "src/dst");
         qgpu::launch_convert(src->ctx, src->data, src->prec, dst->data, dst->prec,
@@ -604,7 +600,7 @@ qgpu_status qgpu_state_convert(const qgpu_state* src, qgpu_state* dst) {
 qgpu_status qgpu_apply(qgpu_state* s, const double* A, uint64_t DA,
                        const uint64_t* target, uint32_t k) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> t = vec(target, k);
@@ -618,7 +614,7 @@ qgpu_status qgpu_apply_ctrl(qgpu_state* s, const double* A, uint64_t DA,
                             const uint64_t* target, uint32_t k,
                             const uint64_t* shift) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> cv = vec(ctrl, nc), t = vec(target, k);
@@ -632,7 +628,7 @@ qgpu_status qgpu_apply_ctrl_fan(qgpu_state* s, const double* A, uint64_t DA,
                                 const uint64_t* target, uint32_t k,
                                 const uint64_t* shift) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> cv = vec(ctrl, nc), t = vec(target, k);
@@ -644,7 +640,7 @@ qgpu_status qgpu_apply_ctrl_fan(qgpu_state* s, const double* A, uint64_t DA,
 qgpu_status qgpu_apply_kraus(qgpu_state* s, const double* Ks, uint32_t nK,
                              uint64_t DA, const uint64_t* target, uint32_t k) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> t = vec(target, k);
@@ -656,7 +652,7 @@ qgpu_status qgpu_apply_kraus(qgpu_state* s, const double* Ks, uint32_t nK,
 qgpu_status qgpu_ptrace(const qgpu_state* s, const uint64_t* target, uint32_t k,
                         qgpu_state** out) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> t = vec(target, k);
@@ -668,7 +664,7 @@ qgpu_status qgpu_ptrace(const qgpu_state* s, const uint64_t* target, uint32_t k,
 qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
                             uint32_t k, qgpu_state** out) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> t = vec(target, k);
@@ -680,7 +676,7 @@ qgpu_status qgpu_ptranspose(const qgpu_state* s, const uint64_t* target,
 qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
                             uint32_t n, qgpu_state** out) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> p = vec(perm, n);
@@ -691,14 +687,14 @@ qgpu_status qgpu_syspermute(const qgpu_state* s, const uint64_t* perm,
 
 qgpu_status qgpu_norm2(const qgpu_state* s, double* out) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         *out = qgpu::op_norm2(s);
     });
 }
 
 qgpu_status qgpu_trace(const qgpu_state* s, double* re, double* im) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         cd t = qgpu::op_trace(s);
         if (re) *re = t.real();
         if (im) *im = t.imag();
@@ -707,7 +703,7 @@ qgpu_status qgpu_trace(const qgpu_state* s, double* re, double* im) {
 
 qgpu_status qgpu_normalize(qgpu_state* s) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         if (!qgpu::op_normalize(s))
             raise(QGPU_ERR_DIVISION_BY_ZERO, "qpp::normalize()", "Division by zero!");
     });
@@ -716,8 +712,8 @@ qgpu_status qgpu_normalize(qgpu_state* s) {
 qgpu_status qgpu_inner(const qgpu_state* a, const qgpu_state* b, double* re,
                        double* im) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(a);
-        check_handle(b);
+        qgpu::need_handle(a);
+        qgpu::need_handle(b);
         if (a->kind != b->kind || a->dims != b->dims || a->prec != b->prec)
             raise(QGPU_ERR_DIMS_NOT_EQUAL, "qgpu_inner()", "a/b");
         cd v = qgpu::reduce_inner(a->ctx, a->prec, a->data, b->data, a->elems);
@@ -732,7 +728,7 @@ qgpu_status qgpu_host_apply(qgpu_ctx* ctx, const double* state, uint64_t rows,
                             uint64_t ac, const uint64_t* target, uint32_t k,
                             const uint64_t* dims, uint32_t n, double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         uint64_t DA = check_apply(rows, cols, ar, ac, t, d);
         Tmp s;
@@ -749,7 +745,7 @@ qgpu_status qgpu_host_apply_ctrl(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* dims, uint32_t n,
                                  const uint64_t* shift, int fan, double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> cv = vec(ctrl, nc), t = vec(target, k), d = vec(dims, n);
         auto sh = check_ctrl(rows, cols, ar, ac, cv, t, d, shift, fan != 0);
         Tmp s;
@@ -766,7 +762,7 @@ qgpu_status qgpu_host_apply_kraus(qgpu_ctx* ctx, const double* state,
                                   const uint64_t* dims, uint32_t n,
                                   double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         uint64_t DA = check_kraus(rows, cols, nK, kr, kc, t, d);
         Tmp s;
@@ -780,7 +776,7 @@ qgpu_status qgpu_host_ptrace(qgpu_ctx* ctx, const double* state, uint64_t rows,
                              uint64_t cols, const uint64_t* target, uint32_t k,
                              const uint64_t* dims, uint32_t n, double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         check_subsys_op("qpp::ptrace()", rows, cols, t, d);
         Tmp s, o;
@@ -796,7 +792,7 @@ qgpu_status qgpu_host_ptranspose(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* dims, uint32_t n,
                                  double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> t = vec(target, k), d = vec(dims, n);
         check_subsys_op("qpp::ptranspose()", rows, cols, t, d);
         Tmp s, o;
@@ -812,7 +808,7 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
                                  const uint64_t* dims, uint32_t n,
                                  double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> p = vec(perm, np), d = vec(dims, n);
         check_perm(rows, cols, p, d);
         Tmp s, o;
@@ -826,7 +822,7 @@ qgpu_status qgpu_host_syspermute(qgpu_ctx* ctx, const double* state,
 qgpu_status qgpu_apply_qft(qgpu_state* s, const uint64_t* target, uint32_t k, uint64_t d,
                            int swap, int inverse) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         std::vector<uint64_t> t = vec(target, k);
@@ -837,7 +833,7 @@ qgpu_status qgpu_apply_qft(qgpu_state* s, const uint64_t* target, uint32_t k, ui
 
 qgpu_status qgpu_qft(qgpu_state* s, uint64_t d, int swap, int inverse) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(s);
+        qgpu::need_handle(s);
         uint64_t r, c;
         shape_of(s, r, c);
         check_qft(inverse ? "qpp::TFQ()" : "qpp::QFT()", true, r, c, {}, d);
@@ -851,7 +847,7 @@ static qgpu_status host_qft(qgpu_ctx* ctx, const double* state, uint64_t rows,
                             uint64_t cols, const uint64_t* target, uint32_t k, bool whole,
                             uint64_t d, int swap, int inverse, double* result) {
     return qgpu::guarded(__func__, [&] {
-        check_handle(ctx);
+        qgpu::need_handle(ctx);
         std::vector<uint64_t> t = vec(target, k);
         const char* W = whole ? (inverse ? "qpp::TFQ()" : "qpp::QFT()")
                               : (inverse ? "qpp::applyTFQ()" : "qpp::applyQFT()");
